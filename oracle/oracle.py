@@ -1,0 +1,323 @@
+"""ctypes wrapper over the CPU oracle (oracle/_build/liboracle_pz.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA product.  Only tests/,
+``__graft_entry__.smoke()`` and ``bench.py``'s cpu_baseline / reference legs
+may import this module.  The oracle restates the reference's Rust path
+(see pz_oracle.h for the file:line map); its equality with the Rust binary
+is unpinned because the Rust reference cannot be built here.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle_pz.so")
+
+u64p = ctypes.POINTER(ctypes.c_uint64)
+u32p = ctypes.POINTER(ctypes.c_uint32)
+u8p = ctypes.POINTER(ctypes.c_uint8)
+i32p = ctypes.POINTER(ctypes.c_int32)
+vp = ctypes.c_void_p
+
+PARAM_IDS = {
+    "I_2P_LB_SR": 0, "I_4P": 1, "I_8P": 2, "NI_2P": 3,
+    "NI_4P_HB_FR": 4, "NI_4P_LB_SR": 5, "NI_8P": 6, "SP_TEST": 7,
+}
+GATES = {"and": 0, "nand": 1, "or": 2, "nor": 3, "xor": 4, "xnor": 5}
+
+
+class ParamInfo(ctypes.Structure):
+    _fields_ = [
+        ("rlwe_q", ctypes.c_uint64), ("lwe_q", ctypes.c_uint64),
+        ("br_q", ctypes.c_uint32), ("rlwe_n", ctypes.c_uint32), ("lwe_n", ctypes.c_uint32),
+        ("lwe_logb", ctypes.c_uint32), ("lwe_d", ctypes.c_uint32),
+        ("rlrg_logb", ctypes.c_uint32), ("rlrg_d_a", ctypes.c_uint32), ("rlrg_d_b", ctypes.c_uint32),
+        ("auto_logb", ctypes.c_uint32), ("auto_d", ctypes.c_uint32),
+        ("g", ctypes.c_uint32), ("w", ctypes.c_uint32),
+        ("lwe_secret_gaussian", ctypes.c_uint32), ("variant", ctypes.c_uint32),
+        ("embedding_factor", ctypes.c_uint32), ("rgsw_rows", ctypes.c_uint32),
+        ("auto_rows", ctypes.c_uint32), ("n_auto_keys", ctypes.c_uint32),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError(f"oracle library missing: {_LIB_PATH} (run `make -C oracle`)")
+        L = ctypes.CDLL(_LIB_PATH)
+        sig = {
+            "orc_param_info_get": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ParamInfo)]),
+            "orc_eval_new": (vp, [ctypes.c_int]),
+            "orc_eval_free": (None, [vp]),
+            "orc_eval_psi": (ctypes.c_uint64, [vp]),
+            "orc_eval_tables": (None, [vp, u64p, u64p, u64p]),
+            "orc_eval_test_vec": (None, [vp, ctypes.c_int, u64p]),
+            "orc_eval_dlog_map": (None, [vp, u32p]),
+            "orc_eval_auto_map": (None, [vp, ctypes.c_int, u32p, u8p]),
+            "orc_ntt_forward": (None, [vp, u64p, ctypes.c_int]),
+            "orc_ntt_backward": (None, [vp, u64p, ctypes.c_int]),
+            "orc_decompose": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_uint64, u64p]),
+            "orc_shoup_matrix_fma": (None, [ctypes.c_uint64, u64p, u64p, u64p, u64p, ctypes.c_size_t, ctypes.c_size_t]),
+            "orc_shoup_repr": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_uint64]),
+            "orc_barrett_mul": (ctypes.c_uint64, [vp, ctypes.c_uint64, ctypes.c_uint64]),
+            "orc_negacyclic_mul": (None, [ctypes.c_uint64, u64p, u64p, u64p, ctypes.c_size_t]),
+            "orc_key_new": (vp, [vp, u64p, u64p, u64p]),
+            "orc_key_free": (None, [vp]),
+            "orc_rlwe_by_rgsw": (None, [vp, vp, u64p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
+            "orc_rlwe_auto": (None, [vp, vp, u64p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int]),
+            "orc_lwe_key_switch": (None, [vp, vp, u64p, u64p]),
+            "orc_pbs": (ctypes.c_int, [vp, vp, ctypes.c_int, u64p, u64p, u64p]),
+            "orc_gate": (None, [vp, vp, ctypes.c_int, u64p, u64p]),
+            "orc_not": (None, [vp, u64p]),
+            "orc_gate_batch": (None, [vp, vp, u8p, u64p, u64p, u64p, ctypes.c_size_t, ctypes.c_int]),
+            "orc_sample_extract": (None, [vp, u64p, u64p, ctypes.c_uint32]),
+            "orc_rng_new": (vp, [u8p]),
+            "orc_rng_free": (None, [vp]),
+            "orc_rng_next_u64": (ctypes.c_uint64, [vp]),
+            "orc_rng_uniform_mod": (None, [vp, ctypes.c_uint64, u64p, ctypes.c_size_t]),
+            "orc_client_keys": (None, [vp, ctypes.c_int, ctypes.c_int, i32p, i32p, i32p, i32p]),
+            "orc_gen_server_key": (None, [vp, i32p, i32p, u8p, u64p, u64p, u64p]),
+            "orc_encrypt_bool": (None, [vp, vp, i32p, ctypes.c_int, u64p]),
+            "orc_decrypt_bool": (ctypes.c_int, [vp, i32p, u64p]),
+            "orc_mp_decryption_share": (ctypes.c_uint64, [vp, vp, i32p, u64p]),
+            "orc_mp_aggregate_decrypt": (ctypes.c_int, [vp, u64p, u64p, ctypes.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a, t=u64p):
+    return a.ctypes.data_as(t)
+
+
+def param_info(name_or_id):
+    pid = PARAM_IDS[name_or_id] if isinstance(name_or_id, str) else int(name_or_id)
+    info = ParamInfo()
+    if lib().orc_param_info_get(pid, ctypes.byref(info)) != 0:
+        raise ValueError(f"unknown parameter set {name_or_id}")
+    return info
+
+
+class Rng:
+    """ChaCha8 stream; seed is 32 bytes."""
+
+    def __init__(self, seed):
+        seed = bytes(seed)
+        assert len(seed) == 32
+        self._seed = (ctypes.c_uint8 * 32)(*seed)
+        self.h = lib().orc_rng_new(self._seed)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_rng_free(self.h)
+            self.h = None
+
+    def uniform_mod(self, q, n):
+        out = np.empty(n, dtype=np.uint64)
+        lib().orc_rng_uniform_mod(self.h, q, _p(out), n)
+        return out
+
+
+class ServerKeyCoeff:
+    """Coefficient-domain expanded server key (layout of orc_key_new)."""
+
+    def __init__(self, rgsw, autos, ksk):
+        self.rgsw, self.autos, self.ksk = rgsw, autos, ksk
+
+
+class Evaluator:
+    """Oracle BoolEvaluator for one parameter set."""
+
+    def __init__(self, param):
+        self.pid = PARAM_IDS[param] if isinstance(param, str) else int(param)
+        self.info = param_info(self.pid)
+        self.h = lib().orc_eval_new(self.pid)
+        i = self.info
+        self.N, self.n, self.Q = i.rlwe_n, i.lwe_n, i.rlwe_q
+        self.L = self.N + 1
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_eval_free(self.h)
+            self.h = None
+
+    # --- tables -------------------------------------------------------------
+    def psi(self):
+        return lib().orc_eval_psi(self.h)
+
+    def tables(self):
+        a = np.empty(self.N, np.uint64)
+        b = np.empty(self.N, np.uint64)
+        ni = (ctypes.c_uint64 * 1)()
+        lib().orc_eval_tables(self.h, _p(a), _p(b), ni)
+        return a, b, int(ni[0])
+
+    def test_vec(self, gate):
+        out = np.empty(self.info.br_q // 2, np.uint64)
+        lib().orc_eval_test_vec(self.h, GATES[gate] if isinstance(gate, str) else gate, _p(out))
+        return out
+
+    def dlog_map(self):
+        out = np.empty(self.info.br_q, np.uint32)
+        lib().orc_eval_dlog_map(self.h, _p(out, u32p))
+        return out
+
+    def auto_map(self, k):
+        idx = np.empty(self.N, np.uint32)
+        sgn = np.empty(self.N, np.uint8)
+        lib().orc_eval_auto_map(self.h, k, _p(idx, u32p), _p(sgn, u8p))
+        return idx, sgn
+
+    # --- arithmetic -------------------------------------------------------------
+    def ntt_forward(self, poly, lazy=False):
+        a = np.ascontiguousarray(poly, dtype=np.uint64).copy()
+        lib().orc_ntt_forward(self.h, _p(a), int(lazy))
+        return a
+
+    def ntt_backward(self, poly, lazy=False):
+        a = np.ascontiguousarray(poly, dtype=np.uint64).copy()
+        lib().orc_ntt_backward(self.h, _p(a), int(lazy))
+        return a
+
+    def decompose(self, which, value):
+        out = np.zeros(64, np.uint64)
+        d = lib().orc_decompose(self.h, which, int(value), _p(out))
+        return out[:d]
+
+    def barrett_mul(self, a, b):
+        return lib().orc_barrett_mul(self.h, int(a), int(b))
+
+    # --- keys ---------------------------------------------------------------
+    def client_keys(self, parties, seed_base=0):
+        N, n = self.N, self.n
+        s = np.empty(N, np.int32)
+        z = np.empty(n, np.int32)
+        sp = np.empty((parties, N), np.int32)
+        zp = np.empty((parties, n), np.int32)
+        lib().orc_client_keys(self.h, parties, seed_base, _p(s, i32p), _p(z, i32p),
+                              _p(sp, i32p), _p(zp, i32p))
+        return s, z, sp, zp
+
+    def gen_server_key(self, s, z, err_seed=b"\x33" * 32):
+        i = self.info
+        N, n = self.N, self.n
+        rgsw = np.empty((n, i.rgsw_rows, N), np.uint64)
+        autos = np.empty((i.n_auto_keys, i.auto_rows, N), np.uint64)
+        ksk = np.empty((i.lwe_d * N, n + 1), np.uint64)
+        seed = (ctypes.c_uint8 * 32)(*bytes(err_seed))
+        lib().orc_gen_server_key(self.h, _p(np.ascontiguousarray(s, np.int32), i32p),
+                                 _p(np.ascontiguousarray(z, np.int32), i32p), seed,
+                                 _p(rgsw), _p(autos), _p(ksk))
+        return ServerKeyCoeff(rgsw, autos, ksk)
+
+    def key(self, coeff):
+        return OracleKey(self, coeff)
+
+    # --- client -----------------------------------------------------------------
+    def encrypt_bool(self, rng, s, bits):
+        bits = np.atleast_1d(np.asarray(bits, dtype=np.int64))
+        out = np.empty((len(bits), self.L), np.uint64)
+        sp = _p(np.ascontiguousarray(s, np.int32), i32p)
+        for k, b in enumerate(bits):
+            row = out[k]
+            lib().orc_encrypt_bool(self.h, rng.h, sp, int(b), _p(row))
+        return out
+
+    def decrypt_bool(self, s, cts):
+        cts = np.atleast_2d(np.ascontiguousarray(cts, np.uint64))
+        sp = _p(np.ascontiguousarray(s, np.int32), i32p)
+        return np.array([lib().orc_decrypt_bool(self.h, sp, _p(np.ascontiguousarray(c))) for c in cts])
+
+    def mp_decrypt_bool(self, rng, s_parts, cts):
+        cts = np.atleast_2d(np.ascontiguousarray(cts, np.uint64))
+        out = []
+        P = len(s_parts)
+        for c in cts:
+            c = np.ascontiguousarray(c)
+            shares = np.array([lib().orc_mp_decryption_share(
+                self.h, rng.h, _p(np.ascontiguousarray(s_parts[p], np.int32), i32p), _p(c))
+                for p in range(P)], dtype=np.uint64)
+            out.append(lib().orc_mp_aggregate_decrypt(self.h, _p(c), _p(shares), P))
+        return np.array(out)
+
+    def sample_extract(self, rlwe, index=0):
+        r = np.ascontiguousarray(rlwe, np.uint64)
+        out = np.empty(self.L, np.uint64)
+        lib().orc_sample_extract(self.h, _p(r), _p(out), index)
+        return out
+
+    def not_(self, c):
+        a = np.ascontiguousarray(c, np.uint64).copy()
+        lib().orc_not(self.h, _p(a))
+        return a
+
+
+class OracleKey:
+    def __init__(self, ev, coeff):
+        self.ev = ev
+        self.coeff = coeff
+        self.h = lib().orc_key_new(ev.h, _p(np.ascontiguousarray(coeff.rgsw)),
+                                   _p(np.ascontiguousarray(coeff.autos)),
+                                   _p(np.ascontiguousarray(coeff.ksk)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_key_free(self.h)
+            self.h = None
+
+    def rlwe_by_rgsw(self, rlwe, lwe_index, trivial=False, shoup=True):
+        a = np.ascontiguousarray(rlwe, np.uint64).copy()
+        lib().orc_rlwe_by_rgsw(self.ev.h, self.h, _p(a), lwe_index, int(trivial), int(shoup))
+        return a
+
+    def rlwe_auto(self, rlwe, k, trivial=False, shoup=True):
+        a = np.ascontiguousarray(rlwe, np.uint64).copy()
+        lib().orc_rlwe_auto(self.ev.h, self.h, _p(a), k, int(trivial), int(shoup))
+        return a
+
+    def lwe_key_switch(self, lwe_in):
+        a = np.ascontiguousarray(lwe_in, np.uint64)
+        out = np.empty(self.ev.n + 1, np.uint64)
+        lib().orc_lwe_key_switch(self.ev.h, self.h, _p(a), _p(out))
+        return out
+
+    def pbs(self, gate, lwe):
+        a = np.ascontiguousarray(lwe, np.uint64).copy()
+        ks = np.empty(self.ev.n + 1, np.uint64)
+        rl = np.empty(2 * self.ev.N, np.uint64)
+        autos = lib().orc_pbs(self.ev.h, self.h, GATES[gate] if isinstance(gate, str) else gate,
+                              _p(a), _p(ks), _p(rl))
+        return a, ks, rl, autos
+
+    def gate(self, gate, c0, c1):
+        a = np.ascontiguousarray(c0, np.uint64).copy()
+        b = np.ascontiguousarray(c1, np.uint64)
+        lib().orc_gate(self.ev.h, self.h, GATES[gate] if isinstance(gate, str) else gate, _p(a), _p(b))
+        return a
+
+    def gate_batch(self, gates, c0, c1, threads=1):
+        gates = np.ascontiguousarray(gates, np.uint8)
+        c0 = np.ascontiguousarray(c0, np.uint64)
+        c1 = np.ascontiguousarray(c1, np.uint64)
+        out = np.empty_like(c0)
+        lib().orc_gate_batch(self.ev.h, self.h, _p(gates, u8p), _p(c0), _p(c1), _p(out),
+                             len(gates), threads)
+        return out
+
+
+def setup(param, parties=2, seed_base=0, err_seed=b"\x33" * 32):
+    """Evaluator + client keys + server key for a parameter set."""
+    ev = Evaluator(param)
+    s, z, sp, zp = ev.client_keys(parties, seed_base)
+    coeff = ev.gen_server_key(s, z, err_seed)
+    key = ev.key(coeff)
+    return ev, (s, z, sp, zp), coeff, key

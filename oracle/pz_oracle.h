@@ -1,0 +1,163 @@
+/*
+ * pz_oracle.h -- CPU oracle for the server-side gate bootstrap of phantom-zone.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker: only tests/, the
+ * smoke() entry point and bench.py's cpu_baseline / reference legs may load
+ * it.  The product (phantom-zone_b200/) never links, loads or calls it.
+ *
+ * It restates, in C++17 with u64 / unsigned __int128 / IEEE double exactly as
+ * the Rust code does, the reference's path:
+ *   src/pbs.rs:104-482            pbs, blind_rotation, mod_switch_odd,
+ *                                 sample_extract, monomial_mul
+ *   src/rgsw/runtime.rs:363-855   decompose_r, rlwe_auto(_shoup),
+ *                                 rlwe_by_rgsw(_shoup)
+ *   src/ntt.rs:24-442             Harvey butterflies, CT forward, GS inverse
+ *   src/decomposer.rs:13-309      signed gadget decomposition
+ *   src/lwe.rs:14-44              lwe_key_switch
+ *   src/backend/modulus_u64.rs    Barrett mul, add/sub/neg, shoup_matrix_fma
+ *   src/backend/power_of_2.rs     mask arithmetic mod 2^k
+ *   src/bool/evaluator.rs:651-784,2118-2245   dlog map, test vectors, gates
+ *   src/bool/parameters.rs:526-726            parameter sets
+ * plus a client-side harness (key generation, encryption, decryption) that
+ * the reference runs on clients and which is out of the GPU path's scope.
+ *
+ * Parity status: the Rust reference cannot be built in this environment (no
+ * cargo/rustc, no crate sources), and it ships no golden vectors: every
+ * reference test draws from an entropy-seeded RNG.  Equality with the Rust
+ * binary's output words is therefore UNPINNED.  The oracle is pinned instead
+ * by the reference's own property tests, restated in tests/test_oracle.py:
+ * NTT vs schoolbook negacyclic product (ntt.rs:510-540), Shoup FMA vs naive
+ * u128 (modulus_u64.rs:284-336), decomposition recomposition
+ * (decomposer.rs:325-370), Shoup vs non-Shoup external product and
+ * automorphism bit-equality (rgsw/mod.rs:526-831), gate truth tables and
+ * FheUint8 plaintext semantics under decryption (mp_api.rs:491-695).
+ */
+#ifndef PZ_ORACLE_H
+#define PZ_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  uint64_t rlwe_q;      /* Q */
+  uint64_t lwe_q;       /* q_ks, a power of two */
+  uint32_t br_q;        /* blind-rotation modulus */
+  uint32_t rlwe_n;      /* N */
+  uint32_t lwe_n;       /* n */
+  uint32_t lwe_logb, lwe_d;          /* key-switch decomposer */
+  uint32_t rlrg_logb, rlrg_d_a, rlrg_d_b; /* RLWE x RGSW decomposer */
+  uint32_t auto_logb, auto_d;        /* automorphism decomposer */
+  uint32_t g, w;                     /* generator, window */
+  uint32_t lwe_secret_gaussian;      /* 1: LWE secret from the error distribution */
+  uint32_t variant;                  /* 0 single, 1 interactive, 2 non-interactive */
+  uint32_t embedding_factor;         /* 2N / br_q */
+  uint32_t rgsw_rows;                /* 2 d_a + 2 d_b */
+  uint32_t auto_rows;                /* 2 d_auto */
+  uint32_t n_auto_keys;              /* w + 1 */
+} orc_param_info;
+
+/* Parameter set ids, in the order of src/bool/parameters.rs:526-726. */
+enum {
+  ORC_I_2P_LB_SR = 0, ORC_I_4P = 1, ORC_I_8P = 2, ORC_NI_2P = 3,
+  ORC_NI_4P_HB_FR = 4, ORC_NI_4P_LB_SR = 5, ORC_NI_8P = 6, ORC_SP_TEST = 7,
+  ORC_NUM_PARAMS = 8
+};
+
+/* Gate ids: and, nand, or, nor, xor, xnor (evaluator.rs:2163-2245). */
+enum { ORC_AND = 0, ORC_NAND = 1, ORC_OR = 2, ORC_NOR = 3, ORC_XOR = 4, ORC_XNOR = 5 };
+
+int orc_param_info_get(int param_id, orc_param_info *out);
+
+/* --- evaluator (BoolEvaluator::new, evaluator.rs:651-784) ------------------ */
+void *orc_eval_new(int param_id);
+void orc_eval_free(void *ev);
+/* psi (the 2N-th root the NTT uses) and its bit-reversed power tables. */
+uint64_t orc_eval_psi(void *ev);
+void orc_eval_tables(void *ev, uint64_t *psi_br, uint64_t *psi_inv_br, uint64_t *n_inv);
+/* test vector (length br_q/2) of a gate, and the dlog map (length br_q) */
+void orc_eval_test_vec(void *ev, int gate, uint64_t *out);
+void orc_eval_dlog_map(void *ev, uint32_t *out);
+/* auto map of key slot k (0 -> -g, k>=1 -> g^k mod br_q): index + sign */
+void orc_eval_auto_map(void *ev, int k, uint32_t *index, uint8_t *sign);
+
+/* --- arithmetic pins --------------------------------------------------------- */
+void orc_ntt_forward(void *ev, uint64_t *poly, int lazy);
+void orc_ntt_backward(void *ev, uint64_t *poly, int lazy);
+/* which: 0 lwe (KS), 1 rlrg a, 2 rlrg b, 3 auto; writes d digits */
+int orc_decompose(void *ev, int which, uint64_t value, uint64_t *digits);
+void orc_shoup_matrix_fma(uint64_t q, uint64_t *out, const uint64_t *a,
+                          const uint64_t *a_shoup, const uint64_t *b,
+                          size_t rows, size_t n);
+uint64_t orc_shoup_repr(uint64_t v, uint64_t q);
+uint64_t orc_barrett_mul(void *ev, uint64_t a, uint64_t b);
+void orc_negacyclic_mul(uint64_t q, const uint64_t *a, const uint64_t *b,
+                        uint64_t *out, size_t n);
+
+/* --- server key ----------------------------------------------------------------
+ * Coefficient-domain, fully expanded server key (what set_server_key holds
+ * before the forward NTT, keys.rs:687-781):
+ *   rgsw  [n][2 d_a + 2 d_b][N]  rows A(-sm), B(-sm), A(m), B(m)
+ *   autos [w+1][2 d_auto][N]      rows A, B; slot 0 = -g, slot k = g^k
+ *   ksk   [d_ks N][n+1]           row = [b, a_1..a_n] mod q_ks
+ */
+void *orc_key_new(void *ev, const uint64_t *rgsw, const uint64_t *autos,
+                  const uint64_t *ksk);
+void orc_key_free(void *key);
+
+/* --- the hot path ------------------------------------------------------------- */
+void orc_rlwe_by_rgsw(void *ev, void *key, uint64_t *rlwe, uint32_t lwe_index,
+                      int trivial, int shoup);
+void orc_rlwe_auto(void *ev, void *key, uint64_t *rlwe, uint32_t k, int trivial,
+                   int shoup);
+void orc_lwe_key_switch(void *ev, void *key, const uint64_t *lwe_in, uint64_t *out);
+/* pbs on lwe (N+1 words, in place) with the gate's test vector.  If ks_out
+ * (n+1 words) / rlwe_out (2N words) are non-NULL they receive the key-switch
+ * output and the blind-rotated accumulator. Returns the number of
+ * non-trivial automorphisms executed. */
+int orc_pbs(void *ev, void *key, int gate, uint64_t *lwe, uint64_t *ks_out,
+            uint64_t *rlwe_out);
+/* gate: c0 <- gate(c0, c1) (evaluator.rs:2163-2245) */
+void orc_gate(void *ev, void *key, int gate, uint64_t *c0, const uint64_t *c1);
+void orc_not(void *ev, uint64_t *c0);
+/* independent gates on `threads` host threads, one evaluator scratch per
+ * thread (the reference's thread-local evaluator model, mp_api.rs:20-22) */
+void orc_gate_batch(void *ev, void *key, const uint8_t *gates, const uint64_t *c0,
+                    const uint64_t *c1, uint64_t *out, size_t count, int threads);
+void orc_sample_extract(void *ev, const uint64_t *rlwe, uint64_t *lwe, uint32_t index);
+
+/* --- client-side harness (reference runs this on clients; out of scope) -------- */
+/* ChaCha8 stream (rand_chacha 0.3 layout), for seeding */
+void *orc_rng_new(const uint8_t seed[32]);
+void orc_rng_free(void *rng);
+uint64_t orc_rng_next_u64(void *rng);
+void orc_rng_uniform_mod(void *rng, uint64_t q, uint64_t *out, size_t n);
+
+/* Client keys of `parties` parties from seeds seed_p = 32 x byte(p + 1 + 16*seed_base).
+ * Writes the ideal (summed) secrets: s [N] as i32, z [n] as i32, and each
+ * party's secrets (s_parts [parties][N], z_parts [parties][n]) if non-NULL. */
+void orc_client_keys(void *ev, int parties, int seed_base, int32_t *s, int32_t *z,
+                     int32_t *s_parts, int32_t *z_parts);
+/* Server key (coefficient domain, layout of orc_key_new) under the ideal
+ * secrets, errors drawn from ChaCha8(err_seed).  See DESIGN.md. */
+void orc_gen_server_key(void *ev, const int32_t *s, const int32_t *z,
+                        const uint8_t err_seed[32], uint64_t *rgsw, uint64_t *autos,
+                        uint64_t *ksk);
+/* LWE_Q encryption of bool under s (lwe.rs:104-137, m = +-Q/8) */
+void orc_encrypt_bool(void *ev, void *rng, const int32_t *s, int bit, uint64_t *lwe);
+/* noisy m = b - <a, s> (lwe.rs:139-162) and the bool decode (evaluator.rs:243-256)
+ * returns 0/1, or -1 when the decode is not 0 or 1 */
+int orc_decrypt_bool(void *ev, const int32_t *s, const uint64_t *lwe);
+/* multi-party decryption share of one party (multi_party.rs:57-87) */
+uint64_t orc_mp_decryption_share(void *ev, void *rng, const int32_t *s_part,
+                                 const uint64_t *lwe);
+int orc_mp_aggregate_decrypt(void *ev, const uint64_t *lwe, const uint64_t *shares,
+                             int parties);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
