@@ -1,0 +1,163 @@
+/*
+ * phantom_zone_b200.h -- C ABI of the B200 gate-bootstrap engine.
+ *
+ * This is the drop-in boundary for phantom-zone's server-side gate
+ * evaluation: a Rust `BooleanGates` implementation (or any other FFI host)
+ * calls these entry points instead of running `pbs()` on the CPU.  Plain
+ * pointers and sizes only; every call returns a pz_status (no panics or
+ * exceptions cross the boundary); pz_last_error() describes the last failure
+ * of a context.
+ *
+ * Data formats (all little-endian u64 words, as in the reference):
+ *   LWE ciphertext mod Q       [N + 1]      b, a_1 .. a_N      (pbs.rs:423-449)
+ *   RLWE ciphertext            [2][N]       a(X), b(X)         (runtime.rs:137-153)
+ *   server key, coefficient domain (pz_server_key_view below)
+ *
+ * Reference interfaces replaced (paths inside gausslabs/phantom-zone):
+ *   pz_param_get          bool/parameters.rs:526-726 (parameter constants)
+ *   pz_ctx_create         BoolEvaluator::new, bool/evaluator.rs:651-784;
+ *                         set_parameter_set, bool/mp_api.rs:35-47,
+ *                         bool/ni_mp_api.rs:39-57
+ *   pz_key_upload         set_server_key, bool/mp_api.rs:136-145 and
+ *                         bool/ni_mp_api.rs:119-132 (ServerKeyEvaluationDomain
+ *                         ::from + Shoup*ServerKeyEvaluationDomain::from,
+ *                         bool/keys.rs:687-781, 869-1004, 1088-1220)
+ *   pz_gate_batch*        BooleanGates::{and,nand,or,nor,xor,xnor}_inplace,
+ *                         bool/mod.rs:22-71 -> evaluator.rs:2163-2245 -> pbs()
+ *                         pbs.rs:104-233 (batched: many gates per call)
+ *   pz_not_batch_device   BooleanGates::not_inplace, evaluator.rs:2247-2250
+ *   pz_pbs_batch_device   pbs(), pbs.rs:104-233, on already-combined LWEs
+ *   pz_ntt_*_device       Ntt::forward / Ntt::backward, ntt.rs:396-442
+ *   pz_rlwe_by_rgsw_device rlwe_by_rgsw_shoup, rgsw/runtime.rs:754-855
+ *   pz_rlwe_auto_device   rlwe_auto_shoup, rgsw/runtime.rs:530-643
+ *   pz_lwe_key_switch_device lwe_key_switch, lwe.rs:14-44
+ */
+#ifndef PHANTOM_ZONE_B200_H
+#define PHANTOM_ZONE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pz_status {
+  PZ_OK = 0,
+  PZ_ERR_INVALID_ARGUMENT = 1,
+  PZ_ERR_CUDA = 2,
+  PZ_ERR_OUT_OF_MEMORY = 3,
+  PZ_ERR_NOT_SUPPORTED = 4,
+  PZ_ERR_KEY_MISMATCH = 5
+} pz_status;
+
+/* Parameter sets, in the order of bool/parameters.rs:526-726. */
+enum {
+  PZ_I_2P_LB_SR = 0,   /* InteractiveLTE2Party */
+  PZ_I_4P = 1,         /* InteractiveLTE4Party */
+  PZ_I_8P = 2,         /* InteractiveLTE8Party */
+  PZ_NI_2P = 3,        /* NonInteractiveLTE2Party */
+  PZ_NI_4P_HB_FR = 4,  /* NonInteractiveLTE4Party */
+  PZ_NI_4P_LB_SR = 5,
+  PZ_NI_8P = 6,        /* NonInteractiveLTE8Party */
+  PZ_SP_TEST = 7,      /* SP_TEST_BOOL_PARAMS (reference test set, N = 512) */
+  PZ_NUM_PARAMS = 8
+};
+
+/* Gate codes of the batched gate entry points. */
+enum { PZ_GATE_AND = 0, PZ_GATE_NAND = 1, PZ_GATE_OR = 2, PZ_GATE_NOR = 3,
+       PZ_GATE_XOR = 4, PZ_GATE_XNOR = 5 };
+
+typedef struct pz_params {
+  uint64_t rlwe_q;   /* Q */
+  uint64_t lwe_q;    /* q_ks (power of two) */
+  uint32_t br_q;     /* blind-rotation modulus */
+  uint32_t rlwe_n;   /* N */
+  uint32_t lwe_n;    /* n */
+  uint32_t lwe_logb, lwe_d;
+  uint32_t rlrg_logb, rlrg_d_a, rlrg_d_b;
+  uint32_t auto_logb, auto_d;
+  uint32_t g, w;
+  uint32_t lwe_secret_gaussian;
+  uint32_t variant;          /* 0 single party, 1 interactive, 2 non-interactive */
+  uint32_t embedding_factor; /* 2N / br_q */
+  uint32_t rgsw_rows;        /* 2 d_a + 2 d_b */
+  uint32_t auto_rows;        /* 2 d_auto */
+  uint32_t n_auto_keys;      /* w + 1 */
+} pz_params;
+
+typedef struct pz_ctx pz_ctx;
+typedef struct pz_key pz_key;
+
+/* Expanded server key in the coefficient domain, host memory:
+ *   rgsw    [n][2 d_a + 2 d_b][N]  RGSW(X^{emb s_i}) rows A(-sm), B(-sm), A(m), B(m)
+ *   autos   [w + 1][2 d_auto][N]   auto keys, rows A then B; slot 0 = -g, slot k = g^k
+ *   lwe_ksk [d_ks N][n + 1]        LWE key-switching key, row = [b, a_1 .. a_n] mod q_ks
+ * (the contents of ServerKeyEvaluationDomain before its forward NTT). */
+typedef struct pz_server_key_view {
+  const uint64_t *rgsw;
+  const uint64_t *autos;
+  const uint64_t *lwe_ksk;
+} pz_server_key_view;
+
+const char *pz_status_string(pz_status s);
+pz_status pz_param_get(int param_id, pz_params *out);
+
+/* Context: parameter set + device tables + a private stream.  ntt_root = 0
+ * selects the library's own 2N-th root of unity; a nonzero value must be a
+ * primitive 2N-th root mod Q (outputs do not depend on the choice; the
+ * option lets tests compare evaluation-domain words). */
+pz_status pz_ctx_create(int param_id, int device, pz_ctx **out);
+pz_status pz_ctx_create_ex(int param_id, int device, uint64_t ntt_root, pz_ctx **out);
+void pz_ctx_destroy(pz_ctx *ctx);
+const char *pz_last_error(const pz_ctx *ctx);
+pz_status pz_ctx_params(const pz_ctx *ctx, pz_params *out);
+uint64_t pz_ctx_ntt_root(const pz_ctx *ctx);
+
+/* Server key: expanded, NTT'd and laid out on the context's device. */
+pz_status pz_key_upload(pz_ctx *ctx, const pz_server_key_view *key, pz_key **out);
+void pz_key_release(pz_key *key);
+size_t pz_key_device_bytes(const pz_key *key);
+
+/* out[i] = gate[i](c0[i], c1[i]); c0, c1, out: [count][N + 1].
+ * Host memory, synchronous (copies in and out inside the call). */
+pz_status pz_gate_batch(pz_ctx *ctx, const pz_key *key, const uint8_t *gates, const uint64_t *c0,
+                        const uint64_t *c1, uint64_t *out, size_t count);
+/* Same on device memory, asynchronous on `stream` (NULL: the CUDA default stream). */
+pz_status pz_gate_batch_device(pz_ctx *ctx, const pz_key *key, const uint8_t *d_gates,
+                               const uint64_t *d_c0, const uint64_t *d_c1, uint64_t *d_out,
+                               size_t count, void *stream);
+/* Diagnostic variant: also writes the key-switched LWE (d_ks_out
+ * [count][n + 1] u32, mod q_ks) and the blind-rotated RLWE (d_rlwe_out
+ * [count][2][N]) of each gate; either may be NULL. */
+pz_status pz_gate_batch_debug_device(pz_ctx *ctx, const pz_key *key, const uint8_t *d_gates,
+                                     const uint64_t *d_c0, const uint64_t *d_c1, uint64_t *d_out,
+                                     size_t count, uint32_t *d_ks_out, uint64_t *d_rlwe_out,
+                                     void *stream);
+/* pbs on combined LWE inputs d_lwe [count][N + 1] with the test vector of
+ * gate test_vec[i] (pbs.rs:104-233, no gate prelude). */
+pz_status pz_pbs_batch_device(pz_ctx *ctx, const pz_key *key, const uint8_t *d_test_vec,
+                              const uint64_t *d_lwe, uint64_t *d_out, size_t count, void *stream);
+/* out = -in (mod Q, unreduced: -0 = Q) on `words` u64 words. */
+pz_status pz_not_batch_device(pz_ctx *ctx, const uint64_t *d_in, uint64_t *d_out, size_t words,
+                              void *stream);
+
+/* Kernel-level entry points (device memory, asynchronous). */
+pz_status pz_ntt_forward_device(pz_ctx *ctx, uint64_t *d_polys, size_t count, void *stream);
+pz_status pz_ntt_backward_device(pz_ctx *ctx, uint64_t *d_polys, size_t count, void *stream);
+pz_status pz_rlwe_by_rgsw_device(pz_ctx *ctx, const pz_key *key, uint64_t *d_rlwe,
+                                 const uint32_t *d_lwe_index, size_t count, int trivial, void *stream);
+pz_status pz_rlwe_auto_device(pz_ctx *ctx, const pz_key *key, uint64_t *d_rlwe,
+                              const uint32_t *d_slot, size_t count, int trivial, void *stream);
+/* d_lwe_in [count][N + 1] mod q_ks -> d_out [count][n + 1] u32 mod q_ks */
+pz_status pz_lwe_key_switch_device(pz_ctx *ctx, const pz_key *key, const uint64_t *d_lwe_in,
+                                   uint32_t *d_out, size_t count, void *stream);
+
+/* Blind-rotation launch shape: 0 = one CTA per ciphertext; > 0 caps the grid
+ * (the kernel then strides over the batch). */
+pz_status pz_ctx_set_pbs_grid_limit(pz_ctx *ctx, int grid_limit);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

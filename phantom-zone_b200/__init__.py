@@ -1,0 +1,12 @@
+"""phantom-zone_b200: B200-native server-side gate bootstrap for phantom-zone.
+
+The hot path (LWE key switch -> automorphism-based blind rotation -> sample
+extraction) runs in hand-written CUDA kernels for sm_100a behind the C ABI
+declared in include/phantom_zone_b200.h; this package is the Python host side
+(ctypes) mirroring the reference's BoolEvaluator / BooleanGates / FheUint8
+interface.  Import it with ``importlib.import_module("phantom-zone_b200")``.
+"""
+from . import _lib
+from .engine import GATES, PARAMETER_SETS, SELECTORS, DeviceKey, Engine, param_id, params
+
+__all__ = ["Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "param_id", "params", "_lib"]

@@ -1,0 +1,93 @@
+"""ctypes binding of the C ABI in include/phantom_zone_b200.h.
+
+The engine is the CUDA library ``libpz_b200.so`` built in this package
+directory (``make -C phantom-zone_b200``).  There is no CPU fallback: if the
+library is missing or a call fails, an exception is raised.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpz_b200.so")
+
+u64p = ctypes.POINTER(ctypes.c_uint64)
+u32p = ctypes.POINTER(ctypes.c_uint32)
+u8p = ctypes.POINTER(ctypes.c_uint8)
+vp = ctypes.c_void_p
+st = ctypes.c_int
+
+
+class PzParams(ctypes.Structure):
+    _fields_ = [
+        ("rlwe_q", ctypes.c_uint64), ("lwe_q", ctypes.c_uint64),
+        ("br_q", ctypes.c_uint32), ("rlwe_n", ctypes.c_uint32), ("lwe_n", ctypes.c_uint32),
+        ("lwe_logb", ctypes.c_uint32), ("lwe_d", ctypes.c_uint32),
+        ("rlrg_logb", ctypes.c_uint32), ("rlrg_d_a", ctypes.c_uint32), ("rlrg_d_b", ctypes.c_uint32),
+        ("auto_logb", ctypes.c_uint32), ("auto_d", ctypes.c_uint32),
+        ("g", ctypes.c_uint32), ("w", ctypes.c_uint32),
+        ("lwe_secret_gaussian", ctypes.c_uint32), ("variant", ctypes.c_uint32),
+        ("embedding_factor", ctypes.c_uint32), ("rgsw_rows", ctypes.c_uint32),
+        ("auto_rows", ctypes.c_uint32), ("n_auto_keys", ctypes.c_uint32),
+    ]
+
+
+class PzServerKeyView(ctypes.Structure):
+    _fields_ = [("rgsw", u64p), ("autos", u64p), ("lwe_ksk", u64p)]
+
+
+# name -> (restype, argtypes); every symbol declared in the public header
+SIGNATURES = {
+    "pz_status_string": (ctypes.c_char_p, [st]),
+    "pz_param_get": (st, [ctypes.c_int, ctypes.POINTER(PzParams)]),
+    "pz_ctx_create": (st, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]),
+    "pz_ctx_create_ex": (st, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(vp)]),
+    "pz_ctx_destroy": (None, [vp]),
+    "pz_last_error": (ctypes.c_char_p, [vp]),
+    "pz_ctx_params": (st, [vp, ctypes.POINTER(PzParams)]),
+    "pz_ctx_ntt_root": (ctypes.c_uint64, [vp]),
+    "pz_key_upload": (st, [vp, ctypes.POINTER(PzServerKeyView), ctypes.POINTER(vp)]),
+    "pz_key_release": (None, [vp]),
+    "pz_key_device_bytes": (ctypes.c_size_t, [vp]),
+    "pz_gate_batch": (st, [vp, vp, u8p, u64p, u64p, u64p, ctypes.c_size_t]),
+    "pz_gate_batch_device": (st, [vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_gate_batch_debug_device": (st, [vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp, vp, vp]),
+    "pz_pbs_batch_device": (st, [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_not_batch_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_ntt_forward_device": (st, [vp, vp, ctypes.c_size_t, vp]),
+    "pz_ntt_backward_device": (st, [vp, vp, ctypes.c_size_t, vp]),
+    "pz_rlwe_by_rgsw_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, ctypes.c_int, vp]),
+    "pz_rlwe_auto_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, ctypes.c_int, vp]),
+    "pz_lwe_key_switch_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_ctx_set_pbs_grid_limit": (st, [vp, ctypes.c_int]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libpz_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"CUDA engine not built: {LIB_PATH} is missing (run `make -C phantom-zone_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class PzError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+def check(status, ctx=None, what=""):
+    if status != 0:
+        L = lib()
+        detail = L.pz_last_error(ctx).decode() if ctx else L.pz_status_string(status).decode()
+        raise PzError(status, f"{what}: {L.pz_status_string(status).decode()}: {detail}")

@@ -1,0 +1,712 @@
+// pz_kernels.cu -- CUDA kernels of the gate bootstrap for sm_100a.
+//
+//   key_convert   coefficient-domain key rows -> device evaluation layout
+//                 (forward NTT, * N^{-1} * 2^64 mod Q), keys.rs:702-757
+//   ntt_fwd/inv   batched negacyclic NTT in the reference's index order
+//                 (ntt.rs:409-441), the kernel microbench
+//   ext_product   batched RLWE x RGSW (runtime.rs:754-855)
+//   rlwe_auto     batched RLWE automorphism (runtime.rs:530-643)
+//   ks            gate prelude (evaluator.rs:2118-2133) + mod-down Q -> q_ks
+//                 (pbs.rs:128-132) + LWE key switch (lwe.rs:14-44), batched
+//   pbs           one CTA per ciphertext: odd mod-switch, dlog buckets, test
+//                 vector rotation, the whole blind rotation with the RLWE
+//                 accumulator resident on chip, sample extraction
+//                 (pbs.rs:146-449)
+#include "pz_kernels.cuh"
+
+namespace pz {
+
+// ---------------------------------------------------------------------------
+// Key conversion and NTT microbench
+// ---------------------------------------------------------------------------
+template <int LOGN>
+__global__ void __launch_bounds__(NttShape<LOGN>::T)
+    key_convert_kernel(const u64 *in, u64 *out, size_t npolys, RingConsts rc, u64 c, u64 cs) {
+  constexpr int N = 1 << LOGN;
+  __shared__ u64 sm[N];
+  const int j = threadIdx.x;
+  for (size_t pidx = blockIdx.x; pidx < npolys; pidx += gridDim.x) {
+    const u64 *src = in + pidx * N;
+    u64 x[1][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) x[0][r] = src[pos_coef<LOGN>(j, r)];
+    ntt_forward<LOGN, 1>(x, sm, rc);
+    u64 *dst = out + pidx * N;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      u64 v = reduce4(x[0][r], rc.q);
+      v = reduce2(shoup_mul(v, c, cs, rc.q), rc.q);
+      dst[dev_index<LOGN>(j, r)] = v;
+    }
+    __syncthreads();
+  }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(NttShape<LOGN>::T)
+    ntt_fwd_kernel(u64 *polys, size_t count, RingConsts rc) {
+  constexpr int N = 1 << LOGN;
+  __shared__ u64 sm[N];
+  const int j = threadIdx.x;
+  for (size_t pidx = blockIdx.x; pidx < count; pidx += gridDim.x) {
+    u64 *p = polys + pidx * N;
+    u64 x[1][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) x[0][r] = p[pos_coef<LOGN>(j, r)];
+    ntt_forward<LOGN, 1>(x, sm, rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++) p[pos_eval<LOGN>(j, r)] = reduce4(x[0][r], rc.q);
+    __syncthreads();
+  }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(NttShape<LOGN>::T)
+    ntt_inv_kernel(u64 *polys, size_t count, RingConsts rc) {
+  constexpr int N = 1 << LOGN;
+  __shared__ u64 sm[N];
+  const int j = threadIdx.x;
+  for (size_t pidx = blockIdx.x; pidx < count; pidx += gridDim.x) {
+    u64 *p = polys + pidx * N;
+    u64 x[1][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) x[0][r] = p[pos_eval<LOGN>(j, r)];
+    ntt_inverse<LOGN, 1>(x, sm, rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+      p[pos_coef<LOGN>(j, r)] = reduce2(shoup_mul(x[0][r], rc.n_inv, rc.n_inv_s, rc.q), rc.q);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RLWE x RGSW (runtime.rs:754-855).  acc: coefficient layout, canonical.
+// sm: 3N words.  Device RGSW rows: A(-sm) x d_a, B(-sm) x d_a, A(m) x d_b,
+// B(m) x d_b (runtime.rs:174-180).
+// ---------------------------------------------------------------------------
+template <int LOGN, bool D1>
+__device__ __forceinline__ void ext_product(u64 (&acc)[2][8], const u64 *ct, bool trivial,
+                                            const BrParams &P, u64 *sm) {
+  constexpr int N = 1 << LOGN;
+  const u64 q = P.rc.q, qi = P.rc.qinv_neg;
+  if (D1) {
+    if (!trivial) {
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        u64 sa = decomp_init(acc[0][r], P.da);
+        acc[0][r] = decomp_next(sa, P.da);
+        u64 sb = decomp_init(acc[1][r], P.db);
+        acc[1][r] = decomp_next(sb, P.db);
+      }
+      ntt_forward<LOGN, 2>(acc, sm, P.rc);
+      const u64 *K0 = ct, *K1 = ct + N, *K2 = ct + 2 * N, *K3 = ct + 3 * N;
+      const int j = threadIdx.x;
+#pragma unroll
+      for (int rr = 0; rr < 4; rr++) {
+        u64 k0[2], k1[2], k2[2], k3[2];
+        const int di = dev_index<LOGN>(j, 2 * rr);
+        ld_key2(K0 + di, k0[0], k0[1]);
+        ld_key2(K1 + di, k1[0], k1[1]);
+        ld_key2(K2 + di, k2[0], k2[1]);
+        ld_key2(K3 + di, k3[0], k3[1]);
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int r = 2 * rr + e;
+          const u64 xa = acc[0][r], xb = acc[1][r];
+          u64 hi, lo;
+          mul128(xa, k0[e], hi, lo);
+          mac128(xb, k2[e], hi, lo);
+          const u64 oa = redc(hi, lo, q, qi);
+          mul128(xa, k1[e], hi, lo);
+          mac128(xb, k3[e], hi, lo);
+          const u64 ob = redc(hi, lo, q, qi);
+          acc[0][r] = oa;
+          acc[1][r] = ob;
+        }
+      }
+    } else {
+      // a = 0: only decomp<b> x RLWE'(m) contributes (runtime.rs:790-818 skipped)
+      u64 x[1][8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        u64 sb = decomp_init(acc[1][r], P.db);
+        x[0][r] = decomp_next(sb, P.db);
+      }
+      ntt_forward<LOGN, 1>(x, sm, P.rc);
+      const u64 *K2 = ct + 2 * N, *K3 = ct + 3 * N;
+      const int j = threadIdx.x;
+#pragma unroll
+      for (int rr = 0; rr < 4; rr++) {
+        u64 k2[2], k3[2];
+        const int di = dev_index<LOGN>(j, 2 * rr);
+        ld_key2(K2 + di, k2[0], k2[1]);
+        ld_key2(K3 + di, k3[0], k3[1]);
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int r = 2 * rr + e;
+          u64 hi, lo;
+          mul128(x[0][r], k2[e], hi, lo);
+          acc[0][r] = redc(hi, lo, q, qi);
+          mul128(x[0][r], k3[e], hi, lo);
+          acc[1][r] = redc(hi, lo, q, qi);
+        }
+      }
+    }
+    ntt_inverse<LOGN, 2>(acc, sm, P.rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      acc[0][r] = reduce2(acc[0][r], q);
+      acc[1][r] = reduce2(acc[1][r], q);
+    }
+  } else {
+    // general decomposition counts (SP_TEST: d_a = d_b = 4)
+    const u32 da = P.d_a, db = P.d_b;
+    const u32 dmax = da > db ? da : db;
+    u64 sa[8], sb[8], o[2][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      sa[r] = trivial ? 0 : decomp_init(acc[0][r], P.da);
+      sb[r] = decomp_init(acc[1][r], P.db);
+      o[0][r] = 0;
+      o[1][r] = 0;
+    }
+    for (u32 jd = 0; jd < dmax; jd++) {
+      const bool ha = !trivial && jd < da, hb = jd < db;
+      u64 x[2][8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        x[0][r] = ha ? decomp_next(sa[r], P.da) : 0;
+        x[1][r] = hb ? decomp_next(sb[r], P.db) : 0;
+      }
+      ntt_forward<LOGN, 2>(x, sm, P.rc);
+      u64 kaa[8], kba[8], kam[8], kbm[8];
+      if (ha) {
+        load_key_row<LOGN>(ct + (size_t)jd * N, kaa);
+        load_key_row<LOGN>(ct + (size_t)(da + jd) * N, kba);
+      }
+      if (hb) {
+        load_key_row<LOGN>(ct + (size_t)(2 * da + jd) * N, kam);
+        load_key_row<LOGN>(ct + (size_t)(2 * da + db + jd) * N, kbm);
+      }
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        u64 hi = 0, lo = 0, hi2 = 0, lo2 = 0;
+        if (ha) { mac128(x[0][r], kaa[r], hi, lo); mac128(x[0][r], kba[r], hi2, lo2); }
+        if (hb) { mac128(x[1][r], kam[r], hi, lo); mac128(x[1][r], kbm[r], hi2, lo2); }
+        u64 va = o[0][r] + redc(hi, lo, q, qi), vb = o[1][r] + redc(hi2, lo2, q, qi);
+        o[0][r] = va >= 2 * q ? va - 2 * q : va;
+        o[1][r] = vb >= 2 * q ? vb - 2 * q : vb;
+      }
+    }
+    ntt_inverse<LOGN, 2>(o, sm, P.rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      acc[0][r] = reduce2(o[0][r], q);
+      acc[1][r] = reduce2(o[1][r], q);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RLWE automorphism (runtime.rs:530-643).  Slot 0 is -g, slot v is g^v.
+// ---------------------------------------------------------------------------
+template <int LOGN, bool D1>
+__device__ __forceinline__ void rlwe_auto(u64 (&acc)[2][8], int slot, bool trivial, const BrParams &P,
+                                          u64 *sm) {
+  constexpr int N = 1 << LOGN;
+  const u64 q = P.rc.q, qi = P.rc.qinv_neg;
+  const u32 k = P.auto_k[slot];
+  const int j = threadIdx.x;
+  u64 *s_a = sm, *s_b = sm + 2 * N;
+  __syncthreads();
+  // a(X) -> a(X^k), b(X) -> b(X^k) with sign (generate_auto_map, keygen.rs:16-41)
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const u32 i = (u32)pos_coef<LOGN>(j, r);
+    u32 t = (i * k) & (2 * N - 1);
+    const bool neg = t >= (u32)N;
+    if (neg) t -= N;
+    if (!trivial) s_a[swz(t)] = neg ? q - acc[0][r] : acc[0][r];
+    s_b[swz(t)] = neg ? q - acc[1][r] : acc[1][r];
+  }
+  __syncthreads();
+  if (trivial) {
+#pragma unroll
+    for (int r = 0; r < 8; r++) acc[1][r] = s_b[swz(pos_coef<LOGN>(j, r))];
+    return;
+  }
+  const u64 *KA = P.autos + (size_t)slot * P.auto_rows * N;
+  if (D1) {
+    u64 x[1][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      u64 st = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
+      x[0][r] = decomp_next(st, P.dauto);
+    }
+    ntt_forward<LOGN, 1>(x, sm, P.rc);
+    const u64 *K0 = KA, *K1 = KA + N;
+#pragma unroll
+    for (int rr = 0; rr < 4; rr++) {
+      u64 k0[2], k1[2];
+      const int di = dev_index<LOGN>(j, 2 * rr);
+      ld_key2(K0 + di, k0[0], k0[1]);
+      ld_key2(K1 + di, k1[0], k1[1]);
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int r = 2 * rr + e;
+        u64 hi, lo;
+        mul128(x[0][r], k0[e], hi, lo);
+        acc[0][r] = redc(hi, lo, q, qi);
+        mul128(x[0][r], k1[e], hi, lo);
+        acc[1][r] = redc(hi, lo, q, qi);
+      }
+    }
+    ntt_inverse<LOGN, 2>(acc, sm, P.rc);
+  } else {
+    const u32 d = P.d_auto;
+    u64 st[8], o[2][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      st[r] = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
+      o[0][r] = 0;
+      o[1][r] = 0;
+    }
+    for (u32 jd = 0; jd < d; jd++) {
+      u64 x[1][8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) x[0][r] = decomp_next(st[r], P.dauto);
+      ntt_forward<LOGN, 1>(x, sm, P.rc);
+      u64 ka[8], kb[8];
+      load_key_row<LOGN>(KA + (size_t)jd * N, ka);
+      load_key_row<LOGN>(KA + (size_t)(d + jd) * N, kb);
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        u64 hi, lo;
+        mul128(x[0][r], ka[r], hi, lo);
+        u64 va = o[0][r] + redc(hi, lo, q, qi);
+        mul128(x[0][r], kb[r], hi, lo);
+        u64 vb = o[1][r] + redc(hi, lo, q, qi);
+        o[0][r] = va >= 2 * q ? va - 2 * q : va;
+        o[1][r] = vb >= 2 * q ? vb - 2 * q : vb;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      acc[0][r] = o[0][r];
+      acc[1][r] = o[1][r];
+    }
+    ntt_inverse<LOGN, 2>(acc, sm, P.rc);
+  }
+  // b' += b(X^k) with sign: add_mod of the signed value == sub_mod_fast /
+  // add_mod_fast of runtime.rs:608-620 (the signed value is q - b or b).
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    acc[0][r] = reduce2(acc[0][r], q);
+    acc[1][r] = add_mod(reduce2(acc[1][r], q), s_b[swz(pos_coef<LOGN>(j, r))], q);
+  }
+}
+
+template <int LOGN, bool D1>
+__global__ void __launch_bounds__(NttShape<LOGN>::T)
+    ext_product_kernel(BrParams P, u64 *rlwe, const u32 *idx, size_t count, int trivial) {
+  constexpr int N = 1 << LOGN;
+  extern __shared__ u64 smem[];
+  const int j = threadIdx.x;
+  for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    u64 *p = rlwe + c * 2 * N;
+    u64 acc[2][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      acc[0][r] = p[pos_coef<LOGN>(j, r)];
+      acc[1][r] = p[N + pos_coef<LOGN>(j, r)];
+    }
+    ext_product<LOGN, D1>(acc, P.rgsw + (size_t)idx[c] * P.rgsw_rows * N, trivial != 0, P, smem);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      p[pos_coef<LOGN>(j, r)] = acc[0][r];
+      p[N + pos_coef<LOGN>(j, r)] = acc[1][r];
+    }
+    __syncthreads();
+  }
+}
+
+template <int LOGN, bool D1>
+__global__ void __launch_bounds__(NttShape<LOGN>::T)
+    auto_kernel(BrParams P, u64 *rlwe, const u32 *slot, size_t count, int trivial) {
+  constexpr int N = 1 << LOGN;
+  extern __shared__ u64 smem[];
+  const int j = threadIdx.x;
+  for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    u64 *p = rlwe + c * 2 * N;
+    u64 acc[2][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      acc[0][r] = p[pos_coef<LOGN>(j, r)];
+      acc[1][r] = p[N + pos_coef<LOGN>(j, r)];
+    }
+    rlwe_auto<LOGN, D1>(acc, (int)slot[c], trivial != 0, P, smem);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      p[pos_coef<LOGN>(j, r)] = acc[0][r];
+      p[N + pos_coef<LOGN>(j, r)] = acc[1][r];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gate prelude + mod-down + LWE key switch
+// ---------------------------------------------------------------------------
+// evaluator.rs:2118-2133 then pbs.rs:128-132 for one coefficient.
+__device__ __forceinline__ u64 prelude_moddown(u64 x0, u64 x1, unsigned char gate, bool is_b,
+                                               const KsParams &P) {
+  u64 v;
+  if (P.raw || (gate & GATE_RAW)) {
+    v = x0;
+  } else if (gate >= 4) {  // xor, xnor: 2 (c0 - c1)
+    v = sub_mod(x0, x1, P.Q);
+    v = add_mod(v, v, P.Q);
+  } else {  // and, nand, or, nor: c0 + c1 (+ Q/4 on b)
+    v = add_mod(x0, x1, P.Q);
+    if (is_b) v = add_mod(v, P.qby4, P.Q);
+  }
+  double f = __ddiv_rn(__dmul_rn(__ull2double_rn(v), P.q_ks_f), P.Q_f);
+  return (u64)round(f);
+}
+
+constexpr int KS_CT = 16;    // ciphertexts per CTA
+constexpr int KS_IC = 32;    // LWE coefficients per digit chunk
+constexpr int KS_COLS = 128; // output columns per CTA
+
+__global__ void __launch_bounds__(KS_COLS)
+    ks_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
+  __shared__ u32 dig[KS_CT][KS_IC][MAX_KS_D];
+  const int tid = threadIdx.x;
+  const int col = blockIdx.y * KS_COLS + tid;
+  const int ct0 = blockIdx.x * KS_CT;
+  const size_t L = (size_t)P.N + 1;
+  const u32 d = P.d;
+  u32 acc[KS_CT];
+#pragma unroll
+  for (int c = 0; c < KS_CT; c++) acc[c] = 0;
+  for (u32 i0 = 0; i0 < P.N; i0 += KS_IC) {
+    __syncthreads();
+    for (int e = tid; e < KS_CT * KS_IC; e += KS_COLS) {
+      const int c = e / KS_IC, ii = e % KS_IC;
+      const int ct = ct0 + c;
+      if (ct < count) {
+        const size_t off = (size_t)ct * L + 1 + i0 + ii;
+        const u64 x = prelude_moddown(c0[off], c1 ? c1[off] : 0, gates ? gates[ct] : 0, false, P);
+        u64 st = decomp_init(x, P.dks);
+        for (u32 jd = 0; jd < d; jd++) dig[c][ii][jd] = (u32)decomp_next(st, P.dks);
+      } else {
+        for (u32 jd = 0; jd < d; jd++) dig[c][ii][jd] = 0;
+      }
+    }
+    __syncthreads();
+    if (col <= (int)P.n) {
+      const u32 *kp = P.ksk + (size_t)i0 * d * P.ksk_stride + col;
+      for (int ii = 0; ii < KS_IC; ii++) {
+        for (u32 jd = 0; jd < d; jd++) {
+          const u32 kv = __ldg(kp);
+          kp += P.ksk_stride;
+#pragma unroll
+          for (int c = 0; c < KS_CT; c++) acc[c] += dig[c][ii][jd] * kv;
+        }
+      }
+    }
+  }
+  if (col <= (int)P.n) {
+#pragma unroll
+    for (int c = 0; c < KS_CT; c++) {
+      const int ct = ct0 + c;
+      if (ct < count) {
+        u32 v = acc[c];
+        if (col == 0) {
+          const size_t off = (size_t)ct * L;
+          v += (u32)prelude_moddown(c0[off], c1 ? c1[off] : 0, gates ? gates[ct] : 0, true, P);
+        }
+        out[(size_t)ct * P.out_stride + col] = v & P.mask;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The bootstrap: one CTA per ciphertext (grid-stride over the batch)
+// ---------------------------------------------------------------------------
+// pbs.rs:416-420
+__device__ __forceinline__ u32 mod_switch_odd(u32 v, double from_q, double to_q) {
+  u64 odd = (u64)floor(__ddiv_rn(__dmul_rn((double)v, to_q), from_q));
+  return (u32)(odd + ((odd & 1ull) ^ 1ull));
+}
+
+size_t pbs_smem_bytes(int logn, u32 br_q, u32 n) {
+  size_t N = (size_t)1 << logn;
+  size_t extra = ((size_t)(br_q / 2 + 1) + n) * 2;
+  extra = (extra + 15) & ~(size_t)15;
+  return 3 * N * 8 + extra;
+}
+
+template <int LOGN, bool D1>
+__global__ void __launch_bounds__(NttShape<LOGN>::T)
+    pbs_kernel(BrParams P, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out, int count,
+               u64 *rlwe_dbg) {
+  constexpr int N = 1 << LOGN, T = NttShape<LOGN>::T;
+  extern __shared__ u64 smem[];
+  u64 *sm = smem;
+  const u32 R = P.br_q >> 1, q4 = P.br_q >> 2, n = P.n;
+  unsigned short *s_start = (unsigned short *)(smem + 3 * N);  // R + 1 entries
+  unsigned short *s_list = s_start + (R + 1);                  // n entries
+  const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
+  const u64 q = P.rc.q;
+
+  for (int ct = blockIdx.x; ct < count; ct += gridDim.x) {
+    const u32 *kso = ks + (size_t)ct * ks_stride;
+    // ---- odd mod-switch + dlog buckets (pbs.rs:147-161), stable in LWE index
+    u32 *cnt = (u32 *)sm;                             // R counters (region 0)
+    unsigned short *keys = (unsigned short *)(sm + N);  // n keys (region 1)
+    u32 *scan = (u32 *)(sm + N) + 512;                // T partial sums (region 1, after keys)
+    u32 *fill = (u32 *)(sm + 2 * N);                  // R fill counters (region 2)
+    __syncthreads();
+    for (u32 b = j; b < R; b += T) { cnt[b] = 0; fill[b] = 0; }
+    __syncthreads();
+    for (u32 i = j; i < n; i += T) {
+      const u32 odd = mod_switch_odd(kso[1 + i], P.q_ks_f, P.br_q_f);
+      const u32 k = P.dlog[odd];
+      keys[i] = (unsigned short)k;
+      atomicAdd(&cnt[k], 1u);
+    }
+    __syncthreads();
+    {  // exclusive scan of cnt[0..R) into s_start, s_start[R] = n
+      const u32 per = (R + T - 1) / T;
+      const u32 b0 = j * per;
+      u32 local = 0;
+      for (u32 b = b0; b < b0 + per && b < R; b++) local += cnt[b];
+      u32 incl = local;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        u32 y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) scan[warp] = incl;
+      __syncthreads();
+      u32 woff = 0;
+      for (int w2 = 0; w2 < warp; w2++) woff += scan[w2];
+      u32 run = woff + incl - local;
+      for (u32 b = b0; b < b0 + per && b < R; b++) {
+        s_start[b] = (unsigned short)run;
+        run += cnt[b];
+      }
+      if (j == 0) s_start[R] = (unsigned short)n;
+    }
+    __syncthreads();
+    if (warp == 0) {  // stable placement: within a bucket, increasing LWE index
+      for (u32 i0 = 0; i0 < n; i0 += 32) {
+        const u32 i = i0 + lane;
+        const bool valid = i < n;
+        const u32 k = valid ? keys[i] : 0xFFFFu;
+        const u32 peers = __match_any_sync(0xffffffffu, k);
+        const u32 rank = __popc(peers & ((1u << lane) - 1u));
+        if (valid) s_list[s_start[k] + fill[k] + rank] = (unsigned short)i;
+        __syncwarp();
+        if (valid && rank == 0) fill[k] += __popc(peers);
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+
+    // ---- trivial test RLWE: X^{g * odd(b)} * tv, embedded (pbs.rs:163-211)
+    const u32 odd_b = mod_switch_odd(kso[0], P.q_ks_f, P.br_q_f);
+    const u32 gb = (u32)(((u64)P.g * odd_b) % P.br_q);
+    u32 mexp = gb;
+    bool msign = true;
+    if (mexp > R) { mexp -= R; msign = false; }
+    u32 gi = gates[ct] & 7u;
+    if (gi > 5) gi = 5;  // codes are validated on the host; never index past the 6 test vectors
+    const u64 *tv = P.tv + (size_t)gi * R;
+    u64 acc[2][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const u32 p = (u32)pos_coef<LOGN>(j, r);
+      acc[0][r] = 0;
+      u64 v = 0;
+      if (p % P.emb == 0) {
+        const u32 o = p / P.emb;
+        u32 s;
+        bool sg;
+        if (o >= mexp) { s = o - mexp; sg = msign; } else { s = o + R - mexp; sg = !msign; }
+        const u64 t = tv[s];
+        v = sg ? t : q - t;
+      }
+      acc[1][r] = v;
+    }
+
+    // ---- blind rotation (pbs.rs:240-414)
+    bool trivial = true;
+    const u64 *rgsw = P.rgsw;
+    const size_t ct_words = (size_t)P.rgsw_rows * N;
+    auto bucket = [&](u32 b) {
+      const u32 e = s_start[b + 1];
+      for (u32 t = s_start[b]; t < e; t++) {
+        ext_product<LOGN, D1>(acc, rgsw + (size_t)s_list[t] * ct_words, trivial, P, sm);
+        trivial = false;
+      }
+    };
+    u32 v = 0;
+    for (u32 i = q4 - 1; i >= 1; i--) {  // -(g^k)
+      bucket(q4 + i);
+      v++;
+      if (s_start[q4 + i] != s_start[q4 + i - 1] || v == P.w || i == 1) {
+        rlwe_auto<LOGN, D1>(acc, (int)v, trivial, P, sm);
+        v = 0;
+      }
+    }
+    bucket(q4);  // -(g^0)
+    rlwe_auto<LOGN, D1>(acc, 0, trivial, P, sm);
+    v = 0;
+    for (u32 i = q4 - 1; i >= 1; i--) {  // +(g^k)
+      bucket(i);
+      v++;
+      if (s_start[i] != s_start[i - 1] || v == P.w || i == 1) {
+        rlwe_auto<LOGN, D1>(acc, (int)v, trivial, P, sm);
+        v = 0;
+      }
+    }
+    bucket(0);  // +(g^0)
+
+    // ---- sample extract at index 0 (pbs.rs:423-449)
+    u64 *o = out + (size_t)ct * (N + 1);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const u32 p = (u32)pos_coef<LOGN>(j, r);
+      if (p == 0) {
+        o[0] = acc[1][r];
+        o[1] = acc[0][r];
+      } else {
+        o[1 + N - p] = q - acc[0][r];
+      }
+    }
+    if (rlwe_dbg) {
+      u64 *d = rlwe_dbg + (size_t)ct * 2 * N;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        d[pos_coef<LOGN>(j, r)] = acc[0][r];
+        d[N + pos_coef<LOGN>(j, r)] = acc[1][r];
+      }
+    }
+  }
+}
+
+__global__ void not_kernel(const u64 *in, u64 *out, size_t words, u64 q) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = q - in[i];  // neg = q - a, evaluator.rs:2247-2250
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+static int grid_for(size_t count) { return (int)(count < 65535 * 16 ? count : 65535 * 16); }
+
+cudaError_t launch_key_convert(int logn, const u64 *in, u64 *out, size_t npolys, const RingConsts &rc,
+                               u64 c, u64 cs, cudaStream_t s) {
+  if (npolys == 0) return cudaSuccess;
+  if (logn == 11) key_convert_kernel<11><<<grid_for(npolys), 256, 0, s>>>(in, out, npolys, rc, c, cs);
+  else if (logn == 9) key_convert_kernel<9><<<grid_for(npolys), 64, 0, s>>>(in, out, npolys, rc, c, cs);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  if (logn == 11) ntt_fwd_kernel<11><<<grid_for(count), 256, 0, s>>>(polys, count, rc);
+  else if (logn == 9) ntt_fwd_kernel<9><<<grid_for(count), 64, 0, s>>>(polys, count, rc);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  if (logn == 11) ntt_inv_kernel<11><<<grid_for(count), 256, 0, s>>>(polys, count, rc);
+  else if (logn == 9) ntt_inv_kernel<9><<<grid_for(count), 64, 0, s>>>(polys, count, rc);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+template <typename K>
+static cudaError_t set_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
+                               size_t count, int trivial, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  const size_t N = (size_t)1 << logn, smem = 3 * N * 8;
+  cudaError_t e;
+#define PZ_LAUNCH(LN, DD, TH)                                                                  \
+  if ((e = set_smem(ext_product_kernel<LN, DD>, smem)) != cudaSuccess) return e;              \
+  ext_product_kernel<LN, DD><<<grid_for(count), TH, smem, s>>>(P, rlwe, idx, count, trivial);
+  if (logn == 11 && d1) { PZ_LAUNCH(11, true, 256) }
+  else if (logn == 11) { PZ_LAUNCH(11, false, 256) }
+  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 64) }
+  else if (logn == 9) { PZ_LAUNCH(9, false, 64) }
+  else return cudaErrorInvalidValue;
+#undef PZ_LAUNCH
+  return cudaGetLastError();
+}
+
+cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *slot, size_t count,
+                        int trivial, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  const size_t N = (size_t)1 << logn, smem = 3 * N * 8;
+  cudaError_t e;
+#define PZ_LAUNCH(LN, DD, TH)                                                           \
+  if ((e = set_smem(auto_kernel<LN, DD>, smem)) != cudaSuccess) return e;              \
+  auto_kernel<LN, DD><<<grid_for(count), TH, smem, s>>>(P, rlwe, slot, count, trivial);
+  if (logn == 11 && d1) { PZ_LAUNCH(11, true, 256) }
+  else if (logn == 11) { PZ_LAUNCH(11, false, 256) }
+  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 64) }
+  else if (logn == 9) { PZ_LAUNCH(9, false, 64) }
+  else return cudaErrorInvalidValue;
+#undef PZ_LAUNCH
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
+                      size_t count, u32 *out, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  if (P.d > (u32)MAX_KS_D) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((count + KS_CT - 1) / KS_CT), (unsigned)((P.n + 1 + KS_COLS - 1) / KS_COLS));
+  ks_kernel<<<grid, KS_COLS, 0, s>>>(P, gates, c0, c1, (int)count, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
+                       const unsigned char *gates, u64 *out, size_t count, u64 *rlwe_dbg, int grid_limit,
+                       cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  const size_t smem = pbs_smem_bytes(logn, P.br_q, P.n);
+  int grid = (int)count;
+  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
+  cudaError_t e;
+#define PZ_LAUNCH(LN, DD, TH)                                                                        \
+  if ((e = set_smem(pbs_kernel<LN, DD>, smem)) != cudaSuccess) return e;                            \
+  pbs_kernel<LN, DD><<<grid, TH, smem, s>>>(P, ks, ks_stride, gates, out, (int)count, rlwe_dbg);
+  if (logn == 11 && d1) { PZ_LAUNCH(11, true, 256) }
+  else if (logn == 11) { PZ_LAUNCH(11, false, 256) }
+  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 64) }
+  else if (logn == 9) { PZ_LAUNCH(9, false, 64) }
+  else return cudaErrorInvalidValue;
+#undef PZ_LAUNCH
+  return cudaGetLastError();
+}
+
+cudaError_t launch_not(const u64 *in, u64 *out, size_t words, u64 q, cudaStream_t s) {
+  if (words == 0) return cudaSuccess;
+  size_t blocks = (words + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  not_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, out, words, q);
+  return cudaGetLastError();
+}
+
+}  // namespace pz

@@ -1,0 +1,59 @@
+// pz_kernels.cuh -- parameter blocks shared by the kernels and the host runtime.
+#pragma once
+#include "pz_device.cuh"
+
+namespace pz {
+
+constexpr int MAX_KS_D = 16;   // key-switch decomposition count bound
+constexpr int MAX_AUTO_SLOTS = 16;
+
+// Everything the blind rotation needs for one parameter set + server key.
+struct BrParams {
+  RingConsts rc;
+  Decomp da, db, dauto;
+  u32 d_a, d_b, d_auto;
+  u32 rgsw_rows, auto_rows;
+  u32 n, br_q, w, g, emb;
+  double q_ks_f, br_q_f;           // mod_switch_odd operands (pbs.rs:416-420)
+  u32 auto_k[MAX_AUTO_SLOTS];      // automorphism element mod 2N per key slot
+  const unsigned short *dlog;      // [br_q]
+  const u64 *tv;                   // [6][br_q/2] test vectors
+  const u64 *rgsw;                 // [n][rgsw_rows][N] device layout, Montgomery form
+  const u64 *autos;                // [w+1][auto_rows][N]
+};
+
+// Gate prelude + mod-down + LWE key switch.
+struct KsParams {
+  u64 Q, qby4;
+  u32 mask;                 // q_ks - 1
+  double q_ks_f, Q_f;       // pbs.rs:128-132 operands
+  Decomp dks;
+  u32 d, n, N;
+  u32 ksk_stride;           // u32 words per KSK row (>= n+1)
+  u32 out_stride;           // u32 words per output LWE (>= n+1)
+  u32 raw;                  // inputs are combined LWEs: skip the gate prelude
+  const u32 *ksk;           // [d N][ksk_stride]
+};
+
+// Gate codes 0..5 (and, nand, or, nor, xor, xnor).  GATE_RAW marks an input
+// that is already the combined LWE (no prelude); the low bits then select
+// the test vector.
+constexpr unsigned char GATE_RAW = 0x80;
+
+cudaError_t launch_key_convert(int logn, const u64 *in, u64 *out, size_t npolys, const RingConsts &rc,
+                               u64 c, u64 cs, cudaStream_t s);
+cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s);
+cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s);
+cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
+                               size_t count, int trivial, cudaStream_t s);
+cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *slot, size_t count,
+                        int trivial, cudaStream_t s);
+cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
+                      size_t count, u32 *out, cudaStream_t s);
+cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
+                       const unsigned char *gates, u64 *out, size_t count, u64 *rlwe_dbg,
+                       int grid_limit, cudaStream_t s);
+cudaError_t launch_not(const u64 *in, u64 *out, size_t words, u64 q, cudaStream_t s);
+size_t pbs_smem_bytes(int logn, u32 br_q, u32 n);
+
+}  // namespace pz

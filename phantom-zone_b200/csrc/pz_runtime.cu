@@ -1,0 +1,578 @@
+// pz_runtime.cu -- host runtime behind the C ABI (include/phantom_zone_b200.h).
+//
+// Owns per-context device tables (twiddles, dlog map, test vectors), device
+// server keys, scratch, and the launch sequence of a gate batch:
+//   ks kernel (prelude + mod-down + LWE key switch)  ->  pbs kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/phantom_zone_b200.h"
+#include "pz_kernels.cuh"
+
+using pz::u32;
+using pz::u64;
+typedef unsigned __int128 u128;
+
+namespace {
+
+// bool/parameters.rs:526-726
+const pz_params PARAMS[PZ_NUM_PARAMS] = {
+    // rlwe_q, lwe_q, br_q, N, n, lwe_logb, lwe_d, rlrg_logb, d_a, d_b, auto_logb, auto_d, g, w, gauss, variant
+    {18014398509404161ULL, 1ULL << 15, 1u << 11, 1u << 11, 580, 1, 12, 17, 1, 1, 24, 1, 5, 10, 0, 1, 0, 0, 0, 0},
+    {18014398509404161ULL, 1ULL << 16, 1u << 11, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 1, 0, 0, 0, 0},
+    {18014398509404161ULL, 1ULL << 17, 1u << 12, 1u << 11, 660, 1, 14, 17, 1, 1, 24, 1, 5, 10, 0, 1, 0, 0, 0, 0},
+    {18014398509404161ULL, 1ULL << 16, 1u << 12, 1u << 11, 520, 1, 13, 17, 1, 1, 24, 1, 5, 10, 1, 2, 0, 0, 0, 0},
+    {18014398509404161ULL, 1ULL << 16, 1u << 11, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 2, 0, 0, 0, 0},
+    {18014398509404161ULL, 1ULL << 16, 1u << 12, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 2, 0, 0, 0, 0},
+    {18014398509404161ULL, 1ULL << 17, 1u << 12, 1u << 11, 660, 1, 14, 17, 1, 1, 24, 1, 5, 10, 0, 2, 0, 0, 0, 0},
+    {268369921ULL, 1ULL << 16, 1u << 9, 1u << 9, 100, 4, 4, 7, 4, 4, 7, 4, 5, 5, 1, 0, 0, 0, 0, 0},
+};
+
+pz_params full_params(int id) {
+  pz_params p = PARAMS[id];
+  p.embedding_factor = 2 * p.rlwe_n / p.br_q;
+  p.rgsw_rows = 2 * p.rlrg_d_a + 2 * p.rlrg_d_b;
+  p.auto_rows = 2 * p.auto_d;
+  p.n_auto_keys = p.w + 1;
+  return p;
+}
+
+u64 mulmod(u64 a, u64 b, u64 q) { return (u64)(((u128)a * b) % q); }
+u64 powmod(u64 a, u64 e, u64 q) {
+  u64 r = 1 % q;
+  a %= q;
+  while (e) {
+    if (e & 1) r = mulmod(r, a, q);
+    a = mulmod(a, a, q);
+    e >>= 1;
+  }
+  return r;
+}
+u64 invmod(u64 a, u64 q) { return powmod(a, q - 2, q); }  // q prime
+u64 shoup(u64 v, u64 q) { return (u64)(((u128)v << 64) / q); }
+u32 log2_exact(u64 v) { return 63 - __builtin_clzll(v); }
+// utils.rs:230-237
+u32 log2_ref(u64 v) { return (v & (v - 1)) == 0 ? 63 - __builtin_clzll(v) : 64 - __builtin_clzll(v); }
+
+// A primitive 2N-th root of unity: c^((Q-1)/2N) for the smallest c >= 2
+// whose power has order exactly 2N (omega^N = -1).
+u64 default_root(u64 q, u64 two_n) {
+  for (u64 c = 2; c < 1000000; c++) {
+    u64 w = powmod(c, (q - 1) / two_n, q);
+    if (powmod(w, two_n / 2, q) == q - 1) return w;
+  }
+  return 0;
+}
+
+pz::Decomp make_decomp(u64 q, u32 logb, u32 d) {  // decomposer.rs:158-178
+  pz::Decomp dp;
+  dp.q = q;
+  dp.logb = logb;
+  dp.d = d;
+  dp.ignore_bits = log2_ref(q) - logb * d;
+  dp.bmask = (1ull << logb) - 1;
+  dp.bby2 = 1ull << (logb - 1);
+  return dp;
+}
+
+}  // namespace
+
+struct pz_ctx {
+  int param_id = 0, device = 0;
+  pz_params P{};
+  u32 logn = 0;
+  u64 root = 0;
+  cudaStream_t stream = nullptr;
+  // device tables
+  u64 *d_tw = nullptr;        // fw | fws | iw | iws  (4N words)
+  unsigned short *d_dlog = nullptr;
+  u64 *d_tv = nullptr;        // 6 x br_q/2
+  // constants
+  pz::RingConsts rc{};
+  u64 conv_c = 0, conv_cs = 0;
+  pz::BrParams br{};
+  pz::KsParams ks{};
+  int grid_limit = 0;
+  // host-API scratch (guarded by mu)
+  std::mutex mu;
+  size_t cap = 0;
+  u64 *d_c0 = nullptr, *d_c1 = nullptr, *d_out = nullptr;
+  unsigned char *d_gates = nullptr;
+  u32 *d_ks = nullptr;
+  std::string err;
+};
+
+struct pz_key {
+  pz_ctx *ctx = nullptr;
+  u64 *d_rgsw = nullptr, *d_autos = nullptr;
+  u32 *d_ksk = nullptr;
+  size_t bytes = 0;
+};
+
+namespace {
+
+pz_status fail(pz_ctx *ctx, pz_status s, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return s;
+}
+pz_status cuda_fail(pz_ctx *ctx, const char *what, cudaError_t e) {
+  pz_status s = (e == cudaErrorMemoryAllocation) ? PZ_ERR_OUT_OF_MEMORY : PZ_ERR_CUDA;
+  return fail(ctx, s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define PZ_CK(ctx, call)                                      \
+  do {                                                        \
+    cudaError_t _e = (call);                                  \
+    if (_e != cudaSuccess) return cuda_fail((ctx), #call, _e); \
+  } while (0)
+
+// Device entry points run on the caller's stream; NULL is the CUDA default
+// stream (the context's private stream only serves the synchronous host API).
+cudaStream_t pick(pz_ctx *, void *stream) { return (cudaStream_t)stream; }
+
+u32 ks_stride(const pz_params &P) { return (P.lwe_n + 1 + 31) & ~31u; }
+
+// evaluator.rs:664-673 dlog map; :688-726 test vectors; :728-743 auto elements
+void build_tables(pz_ctx *c, std::vector<unsigned short> &dlog, std::vector<u64> &tv) {
+  const pz_params &P = c->P;
+  const u32 q = P.br_q, R = q / 2;
+  const u64 Q = P.rlwe_q;
+  dlog.assign(q, 0);
+  for (u32 i = 0; i < q / 4; i++) {
+    u64 v = powmod(P.g, i, q);
+    dlog[v] = (unsigned short)i;
+    dlog[q - v] = (unsigned short)(i + q / 4);
+  }
+  const u64 true_el = Q >> 3, false_el = Q - true_el;
+  // X -> X^{-g} map on the br_q/2 ring (generate_auto_map, keygen.rs:16-41)
+  std::vector<u32> idx(R);
+  std::vector<unsigned char> sgn(R);
+  const u64 k = 2ull * R - (P.g % (2ull * R));
+  for (u32 i = 0; i < R; i++) {
+    u64 t = ((u64)i * k) % (2ull * R);
+    bool s = true;
+    if (t >= R) { t -= R; s = false; }
+    idx[i] = (u32)t;
+    sgn[i] = s;
+  }
+  auto one = [&](u32 part, u64 before, u64 after, u64 *out) {
+    for (u32 i = 0; i < R; i++) {
+      u64 v = i < part ? before : after;
+      out[idx[i]] = sgn[i] ? v : Q - v;
+    }
+  };
+  tv.assign(6ull * R, 0);
+  const u32 qby8 = q >> 3;
+  one(3 * qby8, false_el, true_el, &tv[0 * R]);  // and
+  one(3 * qby8, true_el, false_el, &tv[1 * R]);  // nand
+  one(qby8, false_el, true_el, &tv[2 * R]);      // or
+  one(qby8, true_el, false_el, &tv[3 * R]);      // nor
+  one(qby8, false_el, true_el, &tv[4 * R]);      // xor
+  one(qby8, true_el, false_el, &tv[5 * R]);      // xnor
+  const u64 two_n = 2ull * P.rlwe_n;
+  for (u32 s = 0; s <= P.w; s++) {
+    u64 el = s == 0 ? two_n - (P.g % two_n) : (powmod(P.g, s, 1ull << 62) % q) % two_n;
+    c->br.auto_k[s] = (u32)el;
+  }
+}
+
+pz_status ensure_scratch(pz_ctx *c, size_t count) {
+  if (count <= c->cap) return PZ_OK;
+  size_t cap = std::max(count, c->cap * 2);
+  const size_t L = (size_t)c->P.rlwe_n + 1;
+  cudaFree(c->d_c0); cudaFree(c->d_c1); cudaFree(c->d_out); cudaFree(c->d_gates); cudaFree(c->d_ks);
+  c->d_c0 = c->d_c1 = c->d_out = nullptr; c->d_gates = nullptr; c->d_ks = nullptr;
+  c->cap = 0;
+  PZ_CK(c, cudaMalloc(&c->d_c0, cap * L * 8));
+  PZ_CK(c, cudaMalloc(&c->d_c1, cap * L * 8));
+  PZ_CK(c, cudaMalloc(&c->d_out, cap * L * 8));
+  PZ_CK(c, cudaMalloc(&c->d_gates, cap));
+  PZ_CK(c, cudaMalloc(&c->d_ks, cap * ks_stride(c->P) * 4));
+  c->cap = cap;
+  return PZ_OK;
+}
+
+pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, const u64 *d_c0,
+                    const u64 *d_c1, u64 *d_out, size_t count, u32 *d_ks_out, u64 *d_rlwe, cudaStream_t s,
+                    u32 *d_ks_scratch, bool raw) {
+  pz::BrParams br = c->br;
+  br.rgsw = k->d_rgsw;
+  br.autos = k->d_autos;
+  pz::KsParams ks = c->ks;
+  ks.ksk = k->d_ksk;
+  ks.raw = raw ? 1u : 0u;
+  const u32 stride = ks_stride(c->P);
+  u32 *d_ks = d_ks_out ? d_ks_out : d_ks_scratch;
+  const u32 ks_out_stride = d_ks_out ? c->P.lwe_n + 1 : stride;
+  ks.out_stride = ks_out_stride;
+  cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s);
+  if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s);
+  if (e != cudaSuccess) return cuda_fail(c, "launch_pbs", e);
+  return PZ_OK;
+}
+
+pz_status check_key(pz_ctx *c, const pz_key *k) {
+  if (!k) return fail(c, PZ_ERR_INVALID_ARGUMENT, "key is NULL");
+  if (k->ctx != c) return fail(c, PZ_ERR_KEY_MISMATCH, "key was uploaded through another context");
+  return PZ_OK;
+}
+
+pz_status check_gates_host(pz_ctx *c, const uint8_t *gates, size_t count, bool raw) {
+  for (size_t i = 0; i < count; i++)
+    if ((gates[i] & 0x7f) > 5 || (!raw && (gates[i] & 0x80)))
+      return fail(c, PZ_ERR_INVALID_ARGUMENT, "gate code out of range at index " + std::to_string(i));
+  return PZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pz_status_string(pz_status s) {
+  switch (s) {
+    case PZ_OK: return "ok";
+    case PZ_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case PZ_ERR_CUDA: return "CUDA error";
+    case PZ_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case PZ_ERR_NOT_SUPPORTED: return "not supported";
+    case PZ_ERR_KEY_MISMATCH: return "key does not belong to this context";
+  }
+  return "unknown status";
+}
+
+pz_status pz_param_get(int id, pz_params *out) {
+  if (id < 0 || id >= PZ_NUM_PARAMS || !out) return PZ_ERR_INVALID_ARGUMENT;
+  *out = full_params(id);
+  return PZ_OK;
+}
+
+pz_status pz_ctx_create(int id, int device, pz_ctx **out) { return pz_ctx_create_ex(id, device, 0, out); }
+
+pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
+  if (!out) return PZ_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (id < 0 || id >= PZ_NUM_PARAMS) return PZ_ERR_INVALID_ARGUMENT;
+  pz_ctx *c = new pz_ctx();
+  c->param_id = id;
+  c->device = device;
+  c->P = full_params(id);
+  const pz_params &P = c->P;
+  const u64 Q = P.rlwe_q;
+  const u64 N = P.rlwe_n;
+  c->logn = log2_exact(N);
+  if (c->logn != 9 && c->logn != 11) { delete c; return PZ_ERR_NOT_SUPPORTED; }
+  if (root == 0) root = default_root(Q, 2 * N);
+  if (root == 0 || powmod(root, N, Q) != Q - 1) { delete c; return PZ_ERR_INVALID_ARGUMENT; }
+  c->root = root;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { delete c; return PZ_ERR_CUDA; }
+  // twiddles: psi^{bitrev(i)} and psi^{-bitrev(i)} (ntt.rs:337-369)
+  std::vector<u64> tw(4 * N);
+  const u64 rinv = invmod(root, Q);
+  u64 pw = 1, pwi = 1;
+  for (u64 i = 0; i < N; i++) {
+    u64 bo = 0;
+    for (u32 b = 0; b < c->logn; b++) bo |= ((i >> b) & 1) << (c->logn - 1 - b);
+    tw[bo] = pw;
+    tw[2 * N + bo] = pwi;
+    pw = mulmod(pw, root, Q);
+    pwi = mulmod(pwi, rinv, Q);
+  }
+  for (u64 i = 0; i < N; i++) {
+    tw[N + i] = shoup(tw[i], Q);
+    tw[3 * N + i] = shoup(tw[2 * N + i], Q);
+  }
+  std::vector<unsigned short> dlog;
+  std::vector<u64> tv;
+  build_tables(c, dlog, tv);
+#define CK_CREATE(call)                                   \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) { pz_ctx_destroy(c); return PZ_ERR_CUDA; } \
+  } while (0)
+  CK_CREATE(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK_CREATE(cudaMalloc(&c->d_tw, 4 * N * 8));
+  CK_CREATE(cudaMemcpy(c->d_tw, tw.data(), 4 * N * 8, cudaMemcpyHostToDevice));
+  CK_CREATE(cudaMalloc(&c->d_dlog, dlog.size() * 2));
+  CK_CREATE(cudaMemcpy(c->d_dlog, dlog.data(), dlog.size() * 2, cudaMemcpyHostToDevice));
+  CK_CREATE(cudaMalloc(&c->d_tv, tv.size() * 8));
+  CK_CREATE(cudaMemcpy(c->d_tv, tv.data(), tv.size() * 8, cudaMemcpyHostToDevice));
+#undef CK_CREATE
+  // Montgomery constant -Q^{-1} mod 2^64 (Newton iteration)
+  u64 inv = Q;
+  for (int i = 0; i < 6; i++) inv *= 2 - Q * inv;
+  pz::RingConsts &rc = c->rc;
+  rc.q = Q;
+  rc.qinv_neg = 0 - inv;
+  rc.n_inv = invmod(N, Q);
+  rc.n_inv_s = shoup(rc.n_inv, Q);
+  rc.fw = c->d_tw;
+  rc.fws = c->d_tw + N;
+  rc.iw = c->d_tw + 2 * N;
+  rc.iws = c->d_tw + 3 * N;
+  const u64 r64 = (u64)(((u128)1 << 64) % Q);
+  c->conv_c = mulmod(rc.n_inv, r64, Q);  // keys stored as K * N^{-1} * 2^64
+  c->conv_cs = shoup(c->conv_c, Q);
+  pz::BrParams &br = c->br;
+  br.rc = rc;
+  br.da = make_decomp(Q, P.rlrg_logb, P.rlrg_d_a);
+  br.db = make_decomp(Q, P.rlrg_logb, P.rlrg_d_b);
+  br.dauto = make_decomp(Q, P.auto_logb, P.auto_d);
+  br.d_a = P.rlrg_d_a;
+  br.d_b = P.rlrg_d_b;
+  br.d_auto = P.auto_d;
+  br.rgsw_rows = P.rgsw_rows;
+  br.auto_rows = P.auto_rows;
+  br.n = P.lwe_n;
+  br.br_q = P.br_q;
+  br.w = P.w;
+  br.g = P.g;
+  br.emb = P.embedding_factor;
+  br.q_ks_f = (double)P.lwe_q;
+  br.br_q_f = (double)P.br_q;
+  br.dlog = c->d_dlog;
+  br.tv = c->d_tv;
+  pz::KsParams &ks = c->ks;
+  ks.Q = Q;
+  ks.qby4 = Q >> 2;
+  ks.mask = (u32)(P.lwe_q - 1);
+  ks.q_ks_f = (double)P.lwe_q;
+  ks.Q_f = (double)Q;
+  ks.dks = make_decomp(P.lwe_q, P.lwe_logb, P.lwe_d);
+  ks.d = P.lwe_d;
+  ks.n = P.lwe_n;
+  ks.N = P.rlwe_n;
+  ks.ksk_stride = ks_stride(P);
+  ks.out_stride = ks_stride(P);
+  *out = c;
+  return PZ_OK;
+}
+
+void pz_ctx_destroy(pz_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_tw); cudaFree(c->d_dlog); cudaFree(c->d_tv);
+  cudaFree(c->d_c0); cudaFree(c->d_c1); cudaFree(c->d_out); cudaFree(c->d_gates); cudaFree(c->d_ks);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char *pz_last_error(const pz_ctx *c) { return c ? c->err.c_str() : "no context"; }
+
+pz_status pz_ctx_params(const pz_ctx *c, pz_params *out) {
+  if (!c || !out) return PZ_ERR_INVALID_ARGUMENT;
+  *out = c->P;
+  return PZ_OK;
+}
+uint64_t pz_ctx_ntt_root(const pz_ctx *c) { return c ? c->root : 0; }
+
+pz_status pz_ctx_set_pbs_grid_limit(pz_ctx *c, int g) {
+  if (!c || g < 0) return PZ_ERR_INVALID_ARGUMENT;
+  c->grid_limit = g;
+  return PZ_OK;
+}
+
+pz_status pz_key_upload(pz_ctx *c, const pz_server_key_view *v, pz_key **out) {
+  if (!c || !v || !out || !v->rgsw || !v->autos || !v->lwe_ksk)
+    return fail(c, PZ_ERR_INVALID_ARGUMENT, "pz_key_upload: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(c->mu);
+  PZ_CK(c, cudaSetDevice(c->device));
+  const pz_params &P = c->P;
+  const size_t N = P.rlwe_n;
+  const size_t rgsw_polys = (size_t)P.lwe_n * P.rgsw_rows;
+  const size_t auto_polys = (size_t)P.n_auto_keys * P.auto_rows;
+  const size_t ksk_rows = (size_t)P.lwe_d * N;
+  const u32 stride = ks_stride(P);
+  pz_key *k = new pz_key();
+  k->ctx = c;
+  auto cleanup = [&](pz_status s, const std::string &m) {
+    cudaFree(k->d_rgsw); cudaFree(k->d_autos); cudaFree(k->d_ksk);
+    delete k;
+    return fail(c, s, m);
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&k->d_rgsw, rgsw_polys * N * 8)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "rgsw alloc");
+  if ((e = cudaMalloc(&k->d_autos, auto_polys * N * 8)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "auto alloc");
+  if ((e = cudaMalloc(&k->d_ksk, ksk_rows * stride * 4)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "ksk alloc");
+  k->bytes = (rgsw_polys + auto_polys) * N * 8 + ksk_rows * stride * 4;
+  // coefficient rows -> device staging -> forward NTT + Montgomery/N^{-1} + device layout
+  const size_t chunk = 1024;  // polynomials per staging copy
+  u64 *d_stage = nullptr;
+  if ((e = cudaMalloc(&d_stage, chunk * N * 8)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "staging alloc");
+  auto convert = [&](const u64 *src, u64 *dst, size_t polys) -> cudaError_t {
+    for (size_t p0 = 0; p0 < polys; p0 += chunk) {
+      size_t m = std::min(chunk, polys - p0);
+      cudaError_t e2 = cudaMemcpyAsync(d_stage, src + p0 * N, m * N * 8, cudaMemcpyHostToDevice, c->stream);
+      if (e2 != cudaSuccess) return e2;
+      e2 = pz::launch_key_convert((int)c->logn, d_stage, dst + p0 * N, m, c->rc, c->conv_c, c->conv_cs, c->stream);
+      if (e2 != cudaSuccess) return e2;
+      e2 = cudaStreamSynchronize(c->stream);
+      if (e2 != cudaSuccess) return e2;
+    }
+    return cudaSuccess;
+  };
+  if ((e = convert(v->rgsw, k->d_rgsw, rgsw_polys)) != cudaSuccess ||
+      (e = convert(v->autos, k->d_autos, auto_polys)) != cudaSuccess) {
+    cudaFree(d_stage);
+    return cleanup(PZ_ERR_CUDA, std::string("key conversion: ") + cudaGetErrorString(e));
+  }
+  cudaFree(d_stage);
+  // LWE KSK: u64 rows mod q_ks -> u32 rows padded to `stride` words
+  std::vector<u32> ksk32((size_t)ksk_rows * stride, 0);
+  const size_t cols = P.lwe_n + 1;
+  for (size_t r = 0; r < ksk_rows; r++)
+    for (size_t col = 0; col < cols; col++) ksk32[r * stride + col] = (u32)(v->lwe_ksk[r * cols + col] & (P.lwe_q - 1));
+  if ((e = cudaMemcpy(k->d_ksk, ksk32.data(), ksk32.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cleanup(PZ_ERR_CUDA, std::string("ksk copy: ") + cudaGetErrorString(e));
+  *out = k;
+  return PZ_OK;
+}
+
+void pz_key_release(pz_key *k) {
+  if (!k) return;
+  cudaSetDevice(k->ctx->device);
+  cudaFree(k->d_rgsw); cudaFree(k->d_autos); cudaFree(k->d_ksk);
+  delete k;
+}
+size_t pz_key_device_bytes(const pz_key *k) { return k ? k->bytes : 0; }
+
+pz_status pz_gate_batch(pz_ctx *c, const pz_key *k, const uint8_t *gates, const uint64_t *c0,
+                        const uint64_t *c1, uint64_t *out, size_t count) {
+  if (!c) return PZ_ERR_INVALID_ARGUMENT;
+  if (count == 0) return PZ_OK;
+  if (!gates || !c0 || !c1 || !out) return fail(c, PZ_ERR_INVALID_ARGUMENT, "pz_gate_batch: NULL buffer");
+  pz_status s = check_key(c, k);
+  if (s != PZ_OK) return s;
+  if ((s = check_gates_host(c, gates, count, false)) != PZ_OK) return s;
+  std::lock_guard<std::mutex> lock(c->mu);
+  PZ_CK(c, cudaSetDevice(c->device));
+  if ((s = ensure_scratch(c, count)) != PZ_OK) return s;
+  const size_t bytes = count * ((size_t)c->P.rlwe_n + 1) * 8;
+  PZ_CK(c, cudaMemcpyAsync(c->d_gates, gates, count, cudaMemcpyHostToDevice, c->stream));
+  PZ_CK(c, cudaMemcpyAsync(c->d_c0, c0, bytes, cudaMemcpyHostToDevice, c->stream));
+  PZ_CK(c, cudaMemcpyAsync(c->d_c1, c1, bytes, cudaMemcpyHostToDevice, c->stream));
+  if ((s = run_gates(c, k, c->d_gates, c->d_c0, c->d_c1, c->d_out, count, nullptr, nullptr, c->stream, c->d_ks,
+                     false)) != PZ_OK)
+    return s;
+  PZ_CK(c, cudaMemcpyAsync(out, c->d_out, bytes, cudaMemcpyDeviceToHost, c->stream));
+  PZ_CK(c, cudaStreamSynchronize(c->stream));
+  return PZ_OK;
+}
+
+static pz_status gate_device_common(pz_ctx *c, const pz_key *k, const uint8_t *d_gates, const uint64_t *d_c0,
+                                    const uint64_t *d_c1, uint64_t *d_out, size_t count, uint32_t *d_ks_out,
+                                    uint64_t *d_rlwe, void *stream, bool raw) {
+  if (!c) return PZ_ERR_INVALID_ARGUMENT;
+  if (count == 0) return PZ_OK;
+  if (!d_gates || !d_c0 || !d_out) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL device buffer");
+  pz_status s = check_key(c, k);
+  if (s != PZ_OK) return s;
+  PZ_CK(c, cudaSetDevice(c->device));
+  cudaStream_t st = pick(c, stream);
+  u32 *d_ks = nullptr;
+  if (!d_ks_out) PZ_CK(c, cudaMallocAsync(&d_ks, count * ks_stride(c->P) * 4, st));
+  s = run_gates(c, k, d_gates, d_c0, d_c1, d_out, count, d_ks_out, d_rlwe, st, d_ks, raw);
+  if (d_ks) cudaFreeAsync(d_ks, st);
+  return s;
+}
+
+pz_status pz_gate_batch_device(pz_ctx *c, const pz_key *k, const uint8_t *d_gates, const uint64_t *d_c0,
+                               const uint64_t *d_c1, uint64_t *d_out, size_t count, void *stream) {
+  if (c && count && !d_c1) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL c1");
+  return gate_device_common(c, k, d_gates, d_c0, d_c1, d_out, count, nullptr, nullptr, stream, false);
+}
+
+pz_status pz_gate_batch_debug_device(pz_ctx *c, const pz_key *k, const uint8_t *d_gates, const uint64_t *d_c0,
+                                     const uint64_t *d_c1, uint64_t *d_out, size_t count, uint32_t *d_ks_out,
+                                     uint64_t *d_rlwe_out, void *stream) {
+  if (c && count && !d_c1) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL c1");
+  return gate_device_common(c, k, d_gates, d_c0, d_c1, d_out, count, d_ks_out, d_rlwe_out, stream, false);
+}
+
+pz_status pz_pbs_batch_device(pz_ctx *c, const pz_key *k, const uint8_t *d_test_vec, const uint64_t *d_lwe,
+                              uint64_t *d_out, size_t count, void *stream) {
+  return gate_device_common(c, k, d_test_vec, d_lwe, nullptr, d_out, count, nullptr, nullptr, stream, true);
+}
+
+pz_status pz_not_batch_device(pz_ctx *c, const uint64_t *d_in, uint64_t *d_out, size_t words, void *stream) {
+  if (!c) return PZ_ERR_INVALID_ARGUMENT;
+  if (words == 0) return PZ_OK;
+  if (!d_in || !d_out) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL device buffer");
+  PZ_CK(c, cudaSetDevice(c->device));
+  PZ_CK(c, pz::launch_not(d_in, d_out, words, c->P.rlwe_q, pick(c, stream)));
+  return PZ_OK;
+}
+
+pz_status pz_ntt_forward_device(pz_ctx *c, uint64_t *d, size_t count, void *stream) {
+  if (!c || (count && !d)) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  PZ_CK(c, cudaSetDevice(c->device));
+  PZ_CK(c, pz::launch_ntt_fwd((int)c->logn, d, count, c->rc, pick(c, stream)));
+  return PZ_OK;
+}
+
+pz_status pz_ntt_backward_device(pz_ctx *c, uint64_t *d, size_t count, void *stream) {
+  if (!c || (count && !d)) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  PZ_CK(c, cudaSetDevice(c->device));
+  PZ_CK(c, pz::launch_ntt_inv((int)c->logn, d, count, c->rc, pick(c, stream)));
+  return PZ_OK;
+}
+
+pz_status pz_rlwe_by_rgsw_device(pz_ctx *c, const pz_key *k, uint64_t *d_rlwe, const uint32_t *d_idx, size_t count,
+                                 int trivial, void *stream) {
+  if (!c || (count && (!d_rlwe || !d_idx))) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  pz_status s = check_key(c, k);
+  if (s != PZ_OK) return s;
+  PZ_CK(c, cudaSetDevice(c->device));
+  pz::BrParams br = c->br;
+  br.rgsw = k->d_rgsw;
+  br.autos = k->d_autos;
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  PZ_CK(c, pz::launch_ext_product((int)c->logn, d1, br, d_rlwe, d_idx, count, trivial, pick(c, stream)));
+  return PZ_OK;
+}
+
+pz_status pz_rlwe_auto_device(pz_ctx *c, const pz_key *k, uint64_t *d_rlwe, const uint32_t *d_slot, size_t count,
+                              int trivial, void *stream) {
+  if (!c || (count && (!d_rlwe || !d_slot))) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  pz_status s = check_key(c, k);
+  if (s != PZ_OK) return s;
+  PZ_CK(c, cudaSetDevice(c->device));
+  pz::BrParams br = c->br;
+  br.rgsw = k->d_rgsw;
+  br.autos = k->d_autos;
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  PZ_CK(c, pz::launch_auto((int)c->logn, d1, br, d_rlwe, d_slot, count, trivial, pick(c, stream)));
+  return PZ_OK;
+}
+
+pz_status pz_lwe_key_switch_device(pz_ctx *c, const pz_key *k, const uint64_t *d_in, uint32_t *d_out, size_t count,
+                                   void *stream) {
+  if (!c || (count && (!d_in || !d_out))) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  pz_status s = check_key(c, k);
+  if (s != PZ_OK) return s;
+  if (count == 0) return PZ_OK;
+  PZ_CK(c, cudaSetDevice(c->device));
+  cudaStream_t st = pick(c, stream);
+  // raw inputs already mod q_ks: the mod-down step must be the identity, so
+  // run the key-switch kernel with Q = q_ks and gate code GATE_RAW.
+  pz::KsParams ks = c->ks;
+  ks.ksk = k->d_ksk;
+  ks.Q = c->P.lwe_q;
+  ks.Q_f = (double)c->P.lwe_q;
+  ks.out_stride = c->P.lwe_n + 1;
+  ks.raw = 1;
+  cudaError_t e = pz::launch_ks(ks, nullptr, d_in, nullptr, count, d_out, st);
+  if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
+  return PZ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,181 @@
+"""Python handle over the C ABI: one ``Engine`` per (parameter set, device).
+
+Host-memory calls take and return numpy arrays; ``*_device`` calls take
+torch CUDA tensors (any 8-byte integer dtype for u64 words) and run
+asynchronously on the given stream (default: torch's current stream).
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import PzParams, PzServerKeyView, check, lib, u8p, u64p, vp
+
+PARAMETER_SETS = {
+    "I_2P_LB_SR": 0, "I_4P": 1, "I_8P": 2, "NI_2P": 3,
+    "NI_4P_HB_FR": 4, "NI_4P_LB_SR": 5, "NI_8P": 6, "SP_TEST": 7,
+}
+# ParameterSelector names of the reference (bool/mp_api.rs:28-32,
+# bool/ni_mp_api.rs:39-47) -> parameter sets.
+SELECTORS = {
+    "InteractiveLTE2Party": "I_2P_LB_SR",
+    "InteractiveLTE4Party": "I_4P",
+    "InteractiveLTE8Party": "I_8P",
+    "NonInteractiveLTE2Party": "NI_2P",
+    "NonInteractiveLTE4Party": "NI_4P_HB_FR",
+    "NonInteractiveLTE8Party": "NI_8P",
+}
+GATES = {"and": 0, "nand": 1, "or": 2, "nor": 3, "xor": 4, "xnor": 5}
+
+
+def param_id(param):
+    if isinstance(param, int):
+        return param
+    if param in SELECTORS:
+        param = SELECTORS[param]
+    return PARAMETER_SETS[param]
+
+
+def params(param):
+    p = PzParams()
+    check(lib().pz_param_get(param_id(param), ctypes.byref(p)), None, "pz_param_get")
+    return p
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class DeviceKey:
+    """A server key resident on the engine's device."""
+
+    def __init__(self, engine, handle):
+        self.engine = engine
+        self.h = handle
+
+    @property
+    def device_bytes(self):
+        return lib().pz_key_device_bytes(self.h)
+
+    def release(self):
+        if self.h:
+            lib().pz_key_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class Engine:
+    def __init__(self, param, device=0, ntt_root=0):
+        self.param_id = param_id(param)
+        h = vp()
+        check(lib().pz_ctx_create_ex(self.param_id, device, int(ntt_root), ctypes.byref(h)), None,
+              "pz_ctx_create")
+        self.h = h
+        self.device = device
+        self.p = PzParams()
+        check(lib().pz_ctx_params(self.h, ctypes.byref(self.p)), self.h, "pz_ctx_params")
+        self.N, self.n, self.Q = self.p.rlwe_n, self.p.lwe_n, self.p.rlwe_q
+        self.L = self.N + 1
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().pz_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ntt_root(self):
+        return lib().pz_ctx_ntt_root(self.h)
+
+    def set_pbs_grid_limit(self, g):
+        check(lib().pz_ctx_set_pbs_grid_limit(self.h, int(g)), self.h, "set_pbs_grid_limit")
+
+    # -- keys --------------------------------------------------------------
+    def upload_key(self, rgsw, autos, lwe_ksk):
+        """Upload a coefficient-domain server key (layouts of pz_server_key_view)."""
+        p = self.p
+        rgsw = np.ascontiguousarray(rgsw, dtype=np.uint64)
+        autos = np.ascontiguousarray(autos, dtype=np.uint64)
+        lwe_ksk = np.ascontiguousarray(lwe_ksk, dtype=np.uint64)
+        if rgsw.size != p.lwe_n * p.rgsw_rows * p.rlwe_n:
+            raise ValueError("rgsw has the wrong size for this parameter set")
+        if autos.size != p.n_auto_keys * p.auto_rows * p.rlwe_n:
+            raise ValueError("auto keys have the wrong size for this parameter set")
+        if lwe_ksk.size != p.lwe_d * p.rlwe_n * (p.lwe_n + 1):
+            raise ValueError("lwe ksk has the wrong size for this parameter set")
+        view = PzServerKeyView(rgsw.ctypes.data_as(u64p), autos.ctypes.data_as(u64p),
+                               lwe_ksk.ctypes.data_as(u64p))
+        h = vp()
+        check(lib().pz_key_upload(self.h, ctypes.byref(view), ctypes.byref(h)), self.h, "pz_key_upload")
+        return DeviceKey(self, h)
+
+    # -- gates, host memory --------------------------------------------------
+    def gate_batch(self, key, gates, c0, c1):
+        gates = np.ascontiguousarray(gates, dtype=np.uint8)
+        c0 = np.ascontiguousarray(c0, dtype=np.uint64).reshape(-1, self.L)
+        c1 = np.ascontiguousarray(c1, dtype=np.uint64).reshape(-1, self.L)
+        if not (len(gates) == len(c0) == len(c1)):
+            raise ValueError("gates, c0 and c1 must have the same count")
+        out = np.empty_like(c0)
+        check(lib().pz_gate_batch(self.h, key.h, gates.ctypes.data_as(u8p), c0.ctypes.data_as(u64p),
+                                  c1.ctypes.data_as(u64p), out.ctypes.data_as(u64p), len(gates)),
+              self.h, "pz_gate_batch")
+        return out
+
+    # -- device memory ---------------------------------------------------------
+    def gate_batch_device(self, key, gates, c0, c1, out, stream=None, ks_out=None, rlwe_out=None):
+        count = gates.numel()
+        if ks_out is None and rlwe_out is None:
+            check(lib().pz_gate_batch_device(self.h, key.h, _ptr(gates), _ptr(c0), _ptr(c1), _ptr(out),
+                                             count, _stream(stream)), self.h, "pz_gate_batch_device")
+        else:
+            check(lib().pz_gate_batch_debug_device(self.h, key.h, _ptr(gates), _ptr(c0), _ptr(c1),
+                                                   _ptr(out), count, _ptr(ks_out), _ptr(rlwe_out),
+                                                   _stream(stream)), self.h, "pz_gate_batch_debug_device")
+
+    def pbs_batch_device(self, key, test_vec, lwe, out, stream=None):
+        check(lib().pz_pbs_batch_device(self.h, key.h, _ptr(test_vec), _ptr(lwe), _ptr(out),
+                                        test_vec.numel(), _stream(stream)), self.h, "pz_pbs_batch_device")
+
+    def not_device(self, x, out, stream=None):
+        check(lib().pz_not_batch_device(self.h, _ptr(x), _ptr(out), x.numel(), _stream(stream)),
+              self.h, "pz_not_batch_device")
+
+    def ntt_forward_device(self, polys, stream=None):
+        check(lib().pz_ntt_forward_device(self.h, _ptr(polys), polys.numel() // self.N, _stream(stream)),
+              self.h, "pz_ntt_forward_device")
+
+    def ntt_backward_device(self, polys, stream=None):
+        check(lib().pz_ntt_backward_device(self.h, _ptr(polys), polys.numel() // self.N, _stream(stream)),
+              self.h, "pz_ntt_backward_device")
+
+    def rlwe_by_rgsw_device(self, key, rlwe, lwe_index, trivial=False, stream=None):
+        check(lib().pz_rlwe_by_rgsw_device(self.h, key.h, _ptr(rlwe), _ptr(lwe_index), lwe_index.numel(),
+                                           int(trivial), _stream(stream)), self.h, "pz_rlwe_by_rgsw_device")
+
+    def rlwe_auto_device(self, key, rlwe, slot, trivial=False, stream=None):
+        check(lib().pz_rlwe_auto_device(self.h, key.h, _ptr(rlwe), _ptr(slot), slot.numel(), int(trivial),
+                                        _stream(stream)), self.h, "pz_rlwe_auto_device")
+
+    def lwe_key_switch_device(self, key, lwe_in, out, stream=None):
+        count = lwe_in.numel() // self.L
+        check(lib().pz_lwe_key_switch_device(self.h, key.h, _ptr(lwe_in), _ptr(out), count,
+                                             _stream(stream)), self.h, "pz_lwe_key_switch_device")

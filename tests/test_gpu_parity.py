@@ -1,0 +1,181 @@
+"""Bit-exact parity of the CUDA path with the CPU oracle (through the C ABI).
+
+Every comparison here is exact equality of u64 words: the kernels must
+produce the same ciphertext words as the oracle's restatement of the
+reference on the same key bytes and inputs.
+"""
+import numpy as np
+import pytest
+
+from conftest import combine, oracle, oracle_setup, pz, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = ["SP_TEST", "I_2P_LB_SR", "I_4P", "I_8P", "NI_2P", "NI_4P_HB_FR", "NI_4P_LB_SR", "NI_8P"]
+FAST = ["SP_TEST", "I_2P_LB_SR", "NI_8P"]
+
+_ENGINES = {}
+
+
+def engine_and_key(param):
+    if param not in _ENGINES:
+        ev, secrets, coeff, okey = oracle_setup(param)
+        eng = pz().Engine(param, ntt_root=ev.psi())
+        dkey = eng.upload_key(coeff.rgsw, coeff.autos, coeff.ksk)
+        _ENGINES[param] = (eng, dkey)
+    return _ENGINES[param]
+
+
+def rng(tag):
+    return oracle().Rng(bytes([tag]) * 32)
+
+
+@pytest.mark.parametrize("param", PARAMS)
+def test_ntt_matches_oracle(gpu_available, param):
+    ev, _, _, _ = oracle_setup(param)
+    eng, _ = engine_and_key(param)
+    assert eng.ntt_root == ev.psi()
+    count = 64
+    x = rng(0x11).uniform_mod(ev.Q, count * ev.N).reshape(count, ev.N)
+    want = np.stack([ev.ntt_forward(r) for r in x])
+    t = to_dev(x)
+    eng.ntt_forward_device(t)
+    got = to_host(t).reshape(count, ev.N)
+    assert np.array_equal(got, want)
+    eng.ntt_backward_device(t)
+    assert np.array_equal(to_host(t).reshape(count, ev.N), x)
+
+
+@pytest.mark.parametrize("param", ["SP_TEST", "I_2P_LB_SR"])
+def test_ntt_negacyclic_product_default_root(gpu_available, param):
+    """ntt.rs:510-540 pin: NTT product == schoolbook product (library's own root)."""
+    O = oracle()
+    ev, _, _, _ = oracle_setup(param)
+    eng = pz().Engine(param)
+    r = rng(0x12)
+    a = r.uniform_mod(ev.Q, ev.N)
+    b = r.uniform_mod(ev.Q, ev.N)
+    ta, tb = to_dev(a), to_dev(b)
+    eng.ntt_forward_device(ta)
+    eng.ntt_forward_device(tb)
+    fa, fb = to_host(ta), to_host(tb)
+    prod = np.array([(int(u) * int(v)) % ev.Q for u, v in zip(fa, fb)], dtype=np.uint64)
+    tp = to_dev(prod)
+    eng.ntt_backward_device(tp)
+    want = np.empty(ev.N, np.uint64)
+    O.lib().orc_negacyclic_mul(ev.Q, O._p(a), O._p(b), O._p(want), ev.N)
+    assert np.array_equal(to_host(tp), want)
+
+
+@pytest.mark.parametrize("param", PARAMS)
+@pytest.mark.parametrize("trivial", [False, True])
+def test_rlwe_by_rgsw(gpu_available, param, trivial):
+    ev, _, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    count = 24
+    r = rng(0x21 + trivial)
+    rl = r.uniform_mod(ev.Q, count * 2 * ev.N).reshape(count, 2, ev.N)
+    if trivial:
+        rl[:, 0, :] = 0
+    idx = (r.uniform_mod(ev.n, count)).astype(np.uint32)
+    idx[0], idx[-1] = 0, ev.n - 1
+    want = np.stack([okey.rlwe_by_rgsw(rl[i].reshape(-1), int(idx[i]), trivial=trivial) for i in range(count)])
+    t = to_dev(rl)
+    eng.rlwe_by_rgsw_device(dkey, t, to_dev(idx), trivial=trivial)
+    got = to_host(t).reshape(count, -1)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("param", PARAMS)
+@pytest.mark.parametrize("trivial", [False, True])
+def test_rlwe_auto(gpu_available, param, trivial):
+    ev, _, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    slots = np.arange(ev.info.w + 1, dtype=np.uint32)
+    count = len(slots) * 2
+    slots = np.concatenate([slots, slots])
+    r = rng(0x31 + trivial)
+    rl = r.uniform_mod(ev.Q, count * 2 * ev.N).reshape(count, 2, ev.N)
+    rl[1, 0, :7] = 0  # zeros exercise neg(0) = Q on the a-part
+    if trivial:
+        rl[:, 0, :] = 0
+        rl[2, 1, :5] = 0
+        rl[3, 1, :5] = ev.Q  # trivial autos may carry Q (neg(0)) in b
+    want = np.stack([okey.rlwe_auto(rl[i].reshape(-1), int(slots[i]), trivial=trivial) for i in range(count)])
+    t = to_dev(rl)
+    eng.rlwe_auto_device(dkey, t, to_dev(slots), trivial=trivial)
+    assert np.array_equal(to_host(t).reshape(count, -1), want)
+
+
+@pytest.mark.parametrize("param", PARAMS)
+def test_lwe_key_switch(gpu_available, param):
+    ev, _, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    qk = ev.info.lwe_q
+    count = 20
+    r = rng(0x41)
+    x = r.uniform_mod(qk + 1, count * ev.L).reshape(count, ev.L)  # [0, q_ks] (mod-down may give q_ks)
+    x[0, :] = qk
+    x[1, :] = 0
+    want = np.stack([okey.lwe_key_switch(x[i]) for i in range(count)])
+    out = to_dev(np.zeros((count, ev.n + 1), np.uint32))
+    eng.lwe_key_switch_device(dkey, to_dev(x), out)
+    got = to_host(out, np.uint32).astype(np.uint64)
+    assert np.array_equal(got, want)
+
+
+def _gate_inputs(ev, secrets, count, tag):
+    s = secrets[0]
+    r = rng(tag)
+    bits0 = (r.uniform_mod(2, count)).astype(np.int64)
+    bits1 = (r.uniform_mod(2, count)).astype(np.int64)
+    c0 = ev.encrypt_bool(r, s, bits0)
+    c1 = ev.encrypt_bool(r, s, bits1)
+    return bits0, bits1, c0, c1
+
+
+TRUTH = {
+    "and": lambda a, b: a & b, "nand": lambda a, b: 1 - (a & b), "or": lambda a, b: a | b,
+    "nor": lambda a, b: 1 - (a | b), "xor": lambda a, b: a ^ b, "xnor": lambda a, b: 1 - (a ^ b),
+}
+
+
+@pytest.mark.parametrize("param", PARAMS)
+def test_gate_batch_bit_exact(gpu_available, param):
+    O = oracle()
+    ev, secrets, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    names = list(TRUTH)
+    count = 12 if param in FAST else 6
+    bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, count, 0x51)
+    gates = np.array([O.GATES[names[i % 6]] for i in range(count)], np.uint8)
+    out = to_dev(np.zeros((count, ev.L), np.uint64))
+    ks = to_dev(np.zeros((count, ev.n + 1), np.uint32))
+    rl = to_dev(np.zeros((count, 2 * ev.N), np.uint64))
+    eng.gate_batch_device(dkey, to_dev(gates), to_dev(c0), to_dev(c1), out, ks_out=ks, rlwe_out=rl)
+    got_out, got_ks, got_rl = to_host(out), to_host(ks, np.uint32), to_host(rl)
+    for i in range(count):
+        g = names[i % 6]
+        comb = combine(ev, g, c0[i], c1[i])
+        w_out, w_ks, w_rl, _ = okey.pbs(g, comb)
+        assert np.array_equal(got_ks[i].astype(np.uint64), w_ks), f"key switch mismatch at {i} ({g})"
+        assert np.array_equal(got_rl[i], w_rl), f"blind rotation mismatch at {i} ({g})"
+        assert np.array_equal(got_out[i], w_out), f"output mismatch at {i} ({g})"
+    dec = ev.decrypt_bool(secrets[0], got_out)
+    want = np.array([TRUTH[names[i % 6]](bits0[i], bits1[i]) for i in range(count)])
+    assert np.array_equal(dec, want)
+
+
+@pytest.mark.parametrize("param", ["SP_TEST", "I_2P_LB_SR"])
+def test_gate_batch_host_api(gpu_available, param):
+    """pz_gate_batch (host buffers, synchronous) == oracle gates."""
+    O = oracle()
+    ev, secrets, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    count = 8
+    bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, count, 0x61)
+    gates = np.array([O.GATES["nand"]] * count, np.uint8)
+    got = eng.gate_batch(dkey, gates, c0, c1)
+    want = okey.gate_batch(gates, c0, c1, threads=4)
+    assert np.array_equal(got, want)
+    assert np.array_equal(ev.decrypt_bool(secrets[0], got), 1 - (bits0 & bits1))
