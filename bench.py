@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Gate-bootstrap throughput of the B200 engine (one JSON line on rank 0).
+
+Workload (one step): the batched circuit wavefront at NonInteractiveLTE8Party
+parameters -- 1024 independent FheUint8 a*b (155 gates each) and 1024 a<b (35
+gates each), 194,560 gate bootstraps.  Every circuit level (the gates of all
+2048 circuits at that depth) is one key-switch launch plus one blind-rotation
+launch; the whole circuit is one CUDA graph replayed per step.
+
+  value   gate bootstraps/s with inputs resident in HBM (graph replay, CUDA events)
+  e2e     the same through pz_circuit_run: host buffers in pinned memory,
+          host->device inputs and device->host outputs inside the timed region
+  plain   InteractiveLTE2Party, 128 NAND gates, one gate per launch
+  roofline  blind-rotation kernel: algorithmic 32-bit multiply instructions
+          (BASELINE convention, 10 per 64-bit modmul) per second / the IMAD
+          rate measured on this GPU by pz_probe_imad_rate
+  cpu_baseline  the CPU oracle (a C++ restatement of the reference's pbs path)
+          on all host threads, bounded sample of the same gates
+
+Keys and ciphertexts are seeded synthetic data with the reference's shapes and
+value distribution (uniform mod Q / mod q_ks): RLWE/RGSW/LWE ciphertexts are
+pseudo-random, so the bootstrap schedule and work equal those of real keys.
+Inputs (537 MB of ciphertexts per step) exceed L2; the server key stays
+L2/HBM resident across steps as in steady-state serving.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PARAM = "NI_8P"
+N_MUL = 1024
+N_LT = 1024
+C_MM = 10  # 32-bit multiply instructions per 64-bit Shoup modmul (BASELINE.md convention)
+WORKLOAD_CONFIG = {
+    "workload": "batched circuit wavefront: NI_8P, 1024 FheUint8 a*b + 1024 a<b, "
+                "each level one launch, whole circuit one CUDA graph",
+    "param_set": PARAM,
+}
+
+
+def pz():
+    import importlib
+    return importlib.import_module("phantom-zone_b200")
+
+
+# ---------------------------------------------------------------------------
+def synthetic_key(p, seed):
+    rng = np.random.default_rng(seed)
+    N, n = p.rlwe_n, p.lwe_n
+    rgsw = rng.integers(0, p.rlwe_q, (n, p.rgsw_rows, N), dtype=np.uint64)
+    autos = rng.integers(0, p.rlwe_q, (p.n_auto_keys, p.auto_rows, N), dtype=np.uint64)
+    ksk = rng.integers(0, p.lwe_q, (p.lwe_d * N, n + 1), dtype=np.uint64)
+    return rgsw, autos, ksk
+
+
+def wavefront_circuit(P):
+    C = P.Circuit()
+    pairs = [(C.input_u8(), C.input_u8()) for _ in range(N_MUL + N_LT)]
+    for a, b in pairs[:N_MUL]:
+        C.outputs(C.u8_mul(a, b))
+    for a, b in pairs[N_MUL:]:
+        C.output(C.u8_cmp("lt", a, b))
+    return C
+
+
+def schedule_work(p, ks):
+    """Exact counts of the blind rotation's work per ciphertext (pbs.rs:240-414)
+    from key-switched LWEs ks [count][n+1]: returns modmuls per the BASELINE
+    convention M = F (N/2) logN + I ((N/2) logN + N) + MAC."""
+    br_q, n, N, g, w = p.br_q, p.lwe_n, p.rlwe_n, p.g, p.w
+    dlog = np.zeros(br_q, np.int64)
+    for i in range(br_q // 4):
+        v = pow(g, i, br_q)
+        dlog[v] = i
+        dlog[br_q - v] = i + br_q // 4
+    shift = int(np.log2(p.lwe_q)) - int(np.log2(br_q))
+    q4 = br_q // 4
+    logn = int(np.log2(N))
+    total = 0
+    for row in ks:
+        odd = (row[1:].astype(np.int64) >> shift)
+        odd = odd + ((odd & 1) ^ 1)
+        cnt = np.bincount(dlog[odd], minlength=br_q // 2)
+        trivial, autos_nt = True, 0
+
+        def bucket(b):
+            nonlocal trivial
+            if cnt[b]:
+                trivial = False
+
+        v = 0
+        for i in range(q4 - 1, 0, -1):
+            bucket(q4 + i)
+            v += 1
+            if cnt[q4 + i - 1] or v == w or i == 1:
+                autos_nt += 0 if trivial else 1
+                v = 0
+        bucket(q4)
+        autos_nt += 0 if trivial else 1
+        v = 0
+        for i in range(q4 - 1, 0, -1):
+            bucket(i)
+            v += 1
+            if cnt[i - 1] or v == w or i == 1:
+                autos_nt += 0 if trivial else 1
+                v = 0
+        A = autos_nt
+        F, I = 2 * n - 1 + A, 2 * n + 2 * A
+        MAC = (4 * n - 2) * N + 2 * A * N
+        total += F * (N // 2) * logn + I * ((N // 2) * logn + N) + MAC
+    return total
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if args.impl != "reference" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+        return dist, int(os.environ["RANK"]), world, int(os.environ.get("LOCAL_RANK", "0"))
+    return None, 0, 1, 0
+
+
+def max_over_ranks(dist, x, device=None):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+def cpu_gate_sample(p, key_arrays, threads, gates_per_thread, seed=11):
+    """Time the oracle (CPU restatement of the reference) on independent gates."""
+    from oracle import oracle as O
+    ev = O.Evaluator(PARAM)
+    key = ev.key(O.ServerKeyCoeff(*key_arrays))
+    rng = np.random.default_rng(seed)
+    count = threads * gates_per_thread
+    c0 = rng.integers(0, p.rlwe_q, (count, p.rlwe_n + 1), dtype=np.uint64)
+    c1 = rng.integers(0, p.rlwe_q, (count, p.rlwe_n + 1), dtype=np.uint64)
+    gates = rng.integers(0, 6, count).astype(np.uint8)
+    t0 = time.perf_counter()
+    key.gate_batch(gates, c0, c1, threads=threads)
+    dt = time.perf_counter() - t0
+    return count / dt, count, dt
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference path on host cores."""
+    dist, rank, world, _ = dist_setup(args)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    P = pz()
+    p = P.params(PARAM)
+    threads = os.cpu_count() or 1
+    key_arrays = synthetic_key(p, 0x5EED)
+    per_step = []
+    gates_per_thread = 2
+    for s in range(args.warmup + args.steps):
+        rate, count, dt = cpu_gate_sample(p, key_arrays, threads, gates_per_thread, seed=100 + s)
+        if s >= args.warmup:
+            per_step.append(dt)
+    value = threads * gates_per_thread * len(per_step) / sum(per_step)
+    line = {
+        "impl": "reference", "metric": "gate bootstraps/sec", "value": value, "unit": "gate bootstraps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(per_step) / len(per_step), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": dict(WORKLOAD_CONFIG, sample=f"{threads * gates_per_thread} gates of the wavefront's "
+                                               f"gate mix per step on {threads} host threads"),
+        "cpu_baseline": {"value": value, "unit": "gate bootstraps/s", "cores": threads, "kind": "port",
+                         "sample": f"{threads * gates_per_thread} independent gates per step on {threads} threads"},
+        "e2e": {"value": value, "unit": "gate bootstraps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def plain_form(P, torch, device, seed=7):
+    """InteractiveLTE2Party, 128 NAND bootstraps, one gate per launch."""
+    p = P.params("I_2P_LB_SR")
+    eng = P.Engine("I_2P_LB_SR", device=device)
+    key = eng.upload_key(*synthetic_key(p, seed))
+    rng = np.random.default_rng(seed)
+    L = p.rlwe_n + 1
+    c0 = torch.from_numpy(rng.integers(0, p.rlwe_q, (128, L), dtype=np.uint64).view(np.int64)).cuda()
+    c1 = torch.from_numpy(rng.integers(0, p.rlwe_q, (128, L), dtype=np.uint64).view(np.int64)).cuda()
+    g = torch.full((128,), 1, dtype=torch.uint8, device="cuda")
+    out = torch.empty_like(c0)
+    for i in range(3):
+        eng.gate_batch_device(key, g[i:i + 1], c0[i], c1[i], out[i])
+    torch.cuda.synchronize()
+    lat = []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(128)]
+    for i in range(128):
+        ev[i][0].record()
+        eng.gate_batch_device(key, g[i:i + 1], c0[i], c1[i], out[i])
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    lat = [a.elapsed_time(b) for a, b in ev]
+    total = sum(lat)
+    key.release()
+    eng.close()
+    return {"value": 128 / (total / 1e3), "unit": "gate bootstraps/s", "p50_ms": statistics.median(lat),
+            "p99_ms": float(np.percentile(lat, 99)), "config": "I_2P_LB_SR, 128 NAND, one gate per launch"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    dist, rank, world, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    P = pz()
+    p = P.params(PARAM)
+    L = p.rlwe_n + 1
+
+    eng = P.Engine(PARAM, device=local)
+    key_arrays = synthetic_key(p, 0x5EED + rank)
+    key = eng.upload_key(*key_arrays)
+    C = wavefront_circuit(P)
+    info = C.info()
+    gates_per_step = info["gates"]
+    rng = np.random.default_rng(1234 + rank)
+    h_in = torch.from_numpy(rng.integers(0, p.rlwe_q, (info["inputs"], L), dtype=np.uint64).view(np.int64))
+    h_in = h_in.pin_memory()
+    h_out = torch.empty((info["outputs"], L), dtype=torch.int64).pin_memory()
+    d_in = h_in.cuda()
+    d_out = torch.empty((info["outputs"], L), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    # warm-up step 1 is a direct run (sets kernel attributes, binds the
+    # circuit to the device); the circuit is then captured and replayed
+    C.run_device(eng, key, d_in, d_out)
+    torch.cuda.synchronize()
+    C.capture_graph(eng, key, d_in, d_out)
+    for _ in range(max(args.warmup - 1, 0)):
+        C.replay_graph()
+    torch.cuda.synchronize()
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            evs[i][0].record()
+            C.replay_graph()
+            evs[i][1].record()
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    if dist:
+        dist.barrier()
+    total_ms = max_over_ranks(dist, sum(step_ms), "cuda")
+    value = world * gates_per_step * args.steps / (total_ms / 1e3)
+
+    # e2e: host buffers through the synchronous C-ABI call (copies inside)
+    e2e_ms = []
+    for i in range(args.steps):
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        P._lib.check(P._lib.lib().pz_circuit_run(eng.h, key.h, C.h,
+                                                 P._lib.ctypes.cast(h_in.data_ptr(), P._lib.u64p),
+                                                 P._lib.ctypes.cast(h_out.data_ptr(), P._lib.u64p)),
+                     eng.h, "pz_circuit_run")
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = max_over_ranks(dist, sum(e2e_ms), "cuda")
+    e2e_value = world * gates_per_step * args.steps / (e2e_total / 1e3)
+
+    # dominant kernel: blind rotation alone on 2368 key-switched LWEs (4 waves of 592)
+    B = 2368
+    ks = rng.integers(0, p.lwe_q, (B, p.lwe_n + 1), dtype=np.uint64).astype(np.uint32)
+    d_ks = torch.from_numpy(ks.view(np.int32)).cuda()
+    d_tv = torch.from_numpy(rng.integers(0, 6, B).astype(np.uint8)).cuda()
+    d_br = torch.empty((B, L), dtype=torch.int64, device="cuda")
+    eng.blind_rotate_device(key, d_ks, d_tv, d_br)
+    torch.cuda.synchronize()
+    reps = 3
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ea.record()
+    for _ in range(reps):
+        eng.blind_rotate_device(key, d_ks, d_tv, d_br)
+    eb.record()
+    torch.cuda.synchronize()
+    br_ms = ea.elapsed_time(eb) / reps
+    modmuls = schedule_work(p, ks)
+    achieved = modmuls * C_MM / (br_ms / 1e3) / 1e12  # T IMAD/s
+    peak = P.probe_imad_rate(local) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "pbs_kernel_traffic.json")
+    if os.path.exists(prof):
+        try:
+            tr = json.load(open(prof))
+            traffic = tr["dram_bytes_per_bootstrap"] * B
+        except (ValueError, KeyError):
+            traffic = None
+
+    plain = None
+    if not args.no_plain and rank == 0:
+        plain = plain_form(P, torch, local)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, count, dt = cpu_gate_sample(p, key_arrays, threads, 4)
+        cpu = {"value": rate, "unit": "gate bootstraps/s", "cores": threads, "kind": "port",
+               "sample": f"{count} independent NI_8P gates ({threads} threads x 4) in {dt:.1f} s"}
+
+    if rank == 0:
+        launches_per_step = 2 * info["levels"] + 1
+        line = {
+            "metric": "gate bootstraps/sec", "value": value, "unit": "gate bootstraps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded uniform keys and ciphertexts with the reference's shapes)",
+            "config": {**WORKLOAD_CONFIG, "gates_per_step": gates_per_step, "levels": info["levels"],
+                       "max_level_width": info["max_level_width"],
+                       "l2": "inputs (537 MB/step) larger than L2; server key resident"},
+            "latency_ms": {"p50": statistics.median(step_ms), "p99": float(np.percentile(step_ms, 99)),
+                           "what": "completion time of every circuit in the wavefront"},
+            "e2e": {"value": e2e_value, "unit": "gate bootstraps/s",
+                    "h2d_bytes_per_step": int(info["inputs"] * L * 8),
+                    "d2h_bytes_per_step": int(info["outputs"] * L * 8)},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "int", "kernel": "pbs_kernel (blind rotation)", "achieved": achieved,
+                         "peak": peak, "unit": "TIMAD/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "pz_probe_imad_rate on this GPU (MEASURED_PEAKS.json has no integer peak)",
+                         "launch_ms": br_ms, "bootstraps_per_launch": B,
+                         "modmuls_per_bootstrap": modmuls / B},
+            "plain": plain,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    C.close()
+    key.release()
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -138,6 +138,16 @@ pz_status pz_gate_batch_debug_device(pz_ctx *ctx, const pz_key *key, const uint8
  * gate test_vec[i] (pbs.rs:104-233, no gate prelude). */
 pz_status pz_pbs_batch_device(pz_ctx *ctx, const pz_key *key, const uint8_t *d_test_vec,
                               const uint64_t *d_lwe, uint64_t *d_out, size_t count, void *stream);
+/* Blind rotation + sample extraction from key-switched LWEs (pbs.rs:146-232:
+ * odd mod-switch, dlog buckets, test-vector rotation, blind_rotation,
+ * sample_extract): d_ks [count][n + 1] u32 mod q_ks, gate test vector per
+ * item, d_out [count][N + 1]. */
+pz_status pz_blind_rotate_batch_device(pz_ctx *ctx, const pz_key *key, const uint32_t *d_ks,
+                                       const uint8_t *d_test_vec, uint64_t *d_out, size_t count,
+                                       void *stream);
+/* Measured throughput of 32-bit multiply-add (IMAD) instructions on a device:
+ * the integer-pipe denominator of the bootstrap's roofline. */
+pz_status pz_probe_imad_rate(int device, double *imad_per_second);
 /* out = -in (mod Q, unreduced: -0 = Q) on `words` u64 words. */
 pz_status pz_not_batch_device(pz_ctx *ctx, const uint64_t *d_in, uint64_t *d_out, size_t words,
                               void *stream);
@@ -156,6 +166,55 @@ pz_status pz_lwe_key_switch_device(pz_ctx *ctx, const pz_key *key, const uint64_
 /* Blind-rotation launch shape: 0 = one CTA per ciphertext; > 0 caps the grid
  * (the kernel then strides over the batch). */
 pz_status pz_ctx_set_pbs_grid_limit(pz_ctx *ctx, int grid_limit);
+
+/* ---- circuits ------------------------------------------------------------------
+ * A circuit records gates instead of executing them (the reference executes
+ * each BooleanGates call at once); execution runs the circuit level by level,
+ * every gate of a level in one batched launch.  Wires are uint32_t handles;
+ * PZ_WIRE_NONE marks an invalid/absent wire.  not() is free (it flips a
+ * handle bit).  FheUint8 values are 8 wires, least significant bit first
+ * (shortint/enc_dec.rs:11-29). */
+#define PZ_WIRE_NONE 0xffffffffu
+typedef struct pz_circuit pz_circuit;
+pz_status pz_circuit_create(pz_circuit **out);
+void pz_circuit_destroy(pz_circuit *c);
+const char *pz_circuit_last_error(const pz_circuit *c);
+uint32_t pz_circuit_input(pz_circuit *c);
+/* BooleanGates::{and,...,xnor}(a, b), bool/mod.rs:22-71 */
+uint32_t pz_circuit_gate(pz_circuit *c, int gate, uint32_t a, uint32_t b);
+/* BooleanGates::not, evaluator.rs:2318-2322 */
+uint32_t pz_circuit_not(pz_circuit *c, uint32_t a);
+pz_status pz_circuit_output(pz_circuit *c, uint32_t wire);
+pz_status pz_circuit_info(pz_circuit *c, size_t *inputs, size_t *gates, size_t *outputs, size_t *levels,
+                          size_t *max_level_width);
+pz_status pz_circuit_level_sizes(pz_circuit *c, size_t *sizes, size_t capacity);
+/* FheUint8 operators (shortint/mod.rs:63-292 over shortint/ops.rs) */
+pz_status pz_u8_add(pz_circuit *c, const uint32_t a[8], const uint32_t b[8], uint32_t out[8],
+                    uint32_t *overflow);           /* AddAssign / overflowing_add */
+pz_status pz_u8_sub(pz_circuit *c, const uint32_t a[8], const uint32_t b[8], uint32_t out[8],
+                    uint32_t *overflow);           /* Sub / overflowing_sub */
+pz_status pz_u8_mul(pz_circuit *c, const uint32_t a[8], const uint32_t b[8], uint32_t out[8]);
+/* div_rem; when div_zero_flag is non-NULL it is updated like set_div_by_zero_flag
+ * (PZ_WIRE_NONE on entry: no flag yet) */
+pz_status pz_u8_div_rem(pz_circuit *c, const uint32_t a[8], const uint32_t b[8], uint32_t quotient[8],
+                        uint32_t remainder[8], uint32_t *div_zero_flag);
+/* op: 0 eq, 1 neq, 2 lt, 3 gt, 4 le, 5 ge */
+pz_status pz_u8_cmp(pz_circuit *c, int op, const uint32_t a[8], const uint32_t b[8], uint32_t *out);
+/* mux: selector ? a : b */
+pz_status pz_u8_mux(pz_circuit *c, const uint32_t a[8], const uint32_t b[8], uint32_t selector,
+                    uint32_t out[8]);
+/* Execute: inputs [n_inputs][N + 1] in input order, outputs [n_outputs][N + 1]
+ * in output order.  _device: device buffers, asynchronous on `stream`;
+ * pz_circuit_run: host buffers, synchronous. */
+pz_status pz_circuit_run_device(pz_ctx *ctx, const pz_key *key, pz_circuit *c, const uint64_t *d_inputs,
+                                uint64_t *d_outputs, void *stream);
+pz_status pz_circuit_run(pz_ctx *ctx, const pz_key *key, pz_circuit *c, const uint64_t *inputs,
+                         uint64_t *outputs);
+/* Capture the whole circuit on these device buffers as one CUDA graph, then
+ * replay it with a single launch. */
+pz_status pz_circuit_capture_graph(pz_ctx *ctx, const pz_key *key, pz_circuit *c, const uint64_t *d_inputs,
+                                   uint64_t *d_outputs, void *stream);
+pz_status pz_circuit_replay_graph(pz_circuit *c, void *stream);
 
 #ifdef __cplusplus
 }

@@ -76,6 +76,16 @@ def lib():
             "orc_not": (None, [vp, u64p]),
             "orc_gate_batch": (None, [vp, vp, u8p, u64p, u64p, u64p, ctypes.c_size_t, ctypes.c_int]),
             "orc_sample_extract": (None, [vp, u64p, u64p, ctypes.c_uint32]),
+            "orc_u8_op": (ctypes.c_int, [vp, vp, ctypes.c_int, u64p, u64p, u64p, u64p, u64p, u64p, ctypes.POINTER(ctypes.c_int)]),
+            "orc_generate_prime": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
+            "orc_ntt_custom_new": (vp, [ctypes.c_uint64, ctypes.c_size_t]),
+            "orc_ntt_custom_free": (None, [vp]),
+            "orc_ntt_custom_forward": (None, [vp, u64p, ctypes.c_int]),
+            "orc_ntt_custom_backward": (None, [vp, u64p, ctypes.c_int]),
+            "orc_mul_mod_barrett": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+            "orc_decompose_custom": (ctypes.c_uint32, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, u64p]),
+            "orc_round_value": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_uint32]),
+            "orc_recompose": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, u64p]),
             "orc_rng_new": (vp, [u8p]),
             "orc_rng_free": (None, [vp]),
             "orc_rng_next_u64": (ctypes.c_uint64, [vp]),
@@ -117,8 +127,8 @@ class Rng:
         self.h = lib().orc_rng_new(self._seed)
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().orc_rng_free(self.h)
+        if getattr(self, "h", None) and _lib is not None and lib is not None:
+            _lib.orc_rng_free(self.h)
             self.h = None
 
     def uniform_mod(self, q, n):
@@ -303,6 +313,26 @@ class OracleKey:
         b = np.ascontiguousarray(c1, np.uint64)
         lib().orc_gate(self.ev.h, self.h, GATES[gate] if isinstance(gate, str) else gate, _p(a), _p(b))
         return a
+
+    U8_OPS = {"add": 0, "sub": 1, "mul": 2, "div_rem": 3, "eq": 4, "neq": 5, "lt": 6, "gt": 7,
+              "le": 8, "ge": 9, "mux": 10, "overflowing_add": 11, "overflowing_sub": 12}
+
+    def u8_op(self, op, a, b, sel=None, flag=None):
+        """FheUint8 op, sequential gates.  Returns (out, out2, flag)."""
+        L = self.ev.L
+        a = np.ascontiguousarray(a, np.uint64).reshape(8, L)
+        b = np.ascontiguousarray(b, np.uint64).reshape(8, L)
+        code = self.U8_OPS[op]
+        nout = 1 if code in (4, 5, 6, 7, 8, 9) else 8
+        out = np.zeros((nout, L), np.uint64)
+        out2 = np.zeros((8, L), np.uint64)
+        fl = np.zeros(L, np.uint64) if flag is None else np.ascontiguousarray(flag, np.uint64).copy()
+        fs = ctypes.c_int(0 if flag is None else 1)
+        sp = _p(np.ascontiguousarray(sel, np.uint64)) if sel is not None else None
+        rc = lib().orc_u8_op(self.ev.h, self.h, code, _p(a), _p(b), sp, _p(out), _p(out2), _p(fl),
+                             ctypes.byref(fs))
+        assert rc == 0
+        return out, out2, (fl if fs.value else None)
 
     def gate_batch(self, gates, c0, c1, threads=1):
         gates = np.ascontiguousarray(gates, np.uint8)

@@ -728,6 +728,160 @@ void gate(const Eval &e, const Key &k, Scratch &sc, int g, u64 *c0, const u64 *c
   pbs(e, k, sc, e.test_vec[g].data(), c0, nullptr, nullptr);
 }
 
+// ---------------------------------------------------------------------------
+// shortint/ops.rs restated sequentially: every gate bootstraps immediately,
+// in the reference's order, through gate() above.  A ciphertext is a
+// std::vector<u64> of N+1 words.
+// ---------------------------------------------------------------------------
+typedef std::vector<u64> Ct;
+struct SEval {
+  const Eval &e;
+  const Key &k;
+  Scratch sc;
+  SEval(const Eval &e_, const Key &k_) : e(e_), k(k_), sc(e_) {}
+  Ct g(int t, const Ct &a, const Ct &b) {  // gate(a, b): BooleanGates::* (evaluator.rs:2252-2316)
+    Ct out = a;
+    gate(e, k, sc, t, out.data(), b.data());
+    return out;
+  }
+  Ct not_(const Ct &a) {  // evaluator.rs:2318-2322
+    Ct out = a;
+    for (auto &v : out) v = e.rmod.neg(v);
+    return out;
+  }
+};
+// ops.rs:5-14
+Ct s_half_adder(SEval &s, Ct &a, const Ct &b) {
+  Ct carry = s.g(ORC_AND, a, b);
+  a = s.g(ORC_XOR, a, b);
+  return carry;
+}
+// ops.rs:16-44
+Ct s_full_adder_plain_carry_in(SEval &s, Ct &a, const Ct &b, bool carry_in) {
+  Ct a_and_b = s.g(ORC_AND, a, b);
+  a = s.g(ORC_XOR, a, b);
+  if (carry_in) a_and_b = s.g(ORC_OR, a_and_b, a);
+  if (carry_in) a = s.not_(a);
+  return a_and_b;
+}
+// ops.rs:46-59
+Ct s_full_adder(SEval &s, Ct &a, const Ct &b, const Ct &carry_in) {
+  Ct a_and_b = s.g(ORC_AND, a, b);
+  a = s.g(ORC_XOR, a, b);
+  Ct a_xor_b_and_c = s.g(ORC_AND, a, carry_in);
+  a_and_b = s.g(ORC_OR, a_and_b, a_xor_b_and_c);
+  a = s.g(ORC_XOR, a, carry_in);
+  return a_and_b;
+}
+// ops.rs:61-91
+void s_adder(SEval &s, std::vector<Ct> &a, const std::vector<Ct> &b, bool carry_in, Ct &cl, Ct &cll) {
+  const size_t n = a.size();
+  Ct carry = !carry_in ? s_half_adder(s, a[0], b[0]) : s_full_adder_plain_carry_in(s, a[0], b[0], true);
+  for (size_t i = 1; i + 2 < n; i++) carry = s_full_adder(s, a[i], b[i], carry);
+  cll = s_full_adder(s, a[n - 2], b[n - 2], carry);
+  cl = s_full_adder(s, a[n - 1], b[n - 1], cll);
+}
+// ops.rs:143-187
+std::vector<Ct> s_mul(SEval &s, const std::vector<Ct> &a, const std::vector<Ct> &b) {
+  std::vector<Ct> carries, out;
+  for (int i = 0; i < 8; i++) {
+    if (i == 0) {
+      out.push_back(s.g(ORC_AND, a[0], b[0]));
+    } else if (i == 1) {
+      Ct tmp0 = s.g(ORC_AND, a[1], b[0]);
+      Ct tmp1 = s.g(ORC_AND, a[0], b[1]);
+      carries.push_back(s_half_adder(s, tmp0, tmp1));
+      out.push_back(tmp0);
+    } else {
+      Ct sum = s.g(ORC_AND, a[i], b[0]);
+      Ct tmp = s.g(ORC_AND, a[i - 1], b[1]);
+      carries[0] = s_full_adder(s, sum, tmp, carries[0]);
+      for (int j = 2; j < i; j++) {
+        tmp = s.g(ORC_AND, a[i - j], b[j]);
+        carries[j - 1] = s_full_adder(s, sum, tmp, carries[j - 1]);
+      }
+      tmp = s.g(ORC_AND, a[0], b[i]);
+      carries.push_back(s_half_adder(s, sum, tmp));
+      out.push_back(sum);
+    }
+  }
+  return out;
+}
+// ops.rs:189-259
+void s_division(SEval &s, const std::vector<Ct> &a, const std::vector<Ct> &b, std::vector<Ct> &quot,
+                std::vector<Ct> &rem) {
+  const size_t n = a.size();
+  std::vector<Ct> neg_b;
+  for (auto &x : b) neg_b.push_back(s.not_(x));
+  std::vector<Ct> remainder, quotient;
+  for (size_t i = 0; i < n; i++) {
+    remainder.push_back(a[n - 1 - i]);
+    std::vector<Ct> subtract = remainder;
+    Ct carry = s_full_adder_plain_carry_in(s, subtract[i], neg_b[0], true);
+    for (size_t j = 1; j <= i; j++) carry = s_full_adder(s, subtract[i - j], neg_b[j], carry);
+    for (size_t j = i + 1; j < n; j++) carry = s.g(ORC_AND, carry, neg_b[j]);
+    Ct not_carry = s.not_(carry);
+    for (size_t kk = 0; kk < remainder.size(); kk++) {
+      subtract[kk] = s.g(ORC_AND, subtract[kk], carry);
+      remainder[kk] = s.g(ORC_AND, remainder[kk], not_carry);
+      remainder[kk] = s.g(ORC_OR, remainder[kk], subtract[kk]);
+    }
+    quotient.push_back(carry);
+  }
+  std::reverse(remainder.begin(), remainder.end());
+  std::reverse(quotient.begin(), quotient.end());
+  quot = quotient;
+  rem = remainder;
+}
+// ops.rs:261-272
+Ct s_is_zero(SEval &s, const std::vector<Ct> &a) {
+  std::vector<Ct> na;
+  for (auto &x : a) na.push_back(s.not_(x));
+  Ct out = na[0];
+  for (size_t i = 1; i < na.size(); i++) out = s.g(ORC_AND, out, na[i]);
+  return out;
+}
+// ops.rs:274-287
+Ct s_equality(SEval &s, const std::vector<Ct> &a, const std::vector<Ct> &b) {
+  Ct out = s.g(ORC_XNOR, a[0], b[0]);
+  for (size_t i = 1; i < a.size(); i++) {
+    Ct e = s.g(ORC_XNOR, a[i], b[i]);
+    out = s.g(ORC_AND, out, e);
+  }
+  return out;
+}
+// ops.rs:292-321, :341-356
+Ct s_comparator(SEval &s, const std::vector<Ct> &a, const std::vector<Ct> &b) {
+  const size_t n = a.size();
+  Ct comp = s.not_(b[n - 1]);
+  comp = s.g(ORC_AND, comp, a[n - 1]);
+  Ct casc = s.g(ORC_XNOR, a[n - 1], b[n - 1]);
+  Ct tmp = s.not_(b[n - 2]);
+  tmp = s.g(ORC_AND, tmp, a[n - 2]);
+  tmp = s.g(ORC_AND, tmp, casc);
+  comp = s.g(ORC_OR, comp, tmp);
+  for (size_t i = 2; i < n; i++) {
+    Ct tmp_casc = s.g(ORC_XNOR, a[n - i], b[n - i]);
+    casc = s.g(ORC_AND, casc, tmp_casc);
+    Ct t = s.not_(b[n - 1 - i]);
+    t = s.g(ORC_AND, t, a[n - 1 - i]);
+    t = s.g(ORC_AND, t, casc);
+    comp = s.g(ORC_OR, comp, t);
+  }
+  return comp;
+}
+// ops.rs:123-141
+std::vector<Ct> s_mux(SEval &s, const Ct &sel, const std::vector<Ct> &t, const std::vector<Ct> &f) {
+  Ct ns = s.not_(sel);
+  std::vector<Ct> out;
+  for (size_t i = 0; i < t.size(); i++) {
+    Ct sa = s.g(ORC_AND, sel, t[i]);
+    Ct sb = s.g(ORC_AND, ns, f[i]);
+    out.push_back(s.g(ORC_OR, sa, sb));
+  }
+  return out;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -873,6 +1027,134 @@ void orc_gate_batch(void *ev, void *key, const uint8_t *gates, const uint64_t *c
 }
 void orc_sample_extract(void *ev, const uint64_t *rlwe, uint64_t *lwe, uint32_t index) {
   sample_extract(*(Eval *)ev, rlwe, lwe, index);
+}
+
+// ---- FheUint8 operations (shortint/mod.rs:63-292), sequential ------------
+// a, b: [8][N+1] (LSB first).  op: 0 add, 1 sub, 2 mul, 3 div_rem, 4 eq,
+// 5 neq, 6 lt, 7 gt, 8 le, 9 ge, 10 mux (selector = sel), 11 overflowing_add,
+// 12 overflowing_sub.  out: [8][N+1] or, for comparisons, [1][N+1]; out2:
+// remainder (div_rem) or overflow flag.  flag (div_rem): in/out division by
+// zero flag; *flag_set says whether it holds a ciphertext.
+int orc_u8_op(void *ev, void *key, int op, const uint64_t *a, const uint64_t *b, const uint64_t *sel,
+              uint64_t *out, uint64_t *out2, uint64_t *flag, int *flag_set) {
+  Eval &e = *(Eval *)ev;
+  SEval s(e, *(Key *)key);
+  const size_t L = e.N + 1;
+  std::vector<Ct> A(8), Bv(8);
+  for (int i = 0; i < 8; i++) {
+    A[i].assign(a + i * L, a + (i + 1) * L);
+    Bv[i].assign(b + i * L, b + (i + 1) * L);
+  }
+  auto put = [&](uint64_t *dst, const std::vector<Ct> &v) {
+    for (size_t i = 0; i < v.size(); i++) memcpy(dst + i * L, v[i].data(), L * 8);
+  };
+  Ct cl, cll;
+  switch (op) {
+    case 0: case 11: {  // AddAssign (mod.rs:63-70) / overflowing_add (:157-165)
+      s_adder(s, A, Bv, false, cl, cll);
+      put(out, A);
+      if (op == 11 && out2) memcpy(out2, cl.data(), L * 8);
+      return 0;
+    }
+    case 1: case 12: {  // Sub (mod.rs:81-90) / overflowing_sub (:171-179)
+      std::vector<Ct> nb;
+      for (auto &x : Bv) nb.push_back(s.not_(x));
+      s_adder(s, nb, A, true, cl, cll);
+      put(out, nb);
+      if (op == 12 && out2) { Ct o = s.not_(cl); memcpy(out2, o.data(), L * 8); }
+      return 0;
+    }
+    case 2: put(out, s_mul(s, A, Bv)); return 0;
+    case 3: {  // div_rem (mod.rs:187-202) with set_div_by_zero_flag (:42-56)
+      if (flag && flag_set) {
+        Ct z = s_is_zero(s, Bv);
+        if (!*flag_set) { memcpy(flag, z.data(), L * 8); *flag_set = 1; }
+        else {
+          Ct f(flag, flag + L);
+          f = s.g(ORC_OR, f, z);
+          memcpy(flag, f.data(), L * 8);
+        }
+      }
+      std::vector<Ct> q, r;
+      s_division(s, A, Bv, q, r);
+      put(out, q);
+      if (out2) put(out2, r);
+      return 0;
+    }
+    case 4: put(out, {s_equality(s, A, Bv)}); return 0;
+    case 5: put(out, {s.not_(s_equality(s, A, Bv))}); return 0;
+    case 6: put(out, {s_comparator(s, Bv, A)}); return 0;
+    case 7: put(out, {s_comparator(s, A, Bv)}); return 0;
+    case 8: put(out, {s.not_(s_comparator(s, A, Bv))}); return 0;
+    case 9: put(out, {s.not_(s_comparator(s, Bv, A))}); return 0;
+    case 10: {
+      Ct sl(sel, sel + L);
+      put(out, s_mux(s, sl, A, Bv));
+      return 0;
+    }
+  }
+  return -1;
+}
+
+// ---- generic pins (reference unit tests at their own sizes) -----------------
+// Deterministic Miller-Rabin for 64-bit integers (bases valid below 2^64);
+// stands in for num-bigint-dig's probably_prime used by utils.rs:114-116.
+static bool is_prime_u64(u64 n) {
+  if (n < 2) return false;
+  for (u64 p : {2ull, 3ull, 5ull, 7ull, 11ull, 13ull, 17ull, 19ull, 23ull, 29ull, 31ull, 37ull}) {
+    if (n % p == 0) return n == p;
+  }
+  u64 d = n - 1;
+  int s = 0;
+  while ((d & 1) == 0) { d >>= 1; s++; }
+  for (u64 a : {2ull, 3ull, 5ull, 7ull, 11ull, 13ull, 17ull, 19ull, 23ull, 29ull, 31ull, 37ull}) {
+    u64 x = mod_exponent(a, d, n);
+    if (x == 1 || x == n - 1) continue;
+    bool comp = true;
+    for (int r = 1; r < s; r++) {
+      x = (u64)(((u128)x * x) % n);
+      if (x == n - 1) { comp = false; break; }
+    }
+    if (comp) return false;
+  }
+  return true;
+}
+
+// utils.rs:122-142 generate_prime (0 when none is found)
+uint64_t orc_generate_prime(uint32_t num_bits, uint64_t modulo, uint64_t upper_bound) {
+  const int lz = 64 - (int)num_bits;
+  u64 t = upper_bound - 1;
+  while (t % modulo != 1 && clz64(t) == lz) t -= 1;
+  while (!is_prime_u64(t) && clz64(t) == lz && t >= modulo) t -= modulo;
+  return (is_prime_u64(t) && clz64(t) == lz) ? t : 0;
+}
+
+void *orc_ntt_custom_new(uint64_t q, size_t n) {
+  Ntt *t = new Ntt();
+  t->init(q, n);
+  return t;
+}
+void orc_ntt_custom_free(void *h) { delete (Ntt *)h; }
+void orc_ntt_custom_forward(void *h, uint64_t *a, int lazy) { ((Ntt *)h)->forward(a, lazy != 0); }
+void orc_ntt_custom_backward(void *h, uint64_t *a, int lazy) { ((Ntt *)h)->backward(a, lazy != 0); }
+uint64_t orc_mul_mod_barrett(uint64_t q, uint64_t a, uint64_t b) { return ModU64(q).mul(a, b); }
+
+// DefaultDecomposer with arbitrary (q, logb, d); returns ignore_bits.
+uint32_t orc_decompose_custom(uint64_t q, uint32_t logb, uint32_t d, uint64_t value, uint64_t *out) {
+  Decomposer dc;
+  dc.init(q, logb, d);
+  dc.decompose(value, out);
+  return dc.ignore_bits;
+}
+uint64_t orc_round_value(uint64_t v, uint32_t ignore_bits) { return Decomposer::round_value(v, ignore_bits); }
+// decomposer.rs:129-140 recompose with ModularOpsU64
+uint64_t orc_recompose(uint64_t q, uint32_t logb, uint32_t d, const uint64_t *limbs) {
+  Decomposer dc;
+  dc.init(q, logb, d);
+  ModU64 m(q);
+  u64 v = 0;
+  for (u32 j = 0; j < d; j++) v = m.add(v, m.mul(limbs[j], dc.gadget(j)));
+  return v;
 }
 
 // ---- client harness --------------------------------------------------------

@@ -97,6 +97,24 @@ uint64_t orc_barrett_mul(void *ev, uint64_t a, uint64_t b);
 void orc_negacyclic_mul(uint64_t q, const uint64_t *a, const uint64_t *b,
                         uint64_t *out, size_t n);
 
+/* FheUint8 operations evaluated gate by gate in the reference's order
+ * (shortint/mod.rs:63-292 over shortint/ops.rs).  op: 0 add, 1 sub, 2 mul,
+ * 3 div_rem, 4 eq, 5 neq, 6 lt, 7 gt, 8 le, 9 ge, 10 mux, 11 overflowing_add,
+ * 12 overflowing_sub.  a, b, out, out2: [8][N+1]; comparisons write [1][N+1]. */
+int orc_u8_op(void *ev, void *key, int op, const uint64_t *a, const uint64_t *b, const uint64_t *sel,
+              uint64_t *out, uint64_t *out2, uint64_t *flag, int *flag_set);
+
+/* generic pins: the reference's unit tests at their own sizes */
+uint64_t orc_generate_prime(uint32_t num_bits, uint64_t modulo, uint64_t upper_bound);
+void *orc_ntt_custom_new(uint64_t q, size_t n);
+void orc_ntt_custom_free(void *h);
+void orc_ntt_custom_forward(void *h, uint64_t *a, int lazy);
+void orc_ntt_custom_backward(void *h, uint64_t *a, int lazy);
+uint64_t orc_mul_mod_barrett(uint64_t q, uint64_t a, uint64_t b);
+uint32_t orc_decompose_custom(uint64_t q, uint32_t logb, uint32_t d, uint64_t value, uint64_t *out);
+uint64_t orc_round_value(uint64_t v, uint32_t ignore_bits);
+uint64_t orc_recompose(uint64_t q, uint32_t logb, uint32_t d, const uint64_t *limbs);
+
 /* --- server key ----------------------------------------------------------------
  * Coefficient-domain, fully expanded server key (what set_server_key holds
  * before the forward NTT, keys.rs:687-781):

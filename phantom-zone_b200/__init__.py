@@ -7,6 +7,7 @@ declared in include/phantom_zone_b200.h; this package is the Python host side
 interface.  Import it with ``importlib.import_module("phantom-zone_b200")``.
 """
 from . import _lib
-from .engine import GATES, PARAMETER_SETS, SELECTORS, DeviceKey, Engine, param_id, params
+from .engine import GATES, PARAMETER_SETS, SELECTORS, DeviceKey, Engine, param_id, params, probe_imad_rate
+from .circuits import Circuit
 
-__all__ = ["Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "param_id", "params", "_lib"]
+__all__ = ["Circuit", "Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "param_id", "params", "probe_imad_rate", "_lib"]

@@ -53,12 +53,33 @@ SIGNATURES = {
     "pz_gate_batch_debug_device": (st, [vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp, vp, vp]),
     "pz_pbs_batch_device": (st, [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_not_batch_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_blind_rotate_batch_device": (st, [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_probe_imad_rate": (st, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "pz_ntt_forward_device": (st, [vp, vp, ctypes.c_size_t, vp]),
     "pz_ntt_backward_device": (st, [vp, vp, ctypes.c_size_t, vp]),
     "pz_rlwe_by_rgsw_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, ctypes.c_int, vp]),
     "pz_rlwe_auto_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, ctypes.c_int, vp]),
     "pz_lwe_key_switch_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_ctx_set_pbs_grid_limit": (st, [vp, ctypes.c_int]),
+    "pz_circuit_create": (st, [ctypes.POINTER(vp)]),
+    "pz_circuit_destroy": (None, [vp]),
+    "pz_circuit_last_error": (ctypes.c_char_p, [vp]),
+    "pz_circuit_input": (ctypes.c_uint32, [vp]),
+    "pz_circuit_gate": (ctypes.c_uint32, [vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]),
+    "pz_circuit_not": (ctypes.c_uint32, [vp, ctypes.c_uint32]),
+    "pz_circuit_output": (st, [vp, ctypes.c_uint32]),
+    "pz_circuit_info": (st, [vp] + [ctypes.POINTER(ctypes.c_size_t)] * 5),
+    "pz_circuit_level_sizes": (st, [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t]),
+    "pz_u8_add": (st, [vp, u32p, u32p, u32p, u32p]),
+    "pz_u8_sub": (st, [vp, u32p, u32p, u32p, u32p]),
+    "pz_u8_mul": (st, [vp, u32p, u32p, u32p]),
+    "pz_u8_div_rem": (st, [vp, u32p, u32p, u32p, u32p, u32p]),
+    "pz_u8_cmp": (st, [vp, ctypes.c_int, u32p, u32p, u32p]),
+    "pz_u8_mux": (st, [vp, u32p, u32p, ctypes.c_uint32, u32p]),
+    "pz_circuit_run_device": (st, [vp, vp, vp, vp, vp, vp]),
+    "pz_circuit_run": (st, [vp, vp, vp, u64p, u64p]),
+    "pz_circuit_capture_graph": (st, [vp, vp, vp, vp, vp, vp]),
+    "pz_circuit_replay_graph": (st, [vp, vp]),
 }
 
 _lib = None

@@ -1,0 +1,59 @@
+// pz_internal.h -- host-side state shared by the runtime translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/phantom_zone_b200.h"
+#include "pz_kernels.cuh"
+
+struct pz_ctx {
+  int param_id = 0, device = 0;
+  pz_params P{};
+  pz::u32 logn = 0;
+  pz::u64 root = 0;
+  cudaStream_t stream = nullptr;
+  // device tables
+  pz::u64 *d_tw = nullptr;        // fw | fws | iw | iws  (4N words)
+  unsigned short *d_dlog = nullptr;
+  pz::u64 *d_tv = nullptr;        // 6 x br_q/2
+  // constants
+  pz::RingConsts rc{};
+  pz::u64 conv_c = 0, conv_cs = 0;
+  pz::BrParams br{};
+  pz::KsParams ks{};
+  int grid_limit = 0;
+  // host-API scratch (guarded by mu)
+  std::mutex mu;
+  size_t cap = 0;
+  pz::u64 *d_c0 = nullptr, *d_c1 = nullptr, *d_out = nullptr;
+  unsigned char *d_gates = nullptr;
+  pz::u32 *d_ks = nullptr;
+  std::string err;
+};
+
+struct pz_key {
+  pz_ctx *ctx = nullptr;
+  pz::u64 *d_rgsw = nullptr, *d_autos = nullptr;
+  pz::u32 *d_ksk = nullptr;
+  size_t bytes = 0;
+};
+
+
+namespace pz {
+// Launch sequence of one batch of gate bootstraps (ks kernel -> pbs kernel).
+// Optional wire gather/scatter: in0/in1/out_idx (see KsParams, BrParams).
+pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, const u64 *d_c0, const u64 *d_c1,
+                    u64 *d_out, size_t count, u32 *d_ks_out, u64 *d_rlwe, cudaStream_t s, u32 *d_ks_scratch,
+                    bool raw, const u32 *in0 = nullptr, const u32 *in1 = nullptr, const u32 *out_idx = nullptr);
+pz_status fail(pz_ctx *ctx, pz_status s, const std::string &msg);
+pz_status cuda_fail(pz_ctx *ctx, const char *what, cudaError_t e);
+u32 ks_stride(const pz_params &P);
+}  // namespace pz
+
+#define PZ_CK(ctx, call)                                          \
+  do {                                                            \
+    cudaError_t _e = (call);                                      \
+    if (_e != cudaSuccess) return pz::cuda_fail((ctx), #call, _e); \
+  } while (0)

@@ -378,6 +378,16 @@ constexpr int KS_CT = 16;    // ciphertexts per CTA
 constexpr int KS_IC = 32;    // LWE coefficients per digit chunk
 constexpr int KS_COLS = 128; // output columns per CTA
 
+// Input word `i` of gate ct's operand (gathered through a wire index when
+// given; a set WIRE_NEG bit applies not(): q - x, evaluator.rs:2247-2250).
+__device__ __forceinline__ u64 operand(const u64 *base, const u32 *idx, int ct, size_t i, size_t L, u64 q) {
+  if (!base) return 0;
+  if (!idx) return base[(size_t)ct * L + i];
+  const u32 w = idx[ct];
+  const u64 x = base[(size_t)(w & WIRE_MASK) * L + i];
+  return (w & WIRE_NEG) ? q - x : x;
+}
+
 __global__ void __launch_bounds__(KS_COLS)
     ks_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
   __shared__ u32 dig[KS_CT][KS_IC][MAX_KS_D];
@@ -395,8 +405,9 @@ __global__ void __launch_bounds__(KS_COLS)
       const int c = e / KS_IC, ii = e % KS_IC;
       const int ct = ct0 + c;
       if (ct < count) {
-        const size_t off = (size_t)ct * L + 1 + i0 + ii;
-        const u64 x = prelude_moddown(c0[off], c1 ? c1[off] : 0, gates ? gates[ct] : 0, false, P);
+        const size_t off = 1 + i0 + ii;
+        const u64 x = prelude_moddown(operand(c0, P.in0, ct, off, L, P.Q), operand(c1, P.in1, ct, off, L, P.Q),
+                                      gates ? gates[ct] : 0, false, P);
         u64 st = decomp_init(x, P.dks);
         for (u32 jd = 0; jd < d; jd++) dig[c][ii][jd] = (u32)decomp_next(st, P.dks);
       } else {
@@ -423,8 +434,8 @@ __global__ void __launch_bounds__(KS_COLS)
       if (ct < count) {
         u32 v = acc[c];
         if (col == 0) {
-          const size_t off = (size_t)ct * L;
-          v += (u32)prelude_moddown(c0[off], c1 ? c1[off] : 0, gates ? gates[ct] : 0, true, P);
+          v += (u32)prelude_moddown(operand(c0, P.in0, ct, 0, L, P.Q), operand(c1, P.in1, ct, 0, L, P.Q),
+                                    gates ? gates[ct] : 0, true, P);
         }
         out[(size_t)ct * P.out_stride + col] = v & P.mask;
       }
@@ -576,7 +587,7 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
     bucket(0);  // +(g^0)
 
     // ---- sample extract at index 0 (pbs.rs:423-449)
-    u64 *o = out + (size_t)ct * (N + 1);
+    u64 *o = out + (size_t)(P.out_idx ? P.out_idx[ct] : (u32)ct) * (N + 1);
 #pragma unroll
     for (int r = 0; r < 8; r++) {
       const u32 p = (u32)pos_coef<LOGN>(j, r);
@@ -596,6 +607,32 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
       }
     }
   }
+}
+
+// Throughput probe for the roofline denominator: 8 independent chains of
+// 32-bit multiply-adds per thread (mad.lo.u32, the IMAD the 64-bit modular
+// multiplications are built from).  `sink` keeps the chains live.
+__global__ void imad_probe_kernel(u32 iters, u32 seed, u32 *sink) {
+  u32 x[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) x[i] = seed + threadIdx.x * 8 + i;
+  const u32 m = seed | 1u, c = seed ^ 0x9e3779b9u;
+  for (u32 it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x[i]) : "r"(m), "r"(c));
+    }
+  }
+  u32 acc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) acc ^= x[i];
+  if (acc == 0x12345678u) sink[blockIdx.x] = acc;
+}
+
+cudaError_t launch_imad_probe(int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s) {
+  imad_probe_kernel<<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink);
+  return cudaGetLastError();
 }
 
 __global__ void not_kernel(const u64 *in, u64 *out, size_t words, u64 q) {
@@ -633,9 +670,15 @@ cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts 
   return cudaGetLastError();
 }
 
+// Opt the kernel into its dynamic shared memory once (largest size asked so
+// far), outside of any launch sequence that may be captured into a graph.
 template <typename K>
 static cudaError_t set_smem(K kernel, size_t bytes) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  static size_t done = 0;
+  if (bytes <= done) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done = bytes;
+  return e;
 }
 
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,

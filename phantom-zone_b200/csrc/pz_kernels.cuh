@@ -20,6 +20,7 @@ struct BrParams {
   const u64 *tv;                   // [6][br_q/2] test vectors
   const u64 *rgsw;                 // [n][rgsw_rows][N] device layout, Montgomery form
   const u64 *autos;                // [w+1][auto_rows][N]
+  const u32 *out_idx;              // optional scatter: output of gate ct -> LWE out_idx[ct]
 };
 
 // Gate prelude + mod-down + LWE key switch.
@@ -33,7 +34,13 @@ struct KsParams {
   u32 out_stride;           // u32 words per output LWE (>= n+1)
   u32 raw;                  // inputs are combined LWEs: skip the gate prelude
   const u32 *ksk;           // [d N][ksk_stride]
+  // Optional gather (circuit wires): input i of gate ct is LWE
+  // c{i}[in{i}[ct] & WIRE_MASK], negated (q - x) when bit 31 is set.
+  const u32 *in0, *in1;
 };
+
+constexpr u32 WIRE_NEG = 0x80000000u;
+constexpr u32 WIRE_MASK = 0x7fffffffu;
 
 // Gate codes 0..5 (and, nand, or, nor, xor, xnor).  GATE_RAW marks an input
 // that is already the combined LWE (no prelude); the low bits then select
@@ -54,6 +61,8 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
                        const unsigned char *gates, u64 *out, size_t count, u64 *rlwe_dbg,
                        int grid_limit, cudaStream_t s);
 cudaError_t launch_not(const u64 *in, u64 *out, size_t words, u64 q, cudaStream_t s);
+cudaError_t launch_imad_probe(int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s);
+// per launch: blocks * threads * iters * 16 * 8 multiply-adds
 size_t pbs_smem_bytes(int logn, u32 br_q, u32 n);
 
 }  // namespace pz

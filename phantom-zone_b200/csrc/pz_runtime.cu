@@ -12,8 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/phantom_zone_b200.h"
-#include "pz_kernels.cuh"
+#include "pz_internal.h"
 
 using pz::u32;
 using pz::u64;
@@ -83,40 +82,7 @@ pz::Decomp make_decomp(u64 q, u32 logb, u32 d) {  // decomposer.rs:158-178
 
 }  // namespace
 
-struct pz_ctx {
-  int param_id = 0, device = 0;
-  pz_params P{};
-  u32 logn = 0;
-  u64 root = 0;
-  cudaStream_t stream = nullptr;
-  // device tables
-  u64 *d_tw = nullptr;        // fw | fws | iw | iws  (4N words)
-  unsigned short *d_dlog = nullptr;
-  u64 *d_tv = nullptr;        // 6 x br_q/2
-  // constants
-  pz::RingConsts rc{};
-  u64 conv_c = 0, conv_cs = 0;
-  pz::BrParams br{};
-  pz::KsParams ks{};
-  int grid_limit = 0;
-  // host-API scratch (guarded by mu)
-  std::mutex mu;
-  size_t cap = 0;
-  u64 *d_c0 = nullptr, *d_c1 = nullptr, *d_out = nullptr;
-  unsigned char *d_gates = nullptr;
-  u32 *d_ks = nullptr;
-  std::string err;
-};
-
-struct pz_key {
-  pz_ctx *ctx = nullptr;
-  u64 *d_rgsw = nullptr, *d_autos = nullptr;
-  u32 *d_ksk = nullptr;
-  size_t bytes = 0;
-};
-
-namespace {
-
+namespace pz {
 pz_status fail(pz_ctx *ctx, pz_status s, const std::string &msg) {
   if (ctx) ctx->err = msg;
   return s;
@@ -125,17 +91,15 @@ pz_status cuda_fail(pz_ctx *ctx, const char *what, cudaError_t e) {
   pz_status s = (e == cudaErrorMemoryAllocation) ? PZ_ERR_OUT_OF_MEMORY : PZ_ERR_CUDA;
   return fail(ctx, s, std::string(what) + ": " + cudaGetErrorString(e));
 }
-#define PZ_CK(ctx, call)                                      \
-  do {                                                        \
-    cudaError_t _e = (call);                                  \
-    if (_e != cudaSuccess) return cuda_fail((ctx), #call, _e); \
-  } while (0)
-
-// Device entry points run on the caller's stream; NULL is the CUDA default
-// stream (the context's private stream only serves the synchronous host API).
-cudaStream_t pick(pz_ctx *, void *stream) { return (cudaStream_t)stream; }
-
 u32 ks_stride(const pz_params &P) { return (P.lwe_n + 1 + 31) & ~31u; }
+}  // namespace pz
+
+namespace {
+using pz::cuda_fail;
+using pz::fail;
+using pz::ks_stride;
+
+cudaStream_t pick(pz_ctx *, void *stream) { return (cudaStream_t)stream; }
 
 // evaluator.rs:664-673 dlog map; :688-726 test vectors; :728-743 auto elements
 void build_tables(pz_ctx *c, std::vector<unsigned short> &dlog, std::vector<u64> &tv) {
@@ -197,27 +161,6 @@ pz_status ensure_scratch(pz_ctx *c, size_t count) {
   return PZ_OK;
 }
 
-pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, const u64 *d_c0,
-                    const u64 *d_c1, u64 *d_out, size_t count, u32 *d_ks_out, u64 *d_rlwe, cudaStream_t s,
-                    u32 *d_ks_scratch, bool raw) {
-  pz::BrParams br = c->br;
-  br.rgsw = k->d_rgsw;
-  br.autos = k->d_autos;
-  pz::KsParams ks = c->ks;
-  ks.ksk = k->d_ksk;
-  ks.raw = raw ? 1u : 0u;
-  const u32 stride = ks_stride(c->P);
-  u32 *d_ks = d_ks_out ? d_ks_out : d_ks_scratch;
-  const u32 ks_out_stride = d_ks_out ? c->P.lwe_n + 1 : stride;
-  ks.out_stride = ks_out_stride;
-  cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s);
-  if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
-  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
-  e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s);
-  if (e != cudaSuccess) return cuda_fail(c, "launch_pbs", e);
-  return PZ_OK;
-}
-
 pz_status check_key(pz_ctx *c, const pz_key *k) {
   if (!k) return fail(c, PZ_ERR_INVALID_ARGUMENT, "key is NULL");
   if (k->ctx != c) return fail(c, PZ_ERR_KEY_MISMATCH, "key was uploaded through another context");
@@ -232,6 +175,34 @@ pz_status check_gates_host(pz_ctx *c, const uint8_t *gates, size_t count, bool r
 }
 
 }  // namespace
+
+namespace pz {
+pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, const u64 *d_c0, const u64 *d_c1,
+                    u64 *d_out, size_t count, u32 *d_ks_out, u64 *d_rlwe, cudaStream_t s, u32 *d_ks_scratch,
+                    bool raw, const u32 *in0, const u32 *in1, const u32 *out_idx) {
+  pz::BrParams br = c->br;
+  br.rgsw = k->d_rgsw;
+  br.autos = k->d_autos;
+  br.out_idx = out_idx;
+  pz::KsParams ks = c->ks;
+  ks.ksk = k->d_ksk;
+  ks.raw = raw ? 1u : 0u;
+  ks.in0 = in0;
+  ks.in1 = in1;
+  const u32 stride = ks_stride(c->P);
+  u32 *d_ks = d_ks_out ? d_ks_out : d_ks_scratch;
+  const u32 ks_out_stride = d_ks_out ? c->P.lwe_n + 1 : stride;
+  ks.out_stride = ks_out_stride;
+  cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s);
+  if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s);
+  if (e != cudaSuccess) return cuda_fail(c, "launch_pbs", e);
+  return PZ_OK;
+}
+
+}  // namespace pz
+using pz::run_gates;
 
 extern "C" {
 
@@ -501,6 +472,55 @@ pz_status pz_gate_batch_debug_device(pz_ctx *c, const pz_key *k, const uint8_t *
 pz_status pz_pbs_batch_device(pz_ctx *c, const pz_key *k, const uint8_t *d_test_vec, const uint64_t *d_lwe,
                               uint64_t *d_out, size_t count, void *stream) {
   return gate_device_common(c, k, d_test_vec, d_lwe, nullptr, d_out, count, nullptr, nullptr, stream, true);
+}
+
+pz_status pz_blind_rotate_batch_device(pz_ctx *c, const pz_key *k, const uint32_t *d_ks, const uint8_t *d_test_vec,
+                                       uint64_t *d_out, size_t count, void *stream) {
+  if (!c) return PZ_ERR_INVALID_ARGUMENT;
+  if (count == 0) return PZ_OK;
+  if (!d_ks || !d_test_vec || !d_out) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL device buffer");
+  pz_status s = check_key(c, k);
+  if (s != PZ_OK) return s;
+  PZ_CK(c, cudaSetDevice(c->device));
+  pz::BrParams br = c->br;
+  br.rgsw = k->d_rgsw;
+  br.autos = k->d_autos;
+  br.out_idx = nullptr;
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  PZ_CK(c, pz::launch_pbs((int)c->logn, d1, br, d_ks, c->P.lwe_n + 1, d_test_vec, d_out, count, nullptr,
+                          c->grid_limit, pick(c, stream)));
+  return PZ_OK;
+}
+
+pz_status pz_probe_imad_rate(int device, double *imad_per_second) {
+  if (!imad_per_second) return PZ_ERR_INVALID_ARGUMENT;
+  *imad_per_second = 0;
+  if (cudaSetDevice(device) != cudaSuccess) return PZ_ERR_CUDA;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return PZ_ERR_CUDA;
+  const int blocks = sms * 8, threads = 256;
+  const u32 iters = 2048;
+  u32 *sink = nullptr;
+  cudaEvent_t e0, e1;
+  if (cudaMalloc(&sink, blocks * 4) != cudaSuccess) return PZ_ERR_OUT_OF_MEMORY;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  pz_status st = PZ_OK;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4 && st == PZ_OK; rep++) {
+    cudaEventRecord(e0, 0);
+    if (pz::launch_imad_probe(blocks, threads, iters, sink, 0) != cudaSuccess) st = PZ_ERR_CUDA;
+    cudaEventRecord(e1, 0);
+    if (cudaEventSynchronize(e1) != cudaSuccess) st = PZ_ERR_CUDA;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;  // first launch is a warm-up
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (st == PZ_OK) *imad_per_second = (double)blocks * threads * iters * 16 * 8 / (best * 1e-3);
+  return st;
 }
 
 pz_status pz_not_batch_device(pz_ctx *c, const uint64_t *d_in, uint64_t *d_out, size_t words, void *stream) {

@@ -41,6 +41,13 @@ def params(param):
     return p
 
 
+def probe_imad_rate(device=0):
+    """32-bit IMAD instructions per second measured on `device`."""
+    v = ctypes.c_double()
+    check(lib().pz_probe_imad_rate(device, ctypes.byref(v)), None, "pz_probe_imad_rate")
+    return v.value
+
+
 def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
@@ -154,6 +161,11 @@ class Engine:
     def pbs_batch_device(self, key, test_vec, lwe, out, stream=None):
         check(lib().pz_pbs_batch_device(self.h, key.h, _ptr(test_vec), _ptr(lwe), _ptr(out),
                                         test_vec.numel(), _stream(stream)), self.h, "pz_pbs_batch_device")
+
+    def blind_rotate_device(self, key, ks, test_vec, out, stream=None):
+        check(lib().pz_blind_rotate_batch_device(self.h, key.h, _ptr(ks), _ptr(test_vec), _ptr(out),
+                                                 test_vec.numel(), _stream(stream)), self.h,
+              "pz_blind_rotate_batch_device")
 
     def not_device(self, x, out, stream=None):
         check(lib().pz_not_batch_device(self.h, _ptr(x), _ptr(out), x.numel(), _stream(stream)),

@@ -26,9 +26,14 @@ def oracle():
 
 _SETUPS = {}
 
+# parties each parameter set is designed for (SP_TEST_BOOL_PARAMS is single-party)
+PARTIES = {"SP_TEST": 1, "I_2P_LB_SR": 2, "I_4P": 4, "I_8P": 8, "NI_2P": 2, "NI_4P_HB_FR": 4,
+           "NI_4P_LB_SR": 4, "NI_8P": 8}
 
-def oracle_setup(param, parties=2):
+
+def oracle_setup(param, parties=None):
     """Oracle evaluator + client secrets + coefficient-domain server key (cached)."""
+    parties = PARTIES[param] if parties is None else parties
     key = (param, parties)
     if key not in _SETUPS:
         O = oracle()
@@ -56,15 +61,18 @@ def combine(ev, gate, c0, c1):
     Q = np.uint64(ev.Q)
     c0 = np.asarray(c0, np.uint64)
     c1 = np.asarray(c1, np.uint64)
+
+    def red(x):  # x < 2Q -> [0, Q) without computing the negative branch
+        x = np.array(x, np.uint64, copy=True)
+        x[x >= Q] -= Q
+        return x
+
     if gate in ("xor", "xnor", 4, 5):
-        d = np.where(c0 >= c1, c0 - c1, (Q + c0) - c1)
-        s = d + d
-        return np.where(s >= Q, s - Q, s)
-    s = c0 + c1
-    s = np.where(s >= Q, s - Q, s)
-    s = s.copy()
-    b = s[..., 0] + np.uint64(ev.Q >> 2)
-    s[..., 0] = np.where(b >= Q, b - Q, b)
+        d = (Q + c0) - c1
+        d = red(d)
+        return red(d + d)
+    s = red(c0 + c1)
+    s[..., 0] = red(s[..., 0] + np.uint64(ev.Q >> 2))
     return s
 
 

@@ -1,0 +1,243 @@
+"""Pins of the CPU oracle against the reference's own tests (no GPU).
+
+The reference ships no golden vectors (all its tests draw from entropy-seeded
+RNGs), so the oracle is pinned by restating those tests' properties:
+  ntt.rs:474-508      forward/backward round trip and output ranges
+  ntt.rs:510-540      NTT product == schoolbook negacyclic product (25..60-bit primes)
+  modulus_u64.rs:284-336   shoup_matrix_fma == naive u128 arithmetic
+  decomposer.rs:325-370    signed decomposition recomposes within +-1 after rounding
+  rgsw/mod.rs:526-686      Shoup external product == non-Shoup, bit for bit; decrypts to m0*m1
+  rgsw/mod.rs:688-831      Shoup automorphism == non-Shoup, bit for bit; decrypts to m(X^k)
+  mp_api.rs:662-695        bool gates under (multi-party) decryption
+plus the committed fixtures of tests/golden/ (oracle regression vectors).
+"""
+import numpy as np
+import pytest
+
+from conftest import combine, oracle, oracle_setup
+
+O = oracle()
+
+
+def _rng(tag):
+    return O.Rng(bytes([tag]) * 32)
+
+
+def test_generate_prime_matches_reference_rule():
+    N = 1 << 4
+    for bits in [25, 40, 50, 60]:
+        p = O.lib().orc_generate_prime(bits, 2 * N, 1 << bits)
+        assert p != 0 and p % (2 * N) == 1 and p.bit_length() == bits
+
+
+@pytest.mark.parametrize("bits", [25, 40, 50, 60])
+def test_ntt_negacyclic_mul(bits):
+    """ntt.rs:510-540 (N = 16, K = 128 in the reference; 32 samples here)."""
+    N = 1 << 4
+    p = O.lib().orc_generate_prime(bits, 2 * N, 1 << bits)
+    h = O.lib().orc_ntt_custom_new(p, N)
+    r = _rng(bits)
+    try:
+        for _ in range(32):
+            a = r.uniform_mod(p, N)
+            b = r.uniform_mod(p, N)
+            fa, fb = a.copy(), b.copy()
+            O.lib().orc_ntt_custom_forward(h, O._p(fa), 1)
+            O.lib().orc_ntt_custom_forward(h, O._p(fb), 1)
+            prod = np.array([O.lib().orc_mul_mod_barrett(p, int(x), int(y)) for x, y in zip(fa, fb)],
+                            np.uint64)
+            O.lib().orc_ntt_custom_backward(h, O._p(prod), 0)
+            want = np.empty(N, np.uint64)
+            O.lib().orc_negacyclic_mul(p, O._p(a), O._p(b), O._p(want), N)
+            assert np.array_equal(prod, want)
+    finally:
+        O.lib().orc_ntt_custom_free(h)
+
+
+@pytest.mark.parametrize("param", ["SP_TEST", "I_2P_LB_SR"])
+def test_ntt_roundtrip_and_ranges(param):
+    """ntt.rs:474-508 at the parameter set's own ring."""
+    ev, _, _, _ = oracle_setup(param)
+    r = _rng(3)
+    for _ in range(4):
+        a = r.uniform_mod(ev.Q, ev.N)
+        f = ev.ntt_forward(a)
+        assert (f < ev.Q).all() and not np.array_equal(f, a)
+        assert np.array_equal(ev.ntt_backward(f), a)
+        fl = ev.ntt_forward(a, lazy=True)
+        assert (fl < 2 * ev.Q).all()
+        assert np.array_equal(ev.ntt_backward(fl), a)
+        bl = ev.ntt_backward(f, lazy=True)
+        assert (bl < 2 * ev.Q).all()
+        assert np.array_equal(np.where(bl >= ev.Q, bl - np.uint64(ev.Q), bl), a)
+
+
+def test_shoup_matrix_fma():
+    """modulus_u64.rs:284-336: prime 36028797017456641, ring 8, d = 2."""
+    p = 36028797017456641
+    r = _rng(5)
+    for _ in range(64):
+        a = r.uniform_mod(p, 16)
+        b = r.uniform_mod(p, 16)
+        a_sh = np.array([O.lib().orc_shoup_repr(int(v), p) for v in a], np.uint64)
+        out = np.zeros(8, np.uint64)
+        O.lib().orc_shoup_matrix_fma(p, O._p(out), O._p(a), O._p(a_sh), O._p(b), 2, 8)
+        got = np.where(out >= p, out - np.uint64(p), out)
+        want = [(int(a[i]) * int(b[i]) + int(a[8 + i]) * int(b[8 + i])) % p for i in range(8)]
+        assert list(map(int, got)) == want
+
+
+@pytest.mark.parametrize("logq", [37, 55])
+@pytest.mark.parametrize("prime", [True, False])
+def test_decomposition_recomposes(logq, prime):
+    """decomposer.rs:325-370 (logb 11, d 3; 10^6 samples there, 4000 here)."""
+    logb, d = 11, 3
+    q = O.lib().orc_generate_prime(logq, 2 << 11, 1 << logq) if prime else 1 << logq
+    r = _rng(logq + prime)
+    vals = r.uniform_mod(q, 4000)
+    limbs = np.zeros(8, np.uint64)
+    for v in vals:
+        ib = O.lib().orc_decompose_custom(q, logb, d, int(v), O._p(limbs))
+        back = O.lib().orc_round_value(O.lib().orc_recompose(q, logb, d, O._p(limbs)), ib)
+        rounded = O.lib().orc_round_value(int(v), ib)
+        assert abs(int(rounded) - int(back)) <= 1
+
+
+def test_decompose_edge_values():
+    """Q and 0 decompose identically (the wrapping !(q - v) + 1 of decomposer.rs:219-221)."""
+    ev, _, _, _ = oracle_setup("I_2P_LB_SR")
+    for which in range(4):
+        assert np.array_equal(ev.decompose(which, ev.Q if which else ev.info.lwe_q),
+                              ev.decompose(which, 0))
+
+
+def _rlwe_decrypt(ev, s, rl):
+    """b - a s (negacyclic, mod Q) for an RLWE [a | b] under secret s."""
+    N, Q = ev.N, ev.Q
+    a, b = rl[:N], rl[N:]
+    sq = np.array([(int(x) % Q) if x >= 0 else Q + int(x) for x in s], np.uint64)
+    prod = np.empty(N, np.uint64)
+    O.lib().orc_negacyclic_mul(Q, O._p(np.ascontiguousarray(a)), O._p(sq), O._p(prod), N)
+    return np.array([(int(bb) - int(pp)) % Q for bb, pp in zip(b, prod)], np.uint64)
+
+
+def _signed(v, Q):
+    v = int(v) % Q
+    return v - Q if v > Q // 2 else v
+
+
+@pytest.mark.parametrize("param", ["SP_TEST", "I_2P_LB_SR"])
+def test_rlwe_by_rgsw_shoup_equals_plain_and_decrypts(param):
+    """rgsw/mod.rs:526-686: Shoup == non-Shoup; RLWE(m) x RGSW(X^{emb z_i}) decrypts to m X^{emb z_i}."""
+    ev, (s, z, _, _), _, key = oracle_setup(param)
+    r = _rng(7)
+    N, Q = ev.N, ev.Q
+    delta = Q // 8
+    for trial in range(3):
+        i = [0, ev.n // 2, ev.n - 1][trial]
+        m = r.uniform_mod(4, N)
+        a = r.uniform_mod(Q, N)
+        rl = np.concatenate([a, np.zeros(N, np.uint64)])
+        sa = _rlwe_decrypt(ev, s, np.concatenate([a, np.zeros(N, np.uint64)]))  # = -a s
+        b = np.array([(int(m[k]) * delta - int(sa[k])) % Q for k in range(N)], np.uint64)
+        rl[N:] = b
+        x = key.rlwe_by_rgsw(rl, i, shoup=True)
+        y = key.rlwe_by_rgsw(rl, i, shoup=False)
+        assert np.array_equal(x, y)
+        dec = _rlwe_decrypt(ev, s, x)
+        e = int(z[i]) * ev.info.embedding_factor
+        want = np.zeros(N, np.int64)
+        for k in range(N):  # m(X) * X^e, negacyclic
+            t = k + e
+            sign = 1
+            while t >= N:
+                t -= N
+                sign = -sign
+            while t < 0:
+                t += N
+                sign = -sign
+            want[t] += sign * int(m[k])
+        got = np.array([round(_signed(v, Q) / delta) for v in dec])
+        assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("param", ["SP_TEST", "I_2P_LB_SR"])
+def test_rlwe_auto_shoup_equals_plain_and_decrypts(param):
+    """rgsw/mod.rs:688-831: Shoup == non-Shoup; decrypts to m(X^k)."""
+    ev, (s, _, _, _), _, key = oracle_setup(param)
+    r = _rng(9)
+    N, Q = ev.N, ev.Q
+    delta = Q // 8
+    for slot in [0, 1, ev.info.w]:
+        m = r.uniform_mod(4, N)
+        a = r.uniform_mod(Q, N)
+        sa = _rlwe_decrypt(ev, s, np.concatenate([a, np.zeros(N, np.uint64)]))
+        b = np.array([(int(m[k]) * delta - int(sa[k])) % Q for k in range(N)], np.uint64)
+        rl = np.concatenate([a, b])
+        x = key.rlwe_auto(rl, slot, shoup=True)
+        y = key.rlwe_auto(rl, slot, shoup=False)
+        assert np.array_equal(x, y)
+        idx, sgn = ev.auto_map(slot)
+        want = np.zeros(N, np.int64)
+        for k in range(N):
+            want[idx[k]] = int(m[k]) if sgn[k] else -int(m[k])
+        got = np.array([round(_signed(v, Q) / delta) for v in _rlwe_decrypt(ev, s, x)])
+        assert np.array_equal(np.mod(got, 8), np.mod(want, 8))
+
+
+def test_lwe_key_switch_preserves_message():
+    """lwe.rs:14-44: the key-switched LWE decrypts (under z, mod q_ks) like the input (under s)."""
+    ev, (s, z, _, _), _, key = oracle_setup("I_2P_LB_SR")
+    qk = ev.info.lwe_q
+    r = _rng(11)
+    for bit in [0, 1, 1, 0]:
+        ct = ev.encrypt_bool(r, s, [bit])[0]
+        down = np.array([int(np.round(float(v) * qk / float(ev.Q))) for v in ct], np.uint64)
+        out = key.lwe_key_switch(down)
+        m_in = (int(down[0]) - sum(int(a) * int(x) for a, x in zip(down[1:], s))) % qk
+        m_out = (int(out[0]) - sum(int(a) * int(x) for a, x in zip(out[1:], z))) % qk
+        diff = (m_in - m_out) % qk
+        assert min(diff, qk - diff) < qk // 16
+
+
+TRUTH = {
+    "and": lambda a, b: a & b, "nand": lambda a, b: 1 - (a & b), "or": lambda a, b: a | b,
+    "nor": lambda a, b: 1 - (a | b), "xor": lambda a, b: a ^ b, "xnor": lambda a, b: 1 - (a ^ b),
+}
+
+
+@pytest.mark.parametrize("param", ["SP_TEST", "I_2P_LB_SR"])
+def test_gates_decrypt_correctly(param):
+    """mp_api.rs:662-695: every gate on all four input pairs, single- and multi-party decryption."""
+    ev, (s, _, sp, _), _, key = oracle_setup(param)
+    r = _rng(13)
+    a = np.array([0, 0, 1, 1])
+    b = np.array([0, 1, 0, 1])
+    c0 = ev.encrypt_bool(r, s, a)
+    c1 = ev.encrypt_bool(r, s, b)
+    for g, f in TRUTH.items():
+        out = np.stack([key.gate(g, c0[i], c1[i]) for i in range(4)])
+        assert list(ev.decrypt_bool(s, out)) == list(f(a, b))
+        assert list(ev.mp_decrypt_bool(r, sp, out)) == list(f(a, b))
+    assert list(ev.decrypt_bool(s, np.stack([ev.not_(c) for c in c0]))) == list(1 - a)
+
+
+def test_gate_batch_threads_equal_single():
+    ev, (s, _, _, _), _, key = oracle_setup("SP_TEST")
+    r = _rng(15)
+    c0 = ev.encrypt_bool(r, s, [0, 1, 1, 0, 1, 0])
+    c1 = ev.encrypt_bool(r, s, [1, 1, 0, 0, 1, 1])
+    gates = np.array([0, 1, 2, 3, 4, 5], np.uint8)
+    single = np.stack([key.gate(int(g), c0[i], c1[i]) for i, g in enumerate(gates)])
+    assert np.array_equal(key.gate_batch(gates, c0, c1, threads=3), single)
+
+
+def test_pbs_prelude_is_the_gate():
+    """gate(c0, c1) == pbs(combine(c0, c1)) (evaluator.rs:2163-2245)."""
+    ev, (s, _, _, _), _, key = oracle_setup("SP_TEST")
+    r = _rng(17)
+    c0 = ev.encrypt_bool(r, s, [1])[0]
+    c1 = ev.encrypt_bool(r, s, [0])[0]
+    for g in TRUTH:
+        out, _, _, _ = key.pbs(g, combine(ev, g, c0, c1))
+        assert np.array_equal(out, key.gate(g, c0, c1))
