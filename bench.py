@@ -277,6 +277,47 @@ def plain_form(P, torch, device, seed=7):
             "p99_ms": float(np.percentile(lat, 99)), "config": "I_2P_LB_SR, 128 NAND, one gate per launch"}
 
 
+def kernel_only(args):
+    """One kernel on a batch of synthetic items, --warmup + --steps launches,
+    printing the mean launch time (the small case profiled with ncu)."""
+    import torch
+    P = pz()
+    p = P.params(args.param)
+    L = p.rlwe_n + 1
+    eng = P.Engine(args.param)
+    key = eng.upload_key(*synthetic_key(p, 0x5EED))
+    rng = np.random.default_rng(99)
+    B = args.batch
+    if args.mode == "br-kernel":
+        ks = rng.integers(0, p.lwe_q, (B, p.lwe_n + 1), dtype=np.uint64).astype(np.uint32)
+        d_ks = torch.from_numpy(ks.view(np.int32)).cuda()
+        d_tv = torch.from_numpy(rng.integers(0, 6, B).astype(np.uint8)).cuda()
+        d_out = torch.empty((B, L), dtype=torch.int64, device="cuda")
+
+        def launch():
+            eng.blind_rotate_device(key, d_ks, d_tv, d_out)
+    else:
+        lwe = torch.from_numpy(rng.integers(0, p.lwe_q, (B, L), dtype=np.uint64).view(np.int64)).cuda()
+        d_out = torch.empty((B, p.lwe_n + 1), dtype=torch.int32, device="cuda")
+
+        def launch():
+            eng.lwe_key_switch_device(key, lwe, d_out)
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        launch()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / max(args.steps, 1)
+    out = {"mode": args.mode, "param_set": args.param, "batch": B, "ms_per_launch": ms, "items_per_s": B / ms * 1e3}
+    if args.mode == "br-kernel":
+        out["modmuls_per_item"] = schedule_work(p, ks) / B
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -285,9 +326,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--mode", default="wavefront", choices=["wavefront", "br-kernel", "ks-kernel"],
+                    help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
+    ap.add_argument("--batch", type=int, default=296)
+    ap.add_argument("--param", default=PARAM)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode != "wavefront":
+        return kernel_only(args)
 
     import torch
     dist, rank, world, local = dist_setup(args)
