@@ -127,6 +127,22 @@ pz_status pz_gate_batch(pz_ctx *ctx, const pz_key *key, const uint8_t *gates, co
 pz_status pz_gate_batch_device(pz_ctx *ctx, const pz_key *key, const uint8_t *d_gates,
                                const uint64_t *d_c0, const uint64_t *d_c1, uint64_t *d_out,
                                size_t count, void *stream);
+/* Same as pz_gate_batch_device for callers that cannot allocate device
+ * memory on their gate path (device memory fully reserved by another
+ * allocator, or a serving thread that must not make allocating CUDA calls).
+ * No counterpart in the reference.  The key-switch scratch between the two
+ * kernels is a fixed array compiled into the library (PZ_NOALLOC_KS_WORDS
+ * u32 words, kept on every GPU that loads the library until exit), so this
+ * call allocates nothing; count is limited to PZ_NOALLOC_KS_WORDS / stride
+ * (stride = n + 1 rounded up to 32; 4096 gates at NI_8P) and larger batches
+ * are rejected with PZ_ERR_INVALID_ARGUMENT.  The first call on a device
+ * looks up the array's device address and should come before any stream
+ * capture.  Every call shares the array: calls whose work overlaps on the
+ * GPU race and must be serialized by the caller. */
+#define PZ_NOALLOC_KS_WORDS (4096u * 672u)
+pz_status pz_gate_batch_device_noalloc(pz_ctx *ctx, const pz_key *key, const uint8_t *d_gates,
+                                       const uint64_t *d_c0, const uint64_t *d_c1, uint64_t *d_out,
+                                       size_t count, void *stream);
 /* Diagnostic variant: also writes the key-switched LWE (d_ks_out
  * [count][n + 1] u32, mod q_ks) and the blind-rotated RLWE (d_rlwe_out
  * [count][2][N]) of each gate; either may be NULL. */

@@ -50,6 +50,7 @@ SIGNATURES = {
     "pz_key_device_bytes": (ctypes.c_size_t, [vp]),
     "pz_gate_batch": (st, [vp, vp, u8p, u64p, u64p, u64p, ctypes.c_size_t]),
     "pz_gate_batch_device": (st, [vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_gate_batch_device_noalloc": (st, [vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_gate_batch_debug_device": (st, [vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp, vp, vp]),
     "pz_pbs_batch_device": (st, [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_not_batch_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),

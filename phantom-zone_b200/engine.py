@@ -158,6 +158,13 @@ class Engine:
                                                    _ptr(out), count, _ptr(ks_out), _ptr(rlwe_out),
                                                    _stream(stream)), self.h, "pz_gate_batch_debug_device")
 
+    def gate_batch_device_noalloc(self, key, gates, c0, c1, out, stream=None):
+        """gate_batch_device without any device allocation (fixed in-library
+        scratch; bounded batch size; concurrent calls must not overlap)."""
+        check(lib().pz_gate_batch_device_noalloc(self.h, key.h, _ptr(gates), _ptr(c0), _ptr(c1), _ptr(out),
+                                                 gates.numel(), _stream(stream)), self.h,
+              "pz_gate_batch_device_noalloc")
+
     def pbs_batch_device(self, key, test_vec, lwe, out, stream=None):
         check(lib().pz_pbs_batch_device(self.h, key.h, _ptr(test_vec), _ptr(lwe), _ptr(out),
                                         test_vec.numel(), _stream(stream)), self.h, "pz_pbs_batch_device")
