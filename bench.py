@@ -285,6 +285,8 @@ def kernel_only(args):
     p = P.params(args.param)
     L = p.rlwe_n + 1
     eng = P.Engine(args.param)
+    if args.variant is not None:
+        eng.pbs_variant = args.variant
     key = eng.upload_key(*synthetic_key(p, 0x5EED))
     rng = np.random.default_rng(99)
     B = args.batch
@@ -312,7 +314,8 @@ def kernel_only(args):
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / max(args.steps, 1)
-    out = {"mode": args.mode, "param_set": args.param, "batch": B, "ms_per_launch": ms, "items_per_s": B / ms * 1e3}
+    out = {"mode": args.mode, "param_set": args.param, "batch": B, "variant": eng.pbs_variant,
+           "ms_per_launch": ms, "items_per_s": B / ms * 1e3}
     if args.mode == "br-kernel":
         out["modmuls_per_item"] = schedule_work(p, ks) / B
     print(json.dumps(out), flush=True)
@@ -330,6 +333,7 @@ def main():
                     help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
+    ap.add_argument("--variant", type=int, default=None, help="blind-rotation launch-shape variant")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -62,6 +62,8 @@ SIGNATURES = {
     "pz_rlwe_auto_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, ctypes.c_int, vp]),
     "pz_lwe_key_switch_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_ctx_set_pbs_grid_limit": (st, [vp, ctypes.c_int]),
+    "pz_ctx_set_pbs_variant": (st, [vp, ctypes.c_int]),
+    "pz_ctx_pbs_variant": (ctypes.c_int, [vp]),
     "pz_circuit_create": (st, [ctypes.POINTER(vp)]),
     "pz_circuit_destroy": (None, [vp]),
     "pz_circuit_last_error": (ctypes.c_char_p, [vp]),

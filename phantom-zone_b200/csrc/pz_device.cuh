@@ -2,8 +2,9 @@
 //
 // Modular arithmetic mod the RLWE prime Q (< 2^62):
 //   * NTT butterflies use Shoup multiplication by precomputed twiddles
-//     (Harvey's lazy butterflies, the algorithm of ntt.rs:24-104): forward
-//     values live in [0, 4Q), inverse values in [0, 2Q).
+//     (the butterflies of ntt.rs:24-104): forward values grow without
+//     reduction (below 23Q after the 11 stages of N = 2048), inverse values
+//     stay in [0, 2Q) (Harvey).
 //   * The pointwise key product uses Montgomery REDC with R = 2^64.  Device
 //     keys are stored as K * N^{-1} * R mod Q, so REDC(x * K') = x * K * N^{-1}
 //     and the inverse NTT needs no final N^{-1} scaling.  Two products are
@@ -16,7 +17,8 @@
 // coefficients per thread.  Stages are grouped in rounds of three (a radix-8
 // step per thread); between rounds the coefficients are re-distributed
 // through shared memory.  Only the first forward exchange (last inverse
-// exchange) crosses warps; all other exchanges stay inside a warp.  Shared
+// exchange) crosses warps; all other exchanges stay inside a warp.  Every
+// barrier sits on control flow that is uniform across the block.  Shared
 // memory is addressed through the swizzle  pos ^ ((pos >> 4) & 15)  which
 // makes every read/write pattern used here bank-conflict free for u64 words.
 #pragma once
@@ -32,8 +34,9 @@ struct RingConsts {
   u64 q;         // Q
   u64 qinv_neg;  // -Q^{-1} mod 2^64
   u64 n_inv, n_inv_s;  // N^{-1} mod Q and its Shoup companion
-  const u64 *fw, *fws;  // forward twiddles psi^{bitrev(i)}, Shoup companions
-  const u64 *iw, *iws;  // inverse twiddles psi^{-bitrev(i)}, Shoup companions
+  u64 one_s;            // Shoup companion of 1: reduce_any(v) = v mod Q for any v
+  const u64 *fw;  // forward twiddles: pairs (psi^{bitrev(i)}, Shoup companion)
+  const u64 *iw;  // inverse twiddles: pairs (psi^{-bitrev(i)}, Shoup companion)
 };
 
 // Signed gadget decomposer, decomposer.rs:158-300.
@@ -129,12 +132,14 @@ __device__ __forceinline__ int dev_index(int j, int r) {
   return (r >> 1) * (2 * NttShape<LOGN>::T) + 2 * j + (r & 1);
 }
 
-// Harvey forward butterfly, ntt.rs:31-49 (x, y < 4q -> x', y' < 4q)
+// Forward CT butterfly (the x' = x + wy, y' = x - wy of ntt.rs:31-49) without
+// Harvey's conditional subtraction: wy is a Shoup product in [0, 2q), so both
+// outputs grow by less than 2q per stage.  From inputs < q the 11 stages of
+// N = 2048 stay below 23q < 2^60 (Q < 2^55), and the Shoup product accepts
+// any 64-bit input, so no stage needs a reduction.
 __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
-  const u64 q2 = q << 1;
-  if (x >= q2) x -= q2;
-  u64 t = shoup_mul(y, w, ws, q);
-  y = x + q2 - t;
+  const u64 t = shoup_mul(y, w, ws, q);
+  y = x + (q << 1) - t;
   x = x + t;
 }
 // Harvey inverse butterfly, ntt.rs:84-104 (x, y < 2q -> x', y' < 2q)
@@ -149,179 +154,209 @@ __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
 
 __device__ __forceinline__ u64 ldg(const u64 *p) { return __ldg(p); }
 
-// One forward radix-8 round: stages with m, 2m, 4m groups; blk = group of this thread.
-template <int NP>
-__device__ __forceinline__ void fwd_round8(u64 (&x)[NP][8], int m, int blk, const RingConsts &rc) {
+// ---------------------------------------------------------------------------
+// Single-polynomial block NTT: three radix-8 rounds (plus the trailing
+// 2-stage round for N = 2048).  The transform is called once per polynomial,
+// so the whole blind rotation holds a single forward and a single inverse
+// copy.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sync_exchange(bool cross) {
+  if (cross) __syncthreads();
+  else __syncwarp();
+}
+
+// threadIdx.x read afresh: addresses derived from it are recomputed inside
+// each transform instead of being hoisted out of the blind-rotation loop and
+// kept live in registers for the whole kernel.
+__device__ __forceinline__ int tid_opaque() {
+  int t;
+  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
+  return t;
+}
+
+// Twiddle pair (w, Shoup(w)) at index i of an interleaved table (one 16-byte
+// load).  A volatile asm load, unlike __ldg (an invariant load the compiler
+// may hoist out of the transform and keep live), stays inside its round.
+__device__ __forceinline__ void tw(const u64 *t, int i, u64 &w, u64 &ws) {
+  asm volatile("ld.global.nc.v2.u64 {%0, %1}, [%2];" : "=l"(w), "=l"(ws) : "l"(t + 2 * i));
+}
+
+// Forward radix-8 round k: stages with m = 8^k, 2m and 4m groups; blk is the
+// group index of this thread in the first of them.
+template <int LOGN>
+__device__ __forceinline__ void fwd_round8(u64 (&x)[8], int k, int j, const RingConsts &rc) {
+  const int m = 1 << (3 * k);
+  const int blk = j >> (LOGN - 3 * k - 3);
   const u64 q = rc.q;
-  {
-    u64 w = ldg(rc.fw + m + blk), ws = ldg(rc.fws + m + blk);
+  u64 w, ws;
+  tw(rc.fw, m + blk, w, ws);
 #pragma unroll
-    for (int p = 0; p < NP; p++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) fbf(x[p][r], x[p][r + 4], w, ws, q);
-  }
+  for (int r = 0; r < 4; r++) fbf(x[r], x[r + 4], w, ws, q);
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    int idx = 2 * m + 2 * blk + h;
-    u64 w = ldg(rc.fw + idx), ws = ldg(rc.fws + idx);
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      fbf(x[p][4 * h + 0], x[p][4 * h + 2], w, ws, q);
-      fbf(x[p][4 * h + 1], x[p][4 * h + 3], w, ws, q);
-    }
+    tw(rc.fw, 2 * m + 2 * blk + h, w, ws);
+    fbf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
+    fbf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
   }
 #pragma unroll
   for (int h = 0; h < 4; h++) {
-    int idx = 4 * m + 4 * blk + h;
-    u64 w = ldg(rc.fw + idx), ws = ldg(rc.fws + idx);
-#pragma unroll
-    for (int p = 0; p < NP; p++) fbf(x[p][2 * h], x[p][2 * h + 1], w, ws, q);
+    tw(rc.fw, 4 * m + 4 * blk + h, w, ws);
+    fbf(x[2 * h], x[2 * h + 1], w, ws, q);
   }
 }
 
-template <int NP>
-__device__ __forceinline__ void inv_round8(u64 (&x)[NP][8], int m, int blk, const RingConsts &rc) {
+template <int LOGN>
+__device__ __forceinline__ void inv_round8(u64 (&x)[8], int k, int j, const RingConsts &rc) {
+  const int m = 1 << (3 * k);
+  const int blk = j >> (LOGN - 3 * k - 3);
   const u64 q = rc.q;
+  u64 w, ws;
 #pragma unroll
   for (int h = 0; h < 4; h++) {
-    int idx = 4 * m + 4 * blk + h;
-    u64 w = ldg(rc.iw + idx), ws = ldg(rc.iws + idx);
-#pragma unroll
-    for (int p = 0; p < NP; p++) ibf(x[p][2 * h], x[p][2 * h + 1], w, ws, q);
+    tw(rc.iw, 4 * m + 4 * blk + h, w, ws);
+    ibf(x[2 * h], x[2 * h + 1], w, ws, q);
   }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    int idx = 2 * m + 2 * blk + h;
-    u64 w = ldg(rc.iw + idx), ws = ldg(rc.iws + idx);
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      ibf(x[p][4 * h + 0], x[p][4 * h + 2], w, ws, q);
-      ibf(x[p][4 * h + 1], x[p][4 * h + 3], w, ws, q);
-    }
+    tw(rc.iw, 2 * m + 2 * blk + h, w, ws);
+    ibf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
+    ibf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
   }
-  {
-    u64 w = ldg(rc.iw + m + blk), ws = ldg(rc.iws + m + blk);
+  tw(rc.iw, m + blk, w, ws);
 #pragma unroll
-    for (int p = 0; p < NP; p++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) ibf(x[p][r], x[p][r + 4], w, ws, q);
-  }
+  for (int r = 0; r < 4; r++) ibf(x[r], x[r + 4], w, ws, q);
 }
 
 // Trailing 2-stage round (stages with N/4 and N/2 groups).
-template <int LOGN, int NP>
-__device__ __forceinline__ void fwd_round4(u64 (&x)[NP][8], int j, const RingConsts &rc) {
+template <int LOGN>
+__device__ __forceinline__ void fwd_round4(u64 (&x)[8], int j, const RingConsts &rc) {
   constexpr int N = 1 << LOGN;
   const u64 q = rc.q;
+  u64 w, ws;
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    int g = (j >> 5) * 64 + (j & 31) + (h << 5);
-    u64 w = ldg(rc.fw + N / 4 + g), ws = ldg(rc.fws + N / 4 + g);
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      fbf(x[p][4 * h + 0], x[p][4 * h + 2], w, ws, q);
-      fbf(x[p][4 * h + 1], x[p][4 * h + 3], w, ws, q);
-    }
+    const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
+    tw(rc.fw, N / 4 + g, w, ws);
+    fbf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
+    fbf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
 #pragma unroll
     for (int e = 0; e < 2; e++) {
-      int idx = N / 2 + 2 * g + e;
-      u64 w2 = ldg(rc.fw + idx), ws2 = ldg(rc.fws + idx);
-#pragma unroll
-      for (int p = 0; p < NP; p++) fbf(x[p][4 * h + 2 * e], x[p][4 * h + 2 * e + 1], w2, ws2, q);
+      tw(rc.fw, N / 2 + 2 * g + e, w, ws);
+      fbf(x[4 * h + 2 * e], x[4 * h + 2 * e + 1], w, ws, q);
     }
   }
 }
 
-template <int LOGN, int NP>
-__device__ __forceinline__ void inv_round4(u64 (&x)[NP][8], int j, const RingConsts &rc) {
+template <int LOGN>
+__device__ __forceinline__ void inv_round4(u64 (&x)[8], int j, const RingConsts &rc) {
   constexpr int N = 1 << LOGN;
   const u64 q = rc.q;
+  u64 w, ws;
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    int g = (j >> 5) * 64 + (j & 31) + (h << 5);
+    const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
 #pragma unroll
     for (int e = 0; e < 2; e++) {
-      int idx = N / 2 + 2 * g + e;
-      u64 w2 = ldg(rc.iw + idx), ws2 = ldg(rc.iws + idx);
-#pragma unroll
-      for (int p = 0; p < NP; p++) ibf(x[p][4 * h + 2 * e], x[p][4 * h + 2 * e + 1], w2, ws2, q);
+      tw(rc.iw, N / 2 + 2 * g + e, w, ws);
+      ibf(x[4 * h + 2 * e], x[4 * h + 2 * e + 1], w, ws, q);
     }
-    u64 w = ldg(rc.iw + N / 4 + g), ws = ldg(rc.iws + N / 4 + g);
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      ibf(x[p][4 * h + 0], x[p][4 * h + 2], w, ws, q);
-      ibf(x[p][4 * h + 1], x[p][4 * h + 3], w, ws, q);
-    }
+    tw(rc.iw, N / 4 + g, w, ws);
+    ibf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
+    ibf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
   }
 }
 
-// Re-distribute NP polynomials from layout `from` to layout `to` through
-// shared memory sm (NP * N words).  cross: the exchange crosses warps.
-template <int LOGN, int NP, typename FromF, typename ToF>
-__device__ __forceinline__ void exchange(u64 (&x)[NP][8], u64 *sm, int j, FromF from, ToF to,
-                                         bool cross) {
-  constexpr int N = 1 << LOGN;
-  if (cross) __syncthreads();
-  else __syncwarp();
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-#pragma unroll
-    for (int r = 0; r < 8; r++) sm[p * N + swz(from(j, r))] = x[p][r];
-  if (cross) __syncthreads();
-  else __syncwarp();
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-#pragma unroll
-    for (int r = 0; r < 8; r++) x[p][r] = sm[p * N + swz(to(j, r))];
+// Layout of full round k: thread j holds base + t r, t = N >> (3k + 3).
+template <int LOGN>
+__device__ __forceinline__ int base_full(int k, int j) {
+  const int lt = LOGN - 3 * k - 3;
+  return ((j >> lt) << (lt + 3)) + (j & ((1 << lt) - 1));
 }
 
-// Forward negacyclic NTT (CT, ntt.rs:110-143 without the final reduction):
-// input in the coefficient layout, values < 4q; output in the evaluation
-// layout, values < 4q.
-template <int LOGN, int NP>
-__device__ __forceinline__ void ntt_forward(u64 (&x)[NP][8], u64 *sm, const RingConsts &rc) {
+// Swizzled exchange-buffer address of register r in layout L (0..2: full
+// rounds, 3: trailing round).  For N = 2048 the per-thread base absorbs the
+// swizzle: in every layout the coefficient position is a disjoint union of
+// bit fields from the warp, the lane and r, so swz(pos) reduces to one XOR
+// (and at most an immediate offset) per register.  Other sizes use swz()
+// directly.
+template <int LOGN, int L>
+__device__ __forceinline__ int xbase(int j) {
+  if constexpr (LOGN == 11) {
+    const int w = j >> 5, l = j & 31;
+    if constexpr (L == 0) return j ^ ((j >> 4) & 15);                       // pos = j + 256 r
+    else if constexpr (L == 1) return (w << 8) + (l ^ (l >> 4));            // 256 w + l + 32 r
+    else if constexpr (L == 2) return ((w << 8) + ((l >> 2) << 5) + (l & 3)) ^ ((l >> 2) << 1);  // + 4 r
+    else return ((w << 8) + (l << 2)) ^ (l >> 2);                           // 256 w + 4 l + 128 h + e
+  } else {
+    return L < 3 ? base_full<LOGN>(L, j) : 0;
+  }
+}
+template <int LOGN, int L>
+__device__ __forceinline__ int xaddr(int b, int j, int r) {
+  if constexpr (LOGN == 11) {
+    if constexpr (L == 0) return b + (r << 8);
+    else if constexpr (L == 1) return (b ^ (r << 1)) + (r << 5);
+    else if constexpr (L == 2) return b ^ ((r << 2) ^ (r >> 2));
+    else return b ^ ((r & 3) ^ ((r >> 2) << 3) ^ ((r >> 2) << 7));
+  } else {
+    return L < 3 ? swz(b + (r << (LOGN - 3 * L - 3))) : swz(pos_partial(j, r));
+  }
+}
+
+// Move the polynomial from layout LF to layout LT through sm (N words).
+template <int LOGN, int LF, int LT>
+__device__ __forceinline__ void xchg(u64 (&x)[8], u64 *sm, int j) {
+  constexpr bool cross = (LF == 0 || LT == 0);
+  const int bf = xbase<LOGN, LF>(j), bt = xbase<LOGN, LT>(j);
+  sync_exchange(cross);
+#pragma unroll
+  for (int r = 0; r < 8; r++) sm[xaddr<LOGN, LF>(bf, j, r)] = x[r];
+  sync_exchange(cross);
+#pragma unroll
+  for (int r = 0; r < 8; r++) x[r] = sm[xaddr<LOGN, LT>(bt, j, r)];
+}
+
+// Forward negacyclic NTT (CT, ntt.rs:110-143 without reductions) of one
+// polynomial: coefficient layout in, values < q; evaluation layout out,
+// values < (2 log N + 1) q.  sm: N words.  The rounds run in a loop (one copy
+// of the round body); the exchanges between them are layout-specialised and
+// picked by a block-uniform switch.
+template <int LOGN>
+__device__ __forceinline__ void ntt_fwd(u64 (&x)[8], u64 *sm, const RingConsts &rc) {
   typedef NttShape<LOGN> S;
-  const int j = threadIdx.x;
-#pragma unroll
-  for (int k = 0; k < S::FULL; k++) {
-    if (k > 0) {
-      exchange<LOGN, NP>(
-          x, sm, j, [k](int jj, int r) { return pos_full<LOGN>(k - 1, jj, r); },
-          [k](int jj, int r) { return pos_full<LOGN>(k, jj, r); }, k == 1);
-    }
-    const int t = S::N >> (3 * k + 3);
-    fwd_round8<NP>(x, 1 << (3 * k), j / t, rc);
+  static_assert(S::FULL == 3, "three radix-8 rounds");
+  const int j = tid_opaque();
+#pragma unroll 1
+  for (int k = 0; k < 3; k++) {
+    if (k == 1) xchg<LOGN, 0, 1>(x, sm, j);
+    else if (k == 2) xchg<LOGN, 1, 2>(x, sm, j);
+    fwd_round8<LOGN>(x, k, j, rc);
   }
-  if (S::PARTIAL) {
-    exchange<LOGN, NP>(
-        x, sm, j, [](int jj, int r) { return pos_full<LOGN>(S::FULL - 1, jj, r); },
-        [](int jj, int r) { return pos_partial(jj, r); }, S::FULL == 1);
-    fwd_round4<LOGN, NP>(x, j, rc);
+  if constexpr (S::PARTIAL) {
+    xchg<LOGN, 2, 3>(x, sm, j);
+    fwd_round4<LOGN>(x, j, rc);
   }
 }
 
-// Inverse negacyclic NTT (GS, ntt.rs:187-230 without the N^{-1} factor):
-// input in the evaluation layout, values < 2q; output in the coefficient
-// layout, values < 2q.
-template <int LOGN, int NP>
-__device__ __forceinline__ void ntt_inverse(u64 (&x)[NP][8], u64 *sm, const RingConsts &rc) {
+// Inverse negacyclic NTT (GS, ntt.rs:187-230 without the N^{-1} factor) of
+// one polynomial: evaluation layout in, values < 2q; coefficient layout out,
+// values < 2q.  sm: N words.
+template <int LOGN>
+__device__ __forceinline__ void ntt_inv(u64 (&x)[8], u64 *sm, const RingConsts &rc) {
   typedef NttShape<LOGN> S;
-  const int j = threadIdx.x;
-  if (S::PARTIAL) {
-    inv_round4<LOGN, NP>(x, j, rc);
-    exchange<LOGN, NP>(
-        x, sm, j, [](int jj, int r) { return pos_partial(jj, r); },
-        [](int jj, int r) { return pos_full<LOGN>(S::FULL - 1, jj, r); }, S::FULL == 1);
+  const int j = tid_opaque();
+  // The first exchange below is warp-local, but the previous user of sm may
+  // have read it across warps (a transform's last exchange): full barrier.
+  __syncthreads();
+  if constexpr (S::PARTIAL) {
+    inv_round4<LOGN>(x, j, rc);
+    xchg<LOGN, 3, 2>(x, sm, j);
   }
-#pragma unroll
-  for (int k = S::FULL - 1; k >= 0; k--) {
-    const int t = S::N >> (3 * k + 3);
-    inv_round8<NP>(x, 1 << (3 * k), j / t, rc);
-    if (k > 0) {
-      exchange<LOGN, NP>(
-          x, sm, j, [k](int jj, int r) { return pos_full<LOGN>(k, jj, r); },
-          [k](int jj, int r) { return pos_full<LOGN>(k - 1, jj, r); }, k == 1);
-    }
+#pragma unroll 1
+  for (int k = 2; k >= 0; k--) {
+    inv_round8<LOGN>(x, k, j, rc);
+    if (k == 2) xchg<LOGN, 2, 1>(x, sm, j);
+    else if (k == 1) xchg<LOGN, 1, 0>(x, sm, j);
   }
 }
 
@@ -332,10 +367,14 @@ __device__ __forceinline__ u64 reduce4(u64 v, u64 q) {  // [0,4q) -> [0,q)
   return v;
 }
 __device__ __forceinline__ u64 reduce2(u64 v, u64 q) { return v >= q ? v - q : v; }
+// any 64-bit v -> [0, q)
+__device__ __forceinline__ u64 reduce_any(u64 v, const RingConsts &rc) {
+  return reduce2(shoup_mul(v, 1, rc.one_s, rc.q), rc.q);
+}
 
 // 16-byte read-only load that does not allocate in L1 (keys stream through L2).
 __device__ __forceinline__ void ld_key2(const u64 *p, u64 &a, u64 &b) {
-  asm("ld.global.nc.L1::no_allocate.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
 }
 
 // Load one device-layout key row into the evaluation layout registers.

@@ -8,13 +8,23 @@
 //   rlwe_auto     batched RLWE automorphism (runtime.rs:530-643)
 //   ks            gate prelude (evaluator.rs:2118-2133) + mod-down Q -> q_ks
 //                 (pbs.rs:128-132) + LWE key switch (lwe.rs:14-44), batched
-//   pbs           one CTA per ciphertext: odd mod-switch, dlog buckets, test
-//                 vector rotation, the whole blind rotation with the RLWE
-//                 accumulator resident on chip, sample extraction
-//                 (pbs.rs:146-449)
+//   pbs           one CTA per ciphertext: odd mod-switch, dlog buckets, the
+//                 blind-rotation schedule, test vector rotation, the whole
+//                 blind rotation with the RLWE accumulator in registers,
+//                 sample extraction (pbs.rs:146-449)
 #include "pz_kernels.cuh"
 
 namespace pz {
+
+// Shared memory of the bootstrap operations: region 0 (N words) is the NTT
+// exchange buffer and the permuted a(X^k) of an automorphism; region 1 (N
+// words) holds the permuted b(X^k) until the automorphism's final addition.
+constexpr int OP_REGIONS = 2;
+
+// Operation codes of the blind-rotation schedule: an external product with
+// RGSW key `i` is `i`; an automorphism with key slot v (0 = -g) is
+// OP_AUTO | v, plus OP_TRIVIAL while the accumulator is still trivial.
+constexpr u32 OP_AUTO = 0x8000u, OP_TRIVIAL = 0x4000u, OP_SLOT = 0x00ffu;
 
 // ---------------------------------------------------------------------------
 // Key conversion and NTT microbench
@@ -27,15 +37,14 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
   const int j = threadIdx.x;
   for (size_t pidx = blockIdx.x; pidx < npolys; pidx += gridDim.x) {
     const u64 *src = in + pidx * N;
-    u64 x[1][8];
+    u64 x[8];
 #pragma unroll
-    for (int r = 0; r < 8; r++) x[0][r] = src[pos_coef<LOGN>(j, r)];
-    ntt_forward<LOGN, 1>(x, sm, rc);
+    for (int r = 0; r < 8; r++) x[r] = src[pos_coef<LOGN>(j, r)];
+    ntt_fwd<LOGN>(x, sm, rc);
     u64 *dst = out + pidx * N;
 #pragma unroll
     for (int r = 0; r < 8; r++) {
-      u64 v = reduce4(x[0][r], rc.q);
-      v = reduce2(shoup_mul(v, c, cs, rc.q), rc.q);
+      const u64 v = reduce2(shoup_mul(x[r], c, cs, rc.q), rc.q);  // Shoup accepts any 64-bit input
       dst[dev_index<LOGN>(j, r)] = v;
     }
     __syncthreads();
@@ -50,12 +59,12 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
   const int j = threadIdx.x;
   for (size_t pidx = blockIdx.x; pidx < count; pidx += gridDim.x) {
     u64 *p = polys + pidx * N;
-    u64 x[1][8];
+    u64 x[8];
 #pragma unroll
-    for (int r = 0; r < 8; r++) x[0][r] = p[pos_coef<LOGN>(j, r)];
-    ntt_forward<LOGN, 1>(x, sm, rc);
+    for (int r = 0; r < 8; r++) x[r] = p[pos_coef<LOGN>(j, r)];
+    ntt_fwd<LOGN>(x, sm, rc);
 #pragma unroll
-    for (int r = 0; r < 8; r++) p[pos_eval<LOGN>(j, r)] = reduce4(x[0][r], rc.q);
+    for (int r = 0; r < 8; r++) p[pos_eval<LOGN>(j, r)] = reduce_any(x[r], rc);
     __syncthreads();
   }
 }
@@ -68,241 +77,204 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
   const int j = threadIdx.x;
   for (size_t pidx = blockIdx.x; pidx < count; pidx += gridDim.x) {
     u64 *p = polys + pidx * N;
-    u64 x[1][8];
+    u64 x[8];
 #pragma unroll
-    for (int r = 0; r < 8; r++) x[0][r] = p[pos_eval<LOGN>(j, r)];
-    ntt_inverse<LOGN, 1>(x, sm, rc);
+    for (int r = 0; r < 8; r++) x[r] = p[pos_eval<LOGN>(j, r)];
+    ntt_inv<LOGN>(x, sm, rc);
 #pragma unroll
     for (int r = 0; r < 8; r++)
-      p[pos_coef<LOGN>(j, r)] = reduce2(shoup_mul(x[0][r], rc.n_inv, rc.n_inv_s, rc.q), rc.q);
+      p[pos_coef<LOGN>(j, r)] = reduce2(shoup_mul(x[r], rc.n_inv, rc.n_inv_s, rc.q), rc.q);
     __syncthreads();
   }
 }
 
 // ---------------------------------------------------------------------------
-// RLWE x RGSW (runtime.rs:754-855).  acc: coefficient layout, canonical.
-// sm: 3N words.  Device RGSW rows: A(-sm) x d_a, B(-sm) x d_a, A(m) x d_b,
-// B(m) x d_b (runtime.rs:174-180).
+// One blind-rotation operation on the accumulator acc = (a, b) (coefficient
+// layout, canonical [0, Q)):
+//   op = RGSW index i:  acc <- acc x RGSW_i        (rlwe_by_rgsw_shoup, runtime.rs:754-855)
+//   op = OP_AUTO | v:   acc <- auto_{k_v}(acc)      (rlwe_auto_shoup, runtime.rs:530-643)
+// Both share one copy of the forward and of the inverse NTT: the transforms
+// run in a loop over the polynomials that swaps the two register arrays.
+// The first (trivial) external product of a blind rotation runs the general
+// code with a = 0: the a-digits are 0, their products vanish and, since every
+// result is reduced to the canonical residue, the words equal those of the
+// reference's trivial branch.  Device RGSW rows: A(-sm) x d_a, B(-sm) x d_a,
+// A(m) x d_b, B(m) x d_b (runtime.rs:174-180); auto key rows A x d, B x d.
 // ---------------------------------------------------------------------------
-template <int LOGN, bool D1>
-__device__ __forceinline__ void ext_product(u64 (&acc)[2][8], const u64 *ct, bool trivial,
-                                            const BrParams &P, u64 *sm) {
-  constexpr int N = 1 << LOGN;
-  const u64 q = P.rc.q, qi = P.rc.qinv_neg;
-  if (D1) {
-    if (!trivial) {
+__device__ __forceinline__ void swap8(u64 (&x)[8], u64 (&y)[8]) {
 #pragma unroll
-      for (int r = 0; r < 8; r++) {
-        u64 sa = decomp_init(acc[0][r], P.da);
-        acc[0][r] = decomp_next(sa, P.da);
-        u64 sb = decomp_init(acc[1][r], P.db);
-        acc[1][r] = decomp_next(sb, P.db);
-      }
-      ntt_forward<LOGN, 2>(acc, sm, P.rc);
-      const u64 *K0 = ct, *K1 = ct + N, *K2 = ct + 2 * N, *K3 = ct + 3 * N;
-      const int j = threadIdx.x;
+  for (int r = 0; r < 8; r++) {
+    const u64 t = x[r];
+    x[r] = y[r];
+    y[r] = t;
+  }
+}
+
+// x <- x (pointwise, Montgomery) from two device-layout key rows, y likewise.
+template <int LOGN>
+__device__ __forceinline__ void mac_pair(u64 (&x)[8], u64 (&y)[8], const u64 *ka, const u64 *kb,
+                                         const u64 *kc, const u64 *kd, bool two, const RingConsts &rc) {
+  // x' = x ka + y kc, y' = x kb + y kd   (two == false: x' = x ka, y' = x kb)
+  const int j = threadIdx.x;
+  const u64 q = rc.q, qi = rc.qinv_neg;
 #pragma unroll
-      for (int rr = 0; rr < 4; rr++) {
-        u64 k0[2], k1[2], k2[2], k3[2];
-        const int di = dev_index<LOGN>(j, 2 * rr);
-        ld_key2(K0 + di, k0[0], k0[1]);
-        ld_key2(K1 + di, k1[0], k1[1]);
-        ld_key2(K2 + di, k2[0], k2[1]);
-        ld_key2(K3 + di, k3[0], k3[1]);
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int r = 2 * rr + e;
-          const u64 xa = acc[0][r], xb = acc[1][r];
-          u64 hi, lo;
-          mul128(xa, k0[e], hi, lo);
-          mac128(xb, k2[e], hi, lo);
-          const u64 oa = redc(hi, lo, q, qi);
-          mul128(xa, k1[e], hi, lo);
-          mac128(xb, k3[e], hi, lo);
-          const u64 ob = redc(hi, lo, q, qi);
-          acc[0][r] = oa;
-          acc[1][r] = ob;
-        }
-      }
-    } else {
-      // a = 0: only decomp<b> x RLWE'(m) contributes (runtime.rs:790-818 skipped)
-      u64 x[1][8];
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        u64 sb = decomp_init(acc[1][r], P.db);
-        x[0][r] = decomp_next(sb, P.db);
-      }
-      ntt_forward<LOGN, 1>(x, sm, P.rc);
-      const u64 *K2 = ct + 2 * N, *K3 = ct + 3 * N;
-      const int j = threadIdx.x;
-#pragma unroll
-      for (int rr = 0; rr < 4; rr++) {
-        u64 k2[2], k3[2];
-        const int di = dev_index<LOGN>(j, 2 * rr);
-        ld_key2(K2 + di, k2[0], k2[1]);
-        ld_key2(K3 + di, k3[0], k3[1]);
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-          const int r = 2 * rr + e;
-          u64 hi, lo;
-          mul128(x[0][r], k2[e], hi, lo);
-          acc[0][r] = redc(hi, lo, q, qi);
-          mul128(x[0][r], k3[e], hi, lo);
-          acc[1][r] = redc(hi, lo, q, qi);
-        }
-      }
+  for (int rr = 0; rr < 4; rr++) {
+    const int di = dev_index<LOGN>(j, 2 * rr);
+    u64 a[2], b[2], c[2] = {0, 0}, d[2] = {0, 0};
+    ld_key2(ka + di, a[0], a[1]);
+    ld_key2(kb + di, b[0], b[1]);
+    if (two) {
+      ld_key2(kc + di, c[0], c[1]);
+      ld_key2(kd + di, d[0], d[1]);
     }
-    ntt_inverse<LOGN, 2>(acc, sm, P.rc);
 #pragma unroll
-    for (int r = 0; r < 8; r++) {
-      acc[0][r] = reduce2(acc[0][r], q);
-      acc[1][r] = reduce2(acc[1][r], q);
-    }
-  } else {
-    // general decomposition counts (SP_TEST: d_a = d_b = 4)
-    const u32 da = P.d_a, db = P.d_b;
-    const u32 dmax = da > db ? da : db;
-    u64 sa[8], sb[8], o[2][8];
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-      sa[r] = trivial ? 0 : decomp_init(acc[0][r], P.da);
-      sb[r] = decomp_init(acc[1][r], P.db);
-      o[0][r] = 0;
-      o[1][r] = 0;
-    }
-    for (u32 jd = 0; jd < dmax; jd++) {
-      const bool ha = !trivial && jd < da, hb = jd < db;
-      u64 x[2][8];
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        x[0][r] = ha ? decomp_next(sa[r], P.da) : 0;
-        x[1][r] = hb ? decomp_next(sb[r], P.db) : 0;
+    for (int e = 0; e < 2; e++) {
+      const int r = 2 * rr + e;
+      const u64 xv = x[r], yv = y[r];
+      u64 hi, lo, hi2, lo2;
+      mul128(xv, a[e], hi, lo);
+      mul128(xv, b[e], hi2, lo2);
+      if (two) {
+        mac128(yv, c[e], hi, lo);
+        mac128(yv, d[e], hi2, lo2);
       }
-      ntt_forward<LOGN, 2>(x, sm, P.rc);
-      u64 kaa[8], kba[8], kam[8], kbm[8];
-      if (ha) {
-        load_key_row<LOGN>(ct + (size_t)jd * N, kaa);
-        load_key_row<LOGN>(ct + (size_t)(da + jd) * N, kba);
-      }
-      if (hb) {
-        load_key_row<LOGN>(ct + (size_t)(2 * da + jd) * N, kam);
-        load_key_row<LOGN>(ct + (size_t)(2 * da + db + jd) * N, kbm);
-      }
-#pragma unroll
-      for (int r = 0; r < 8; r++) {
-        u64 hi = 0, lo = 0, hi2 = 0, lo2 = 0;
-        if (ha) { mac128(x[0][r], kaa[r], hi, lo); mac128(x[0][r], kba[r], hi2, lo2); }
-        if (hb) { mac128(x[1][r], kam[r], hi, lo); mac128(x[1][r], kbm[r], hi2, lo2); }
-        u64 va = o[0][r] + redc(hi, lo, q, qi), vb = o[1][r] + redc(hi2, lo2, q, qi);
-        o[0][r] = va >= 2 * q ? va - 2 * q : va;
-        o[1][r] = vb >= 2 * q ? vb - 2 * q : vb;
-      }
-    }
-    ntt_inverse<LOGN, 2>(o, sm, P.rc);
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-      acc[0][r] = reduce2(o[0][r], q);
-      acc[1][r] = reduce2(o[1][r], q);
+      x[r] = redc(hi, lo, q, qi);
+      y[r] = redc(hi2, lo2, q, qi);
     }
   }
 }
 
-// ---------------------------------------------------------------------------
-// RLWE automorphism (runtime.rs:530-643).  Slot 0 is -g, slot v is g^v.
-// ---------------------------------------------------------------------------
-template <int LOGN, bool D1>
-__device__ __forceinline__ void rlwe_auto(u64 (&acc)[2][8], int slot, bool trivial, const BrParams &P,
-                                          u64 *sm) {
-  constexpr int N = 1 << LOGN;
-  const u64 q = P.rc.q, qi = P.rc.qinv_neg;
-  const u32 k = P.auto_k[slot];
-  const int j = threadIdx.x;
-  u64 *s_a = sm, *s_b = sm + 2 * N;
-  __syncthreads();
-  // a(X) -> a(X^k), b(X) -> b(X^k) with sign (generate_auto_map, keygen.rs:16-41)
+// Lazy accumulation for the general decomposition path: o += REDC(...) in [0, 2q).
+template <int LOGN>
+__device__ __forceinline__ void mac_accum(u64 (&oa)[8], u64 (&ob)[8], const u64 (&x)[8], const u64 (&y)[8],
+                                          const u64 *ka, const u64 *kb, const u64 *kc, const u64 *kd, bool hx,
+                                          bool hy, const RingConsts &rc) {
+  const u64 q = rc.q, qi = rc.qinv_neg;
+  u64 a[8], b[8], c[8], d[8];
+  if (hx) { load_key_row<LOGN>(ka, a); load_key_row<LOGN>(kb, b); }
+  if (hy) { load_key_row<LOGN>(kc, c); load_key_row<LOGN>(kd, d); }
 #pragma unroll
   for (int r = 0; r < 8; r++) {
-    const u32 i = (u32)pos_coef<LOGN>(j, r);
-    u32 t = (i * k) & (2 * N - 1);
-    const bool neg = t >= (u32)N;
-    if (neg) t -= N;
-    if (!trivial) s_a[swz(t)] = neg ? q - acc[0][r] : acc[0][r];
-    s_b[swz(t)] = neg ? q - acc[1][r] : acc[1][r];
+    u64 hi = 0, lo = 0, hi2 = 0, lo2 = 0;
+    if (hx) { mac128(x[r], a[r], hi, lo); mac128(x[r], b[r], hi2, lo2); }
+    if (hy) { mac128(y[r], c[r], hi, lo); mac128(y[r], d[r], hi2, lo2); }
+    const u64 va = oa[r] + redc(hi, lo, q, qi), vb = ob[r] + redc(hi2, lo2, q, qi);
+    oa[r] = va >= 2 * q ? va - 2 * q : va;
+    ob[r] = vb >= 2 * q ? vb - 2 * q : vb;
   }
-  __syncthreads();
-  if (trivial) {
+}
+
+template <int LOGN, bool D1>
+__device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrParams &P, u64 *sm) {
+  constexpr int N = 1 << LOGN;
+  const u64 q = P.rc.q;
+  const int j = threadIdx.x;
+  u64(&x)[8] = acc[0];
+  u64(&y)[8] = acc[1];
+  const bool is_auto = (op & OP_AUTO) != 0;
+  u64 *s_a = sm, *s_b = sm + N;
+  if (is_auto) {
+    // a(X) -> a(X^k), b(X) -> b(X^k) with sign (generate_auto_map, keygen.rs:16-41)
+    const u32 k = P.auto_k[op & OP_SLOT];
+    const bool trivial = (op & OP_TRIVIAL) != 0;
+    __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 8; r++) acc[1][r] = s_b[swz(pos_coef<LOGN>(j, r))];
-    return;
+    for (int r = 0; r < 8; r++) {
+      const u32 i = (u32)pos_coef<LOGN>(j, r);
+      u32 t = (i * k) & (2 * N - 1);
+      const bool neg = t >= (u32)N;
+      if (neg) t -= N;
+      if (!trivial) s_a[swz(t)] = neg ? q - x[r] : x[r];
+      s_b[swz(t)] = neg ? q - y[r] : y[r];
+    }
+    __syncthreads();
+    if (trivial) {  // runtime.rs:625-642: only b is permuted (neg(0) = q kept)
+#pragma unroll
+      for (int r = 0; r < 8; r++) y[r] = s_b[swz(pos_coef<LOGN>(j, r))];
+      return;
+    }
   }
-  const u64 *KA = P.autos + (size_t)slot * P.auto_rows * N;
+  const u64 *K = is_auto ? P.autos + (size_t)(op & OP_SLOT) * P.auto_rows * N
+                         : P.rgsw + (size_t)op * P.rgsw_rows * N;
   if (D1) {
-    u64 x[1][8];
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-      u64 st = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
-      x[0][r] = decomp_next(st, P.dauto);
-    }
-    ntt_forward<LOGN, 1>(x, sm, P.rc);
-    const u64 *K0 = KA, *K1 = KA + N;
-#pragma unroll
-    for (int rr = 0; rr < 4; rr++) {
-      u64 k0[2], k1[2];
-      const int di = dev_index<LOGN>(j, 2 * rr);
-      ld_key2(K0 + di, k0[0], k0[1]);
-      ld_key2(K1 + di, k1[0], k1[1]);
-#pragma unroll
-      for (int e = 0; e < 2; e++) {
-        const int r = 2 * rr + e;
-        u64 hi, lo;
-        mul128(x[0][r], k0[e], hi, lo);
-        acc[0][r] = redc(hi, lo, q, qi);
-        mul128(x[0][r], k1[e], hi, lo);
-        acc[1][r] = redc(hi, lo, q, qi);
-      }
-    }
-    ntt_inverse<LOGN, 2>(acc, sm, P.rc);
-  } else {
-    const u32 d = P.d_auto;
-    u64 st[8], o[2][8];
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-      st[r] = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
-      o[0][r] = 0;
-      o[1][r] = 0;
-    }
-    for (u32 jd = 0; jd < d; jd++) {
-      u64 x[1][8];
-#pragma unroll
-      for (int r = 0; r < 8; r++) x[0][r] = decomp_next(st[r], P.dauto);
-      ntt_forward<LOGN, 1>(x, sm, P.rc);
-      u64 ka[8], kb[8];
-      load_key_row<LOGN>(KA + (size_t)jd * N, ka);
-      load_key_row<LOGN>(KA + (size_t)(d + jd) * N, kb);
+    if (is_auto) {
 #pragma unroll
       for (int r = 0; r < 8; r++) {
-        u64 hi, lo;
-        mul128(x[0][r], ka[r], hi, lo);
-        u64 va = o[0][r] + redc(hi, lo, q, qi);
-        mul128(x[0][r], kb[r], hi, lo);
-        u64 vb = o[1][r] + redc(hi, lo, q, qi);
-        o[0][r] = va >= 2 * q ? va - 2 * q : va;
-        o[1][r] = vb >= 2 * q ? vb - 2 * q : vb;
+        u64 st = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
+        x[r] = decomp_next(st, P.dauto);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        u64 sa = decomp_init(x[r], P.da);
+        x[r] = decomp_next(sa, P.da);
+        u64 sb = decomp_init(y[r], P.db);
+        y[r] = decomp_next(sb, P.db);
+      }
+    }
+    const int np = is_auto ? 1 : 2;
+#pragma unroll 1
+    for (int p = 0; p < np; p++) {
+      ntt_fwd<LOGN>(x, sm, P.rc);
+      swap8(x, y);
+    }
+    if (np == 1) swap8(x, y);
+    if (is_auto) mac_pair<LOGN>(x, y, K, K + N, nullptr, nullptr, false, P.rc);
+    else mac_pair<LOGN>(x, y, K, K + N, K + 2 * N, K + 3 * N, true, P.rc);
+  } else {
+    // general decomposition counts (SP_TEST: d = 4): digit by digit, lazily
+    // accumulated in [0, 2q), one inverse transform at the end
+    const u32 da = is_auto ? P.d_auto : P.d_a, db = is_auto ? 0 : P.d_b;
+    const Decomp &dpa = is_auto ? P.dauto : P.da;
+    u64 sa[8], sb[8], oa[8], ob[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      sa[r] = decomp_init(is_auto ? s_a[swz(pos_coef<LOGN>(j, r))] : x[r], dpa);
+      sb[r] = is_auto ? 0 : decomp_init(y[r], P.db);
+      oa[r] = 0;
+      ob[r] = 0;
+    }
+    const u32 dmax = da > db ? da : db;
+    for (u32 jd = 0; jd < dmax; jd++) {
+      const bool hx = jd < da, hy = jd < db;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        x[r] = hx ? decomp_next(sa[r], dpa) : 0;
+        y[r] = hy ? decomp_next(sb[r], P.db) : 0;
+      }
+      const int np = hy ? 2 : 1;
+#pragma unroll 1
+      for (int p = 0; p < np; p++) {
+        ntt_fwd<LOGN>(x, sm, P.rc);
+        swap8(x, y);
+      }
+      if (np == 1) swap8(x, y);
+      if (is_auto) {
+        mac_accum<LOGN>(oa, ob, x, y, K + (size_t)jd * N, K + (size_t)(da + jd) * N, nullptr, nullptr, hx,
+                        false, P.rc);
+      } else {
+        mac_accum<LOGN>(oa, ob, x, y, K + (size_t)jd * N, K + (size_t)(da + jd) * N,
+                        K + (size_t)(2 * da + jd) * N, K + (size_t)(2 * da + db + jd) * N, hx, hy, P.rc);
       }
     }
 #pragma unroll
     for (int r = 0; r < 8; r++) {
-      acc[0][r] = o[0][r];
-      acc[1][r] = o[1][r];
+      x[r] = oa[r];
+      y[r] = ob[r];
     }
-    ntt_inverse<LOGN, 2>(acc, sm, P.rc);
   }
-  // b' += b(X^k) with sign: add_mod of the signed value == sub_mod_fast /
-  // add_mod_fast of runtime.rs:608-620 (the signed value is q - b or b).
+#pragma unroll 1
+  for (int p = 0; p < 2; p++) {
+    ntt_inv<LOGN>(x, sm, P.rc);
+    swap8(x, y);
+  }
 #pragma unroll
   for (int r = 0; r < 8; r++) {
-    acc[0][r] = reduce2(acc[0][r], q);
-    acc[1][r] = add_mod(reduce2(acc[1][r], q), s_b[swz(pos_coef<LOGN>(j, r))], q);
+    x[r] = reduce2(x[r], q);
+    y[r] = reduce2(y[r], q);
+    // b' += b(X^k) with sign: add_mod of the signed value == sub_mod_fast /
+    // add_mod_fast of runtime.rs:608-620 (the signed value is q - b or b)
+    if (is_auto) y[r] = add_mod(y[r], s_b[swz(pos_coef<LOGN>(j, r))], q);
   }
 }
 
@@ -317,10 +289,10 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
     u64 acc[2][8];
 #pragma unroll
     for (int r = 0; r < 8; r++) {
-      acc[0][r] = p[pos_coef<LOGN>(j, r)];
+      acc[0][r] = trivial ? 0 : p[pos_coef<LOGN>(j, r)];  // trivial: a = 0 (runtime.rs:790)
       acc[1][r] = p[N + pos_coef<LOGN>(j, r)];
     }
-    ext_product<LOGN, D1>(acc, P.rgsw + (size_t)idx[c] * P.rgsw_rows * N, trivial != 0, P, smem);
+    bootstrap_op<LOGN, D1>(acc, idx[c], P, smem);
 #pragma unroll
     for (int r = 0; r < 8; r++) {
       p[pos_coef<LOGN>(j, r)] = acc[0][r];
@@ -344,7 +316,7 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
       acc[0][r] = p[pos_coef<LOGN>(j, r)];
       acc[1][r] = p[N + pos_coef<LOGN>(j, r)];
     }
-    rlwe_auto<LOGN, D1>(acc, (int)slot[c], trivial != 0, P, smem);
+    bootstrap_op<LOGN, D1>(acc, OP_AUTO | (trivial ? OP_TRIVIAL : 0u) | (slot[c] & OP_SLOT), P, smem);
 #pragma unroll
     for (int r = 0; r < 8; r++) {
       p[pos_coef<LOGN>(j, r)] = acc[0][r];
@@ -452,33 +424,40 @@ __device__ __forceinline__ u32 mod_switch_odd(u32 v, double from_q, double to_q)
   return (u32)(odd + ((odd & 1ull) ^ 1ull));
 }
 
+// Shared memory of pbs_kernel: OP_REGIONS x N words, then u16 arrays:
+// bucket starts (R + 1), bucket members (n), the schedule (n + R + 1), and
+// the schedule length.
 size_t pbs_smem_bytes(int logn, u32 br_q, u32 n) {
-  size_t N = (size_t)1 << logn;
-  size_t extra = ((size_t)(br_q / 2 + 1) + n) * 2;
+  const size_t N = (size_t)1 << logn, R = br_q / 2;
+  size_t extra = ((R + 1) + n + (n + R + 1)) * 2 + 4;
   extra = (extra + 15) & ~(size_t)15;
-  return 3 * N * 8 + extra;
+  return OP_REGIONS * N * 8 + extra;
 }
 
-template <int LOGN, bool D1>
-__global__ void __launch_bounds__(NttShape<LOGN>::T)
+// MINB: CTAs per SM the register allocation must allow (launch-shape
+// variants chosen at run time, see pz_ctx_set_pbs_variant).
+template <int LOGN, bool D1, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
     pbs_kernel(BrParams P, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out, int count,
                u64 *rlwe_dbg) {
   constexpr int N = 1 << LOGN, T = NttShape<LOGN>::T;
   extern __shared__ u64 smem[];
   u64 *sm = smem;
   const u32 R = P.br_q >> 1, q4 = P.br_q >> 2, n = P.n;
-  unsigned short *s_start = (unsigned short *)(smem + 3 * N);  // R + 1 entries
-  unsigned short *s_list = s_start + (R + 1);                  // n entries
+  unsigned short *s_start = (unsigned short *)(smem + OP_REGIONS * N);  // R + 1
+  unsigned short *s_list = s_start + (R + 1);                           // n
+  unsigned short *s_ops = s_list + n;                                   // n + R + 1
+  u32 *s_nops = (u32 *)(((size_t)(s_ops + n + R + 1) + 3) & ~(size_t)3);
   const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
   const u64 q = P.rc.q;
 
   for (int ct = blockIdx.x; ct < count; ct += gridDim.x) {
     const u32 *kso = ks + (size_t)ct * ks_stride;
     // ---- odd mod-switch + dlog buckets (pbs.rs:147-161), stable in LWE index
-    u32 *cnt = (u32 *)sm;                             // R counters (region 0)
-    unsigned short *keys = (unsigned short *)(sm + N);  // n keys (region 1)
-    u32 *scan = (u32 *)(sm + N) + 512;                // T partial sums (region 1, after keys)
-    u32 *fill = (u32 *)(sm + 2 * N);                  // R fill counters (region 2)
+    u32 *cnt = (u32 *)sm;                                 // R counters (region 0)
+    unsigned short *keys = (unsigned short *)(cnt + R);   // n keys (region 0)
+    u32 *fill = (u32 *)(sm + N);                          // R fill counters (region 1)
+    u32 *scan = fill + R;                                 // T partial sums (region 1)
     __syncthreads();
     for (u32 b = j; b < R; b += T) { cnt[b] = 0; fill[b] = 0; }
     __syncthreads();
@@ -526,6 +505,42 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
       }
     }
     __syncthreads();
+    // ---- the blind-rotation schedule (pbs.rs:240-414): buckets of -g^k for
+    // k = q/4-1..1, -g^0, +g^k, +g^0, each followed by an automorphism when
+    // the next bucket is non-empty, the window w is reached or k == 1; the
+    // automorphisms before the first external product act on a trivial RLWE.
+    if (j == 0) {
+      u32 no = 0;
+      bool trivial = true;
+      auto bucket = [&](u32 b) {
+        const u32 e = s_start[b + 1];
+        for (u32 t = s_start[b]; t < e; t++) s_ops[no++] = s_list[t];
+        if (e != s_start[b]) trivial = false;
+      };
+      auto autom = [&](u32 v) { s_ops[no++] = (unsigned short)(OP_AUTO | (trivial ? OP_TRIVIAL : 0u) | v); };
+      u32 v = 0;
+      for (u32 i = q4 - 1; i >= 1; i--) {  // -(g^k)
+        bucket(q4 + i);
+        v++;
+        if (s_start[q4 + i] != s_start[q4 + i - 1] || v == P.w || i == 1) {
+          autom(v);
+          v = 0;
+        }
+      }
+      bucket(q4);  // -(g^0)
+      autom(0);
+      v = 0;
+      for (u32 i = q4 - 1; i >= 1; i--) {  // +(g^k)
+        bucket(i);
+        v++;
+        if (s_start[i] != s_start[i - 1] || v == P.w || i == 1) {
+          autom(v);
+          v = 0;
+        }
+      }
+      bucket(0);  // +(g^0)
+      *s_nops = no;
+    }
 
     // ---- trivial test RLWE: X^{g * odd(b)} * tv, embedded (pbs.rs:163-211)
     const u32 odd_b = mod_switch_odd(kso[0], P.q_ks_f, P.br_q_f);
@@ -552,39 +567,12 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
       }
       acc[1][r] = v;
     }
+    __syncthreads();
 
-    // ---- blind rotation (pbs.rs:240-414)
-    bool trivial = true;
-    const u64 *rgsw = P.rgsw;
-    const size_t ct_words = (size_t)P.rgsw_rows * N;
-    auto bucket = [&](u32 b) {
-      const u32 e = s_start[b + 1];
-      for (u32 t = s_start[b]; t < e; t++) {
-        ext_product<LOGN, D1>(acc, rgsw + (size_t)s_list[t] * ct_words, trivial, P, sm);
-        trivial = false;
-      }
-    };
-    u32 v = 0;
-    for (u32 i = q4 - 1; i >= 1; i--) {  // -(g^k)
-      bucket(q4 + i);
-      v++;
-      if (s_start[q4 + i] != s_start[q4 + i - 1] || v == P.w || i == 1) {
-        rlwe_auto<LOGN, D1>(acc, (int)v, trivial, P, sm);
-        v = 0;
-      }
-    }
-    bucket(q4);  // -(g^0)
-    rlwe_auto<LOGN, D1>(acc, 0, trivial, P, sm);
-    v = 0;
-    for (u32 i = q4 - 1; i >= 1; i--) {  // +(g^k)
-      bucket(i);
-      v++;
-      if (s_start[i] != s_start[i - 1] || v == P.w || i == 1) {
-        rlwe_auto<LOGN, D1>(acc, (int)v, trivial, P, sm);
-        v = 0;
-      }
-    }
-    bucket(0);  // +(g^0)
+    // ---- blind rotation: one operation per schedule entry
+    const u32 nops = *s_nops;
+#pragma unroll 1
+    for (u32 t = 0; t < nops; t++) bootstrap_op<LOGN, D1>(acc, s_ops[t], P, sm);
 
     // ---- sample extract at index 0 (pbs.rs:423-449)
     u64 *o = out + (size_t)(P.out_idx ? P.out_idx[ct] : (u32)ct) * (N + 1);
@@ -684,7 +672,7 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
                                size_t count, int trivial, cudaStream_t s) {
   if (count == 0) return cudaSuccess;
-  const size_t N = (size_t)1 << logn, smem = 3 * N * 8;
+  const size_t N = (size_t)1 << logn, smem = OP_REGIONS * N * 8;
   cudaError_t e;
 #define PZ_LAUNCH(LN, DD, TH)                                                                  \
   if ((e = set_smem(ext_product_kernel<LN, DD>, smem)) != cudaSuccess) return e;              \
@@ -701,7 +689,7 @@ cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, 
 cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *slot, size_t count,
                         int trivial, cudaStream_t s) {
   if (count == 0) return cudaSuccess;
-  const size_t N = (size_t)1 << logn, smem = 3 * N * 8;
+  const size_t N = (size_t)1 << logn, smem = OP_REGIONS * N * 8;
   cudaError_t e;
 #define PZ_LAUNCH(LN, DD, TH)                                                           \
   if ((e = set_smem(auto_kernel<LN, DD>, smem)) != cudaSuccess) return e;              \
@@ -726,19 +714,23 @@ cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *
 
 cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
                        const unsigned char *gates, u64 *out, size_t count, u64 *rlwe_dbg, int grid_limit,
-                       cudaStream_t s) {
+                       cudaStream_t s, int variant) {
   if (count == 0) return cudaSuccess;
   const size_t smem = pbs_smem_bytes(logn, P.br_q, P.n);
   int grid = (int)count;
   if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
   cudaError_t e;
-#define PZ_LAUNCH(LN, DD, TH)                                                                        \
-  if ((e = set_smem(pbs_kernel<LN, DD>, smem)) != cudaSuccess) return e;                            \
-  pbs_kernel<LN, DD><<<grid, TH, smem, s>>>(P, ks, ks_stride, gates, out, (int)count, rlwe_dbg);
-  if (logn == 11 && d1) { PZ_LAUNCH(11, true, 256) }
-  else if (logn == 11) { PZ_LAUNCH(11, false, 256) }
-  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 64) }
-  else if (logn == 9) { PZ_LAUNCH(9, false, 64) }
+#define PZ_LAUNCH(LN, DD, MB, TH)                                                                    \
+  if ((e = set_smem(pbs_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;                        \
+  pbs_kernel<LN, DD, MB><<<grid, TH, smem, s>>>(P, ks, ks_stride, gates, out, (int)count, rlwe_dbg);
+  if (logn == 11 && d1) {
+    if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
+    else if (variant == 1) { PZ_LAUNCH(11, true, 3, 256) }
+    else { PZ_LAUNCH(11, true, 4, 256) }
+  }
+  else if (logn == 11) { PZ_LAUNCH(11, false, 1, 256) }
+  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 1, 64) }
+  else if (logn == 9) { PZ_LAUNCH(9, false, 1, 64) }
   else return cudaErrorInvalidValue;
 #undef PZ_LAUNCH
   return cudaGetLastError();

@@ -59,7 +59,10 @@ cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *
                       size_t count, u32 *out, cudaStream_t s);
 cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
                        const unsigned char *gates, u64 *out, size_t count, u64 *rlwe_dbg,
-                       int grid_limit, cudaStream_t s);
+                       int grid_limit, cudaStream_t s, int variant);
+// launch-shape variants of the production blind rotation (registers per
+// thread capped for 2, 3 or 4 CTAs of 256 threads per SM)
+constexpr int PBS_VARIANTS = 3;
 cudaError_t launch_not(const u64 *in, u64 *out, size_t words, u64 q, cudaStream_t s);
 cudaError_t launch_imad_probe(int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s);
 // per launch: blocks * threads * iters * 16 * 8 multiply-adds

@@ -196,7 +196,8 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
   cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s);
   if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
-  e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s);
+  e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s,
+                     c->pbs_variant);
   if (e != cudaSuccess) return cuda_fail(c, "launch_pbs", e);
   return PZ_OK;
 }
@@ -244,21 +245,20 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   c->root = root;
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) { delete c; return PZ_ERR_CUDA; }
-  // twiddles: psi^{bitrev(i)} and psi^{-bitrev(i)} (ntt.rs:337-369)
+  // twiddles: psi^{bitrev(i)} and psi^{-bitrev(i)} (ntt.rs:337-369), each
+  // interleaved with its Shoup companion: [w_0, ws_0, w_1, ws_1, ...]
   std::vector<u64> tw(4 * N);
   const u64 rinv = invmod(root, Q);
   u64 pw = 1, pwi = 1;
   for (u64 i = 0; i < N; i++) {
     u64 bo = 0;
     for (u32 b = 0; b < c->logn; b++) bo |= ((i >> b) & 1) << (c->logn - 1 - b);
-    tw[bo] = pw;
-    tw[2 * N + bo] = pwi;
+    tw[2 * bo] = pw;
+    tw[2 * bo + 1] = shoup(pw, Q);
+    tw[2 * N + 2 * bo] = pwi;
+    tw[2 * N + 2 * bo + 1] = shoup(pwi, Q);
     pw = mulmod(pw, root, Q);
     pwi = mulmod(pwi, rinv, Q);
-  }
-  for (u64 i = 0; i < N; i++) {
-    tw[N + i] = shoup(tw[i], Q);
-    tw[3 * N + i] = shoup(tw[2 * N + i], Q);
   }
   std::vector<unsigned short> dlog;
   std::vector<u64> tv;
@@ -284,10 +284,9 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   rc.qinv_neg = 0 - inv;
   rc.n_inv = invmod(N, Q);
   rc.n_inv_s = shoup(rc.n_inv, Q);
+  rc.one_s = shoup(1, Q);
   rc.fw = c->d_tw;
-  rc.fws = c->d_tw + N;
   rc.iw = c->d_tw + 2 * N;
-  rc.iws = c->d_tw + 3 * N;
   const u64 r64 = (u64)(((u128)1 << 64) % Q);
   c->conv_c = mulmod(rc.n_inv, r64, Q);  // keys stored as K * N^{-1} * 2^64
   c->conv_cs = shoup(c->conv_c, Q);
@@ -344,6 +343,13 @@ pz_status pz_ctx_params(const pz_ctx *c, pz_params *out) {
   return PZ_OK;
 }
 uint64_t pz_ctx_ntt_root(const pz_ctx *c) { return c ? c->root : 0; }
+
+pz_status pz_ctx_set_pbs_variant(pz_ctx *c, int v) {
+  if (!c || v < 0 || v >= pz::PBS_VARIANTS) return PZ_ERR_INVALID_ARGUMENT;
+  c->pbs_variant = v;
+  return PZ_OK;
+}
+int pz_ctx_pbs_variant(const pz_ctx *c) { return c ? c->pbs_variant : -1; }
 
 pz_status pz_ctx_set_pbs_grid_limit(pz_ctx *c, int g) {
   if (!c || g < 0) return PZ_ERR_INVALID_ARGUMENT;
@@ -488,7 +494,7 @@ pz_status pz_blind_rotate_batch_device(pz_ctx *c, const pz_key *k, const uint32_
   br.out_idx = nullptr;
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   PZ_CK(c, pz::launch_pbs((int)c->logn, d1, br, d_ks, c->P.lwe_n + 1, d_test_vec, d_out, count, nullptr,
-                          c->grid_limit, pick(c, stream)));
+                          c->grid_limit, pick(c, stream), c->pbs_variant));
   return PZ_OK;
 }
 

@@ -115,6 +115,14 @@ class Engine:
     def set_pbs_grid_limit(self, g):
         check(lib().pz_ctx_set_pbs_grid_limit(self.h, int(g)), self.h, "set_pbs_grid_limit")
 
+    @property
+    def pbs_variant(self):
+        return lib().pz_ctx_pbs_variant(self.h)
+
+    @pbs_variant.setter
+    def pbs_variant(self, v):
+        check(lib().pz_ctx_set_pbs_variant(self.h, int(v)), self.h, "set_pbs_variant")
+
     # -- keys --------------------------------------------------------------
     def upload_key(self, rgsw, autos, lwe_ksk):
         """Upload a coefficient-domain server key (layouts of pz_server_key_view)."""

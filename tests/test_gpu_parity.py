@@ -179,3 +179,25 @@ def test_gate_batch_host_api(gpu_available, param):
     want = okey.gate_batch(gates, c0, c1, threads=4)
     assert np.array_equal(got, want)
     assert np.array_equal(ev.decrypt_bool(secrets[0], got), 1 - (bits0 & bits1))
+
+
+@pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_pbs_variants_bit_exact(gpu_available, param, variant):
+    """Every launch-shape variant of the blind rotation gives the oracle's words."""
+    O = oracle()
+    ev, secrets, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    count = 4
+    bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, count, 0x71 + variant)
+    gates = np.array([O.GATES[g] for g in ["nand", "xor", "or", "xnor"]], np.uint8)
+    old = eng.pbs_variant
+    eng.pbs_variant = variant
+    try:
+        out = to_dev(np.zeros((count, ev.L), np.uint64))
+        eng.gate_batch_device(dkey, to_dev(gates), to_dev(c0), to_dev(c1), out)
+        got = to_host(out)
+    finally:
+        eng.pbs_variant = old
+    want = okey.gate_batch(gates, c0, c1, threads=4)
+    assert np.array_equal(got, want)
