@@ -420,13 +420,11 @@ def main():
     achieved = modmuls * C_MM / (br_ms / 1e3) / 1e12  # T IMAD/s
     peak = P.probe_imad_rate(local) / 1e12
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "pbs_kernel_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "pbs_kernel_traffic_ni8p_2368.md")
     if os.path.exists(prof):
-        try:
-            tr = json.load(open(prof))
-            traffic = tr["dram_bytes_per_bootstrap"] * B
-        except (ValueError, KeyError):
-            traffic = None
+        for ln in open(prof):
+            if ln.startswith("traffic_bytes_per_bootstrap:"):
+                traffic = int(ln.split(":")[1]) * B  # ncu dram read+write, warm launch of B items
 
     plain = None
     if not args.no_plain and rank == 0:
@@ -435,9 +433,12 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, count, dt = cpu_gate_sample(p, key_arrays, threads, 4)
+        # calibrate on one gate per thread, then size the sample to ~12 s of CPU work
+        rate0, _, _ = cpu_gate_sample(p, key_arrays, threads, 1, seed=10)
+        per_thread = int(min(max(12.0 * rate0 / threads, 2), 256))
+        rate, count, dt = cpu_gate_sample(p, key_arrays, threads, per_thread)
         cpu = {"value": rate, "unit": "gate bootstraps/s", "cores": threads, "kind": "port",
-               "sample": f"{count} independent NI_8P gates ({threads} threads x 4) in {dt:.1f} s"}
+               "sample": f"{count} independent NI_8P gates ({threads} threads x {per_thread}) in {dt:.1f} s"}
 
     if rank == 0:
         launches_per_step = 2 * info["levels"] + 1

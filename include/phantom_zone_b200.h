@@ -183,7 +183,7 @@ pz_status pz_lwe_key_switch_device(pz_ctx *ctx, const pz_key *key, const uint64_
  * (the kernel then strides over the batch). */
 pz_status pz_ctx_set_pbs_grid_limit(pz_ctx *ctx, int grid_limit);
 /* Blind-rotation kernel variant for N = 2048: registers capped for 2, 3 or 4
- * resident CTAs per SM (variant 0, 1, 2); default 1. */
+ * resident CTAs per SM (variant 0, 1, 2); default 0. */
 pz_status pz_ctx_set_pbs_variant(pz_ctx *ctx, int variant);
 int pz_ctx_pbs_variant(const pz_ctx *ctx);
 

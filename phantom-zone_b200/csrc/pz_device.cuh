@@ -181,32 +181,48 @@ __device__ __forceinline__ void tw(const u64 *t, int i, u64 &w, u64 &ws) {
   asm volatile("ld.global.nc.v2.u64 {%0, %1}, [%2];" : "=l"(w), "=l"(ws) : "l"(t + 2 * i));
 }
 
+// The transforms below act on one polynomial (x) or, with TWO, on two (x and
+// y) at once: both use the same twiddle loads, the same barriers and the same
+// exchange steps (y through the second N words of sm), and their butterflies
+// are independent instruction streams.  A single-polynomial call passes its
+// array as both x and y.
+template <bool TWO>
+__device__ __forceinline__ void fbf2(u64 (&x)[8], u64 (&y)[8], int a, int b, u64 w, u64 ws, u64 q) {
+  fbf(x[a], x[b], w, ws, q);
+  if (TWO) fbf(y[a], y[b], w, ws, q);
+}
+template <bool TWO>
+__device__ __forceinline__ void ibf2(u64 (&x)[8], u64 (&y)[8], int a, int b, u64 w, u64 ws, u64 q) {
+  ibf(x[a], x[b], w, ws, q);
+  if (TWO) ibf(y[a], y[b], w, ws, q);
+}
+
 // Forward radix-8 round k: stages with m = 8^k, 2m and 4m groups; blk is the
 // group index of this thread in the first of them.
-template <int LOGN>
-__device__ __forceinline__ void fwd_round8(u64 (&x)[8], int k, int j, const RingConsts &rc) {
+template <int LOGN, bool TWO>
+__device__ __forceinline__ void fwd_round8(u64 (&x)[8], u64 (&y)[8], int k, int j, const RingConsts &rc) {
   const int m = 1 << (3 * k);
   const int blk = j >> (LOGN - 3 * k - 3);
   const u64 q = rc.q;
   u64 w, ws;
   tw(rc.fw, m + blk, w, ws);
 #pragma unroll
-  for (int r = 0; r < 4; r++) fbf(x[r], x[r + 4], w, ws, q);
+  for (int r = 0; r < 4; r++) fbf2<TWO>(x, y, r, r + 4, w, ws, q);
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     tw(rc.fw, 2 * m + 2 * blk + h, w, ws);
-    fbf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
-    fbf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
+    fbf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    fbf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
 #pragma unroll
   for (int h = 0; h < 4; h++) {
     tw(rc.fw, 4 * m + 4 * blk + h, w, ws);
-    fbf(x[2 * h], x[2 * h + 1], w, ws, q);
+    fbf2<TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
   }
 }
 
-template <int LOGN>
-__device__ __forceinline__ void inv_round8(u64 (&x)[8], int k, int j, const RingConsts &rc) {
+template <int LOGN, bool TWO>
+__device__ __forceinline__ void inv_round8(u64 (&x)[8], u64 (&y)[8], int k, int j, const RingConsts &rc) {
   const int m = 1 << (3 * k);
   const int blk = j >> (LOGN - 3 * k - 3);
   const u64 q = rc.q;
@@ -214,22 +230,22 @@ __device__ __forceinline__ void inv_round8(u64 (&x)[8], int k, int j, const Ring
 #pragma unroll
   for (int h = 0; h < 4; h++) {
     tw(rc.iw, 4 * m + 4 * blk + h, w, ws);
-    ibf(x[2 * h], x[2 * h + 1], w, ws, q);
+    ibf2<TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
   }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     tw(rc.iw, 2 * m + 2 * blk + h, w, ws);
-    ibf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
-    ibf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
+    ibf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    ibf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
   tw(rc.iw, m + blk, w, ws);
 #pragma unroll
-  for (int r = 0; r < 4; r++) ibf(x[r], x[r + 4], w, ws, q);
+  for (int r = 0; r < 4; r++) ibf2<TWO>(x, y, r, r + 4, w, ws, q);
 }
 
 // Trailing 2-stage round (stages with N/4 and N/2 groups).
-template <int LOGN>
-__device__ __forceinline__ void fwd_round4(u64 (&x)[8], int j, const RingConsts &rc) {
+template <int LOGN, bool TWO>
+__device__ __forceinline__ void fwd_round4(u64 (&x)[8], u64 (&y)[8], int j, const RingConsts &rc) {
   constexpr int N = 1 << LOGN;
   const u64 q = rc.q;
   u64 w, ws;
@@ -237,18 +253,18 @@ __device__ __forceinline__ void fwd_round4(u64 (&x)[8], int j, const RingConsts 
   for (int h = 0; h < 2; h++) {
     const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
     tw(rc.fw, N / 4 + g, w, ws);
-    fbf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
-    fbf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
+    fbf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    fbf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       tw(rc.fw, N / 2 + 2 * g + e, w, ws);
-      fbf(x[4 * h + 2 * e], x[4 * h + 2 * e + 1], w, ws, q);
+      fbf2<TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
     }
   }
 }
 
-template <int LOGN>
-__device__ __forceinline__ void inv_round4(u64 (&x)[8], int j, const RingConsts &rc) {
+template <int LOGN, bool TWO>
+__device__ __forceinline__ void inv_round4(u64 (&x)[8], u64 (&y)[8], int j, const RingConsts &rc) {
   constexpr int N = 1 << LOGN;
   const u64 q = rc.q;
   u64 w, ws;
@@ -258,11 +274,11 @@ __device__ __forceinline__ void inv_round4(u64 (&x)[8], int j, const RingConsts 
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       tw(rc.iw, N / 2 + 2 * g + e, w, ws);
-      ibf(x[4 * h + 2 * e], x[4 * h + 2 * e + 1], w, ws, q);
+      ibf2<TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
     }
     tw(rc.iw, N / 4 + g, w, ws);
-    ibf(x[4 * h + 0], x[4 * h + 2], w, ws, q);
-    ibf(x[4 * h + 1], x[4 * h + 3], w, ws, q);
+    ibf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    ibf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
 }
 
@@ -303,61 +319,92 @@ __device__ __forceinline__ int xaddr(int b, int j, int r) {
   }
 }
 
-// Move the polynomial from layout LF to layout LT through sm (N words).
-template <int LOGN, int LF, int LT>
-__device__ __forceinline__ void xchg(u64 (&x)[8], u64 *sm, int j) {
+// Move the polynomial(s) from layout LF to layout LT through sm (N words per
+// polynomial).
+template <int LOGN, int LF, int LT, bool TWO>
+__device__ __forceinline__ void xchg(u64 (&x)[8], u64 (&y)[8], u64 *sm, int j) {
+  constexpr int N = 1 << LOGN;
   constexpr bool cross = (LF == 0 || LT == 0);
   const int bf = xbase<LOGN, LF>(j), bt = xbase<LOGN, LT>(j);
   sync_exchange(cross);
 #pragma unroll
-  for (int r = 0; r < 8; r++) sm[xaddr<LOGN, LF>(bf, j, r)] = x[r];
+  for (int r = 0; r < 8; r++) {
+    const int a = xaddr<LOGN, LF>(bf, j, r);
+    sm[a] = x[r];
+    if (TWO) sm[N + a] = y[r];
+  }
   sync_exchange(cross);
 #pragma unroll
-  for (int r = 0; r < 8; r++) x[r] = sm[xaddr<LOGN, LT>(bt, j, r)];
+  for (int r = 0; r < 8; r++) {
+    const int a = xaddr<LOGN, LT>(bt, j, r);
+    x[r] = sm[a];
+    if (TWO) y[r] = sm[N + a];
+  }
 }
 
-// Forward negacyclic NTT (CT, ntt.rs:110-143 without reductions) of one
-// polynomial: coefficient layout in, values < q; evaluation layout out,
-// values < (2 log N + 1) q.  sm: N words.  The rounds run in a loop (one copy
-// of the round body); the exchanges between them are layout-specialised and
-// picked by a block-uniform switch.
-template <int LOGN>
-__device__ __forceinline__ void ntt_fwd(u64 (&x)[8], u64 *sm, const RingConsts &rc) {
+// Forward negacyclic NTT (CT, ntt.rs:110-143 without reductions): coefficient
+// layout in, values < q; evaluation layout out, values < (2 log N + 1) q.
+// sm: N words (2N with TWO).  The rounds run in a loop (one copy of the round
+// body); the exchanges between them are layout-specialised and picked by a
+// block-uniform switch.
+template <int LOGN, bool TWO>
+__device__ __forceinline__ void ntt_fwd(u64 (&x)[8], u64 (&y)[8], u64 *sm, const RingConsts &rc) {
   typedef NttShape<LOGN> S;
   static_assert(S::FULL == 3, "three radix-8 rounds");
   const int j = tid_opaque();
 #pragma unroll 1
   for (int k = 0; k < 3; k++) {
-    if (k == 1) xchg<LOGN, 0, 1>(x, sm, j);
-    else if (k == 2) xchg<LOGN, 1, 2>(x, sm, j);
-    fwd_round8<LOGN>(x, k, j, rc);
+    if (k == 1) xchg<LOGN, 0, 1, TWO>(x, y, sm, j);
+    else if (k == 2) xchg<LOGN, 1, 2, TWO>(x, y, sm, j);
+    fwd_round8<LOGN, TWO>(x, y, k, j, rc);
   }
   if constexpr (S::PARTIAL) {
-    xchg<LOGN, 2, 3>(x, sm, j);
-    fwd_round4<LOGN>(x, j, rc);
+    xchg<LOGN, 2, 3, TWO>(x, y, sm, j);
+    fwd_round4<LOGN, TWO>(x, y, j, rc);
   }
 }
 
-// Inverse negacyclic NTT (GS, ntt.rs:187-230 without the N^{-1} factor) of
-// one polynomial: evaluation layout in, values < 2q; coefficient layout out,
-// values < 2q.  sm: N words.
-template <int LOGN>
-__device__ __forceinline__ void ntt_inv(u64 (&x)[8], u64 *sm, const RingConsts &rc) {
+// Inverse negacyclic NTT (GS, ntt.rs:187-230 without the N^{-1} factor):
+// evaluation layout in, values < 2q; coefficient layout out, values < 2q.
+// sm: N words (2N with TWO).
+template <int LOGN, bool TWO>
+__device__ __forceinline__ void ntt_inv(u64 (&x)[8], u64 (&y)[8], u64 *sm, const RingConsts &rc) {
   typedef NttShape<LOGN> S;
   const int j = tid_opaque();
   // The first exchange below is warp-local, but the previous user of sm may
   // have read it across warps (a transform's last exchange): full barrier.
   __syncthreads();
   if constexpr (S::PARTIAL) {
-    inv_round4<LOGN>(x, j, rc);
-    xchg<LOGN, 3, 2>(x, sm, j);
+    inv_round4<LOGN, TWO>(x, y, j, rc);
+    xchg<LOGN, 3, 2, TWO>(x, y, sm, j);
   }
 #pragma unroll 1
   for (int k = 2; k >= 0; k--) {
-    inv_round8<LOGN>(x, k, j, rc);
-    if (k == 2) xchg<LOGN, 2, 1>(x, sm, j);
-    else if (k == 1) xchg<LOGN, 1, 0>(x, sm, j);
+    inv_round8<LOGN, TWO>(x, y, k, j, rc);
+    if (k == 2) xchg<LOGN, 2, 1, TWO>(x, y, sm, j);
+    else if (k == 1) xchg<LOGN, 1, 0, TWO>(x, y, sm, j);
   }
+}
+
+// Single-polynomial forms.
+template <int LOGN>
+__device__ __forceinline__ void ntt_fwd(u64 (&x)[8], u64 *sm, const RingConsts &rc) {
+  ntt_fwd<LOGN, false>(x, x, sm, rc);
+}
+template <int LOGN>
+__device__ __forceinline__ void ntt_inv(u64 (&x)[8], u64 *sm, const RingConsts &rc) {
+  ntt_inv<LOGN, false>(x, x, sm, rc);
+}
+
+// Automorphism X -> X^k (k odd) in the evaluation domain.  The forward
+// transform leaves a(psi^(2 brv(p) + 1)) at position p, so a(X^k) holds at p
+// the value found at p' with 2 brv(p') + 1 = (2 brv(p) + 1) k mod 2N: a
+// permutation of positions (the ring automorphism, signs included).
+template <int LOGN>
+__device__ __forceinline__ int auto_eval_src(int p, u32 k) {
+  const u32 e = 2u * (__brev((u32)p) >> (32 - LOGN)) + 1u;
+  const u32 e2 = (e * k) & ((2u << LOGN) - 1u);
+  return (int)(__brev((e2 - 1u) >> 1) >> (32 - LOGN));
 }
 
 __device__ __forceinline__ u64 reduce4(u64 v, u64 q) {  // [0,4q) -> [0,q)

@@ -24,7 +24,7 @@ struct pz_ctx {
   pz::BrParams br{};
   pz::KsParams ks{};
   int grid_limit = 0;
-  int pbs_variant = 1;  // blind-rotation launch shape (see pz::PBS_VARIANTS)
+  int pbs_variant = 0;  // blind-rotation launch shape (see pz::PBS_VARIANTS)
   // host-API scratch (guarded by mu)
   std::mutex mu;
   size_t cap = 0;

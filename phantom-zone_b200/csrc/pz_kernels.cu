@@ -16,15 +16,22 @@
 
 namespace pz {
 
-// Shared memory of the bootstrap operations: region 0 (N words) is the NTT
-// exchange buffer and the permuted a(X^k) of an automorphism; region 1 (N
-// words) holds the permuted b(X^k) until the automorphism's final addition.
+// Shared memory of the bootstrap operations: 2N words.  Region 0 (N words)
+// holds the permuted a(X^k) of an automorphism, region 1 (N words) its b
+// before the evaluation-domain permutation; both together are the exchange
+// buffer of the two-polynomial transforms (region 0 alone of the
+// single-polynomial ones).
 constexpr int OP_REGIONS = 2;
 
 // Operation codes of the blind-rotation schedule: an external product with
 // RGSW key `i` is `i`; an automorphism with key slot v (0 = -g) is
 // OP_AUTO | v, plus OP_TRIVIAL while the accumulator is still trivial.
-constexpr u32 OP_AUTO = 0x8000u, OP_TRIVIAL = 0x4000u, OP_SLOT = 0x00ffu;
+// OP_KEEPB marks an operation whose successor is a non-trivial automorphism:
+// it leaves b in the evaluation domain (scaled by N^{-1}, values < 2q), where
+// the automorphism permutes it and adds it before its own inverse transform,
+// so b skips one inverse and one forward-domain round trip.
+constexpr u32 OP_AUTO = 0x8000u, OP_TRIVIAL = 0x4000u, OP_KEEPB = 0x2000u, OP_SLOT = 0x00ffu,
+              OP_INDEX = 0x1fffu;
 
 // ---------------------------------------------------------------------------
 // Key conversion and NTT microbench
@@ -89,44 +96,39 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
 }
 
 // ---------------------------------------------------------------------------
-// One blind-rotation operation on the accumulator acc = (a, b) (coefficient
-// layout, canonical [0, Q)):
+// One blind-rotation operation on the accumulator acc = (a, b):
 //   op = RGSW index i:  acc <- acc x RGSW_i        (rlwe_by_rgsw_shoup, runtime.rs:754-855)
 //   op = OP_AUTO | v:   acc <- auto_{k_v}(acc)      (rlwe_auto_shoup, runtime.rs:530-643)
-// Both share one copy of the forward and of the inverse NTT: the transforms
-// run in a loop over the polynomials that swaps the two register arrays.
+// a is always in the coefficient layout, canonical [0, Q).  b is too, except
+// on entry to a non-trivial automorphism (evaluation domain, see OP_KEEPB)
+// and on exit from an operation marked OP_KEEPB.  The external product
+// transforms its two digit polynomials together and inverts both outputs
+// together; the automorphism transforms its single digit polynomial alone.
 // The first (trivial) external product of a blind rotation runs the general
 // code with a = 0: the a-digits are 0, their products vanish and, since every
 // result is reduced to the canonical residue, the words equal those of the
-// reference's trivial branch.  Device RGSW rows: A(-sm) x d_a, B(-sm) x d_a,
-// A(m) x d_b, B(m) x d_b (runtime.rs:174-180); auto key rows A x d, B x d.
+// reference's trivial branch.  Every output is the canonical residue of the
+// same polynomial the reference computes (all steps are exact mod Q), so the
+// domain in which b(X^k) is added does not change a word.  Device RGSW rows:
+// A(-sm) x d_a, B(-sm) x d_a, A(m) x d_b, B(m) x d_b (runtime.rs:174-180);
+// auto key rows A x d, B x d.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void swap8(u64 (&x)[8], u64 (&y)[8]) {
-#pragma unroll
-  for (int r = 0; r < 8; r++) {
-    const u64 t = x[r];
-    x[r] = y[r];
-    y[r] = t;
-  }
-}
 
 // x <- x (pointwise, Montgomery) from two device-layout key rows, y likewise.
 template <int LOGN>
 __device__ __forceinline__ void mac_pair(u64 (&x)[8], u64 (&y)[8], const u64 *ka, const u64 *kb,
-                                         const u64 *kc, const u64 *kd, bool two, const RingConsts &rc) {
-  // x' = x ka + y kc, y' = x kb + y kd   (two == false: x' = x ka, y' = x kb)
+                                         const u64 *kc, const u64 *kd, const RingConsts &rc) {
+  // x' = x ka + y kc, y' = x kb + y kd
   const int j = threadIdx.x;
   const u64 q = rc.q, qi = rc.qinv_neg;
 #pragma unroll
   for (int rr = 0; rr < 4; rr++) {
     const int di = dev_index<LOGN>(j, 2 * rr);
-    u64 a[2], b[2], c[2] = {0, 0}, d[2] = {0, 0};
+    u64 a[2], b[2], c[2], d[2];
     ld_key2(ka + di, a[0], a[1]);
     ld_key2(kb + di, b[0], b[1]);
-    if (two) {
-      ld_key2(kc + di, c[0], c[1]);
-      ld_key2(kd + di, d[0], d[1]);
-    }
+    ld_key2(kc + di, c[0], c[1]);
+    ld_key2(kd + di, d[0], d[1]);
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       const int r = 2 * rr + e;
@@ -134,12 +136,36 @@ __device__ __forceinline__ void mac_pair(u64 (&x)[8], u64 (&y)[8], const u64 *ka
       u64 hi, lo, hi2, lo2;
       mul128(xv, a[e], hi, lo);
       mul128(xv, b[e], hi2, lo2);
-      if (two) {
-        mac128(yv, c[e], hi, lo);
-        mac128(yv, d[e], hi2, lo2);
-      }
+      mac128(yv, c[e], hi, lo);
+      mac128(yv, d[e], hi2, lo2);
       x[r] = redc(hi, lo, q, qi);
       y[r] = redc(hi2, lo2, q, qi);
+    }
+  }
+}
+
+// Automorphism product: x' = x ka, y' = x kb + y, with y the permuted b in
+// the evaluation domain (< 2q); outputs < 2q.
+template <int LOGN>
+__device__ __forceinline__ void mac_auto(u64 (&x)[8], u64 (&y)[8], const u64 *ka, const u64 *kb,
+                                         const RingConsts &rc) {
+  const int j = threadIdx.x;
+  const u64 q = rc.q, qi = rc.qinv_neg, q2 = rc.q << 1;
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    const int di = dev_index<LOGN>(j, 2 * rr);
+    u64 a[2], b[2];
+    ld_key2(ka + di, a[0], a[1]);
+    ld_key2(kb + di, b[0], b[1]);
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int r = 2 * rr + e;
+      u64 hi, lo, hi2, lo2;
+      mul128(x[r], a[e], hi, lo);
+      mul128(x[r], b[e], hi2, lo2);
+      x[r] = redc(hi, lo, q, qi);
+      const u64 v = redc(hi2, lo2, q, qi) + y[r];
+      y[r] = v >= q2 ? v - q2 : v;
     }
   }
 }
@@ -172,30 +198,39 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
   u64(&x)[8] = acc[0];
   u64(&y)[8] = acc[1];
   const bool is_auto = (op & OP_AUTO) != 0;
+  const bool keep_b = (op & OP_KEEPB) != 0;
   u64 *s_a = sm, *s_b = sm + N;
   if (is_auto) {
-    // a(X) -> a(X^k), b(X) -> b(X^k) with sign (generate_auto_map, keygen.rs:16-41)
+    // a(X) -> a(X^k) with sign (generate_auto_map, keygen.rs:16-41)
     const u32 k = P.auto_k[op & OP_SLOT];
-    const bool trivial = (op & OP_TRIVIAL) != 0;
     __syncthreads();
+    if (op & OP_TRIVIAL) {  // runtime.rs:625-642: only b is permuted (neg(0) = q kept)
 #pragma unroll
-    for (int r = 0; r < 8; r++) {
-      const u32 i = (u32)pos_coef<LOGN>(j, r);
-      u32 t = (i * k) & (2 * N - 1);
-      const bool neg = t >= (u32)N;
-      if (neg) t -= N;
-      if (!trivial) s_a[swz(t)] = neg ? q - x[r] : x[r];
-      s_b[swz(t)] = neg ? q - y[r] : y[r];
-    }
-    __syncthreads();
-    if (trivial) {  // runtime.rs:625-642: only b is permuted (neg(0) = q kept)
+      for (int r = 0; r < 8; r++) {
+        u32 t = ((u32)pos_coef<LOGN>(j, r) * k) & (2 * N - 1);
+        const bool neg = t >= (u32)N;
+        if (neg) t -= N;
+        s_b[swz(t)] = neg ? q - y[r] : y[r];
+      }
+      __syncthreads();
 #pragma unroll
       for (int r = 0; r < 8; r++) y[r] = s_b[swz(pos_coef<LOGN>(j, r))];
       return;
     }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      u32 t = ((u32)pos_coef<LOGN>(j, r) * k) & (2 * N - 1);
+      const bool neg = t >= (u32)N;
+      if (neg) t -= N;
+      s_a[swz(t)] = neg ? q - x[r] : x[r];
+      s_b[swz(pos_eval<LOGN>(j, r))] = y[r];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; r++) y[r] = s_b[swz(auto_eval_src<LOGN>(pos_eval<LOGN>(j, r), k))];
   }
   const u64 *K = is_auto ? P.autos + (size_t)(op & OP_SLOT) * P.auto_rows * N
-                         : P.rgsw + (size_t)op * P.rgsw_rows * N;
+                         : P.rgsw + (size_t)(op & OP_INDEX) * P.rgsw_rows * N;
   if (D1) {
     if (is_auto) {
 #pragma unroll
@@ -203,6 +238,8 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
         u64 st = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
         x[r] = decomp_next(st, P.dauto);
       }
+      ntt_fwd<LOGN, false>(x, x, sm, P.rc);
+      mac_auto<LOGN>(x, y, K, K + N, P.rc);
     } else {
 #pragma unroll
       for (int r = 0; r < 8; r++) {
@@ -211,16 +248,9 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
         u64 sb = decomp_init(y[r], P.db);
         y[r] = decomp_next(sb, P.db);
       }
+      ntt_fwd<LOGN, true>(x, y, sm, P.rc);
+      mac_pair<LOGN>(x, y, K, K + N, K + 2 * N, K + 3 * N, P.rc);
     }
-    const int np = is_auto ? 1 : 2;
-#pragma unroll 1
-    for (int p = 0; p < np; p++) {
-      ntt_fwd<LOGN>(x, sm, P.rc);
-      swap8(x, y);
-    }
-    if (np == 1) swap8(x, y);
-    if (is_auto) mac_pair<LOGN>(x, y, K, K + N, nullptr, nullptr, false, P.rc);
-    else mac_pair<LOGN>(x, y, K, K + N, K + 2 * N, K + 3 * N, true, P.rc);
   } else {
     // general decomposition counts (SP_TEST: d = 4): digit by digit, lazily
     // accumulated in [0, 2q), one inverse transform at the end
@@ -232,7 +262,7 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
       sa[r] = decomp_init(is_auto ? s_a[swz(pos_coef<LOGN>(j, r))] : x[r], dpa);
       sb[r] = is_auto ? 0 : decomp_init(y[r], P.db);
       oa[r] = 0;
-      ob[r] = 0;
+      ob[r] = is_auto ? y[r] : 0;  // the automorphism's permuted b (< 2q)
     }
     const u32 dmax = da > db ? da : db;
     for (u32 jd = 0; jd < dmax; jd++) {
@@ -242,13 +272,8 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
         x[r] = hx ? decomp_next(sa[r], dpa) : 0;
         y[r] = hy ? decomp_next(sb[r], P.db) : 0;
       }
-      const int np = hy ? 2 : 1;
-#pragma unroll 1
-      for (int p = 0; p < np; p++) {
-        ntt_fwd<LOGN>(x, sm, P.rc);
-        swap8(x, y);
-      }
-      if (np == 1) swap8(x, y);
+      if (hy) ntt_fwd<LOGN, true>(x, y, sm, P.rc);
+      else ntt_fwd<LOGN, false>(x, x, sm, P.rc);
       if (is_auto) {
         mac_accum<LOGN>(oa, ob, x, y, K + (size_t)jd * N, K + (size_t)(da + jd) * N, nullptr, nullptr, hx,
                         false, P.rc);
@@ -263,18 +288,17 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
       y[r] = ob[r];
     }
   }
-#pragma unroll 1
-  for (int p = 0; p < 2; p++) {
-    ntt_inv<LOGN>(x, sm, P.rc);
-    swap8(x, y);
-  }
+  if (keep_b) {
+    ntt_inv<LOGN, false>(x, x, sm, P.rc);
 #pragma unroll
-  for (int r = 0; r < 8; r++) {
-    x[r] = reduce2(x[r], q);
-    y[r] = reduce2(y[r], q);
-    // b' += b(X^k) with sign: add_mod of the signed value == sub_mod_fast /
-    // add_mod_fast of runtime.rs:608-620 (the signed value is q - b or b)
-    if (is_auto) y[r] = add_mod(y[r], s_b[swz(pos_coef<LOGN>(j, r))], q);
+    for (int r = 0; r < 8; r++) x[r] = reduce2(x[r], q);
+  } else {
+    ntt_inv<LOGN, true>(x, y, sm, P.rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      x[r] = reduce2(x[r], q);
+      y[r] = reduce2(y[r], q);
+    }
   }
 }
 
@@ -285,6 +309,7 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
   extern __shared__ u64 smem[];
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    if (idx[c] >= P.n) continue;  // out-of-range key index: the ciphertext is left unchanged
     u64 *p = rlwe + c * 2 * N;
     u64 acc[2][8];
 #pragma unroll
@@ -309,12 +334,18 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
   extern __shared__ u64 smem[];
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    if (slot[c] > P.w) continue;  // out-of-range key slot: the ciphertext is left unchanged
     u64 *p = rlwe + c * 2 * N;
     u64 acc[2][8];
 #pragma unroll
     for (int r = 0; r < 8; r++) {
       acc[0][r] = p[pos_coef<LOGN>(j, r)];
       acc[1][r] = p[N + pos_coef<LOGN>(j, r)];
+    }
+    if (!trivial) {  // a non-trivial automorphism takes b as N^{-1} NTT(b) (< 2q)
+      ntt_fwd<LOGN>(acc[1], smem, P.rc);
+#pragma unroll
+      for (int r = 0; r < 8; r++) acc[1][r] = shoup_mul(acc[1][r], P.rc.n_inv, P.rc.n_inv_s, P.rc.q);
     }
     bootstrap_op<LOGN, D1>(acc, OP_AUTO | (trivial ? OP_TRIVIAL : 0u) | (slot[c] & OP_SLOT), P, smem);
 #pragma unroll
@@ -517,7 +548,10 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
         for (u32 t = s_start[b]; t < e; t++) s_ops[no++] = s_list[t];
         if (e != s_start[b]) trivial = false;
       };
-      auto autom = [&](u32 v) { s_ops[no++] = (unsigned short)(OP_AUTO | (trivial ? OP_TRIVIAL : 0u) | v); };
+      auto autom = [&](u32 v) {
+        if (!trivial) s_ops[no - 1] |= (unsigned short)OP_KEEPB;  // b stays in the evaluation domain
+        s_ops[no++] = (unsigned short)(OP_AUTO | (trivial ? OP_TRIVIAL : 0u) | v);
+      };
       u32 v = 0;
       for (u32 i = q4 - 1; i >= 1; i--) {  // -(g^k)
         bucket(q4 + i);
