@@ -236,6 +236,56 @@ pz_status pz_circuit_capture_graph(pz_ctx *ctx, const pz_key *key, pz_circuit *c
                                    uint64_t *d_outputs, void *stream);
 pz_status pz_circuit_replay_graph(pz_circuit *c, void *stream);
 
+/* ---- multi-session executor (serving) ---------------------------------------------
+ * No reference counterpart: the reference evaluates one gate at a time, in
+ * the calling thread, against its thread's one global server key
+ * (bool/mp_api.rs:20-26).  A server runs on one device.  A session is a
+ * (context, device key) pair of any parameter set sharing the server's ring
+ * (all production sets: N = 2048, the same Q); a job is a circuit submitted
+ * to a session.  pz_server_step admits pending jobs in arrival order while
+ * their wires fit the device arena (admission by device bytes; keys are
+ * resident already), then advances every admitted job by one circuit level:
+ * the gates of all sessions run as one ragged key-switch launch and one
+ * ragged blind-rotation launch per max_items gates, each gate with its own
+ * session's parameters and key.  A job admitted while others are mid-circuit
+ * starts at its level 1 in the same launches (continuous batching).  Not
+ * thread-safe: one host thread drives a server.  Job buffers must stay valid
+ * and the circuit unchanged until the job is done. */
+typedef struct pz_server pz_server;
+typedef struct {
+  size_t pending, active, done, failed;
+  size_t arena_slots, arena_slots_used, arena_bytes;
+  size_t sessions, key_bytes;
+  uint64_t steps, gates, launches;
+} pz_server_stats;
+#define PZ_SERVER_DRY_RUN (-1) /* device id of a host-only server: bookkeeping, no GPU work */
+/* arena_bytes: device bytes for job wires ((n_inputs + n_gates) x (N + 1) x 8 per job);
+ * max_items: gates per ragged launch (larger steps are split) */
+pz_status pz_server_create(int device, size_t arena_bytes, size_t max_items, pz_server **out);
+void pz_server_destroy(pz_server *s);
+const char *pz_server_last_error(const pz_server *s);
+pz_status pz_server_add_session(pz_server *s, pz_ctx *ctx, const pz_key *key, uint32_t *session);
+/* dry-run servers only: a session of parameter set param_id without a key */
+pz_status pz_server_add_virtual_session(pz_server *s, int param_id, uint32_t *session);
+/* inputs [n_inputs][N + 1], outputs [n_outputs][N + 1]; device_io = 1: device pointers */
+pz_status pz_server_submit(pz_server *s, uint32_t session, pz_circuit *c, const uint64_t *inputs,
+                           uint64_t *outputs, int device_io, uint64_t *job);
+/* One scheduling step (admit, one level of every admitted job, retire);
+ * returns when its device work is complete.  *gates: bootstraps run. */
+pz_status pz_server_step(pz_server *s, size_t *gates);
+/* state: 0 pending, 1 running, 2 done, 3 failed (needs more than the whole
+ * arena); latency = done - submit, queue = admit - submit (ms, -1 if n/a) */
+pz_status pz_server_job_status(pz_server *s, uint64_t job, int *state, double *latency_ms, double *queue_ms);
+pz_status pz_server_forget(pz_server *s, uint64_t job);
+pz_status pz_server_stats_get(pz_server *s, pz_server_stats *out);
+/* Ragged blind-rotation launch shape (variant as pz_ctx_set_pbs_variant; grid
+ * limit 0 = one CTA per gate) */
+pz_status pz_server_set_launch(pz_server *s, int pbs_variant, int grid_limit);
+/* Autotuner: times every variant x {one CTA per gate, persistent 2 x SMs}
+ * on `batch` synthetic gates spread over the sessions and keeps the fastest.
+ * Needs an idle server (no admitted job). */
+pz_status pz_server_autotune(pz_server *s, size_t batch, int *variant, int *grid_limit, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

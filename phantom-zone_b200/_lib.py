@@ -35,6 +35,12 @@ class PzServerKeyView(ctypes.Structure):
     _fields_ = [("rgsw", u64p), ("autos", u64p), ("lwe_ksk", u64p)]
 
 
+class PzServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_size_t) for n in ("pending", "active", "done", "failed", "arena_slots",
+                                                "arena_slots_used", "arena_bytes", "sessions", "key_bytes")] + \
+               [(n, ctypes.c_uint64) for n in ("steps", "gates", "launches")]
+
+
 # name -> (restype, argtypes); every symbol declared in the public header
 SIGNATURES = {
     "pz_status_string": (ctypes.c_char_p, [st]),
@@ -64,6 +70,20 @@ SIGNATURES = {
     "pz_ctx_set_pbs_grid_limit": (st, [vp, ctypes.c_int]),
     "pz_ctx_set_pbs_variant": (st, [vp, ctypes.c_int]),
     "pz_ctx_pbs_variant": (ctypes.c_int, [vp]),
+    "pz_server_create": (st, [ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(vp)]),
+    "pz_server_destroy": (None, [vp]),
+    "pz_server_last_error": (ctypes.c_char_p, [vp]),
+    "pz_server_add_session": (st, [vp, vp, vp, u32p]),
+    "pz_server_add_virtual_session": (st, [vp, ctypes.c_int, u32p]),
+    "pz_server_submit": (st, [vp, ctypes.c_uint32, vp, vp, vp, ctypes.c_int, u64p]),
+    "pz_server_step": (st, [vp, ctypes.POINTER(ctypes.c_size_t)]),
+    "pz_server_job_status": (st, [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "pz_server_forget": (st, [vp, ctypes.c_uint64]),
+    "pz_server_stats_get": (st, [vp, ctypes.POINTER(PzServerStats)]),
+    "pz_server_set_launch": (st, [vp, ctypes.c_int, ctypes.c_int]),
+    "pz_server_autotune": (st, [vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                ctypes.POINTER(ctypes.c_double)]),
     "pz_circuit_create": (st, [ctypes.POINTER(vp)]),
     "pz_circuit_destroy": (None, [vp]),
     "pz_circuit_last_error": (ctypes.c_char_p, [vp]),

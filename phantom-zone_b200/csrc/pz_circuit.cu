@@ -353,6 +353,32 @@ pz_status enqueue(pz_ctx *ctx, const pz_key *k, pz_circuit *c, const u64 *d_in, 
 
 }  // namespace
 
+namespace pz {
+bool circuit_view(pz_circuit *c, CircuitView *v) {
+  if (!c || !v) return false;
+  compile(c);
+  v->n_inputs = c->n_inputs;
+  v->n_gates = c->gates.size();
+  v->n_outputs = c->outputs.size();
+  v->levels = c->level_off.empty() ? 0 : c->level_off.size() - 1;
+  v->level_off = c->level_off.data();
+  v->type = c->h_type.data();
+  v->in0 = c->h_in0.data();
+  v->in1 = c->h_in1.data();
+  v->out = c->h_out.data();
+  v->outref = c->h_outref.data();
+  return true;
+}
+
+cudaError_t launch_gather(const u64 *wires, const u32 *refs, u64 *out, size_t count, size_t L, u64 q,
+                          cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  const size_t blocks = std::min<size_t>(count, 4096);
+  gather_kernel<<<(unsigned)blocks, 256, 0, s>>>(wires, refs, out, count, L, q);
+  return cudaGetLastError();
+}
+}  // namespace pz
+
 extern "C" {
 
 pz_status pz_circuit_create(pz_circuit **out) {

@@ -51,6 +51,19 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
 pz_status fail(pz_ctx *ctx, pz_status s, const std::string &msg);
 pz_status cuda_fail(pz_ctx *ctx, const char *what, cudaError_t e);
 u32 ks_stride(const pz_params &P);
+
+// Compiled (levelized) form of a circuit, read by the multi-session executor.
+// Wire slots: inputs first (input order), then gate outputs; bit 31 = not().
+struct CircuitView {
+  size_t n_inputs = 0, n_gates = 0, n_outputs = 0, levels = 0;
+  const size_t *level_off = nullptr;  // level l (1..levels) = gates [off[l-1], off[l])
+  const unsigned char *type = nullptr;
+  const u32 *in0 = nullptr, *in1 = nullptr, *out = nullptr, *outref = nullptr;
+};
+bool circuit_view(pz_circuit *c, CircuitView *v);
+// out[i] = wires[refs[i]] (q - x when bit 31 of refs[i] is set), L words each
+cudaError_t launch_gather(const u64 *wires, const u32 *refs, u64 *out, size_t count, size_t L, u64 q,
+                          cudaStream_t s);
 }  // namespace pz
 
 #define PZ_CK(ctx, call)                                          \

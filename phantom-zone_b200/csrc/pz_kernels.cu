@@ -12,6 +12,10 @@
 //                 blind-rotation schedule, test vector rotation, the whole
 //                 blind rotation with the RLWE accumulator in registers,
 //                 sample extraction (pbs.rs:146-449)
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "pz_kernels.cuh"
 
 namespace pz {
@@ -377,7 +381,7 @@ __device__ __forceinline__ u64 prelude_moddown(u64 x0, u64 x1, unsigned char gat
   return (u64)round(f);
 }
 
-constexpr int KS_CT = 16;    // ciphertexts per CTA
+constexpr int KS_CT = KS_TILE_CT;  // ciphertexts per CTA
 constexpr int KS_IC = 32;    // LWE coefficients per digit chunk
 constexpr int KS_COLS = 128; // output columns per CTA
 
@@ -391,12 +395,12 @@ __device__ __forceinline__ u64 operand(const u64 *base, const u32 *idx, int ct, 
   return (w & WIRE_NEG) ? q - x : x;
 }
 
-__global__ void __launch_bounds__(KS_COLS)
-    ks_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
-  __shared__ u32 dig[KS_CT][KS_IC][MAX_KS_D];
+// Key switch of ciphertexts [ct0, min(ct0 + KS_CT, count)) for the output
+// columns of this CTA (blockIdx.y).
+__device__ __forceinline__ void ks_tile(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
+                                        int ct0, int count, u32 *out, u32 (*dig)[KS_IC][MAX_KS_D]) {
   const int tid = threadIdx.x;
   const int col = blockIdx.y * KS_COLS + tid;
-  const int ct0 = blockIdx.x * KS_CT;
   const size_t L = (size_t)P.N + 1;
   const u32 d = P.d;
   u32 acc[KS_CT];
@@ -446,6 +450,33 @@ __global__ void __launch_bounds__(KS_COLS)
   }
 }
 
+__global__ void __launch_bounds__(KS_COLS)
+    ks_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
+  __shared__ u32 dig[KS_CT][KS_IC][MAX_KS_D];
+  ks_tile(P, gates, c0, c1, blockIdx.x * KS_CT, count, out, dig);
+}
+
+// Ragged batch: tile blockIdx.x holds up to KS_CT ciphertexts of one session
+// (descriptor) -- the KSK rows it streams are that session's.  Ciphertext
+// operands are gathered from `wires` through in0/in1 (bit 31 = not()).
+__global__ void __launch_bounds__(KS_COLS)
+    ks_ragged_kernel(const KsParams *descs, const KsTile *tiles, const unsigned char *gates, const u64 *wires,
+                     const u32 *in0, const u32 *in1, u32 *out, u32 out_stride) {
+  __shared__ u32 dig[KS_CT][KS_IC][MAX_KS_D];
+  __shared__ KsParams sp;
+  const KsTile t = tiles[blockIdx.x];
+  if (threadIdx.x == 0) {
+    sp = descs[t.desc];
+    sp.in0 = in0;
+    sp.in1 = in1;
+    sp.out_stride = out_stride;
+    sp.raw = 0;
+  }
+  __syncthreads();
+  if (blockIdx.y * KS_COLS > sp.n) return;  // no columns of this session here (uniform per CTA)
+  ks_tile(sp, gates, wires, wires, (int)t.first, (int)(t.first + t.count), out, dig);
+}
+
 // ---------------------------------------------------------------------------
 // The bootstrap: one CTA per ciphertext (grid-stride over the batch)
 // ---------------------------------------------------------------------------
@@ -467,12 +498,12 @@ size_t pbs_smem_bytes(int logn, u32 br_q, u32 n) {
 
 // MINB: CTAs per SM the register allocation must allow (launch-shape
 // variants chosen at run time, see pz_ctx_set_pbs_variant).
-template <int LOGN, bool D1, int MINB>
-__global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
-    pbs_kernel(BrParams P, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out, int count,
-               u64 *rlwe_dbg) {
+// One gate bootstrap of ciphertext ct (key-switched LWE kso, gate code
+// gcode) with the parameters and key of P; the whole CTA takes part.
+template <int LOGN, bool D1>
+__device__ __forceinline__ void pbs_item(const BrParams &P, int ct, const u32 *kso, u32 gcode, u64 *out,
+                                         u64 *rlwe_dbg, u64 *smem) {
   constexpr int N = 1 << LOGN, T = NttShape<LOGN>::T;
-  extern __shared__ u64 smem[];
   u64 *sm = smem;
   const u32 R = P.br_q >> 1, q4 = P.br_q >> 2, n = P.n;
   unsigned short *s_start = (unsigned short *)(smem + OP_REGIONS * N);  // R + 1
@@ -481,9 +512,7 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
   u32 *s_nops = (u32 *)(((size_t)(s_ops + n + R + 1) + 3) & ~(size_t)3);
   const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
   const u64 q = P.rc.q;
-
-  for (int ct = blockIdx.x; ct < count; ct += gridDim.x) {
-    const u32 *kso = ks + (size_t)ct * ks_stride;
+  {
     // ---- odd mod-switch + dlog buckets (pbs.rs:147-161), stable in LWE index
     u32 *cnt = (u32 *)sm;                                 // R counters (region 0)
     unsigned short *keys = (unsigned short *)(cnt + R);   // n keys (region 0)
@@ -582,7 +611,7 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
     u32 mexp = gb;
     bool msign = true;
     if (mexp > R) { mexp -= R; msign = false; }
-    u32 gi = gates[ct] & 7u;
+    u32 gi = gcode & 7u;
     if (gi > 5) gi = 5;  // codes are validated on the host; never index past the 6 test vectors
     const u64 *tv = P.tv + (size_t)gi * R;
     u64 acc[2][8];
@@ -628,6 +657,35 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
         d[N + pos_coef<LOGN>(j, r)] = acc[1][r];
       }
     }
+  }
+}
+
+template <int LOGN, bool D1, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
+    pbs_kernel(BrParams P, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out, int count,
+               u64 *rlwe_dbg) {
+  extern __shared__ u64 smem[];
+  for (int ct = blockIdx.x; ct < count; ct += gridDim.x)
+    pbs_item<LOGN, D1>(P, ct, ks + (size_t)ct * ks_stride, gates[ct], out, rlwe_dbg, smem);
+}
+
+// Ragged batch: ciphertext ct uses the parameter set and server key of
+// descriptor item_desc[ct] (sessions of different parameter sets in one
+// launch); outputs scatter to out_idx[ct].
+template <int LOGN, bool D1, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
+    pbs_ragged_kernel(const BrParams *descs, const u32 *item_desc, const u32 *ks, u32 ks_stride,
+                      const unsigned char *gates, u64 *out, const u32 *out_idx, int count) {
+  extern __shared__ u64 smem[];
+  __shared__ BrParams sp;
+  for (int ct = blockIdx.x; ct < count; ct += gridDim.x) {
+    __syncthreads();  // the previous item is done with sp
+    if (threadIdx.x == 0) {
+      sp = descs[item_desc[ct]];
+      sp.out_idx = out_idx;
+    }
+    __syncthreads();
+    pbs_item<LOGN, D1>(sp, ct, ks + (size_t)ct * ks_stride, gates[ct], out, nullptr, smem);
   }
 }
 
@@ -696,13 +754,19 @@ cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts 
 // far), outside of any launch sequence that may be captured into a graph.
 template <typename K>
 static cudaError_t set_smem(K kernel, size_t bytes) {
-  static size_t done = 0;
-  if (bytes <= done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) done = bytes;
+  // the attribute is per kernel and per device: remember the largest size set
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &have = done[{(const void *)kernel, dev}];
+  if (bytes <= have) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
   return e;
 }
-
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
                                size_t count, int trivial, cudaStream_t s) {
   if (count == 0) return cudaSuccess;
@@ -757,6 +821,41 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                                    \
   if ((e = set_smem(pbs_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;                        \
   pbs_kernel<LN, DD, MB><<<grid, TH, smem, s>>>(P, ks, ks_stride, gates, out, (int)count, rlwe_dbg);
+  if (logn == 11 && d1) {
+    if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
+    else if (variant == 1) { PZ_LAUNCH(11, true, 3, 256) }
+    else { PZ_LAUNCH(11, true, 4, 256) }
+  }
+  else if (logn == 11) { PZ_LAUNCH(11, false, 1, 256) }
+  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 1, 64) }
+  else if (logn == 9) { PZ_LAUNCH(9, false, 1, 64) }
+  else return cudaErrorInvalidValue;
+#undef PZ_LAUNCH
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, u32 max_n,
+                             u32 max_d, const unsigned char *gates, const u64 *wires, const u32 *in0,
+                             const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s) {
+  if (ntiles == 0) return cudaSuccess;
+  if (max_d > (u32)MAX_KS_D) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)ntiles, (unsigned)((max_n + 1 + KS_COLS - 1) / KS_COLS));
+  ks_ragged_kernel<<<grid, KS_COLS, 0, s>>>(d_descs, d_tiles, gates, wires, in0, in1, out, out_stride);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pbs_ragged(int logn, bool d1, const BrParams *d_descs, const u32 *item_desc, u32 max_br_q,
+                              u32 max_n, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out,
+                              const u32 *out_idx, size_t count, int grid_limit, cudaStream_t s, int variant) {
+  if (count == 0) return cudaSuccess;
+  const size_t smem = pbs_smem_bytes(logn, max_br_q, max_n);
+  int grid = (int)count;
+  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
+  cudaError_t e;
+#define PZ_LAUNCH(LN, DD, MB, TH)                                                                    \
+  if ((e = set_smem(pbs_ragged_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;                 \
+  pbs_ragged_kernel<LN, DD, MB><<<grid, TH, smem, s>>>(d_descs, item_desc, ks, ks_stride, gates, out, out_idx, \
+                                                       (int)count);
   if (logn == 11 && d1) {
     if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
     else if (variant == 1) { PZ_LAUNCH(11, true, 3, 256) }

@@ -39,6 +39,13 @@ struct KsParams {
   const u32 *in0, *in1;
 };
 
+// One CTA of the ragged key switch: `count` (<= 16) consecutive items of
+// one session descriptor, starting at item `first`.
+struct KsTile {
+  u32 desc, first, count;
+};
+constexpr int KS_TILE_CT = 16;
+
 constexpr u32 WIRE_NEG = 0x80000000u;
 constexpr u32 WIRE_MASK = 0x7fffffffu;
 
@@ -63,6 +70,14 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
 // launch-shape variants of the production blind rotation (registers per
 // thread capped for 2, 3 or 4 CTAs of 256 threads per SM)
 constexpr int PBS_VARIANTS = 3;
+// Ragged batches (several sessions / parameter sets in one launch): per-item
+// descriptors in device memory; max_* bound the sizes over the descriptors.
+cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, u32 max_n,
+                             u32 max_d, const unsigned char *gates, const u64 *wires, const u32 *in0,
+                             const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s);
+cudaError_t launch_pbs_ragged(int logn, bool d1, const BrParams *d_descs, const u32 *item_desc, u32 max_br_q,
+                              u32 max_n, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out,
+                              const u32 *out_idx, size_t count, int grid_limit, cudaStream_t s, int variant);
 cudaError_t launch_not(const u64 *in, u64 *out, size_t words, u64 q, cudaStream_t s);
 cudaError_t launch_imad_probe(int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s);
 // per launch: blocks * threads * iters * 16 * 8 multiply-adds

@@ -1,0 +1,673 @@
+// pz_server.cu -- multi-session executor: continuous batching of circuits
+// from many sessions (each with its own server key, any production parameter
+// set) on one device.
+//
+// The reference evaluates one gate at a time, in the calling thread, against
+// the one global server key of that thread's parameter set
+// (bool/mp_api.rs:20-26, evaluator.rs:2136-2323).  Here every submitted
+// circuit is a job bound to a session (a context + a device-resident server
+// key).  A step
+//   1. admits pending jobs in arrival order while their wires fit the device
+//      arena (admission by device bytes; keys are already resident),
+//   2. collects the next level of every admitted job, sorts the gates by
+//      session and runs them as ONE ragged key-switch launch (tiles of one
+//      session each) plus ONE ragged blind-rotation launch (each CTA loads
+//      its gate's parameter set and key from a descriptor table), chunked at
+//      max_items gates,
+//   3. retires jobs whose last level ran: outputs are gathered (not() applied)
+//      and copied out, their arena ranges are freed.
+// Jobs admitted while others are mid-circuit join at their own level 1, so
+// work of requests arriving at different times overlaps on the device.
+// A dry-run server (device PZ_SERVER_DRY_RUN) runs the same admission and
+// level bookkeeping without a GPU.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <random>
+#include <unordered_map>
+#include <vector>
+
+#include "pz_internal.h"
+
+using pz::u32;
+using pz::u64;
+
+namespace {
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+struct pz_server {
+  int device = 0;
+  bool dry = false;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  struct Session {
+    pz_ctx *ctx = nullptr;
+    const pz_key *key = nullptr;
+    int param_id = 0;
+    size_t key_bytes = 0;
+  };
+  std::vector<Session> sessions;
+  int logn = -1;
+  bool d1 = true;
+  size_t L = 0;
+  u64 q = 0;
+  u32 max_n = 0, max_br_q = 0, max_d = 0, ks_stride = 0;
+  pz::BrParams *d_br = nullptr;
+  pz::KsParams *d_ksp = nullptr;
+
+  // wire arena: slots of L words
+  u64 *d_arena = nullptr;
+  size_t arena_slots = 0, slots_used = 0;
+  std::map<size_t, size_t> free_ranges;  // start -> length
+
+  // per-chunk staging (double-buffered host->device item arrays)
+  size_t max_items = 0;
+  size_t arena_bytes_req = 0;
+  int flip = 0;
+  u32 ksout_stride = 0;
+  unsigned char *h_buf[2] = {nullptr, nullptr};
+  unsigned char *d_buf[2] = {nullptr, nullptr};
+  cudaEvent_t buf_free[2] = {nullptr, nullptr};
+  u32 *d_ksout = nullptr;
+  u64 *d_gather = nullptr;
+  size_t gather_cap = 0;  // ciphertexts
+  u32 *d_outref = nullptr;
+  size_t outref_cap = 0;
+
+  int pbs_variant = 0, grid_limit = 0;
+
+  struct Job {
+    u64 id = 0;
+    u32 session = 0;
+    pz_circuit *c = nullptr;
+    pz::CircuitView v;
+    const u64 *in = nullptr;
+    u64 *out = nullptr;
+    int device_io = 0;
+    size_t base = 0, slots = 0, level = 0;
+    int state = 0;  // 0 pending, 1 running, 2 done, 3 failed
+    double t_submit = 0, t_admit = 0, t_done = 0;
+  };
+  std::deque<Job *> pending;
+  std::vector<Job *> active;
+  std::unordered_map<u64, Job *> jobs;
+  u64 next_id = 1;
+  size_t n_done = 0, n_failed = 0;
+  u64 steps = 0, gates = 0, launches = 0;
+
+  pz_status fail(pz_status st, const std::string &m) {
+    err = m;
+    return st;
+  }
+  pz_status cuda(const char *what, cudaError_t e) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return PZ_ERR_CUDA;
+  }
+
+  // first fit over the free slot ranges
+  bool alloc(size_t n, size_t *base) {
+    for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it) {
+      if (it->second >= n) {
+        *base = it->first;
+        const size_t rest = it->second - n, start = it->first + n;
+        free_ranges.erase(it);
+        if (rest) free_ranges[start] = rest;
+        slots_used += n;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t base, size_t n) {
+    if (!n) return;
+    slots_used -= n;
+    auto it = free_ranges.emplace(base, n).first;
+    auto next = std::next(it);
+    if (next != free_ranges.end() && it->first + it->second == next->first) {
+      it->second += next->second;
+      free_ranges.erase(next);
+    }
+    if (it != free_ranges.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) {
+        prev->second += it->second;
+        free_ranges.erase(it);
+      }
+    }
+  }
+
+  // packed item arrays of one chunk: gates | in0 | in1 | out | desc | tiles
+  struct Layout {
+    size_t gate, in0, in1, out, desc, tiles, total;
+  };
+  Layout layout(size_t cap) const {
+    Layout l;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+      const size_t at = o;
+      o += (bytes + 255) & ~(size_t)255;
+      return at;
+    };
+    l.gate = take(cap);
+    l.in0 = take(cap * 4);
+    l.in1 = take(cap * 4);
+    l.out = take(cap * 4);
+    l.desc = take(cap * 4);
+    l.tiles = take((cap + 1) * sizeof(pz::KsTile));
+    l.total = o;
+    return l;
+  }
+
+  ~pz_server() {
+    for (auto &kv : jobs) delete kv.second;
+    if (!dry) {
+      cudaSetDevice(device);
+      if (stream) cudaStreamSynchronize(stream);
+      for (int b = 0; b < 2; b++) {
+        if (h_buf[b]) cudaFreeHost(h_buf[b]);
+        if (d_buf[b]) cudaFree(d_buf[b]);
+        if (buf_free[b]) cudaEventDestroy(buf_free[b]);
+      }
+      cudaFree(d_arena);
+      cudaFree(d_ksout);
+      cudaFree(d_gather);
+      cudaFree(d_outref);
+      cudaFree(d_br);
+      cudaFree(d_ksp);
+      if (stream) cudaStreamDestroy(stream);
+    }
+  }
+};
+
+namespace {
+
+size_t key_bytes_of(const pz_params &P) {
+  // RGSW + auto keys (u64, device form) + KSK (u32 rows of ks_stride words)
+  return (size_t)P.lwe_n * P.rgsw_rows * P.rlwe_n * 8 + (size_t)P.n_auto_keys * P.auto_rows * P.rlwe_n * 8 +
+         (size_t)P.lwe_d * P.rlwe_n * pz::ks_stride(P) * 4;
+}
+
+// Re-upload the descriptor tables after a session was added.
+pz_status upload_descs(pz_server *s) {
+  if (s->dry) return PZ_OK;
+  cudaError_t e = cudaStreamSynchronize(s->stream);  // no launch may still read the old tables
+  if (e != cudaSuccess) return s->cuda("cudaStreamSynchronize", e);
+  std::vector<pz::BrParams> br(s->sessions.size());
+  std::vector<pz::KsParams> ks(s->sessions.size());
+  for (size_t i = 0; i < s->sessions.size(); i++) {
+    const auto &se = s->sessions[i];
+    br[i] = se.ctx->br;
+    br[i].rgsw = se.key->d_rgsw;
+    br[i].autos = se.key->d_autos;
+    br[i].out_idx = nullptr;
+    ks[i] = se.ctx->ks;
+    ks[i].ksk = se.key->d_ksk;
+  }
+  cudaFree(s->d_br);
+  cudaFree(s->d_ksp);
+  s->d_br = nullptr;
+  s->d_ksp = nullptr;
+  if ((e = cudaMalloc(&s->d_br, br.size() * sizeof(pz::BrParams))) != cudaSuccess) return s->cuda("cudaMalloc", e);
+  if ((e = cudaMalloc(&s->d_ksp, ks.size() * sizeof(pz::KsParams))) != cudaSuccess) return s->cuda("cudaMalloc", e);
+  if ((e = cudaMemcpy(s->d_br, br.data(), br.size() * sizeof(pz::BrParams), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return s->cuda("cudaMemcpy", e);
+  if ((e = cudaMemcpy(s->d_ksp, ks.data(), ks.size() * sizeof(pz::KsParams), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return s->cuda("cudaMemcpy", e);
+  return PZ_OK;
+}
+
+pz_status add_session_common(pz_server *s, int param_id, pz_ctx *ctx, const pz_key *key, uint32_t *session) {
+  pz_params P;
+  if (pz_param_get(param_id, &P) != PZ_OK) return s->fail(PZ_ERR_INVALID_ARGUMENT, "bad parameter set");
+  const int logn = (int)__builtin_ctzll(P.rlwe_n);
+  const bool d1 = P.rlrg_d_a == 1 && P.rlrg_d_b == 1 && P.auto_d == 1;
+  if (s->logn >= 0 && (logn != s->logn || d1 != s->d1 || P.rlwe_q != s->q))
+    return s->fail(PZ_ERR_NOT_SUPPORTED, "all sessions of a server share the ring (N, Q) and decomposition shape");
+  if (s->logn < 0) {
+    s->logn = logn;
+    s->d1 = d1;
+    s->L = (size_t)P.rlwe_n + 1;
+    s->q = P.rlwe_q;
+  }
+  pz_server::Session se;
+  se.ctx = ctx;
+  se.key = key;
+  se.param_id = param_id;
+  se.key_bytes = key ? key->bytes : key_bytes_of(P);
+  s->sessions.push_back(se);
+  s->max_n = std::max(s->max_n, P.lwe_n);
+  s->max_br_q = std::max(s->max_br_q, P.br_q);
+  s->max_d = std::max(s->max_d, P.lwe_d);
+  s->ks_stride = std::max(s->ks_stride, pz::ks_stride(P));
+  pz_status st = upload_descs(s);
+  if (st != PZ_OK) {
+    s->sessions.pop_back();
+    return st;
+  }
+  if (session) *session = (uint32_t)(s->sessions.size() - 1);
+  return PZ_OK;
+}
+
+pz_status ensure_arena(pz_server *s, size_t arena_bytes) {
+  if (s->arena_slots) return PZ_OK;
+  s->arena_slots = arena_bytes / (s->L * 8);
+  if (s->arena_slots == 0) return s->fail(PZ_ERR_INVALID_ARGUMENT, "arena smaller than one ciphertext");
+  s->free_ranges.clear();
+  s->free_ranges[0] = s->arena_slots;
+  if (s->dry) return PZ_OK;
+  cudaError_t e = cudaMalloc(&s->d_arena, s->arena_slots * s->L * 8);
+  if (e != cudaSuccess) {
+    s->arena_slots = 0;
+    return s->cuda("arena cudaMalloc", e);
+  }
+  return PZ_OK;
+}
+
+// Admit pending jobs in arrival order while their wires fit.
+pz_status admit(pz_server *s) {
+  while (!s->pending.empty()) {
+    pz_server::Job *j = s->pending.front();
+    const size_t need = j->v.n_inputs + j->v.n_gates;
+    if (need > s->arena_slots) {  // can never fit
+      j->state = 3;
+      j->t_done = now_ms();
+      s->n_failed++;
+      s->pending.pop_front();
+      continue;
+    }
+    size_t base;
+    if (!s->alloc(std::max<size_t>(need, 1), &base)) break;
+    j->base = base;
+    j->slots = std::max<size_t>(need, 1);
+    j->level = 0;
+    j->state = 1;
+    j->t_admit = now_ms();
+    if (!s->dry && j->v.n_inputs) {
+      cudaError_t e = cudaMemcpyAsync(s->d_arena + base * s->L, j->in, j->v.n_inputs * s->L * 8,
+                                      j->device_io ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->stream);
+      if (e != cudaSuccess) return s->cuda("input copy", e);
+    }
+    s->pending.pop_front();
+    s->active.push_back(j);
+  }
+  return PZ_OK;
+}
+
+struct Item {
+  u32 session;
+  unsigned char gate;
+  u32 in0, in1, out;
+};
+
+// Run the sorted items of one step, in chunks of max_items.
+pz_status run_items(pz_server *s, const std::vector<Item> &items) {
+  if (s->dry || items.empty()) return PZ_OK;
+  const pz_server::Layout lay = s->layout(s->max_items);
+  for (size_t c0 = 0; c0 < items.size(); c0 += s->max_items) {
+    const size_t n = std::min(s->max_items, items.size() - c0);
+    const int b = s->flip;
+    s->flip ^= 1;
+    cudaError_t e = cudaEventSynchronize(s->buf_free[b]);  // its previous chunk has been read
+    if (e != cudaSuccess) return s->cuda("cudaEventSynchronize", e);
+    unsigned char *h = s->h_buf[b];
+    unsigned char *hg = h + lay.gate;
+    u32 *h0 = (u32 *)(h + lay.in0), *h1 = (u32 *)(h + lay.in1), *ho = (u32 *)(h + lay.out);
+    u32 *hd = (u32 *)(h + lay.desc);
+    pz::KsTile *ht = (pz::KsTile *)(h + lay.tiles);
+    size_t ntiles = 0;
+    for (size_t i = 0; i < n; i++) {
+      const Item &it = items[c0 + i];
+      hg[i] = it.gate;
+      h0[i] = it.in0;
+      h1[i] = it.in1;
+      ho[i] = it.out;
+      hd[i] = it.session;
+      if (ntiles == 0 || ht[ntiles - 1].desc != it.session || ht[ntiles - 1].count == (u32)pz::KS_TILE_CT)
+        ht[ntiles++] = pz::KsTile{it.session, (u32)i, 0};
+      ht[ntiles - 1].count++;
+    }
+    unsigned char *d = s->d_buf[b];
+    if ((e = cudaMemcpyAsync(d, h, lay.total, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess)
+      return s->cuda("item upload", e);
+    if ((e = cudaEventRecord(s->buf_free[b], s->stream)) != cudaSuccess) return s->cuda("cudaEventRecord", e);
+    e = pz::launch_ks_ragged(s->d_ksp, (const pz::KsTile *)(d + lay.tiles), ntiles, s->max_n, s->max_d,
+                             d + lay.gate, s->d_arena, (const u32 *)(d + lay.in0), (const u32 *)(d + lay.in1),
+                             s->d_ksout, s->ks_stride, s->stream);
+    if (e != cudaSuccess) return s->cuda("launch_ks_ragged", e);
+    e = pz::launch_pbs_ragged(s->logn, s->d1, s->d_br, (const u32 *)(d + lay.desc), s->max_br_q, s->max_n,
+                              s->d_ksout, s->ks_stride, d + lay.gate, s->d_arena, (const u32 *)(d + lay.out), n,
+                              s->grid_limit, s->stream, s->pbs_variant);
+    if (e != cudaSuccess) return s->cuda("launch_pbs_ragged", e);
+    s->launches += 2;
+  }
+  return PZ_OK;
+}
+
+// Gather the outputs of finished jobs (on the stream; copies complete at the
+// step's final synchronisation).
+pz_status finish_outputs(pz_server *s, const std::vector<pz_server::Job *> &fin) {
+  if (s->dry || fin.empty()) return PZ_OK;
+  size_t host_outs = 0, refs = 0;
+  for (auto *j : fin) {
+    refs += j->v.n_outputs;
+    if (!j->device_io) host_outs += j->v.n_outputs;
+  }
+  cudaError_t e;
+  if (refs > s->outref_cap) {
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return s->cuda("cudaStreamSynchronize", e);
+    cudaFree(s->d_outref);
+    s->d_outref = nullptr;
+    s->outref_cap = 0;
+    if ((e = cudaMalloc(&s->d_outref, refs * 4)) != cudaSuccess) return s->cuda("cudaMalloc", e);
+    s->outref_cap = refs;
+  }
+  if (host_outs > s->gather_cap) {
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return s->cuda("cudaStreamSynchronize", e);
+    cudaFree(s->d_gather);
+    s->d_gather = nullptr;
+    s->gather_cap = 0;
+    if ((e = cudaMalloc(&s->d_gather, host_outs * s->L * 8)) != cudaSuccess) return s->cuda("cudaMalloc", e);
+    s->gather_cap = host_outs;
+  }
+  std::vector<u32> h(refs);
+  size_t r = 0;
+  for (auto *j : fin)
+    for (size_t i = 0; i < j->v.n_outputs; i++) {
+      const u32 ref = j->v.outref[i];
+      h[r++] = (u32)(j->base + (ref & pz::WIRE_MASK)) | (ref & pz::WIRE_NEG);
+    }
+  if (refs && (e = cudaMemcpyAsync(s->d_outref, h.data(), refs * 4, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess)
+    return s->cuda("outref upload", e);
+  size_t ro = 0, go = 0;
+  for (auto *j : fin) {
+    const size_t no = j->v.n_outputs;
+    if (!no) continue;
+    u64 *dst = j->device_io ? j->out : s->d_gather + go * s->L;
+    if ((e = pz::launch_gather(s->d_arena, s->d_outref + ro, dst, no, s->L, s->q, s->stream)) != cudaSuccess)
+      return s->cuda("gather", e);
+    if (!j->device_io) {
+      if ((e = cudaMemcpyAsync(j->out, dst, no * s->L * 8, cudaMemcpyDeviceToHost, s->stream)) != cudaSuccess)
+        return s->cuda("output copy", e);
+      go += no;
+    }
+    ro += no;
+  }
+  return PZ_OK;  // complete at the step's stream synchronisation
+}
+
+}  // namespace
+
+extern "C" {
+
+pz_status pz_server_create(int device, size_t arena_bytes, size_t max_items, pz_server **out) {
+  if (!out || max_items == 0) return PZ_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  pz_server *s = new pz_server();
+  s->dry = device == PZ_SERVER_DRY_RUN;
+  s->device = s->dry ? 0 : device;
+  s->max_items = max_items;
+  s->arena_slots = 0;
+  s->arena_bytes_req = arena_bytes;  // slots are sized by the first session's ring (L words)
+  if (!s->dry) {
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      s->dry = true;  // nothing device-side to release
+      delete s;
+      return PZ_ERR_CUDA;
+    }
+    const pz_server::Layout lay = s->layout(max_items);
+    for (int b = 0; b < 2; b++) {
+      if (cudaMallocHost(&s->h_buf[b], lay.total) != cudaSuccess || cudaMalloc(&s->d_buf[b], lay.total) != cudaSuccess ||
+          cudaEventCreateWithFlags(&s->buf_free[b], cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventRecord(s->buf_free[b], s->stream) != cudaSuccess) {
+        delete s;
+        return PZ_ERR_OUT_OF_MEMORY;
+      }
+    }
+  }
+  *out = s;
+  return PZ_OK;
+}
+
+void pz_server_destroy(pz_server *s) { delete s; }
+
+const char *pz_server_last_error(const pz_server *s) { return s ? s->err.c_str() : "no server"; }
+
+pz_status pz_server_add_session(pz_server *s, pz_ctx *ctx, const pz_key *key, uint32_t *session) {
+  if (!s || !ctx || !key) return PZ_ERR_INVALID_ARGUMENT;
+  if (s->dry) return s->fail(PZ_ERR_INVALID_ARGUMENT, "dry-run server: use pz_server_add_virtual_session");
+  if (key->ctx != ctx) return s->fail(PZ_ERR_KEY_MISMATCH, "key does not belong to this context");
+  if (ctx->device != s->device) return s->fail(PZ_ERR_INVALID_ARGUMENT, "context is on another device");
+  cudaSetDevice(s->device);
+  pz_status st = add_session_common(s, ctx->param_id, ctx, key, session);
+  if (st != PZ_OK) return st;
+  st = ensure_arena(s, s->arena_bytes_req);
+  if (st != PZ_OK) return st;
+  if (s->ks_stride > s->ksout_stride) {  // key-switch scratch for the widest session
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->d_ksout);
+    s->d_ksout = nullptr;
+    s->ksout_stride = 0;
+    cudaError_t e = cudaMalloc(&s->d_ksout, s->max_items * (size_t)s->ks_stride * 4);
+    if (e != cudaSuccess) return s->cuda("cudaMalloc", e);
+    s->ksout_stride = s->ks_stride;
+  }
+  return PZ_OK;
+}
+
+pz_status pz_server_add_virtual_session(pz_server *s, int param_id, uint32_t *session) {
+  if (!s) return PZ_ERR_INVALID_ARGUMENT;
+  if (!s->dry) return s->fail(PZ_ERR_INVALID_ARGUMENT, "virtual sessions exist only on a dry-run server");
+  pz_status st = add_session_common(s, param_id, nullptr, nullptr, session);
+  if (st != PZ_OK) return st;
+  return ensure_arena(s, s->arena_bytes_req);
+}
+
+pz_status pz_server_submit(pz_server *s, uint32_t session, pz_circuit *c, const uint64_t *inputs,
+                           uint64_t *outputs, int device_io, uint64_t *job) {
+  if (!s || !c) return PZ_ERR_INVALID_ARGUMENT;
+  if (session >= s->sessions.size()) return s->fail(PZ_ERR_INVALID_ARGUMENT, "unknown session");
+  pz_server::Job *j = new pz_server::Job();
+  if (!pz::circuit_view(c, &j->v)) {
+    delete j;
+    return s->fail(PZ_ERR_INVALID_ARGUMENT, "bad circuit");
+  }
+  if (!s->dry && ((j->v.n_inputs && !inputs) || (j->v.n_outputs && !outputs))) {
+    delete j;
+    return s->fail(PZ_ERR_INVALID_ARGUMENT, "NULL job buffer");
+  }
+  j->id = s->next_id++;
+  j->session = session;
+  j->c = c;
+  j->in = inputs;
+  j->out = outputs;
+  j->device_io = device_io;
+  j->t_submit = now_ms();
+  s->jobs[j->id] = j;
+  s->pending.push_back(j);
+  if (job) *job = j->id;
+  return PZ_OK;
+}
+
+pz_status pz_server_step(pz_server *s, size_t *gates_run) {
+  if (!s) return PZ_ERR_INVALID_ARGUMENT;
+  if (gates_run) *gates_run = 0;
+  if (!s->dry) cudaSetDevice(s->device);
+  pz_status st = admit(s);
+  if (st != PZ_OK) return st;
+  // next level of every admitted job, sorted by session (counting sort)
+  std::vector<size_t> per(s->sessions.size() + 1, 0);
+  for (auto *j : s->active)
+    if (j->level < j->v.levels) per[j->session + 1] += j->v.level_off[j->level + 1] - j->v.level_off[j->level];
+  for (size_t i = 1; i < per.size(); i++) per[i] += per[i - 1];
+  const size_t total = per.back();
+  std::vector<Item> items(total);
+  for (auto *j : s->active) {
+    if (j->level >= j->v.levels) continue;
+    const size_t a = j->v.level_off[j->level], b = j->v.level_off[j->level + 1];
+    size_t &pos = per[j->session];
+    for (size_t g = a; g < b; g++) {
+      Item &it = items[pos++];
+      it.session = j->session;
+      it.gate = j->v.type[g];
+      it.in0 = (u32)(j->base + (j->v.in0[g] & pz::WIRE_MASK)) | (j->v.in0[g] & pz::WIRE_NEG);
+      it.in1 = (u32)(j->base + (j->v.in1[g] & pz::WIRE_MASK)) | (j->v.in1[g] & pz::WIRE_NEG);
+      it.out = (u32)(j->base + j->v.out[g]);
+    }
+    j->level++;
+  }
+  st = run_items(s, items);
+  if (st != PZ_OK) return st;
+  std::vector<pz_server::Job *> fin, still;
+  for (auto *j : s->active) (j->level >= j->v.levels ? fin : still).push_back(j);
+  st = finish_outputs(s, fin);
+  if (st != PZ_OK) return st;
+  if (!s->dry) {
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return s->cuda("step", e);
+  }
+  const double t = now_ms();
+  for (auto *j : fin) {
+    j->state = 2;
+    j->t_done = t;
+    s->release(j->base, j->slots);
+    s->n_done++;
+  }
+  s->active.swap(still);
+  s->steps++;
+  s->gates += total;
+  if (gates_run) *gates_run = total;
+  return PZ_OK;
+}
+
+pz_status pz_server_job_status(pz_server *s, uint64_t job, int *state, double *latency_ms, double *queue_ms) {
+  if (!s) return PZ_ERR_INVALID_ARGUMENT;
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) return s->fail(PZ_ERR_INVALID_ARGUMENT, "unknown job");
+  const pz_server::Job *j = it->second;
+  if (state) *state = j->state;
+  if (latency_ms) *latency_ms = j->state >= 2 ? j->t_done - j->t_submit : -1.0;
+  if (queue_ms) *queue_ms = j->state >= 1 && j->state != 3 ? j->t_admit - j->t_submit : -1.0;
+  return PZ_OK;
+}
+
+pz_status pz_server_forget(pz_server *s, uint64_t job) {
+  if (!s) return PZ_ERR_INVALID_ARGUMENT;
+  auto it = s->jobs.find(job);
+  if (it == s->jobs.end()) return s->fail(PZ_ERR_INVALID_ARGUMENT, "unknown job");
+  if (it->second->state < 2) return s->fail(PZ_ERR_INVALID_ARGUMENT, "job not finished");
+  delete it->second;
+  s->jobs.erase(it);
+  return PZ_OK;
+}
+
+pz_status pz_server_stats_get(pz_server *s, pz_server_stats *out) {
+  if (!s || !out) return PZ_ERR_INVALID_ARGUMENT;
+  std::memset(out, 0, sizeof(*out));
+  out->pending = s->pending.size();
+  out->active = s->active.size();
+  out->done = s->n_done;
+  out->failed = s->n_failed;
+  out->arena_slots = s->arena_slots;
+  out->arena_slots_used = s->slots_used;
+  out->arena_bytes = s->arena_slots * s->L * 8;
+  out->sessions = s->sessions.size();
+  for (auto &se : s->sessions) out->key_bytes += se.key_bytes;
+  out->steps = s->steps;
+  out->gates = s->gates;
+  out->launches = s->launches;
+  return PZ_OK;
+}
+
+pz_status pz_server_set_launch(pz_server *s, int pbs_variant, int grid_limit) {
+  if (!s || pbs_variant < 0 || pbs_variant >= pz::PBS_VARIANTS || grid_limit < 0) return PZ_ERR_INVALID_ARGUMENT;
+  s->pbs_variant = pbs_variant;
+  s->grid_limit = grid_limit;
+  return PZ_OK;
+}
+
+pz_status pz_server_autotune(pz_server *s, size_t batch, int *variant, int *grid_limit, double *best_ms) {
+  if (!s || batch == 0) return PZ_ERR_INVALID_ARGUMENT;
+  if (s->dry) return s->fail(PZ_ERR_NOT_SUPPORTED, "dry-run server");
+  if (s->sessions.empty()) return s->fail(PZ_ERR_INVALID_ARGUMENT, "no session");
+  if (!s->active.empty()) return s->fail(PZ_ERR_INVALID_ARGUMENT, "autotune needs an idle server");
+  batch = std::min(batch, std::min(s->max_items, s->arena_slots));
+  cudaSetDevice(s->device);
+  // synthetic key-switched LWEs (uniform mod each session's q_ks), gates
+  // spread over the sessions, outputs into arena slots [0, batch)
+  std::mt19937_64 rng(0x7A11u);
+  std::vector<u32> ks((size_t)batch * s->ks_stride, 0), desc(batch), outi(batch);
+  std::vector<unsigned char> g(batch);
+  for (size_t i = 0; i < batch; i++) {
+    desc[i] = (u32)(i % s->sessions.size());
+    const pz_params &P = s->sessions[desc[i]].ctx->P;
+    for (u32 c = 0; c <= P.lwe_n; c++) ks[i * s->ks_stride + c] = (u32)(rng() % P.lwe_q);
+    g[i] = (unsigned char)(rng() % 6);
+    outi[i] = (u32)i;
+  }
+  u32 *d_ks = nullptr, *d_desc = nullptr, *d_out = nullptr;
+  unsigned char *d_g = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  pz_status st = PZ_OK;
+  double best = 1e30;
+  int bv = s->pbs_variant, bg = s->grid_limit;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  const int grids[2] = {0, 2 * sms};
+  auto CK = [&](cudaError_t e, const char *w) {
+    if (e != cudaSuccess && st == PZ_OK) st = s->cuda(w, e);
+    return e == cudaSuccess;
+  };
+  if (CK(cudaMalloc(&d_ks, ks.size() * 4), "cudaMalloc") && CK(cudaMalloc(&d_desc, batch * 4), "cudaMalloc") &&
+      CK(cudaMalloc(&d_out, batch * 4), "cudaMalloc") && CK(cudaMalloc(&d_g, batch), "cudaMalloc") &&
+      CK(cudaMemcpy(d_ks, ks.data(), ks.size() * 4, cudaMemcpyHostToDevice), "cudaMemcpy") &&
+      CK(cudaMemcpy(d_desc, desc.data(), batch * 4, cudaMemcpyHostToDevice), "cudaMemcpy") &&
+      CK(cudaMemcpy(d_out, outi.data(), batch * 4, cudaMemcpyHostToDevice), "cudaMemcpy") &&
+      CK(cudaMemcpy(d_g, g.data(), batch, cudaMemcpyHostToDevice), "cudaMemcpy") &&
+      CK(cudaEventCreate(&a), "cudaEventCreate") && CK(cudaEventCreate(&b), "cudaEventCreate")) {
+    const int nv = (s->logn == 11 && s->d1) ? pz::PBS_VARIANTS : 1;
+    for (int v = 0; v < nv && st == PZ_OK; v++) {
+      for (int gi = 0; gi < 2 && st == PZ_OK; gi++) {
+        auto launch = [&]() {
+          return pz::launch_pbs_ragged(s->logn, s->d1, s->d_br, d_desc, s->max_br_q, s->max_n, d_ks, s->ks_stride,
+                                       d_g, s->d_arena, d_out, batch, grids[gi], s->stream, v);
+        };
+        if (!CK(launch(), "launch_pbs_ragged")) break;  // warm-up
+        if (!CK(cudaEventRecord(a, s->stream), "cudaEventRecord")) break;
+        for (int r = 0; r < 2; r++)
+          if (!CK(launch(), "launch_pbs_ragged")) break;
+        if (!CK(cudaEventRecord(b, s->stream), "cudaEventRecord")) break;
+        if (!CK(cudaEventSynchronize(b), "cudaEventSynchronize")) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms / 2 < best) {
+          best = ms / 2;
+          bv = v;
+          bg = grids[gi];
+        }
+      }
+    }
+  }
+  cudaStreamSynchronize(s->stream);
+  cudaFree(d_ks);
+  cudaFree(d_desc);
+  cudaFree(d_out);
+  cudaFree(d_g);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (st != PZ_OK) return st;
+  s->pbs_variant = bv;
+  s->grid_limit = bg;
+  if (variant) *variant = bv;
+  if (grid_limit) *grid_limit = bg;
+  if (best_ms) *best_ms = best;
+  return PZ_OK;
+}
+
+}  // extern "C"

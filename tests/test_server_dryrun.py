@@ -1,0 +1,122 @@
+"""Multi-session executor bookkeeping on the host (dry-run server, no GPU):
+admission by device bytes in arrival order, one circuit level per job per
+step, continuous batching of late arrivals, latency accounting."""
+import pytest
+
+from conftest import pz
+
+
+def u8_circuit(op):
+    P = pz()
+    C = P.Circuit()
+    a, b = C.input_u8(), C.input_u8()
+    if op == "add":
+        C.outputs(C.u8_add(a, b))
+    elif op == "mul":
+        C.outputs(C.u8_mul(a, b))
+    elif op == "lt":
+        C.output(C.u8_cmp("lt", a, b))
+    elif op == "div_rem":
+        q, r, f = C.u8_div_rem(a, b)
+        C.outputs(q)
+        C.outputs(r)
+        C.output(f)
+    return C
+
+
+def slots(C):
+    i = C.info()
+    return i["inputs"] + i["gates"]
+
+
+def L_of(param):
+    return pz().params(param).rlwe_n + 1
+
+
+def make_server(arena_slots, params=("I_2P_LB_SR", "NI_8P"), max_items=4096):
+    P = pz()
+    S = P.Server(device=P.DRY_RUN, arena_bytes=arena_slots * L_of(params[0]) * 8, max_items=max_items)
+    sids = [S.add_virtual_session(P.param_id(p)) for p in params]
+    return S, sids
+
+
+def test_levels_advance_one_per_step():
+    S, (s0, s1) = make_server(1 << 16)
+    circs = [u8_circuit("add"), u8_circuit("lt"), u8_circuit("mul")]
+    jobs = [S.submit(s0 if i % 2 == 0 else s1, c) for i, c in enumerate(circs)]
+    sizes = [c.level_sizes() for c in circs]
+    depth = max(len(s) for s in sizes)
+    for step in range(depth):
+        ran = S.step()
+        assert ran == sum(s[step] for s in sizes if step < len(s))
+        for j, s in zip(jobs, sizes):
+            want = pz().server.DONE if step + 1 >= len(s) else pz().server.RUNNING
+            assert S.status(j)["state"] == want
+    st = S.stats()
+    assert st["done"] == 3 and st["active"] == 0 and st["pending"] == 0
+    assert st["arena_slots_used"] == 0
+    assert st["gates"] == sum(c.info()["gates"] for c in circs)
+
+
+def test_admission_by_device_bytes_fifo():
+    a = u8_circuit("mul")
+    need = slots(a)
+    S, (s0, _) = make_server(2 * need + need // 2)  # room for two such jobs, not three
+    jobs = [S.submit(s0, a) for _ in range(3)]
+    S.step()
+    states = [S.status(j)["state"] for j in jobs]
+    assert states == [pz().server.RUNNING, pz().server.RUNNING, pz().server.PENDING]
+    assert S.stats()["arena_slots_used"] == 2 * need
+    S.run_until_idle()
+    assert all(S.status(j)["state"] == pz().server.DONE for j in jobs)
+    # the third job waited for a whole circuit: it queued, the first two did not
+    assert S.status(jobs[2])["queue_ms"] >= S.status(jobs[0])["queue_ms"]
+    assert S.stats()["arena_slots_used"] == 0
+
+
+def test_job_larger_than_arena_fails_without_blocking_others():
+    big, small = u8_circuit("mul"), u8_circuit("lt")
+    S, (s0, s1) = make_server(slots(big) - 1)
+    jb = S.submit(s0, big)
+    js = S.submit(s1, small)
+    S.run_until_idle()
+    assert S.status(jb)["state"] == pz().server.FAILED
+    assert S.status(js)["state"] == pz().server.DONE
+    assert S.stats()["failed"] == 1
+
+
+def test_late_arrival_joins_running_batch():
+    m, l = u8_circuit("mul"), u8_circuit("lt")
+    ms, ls = m.level_sizes(), l.level_sizes()
+    S, (s0, s1) = make_server(1 << 16)
+    S.submit(s0, m)
+    for k in range(3):
+        assert S.step() == ms[k]
+    S.submit(s1, l)  # arrives while the multiplication is mid-circuit
+    assert S.step() == ms[3] + ls[0]  # one step carries both sessions' gates
+    assert S.step() == ms[4] + ls[1]
+
+
+def test_stats_and_forget():
+    S, (s0, s1) = make_server(1 << 14)
+    st = S.stats()
+    assert st["sessions"] == 2
+    P = pz()
+    assert st["key_bytes"] > 2 * P.params("I_2P_LB_SR").lwe_n * 4 * 2048 * 8
+    j = S.submit(s0, u8_circuit("add"))
+    with pytest.raises(RuntimeError):
+        S.forget(j)  # not finished
+    S.run_until_idle()
+    lat = S.status(j)["latency_ms"]
+    assert lat >= 0
+    S.forget(j)
+    with pytest.raises(RuntimeError):
+        S.status(j)
+
+
+def test_mixed_ring_rejected():
+    P = pz()
+    S = P.Server(device=P.DRY_RUN, arena_bytes=1 << 24, max_items=64)
+    S.add_virtual_session(P.param_id("NI_8P"))
+    with pytest.raises(RuntimeError):
+        S.add_virtual_session(P.param_id("SP_TEST"))  # N = 512: another ring
