@@ -277,6 +277,218 @@ def plain_form(P, torch, device, seed=7):
             "p99_ms": float(np.percentile(lat, 99)), "config": "I_2P_LB_SR, 128 NAND, one gate per launch"}
 
 
+SERVING_PARAMS = ["I_2P_LB_SR", "I_4P", "I_8P", "NI_2P", "NI_4P_HB_FR", "NI_8P"]
+
+
+def microbench(P, torch, device, count=4096, reps=5):
+    """Kernel microbench: forward+inverse negacyclic NTT of `count` polynomials
+    (N = 2048, mod Q, seeded uniform), and `count` RLWE x RGSW external
+    products at InteractiveLTE2Party (key index i mod n)."""
+    p = P.params("I_2P_LB_SR")
+    N = p.rlwe_n
+    eng = P.Engine("I_2P_LB_SR", device=device)
+    rng = np.random.default_rng(0x11)
+    x = torch.from_numpy(rng.integers(0, p.rlwe_q, (count, N), dtype=np.uint64).view(np.int64)).cuda()
+    t = x.clone()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    eng.ntt_forward_device(t)
+    eng.ntt_backward_device(t)
+    torch.cuda.synchronize()
+    roundtrip_ok = bool(torch.equal(t, x))
+    ev[0].record()
+    for _ in range(reps):
+        eng.ntt_forward_device(t)
+    ev[1].record()
+    for _ in range(reps):
+        eng.ntt_backward_device(t)
+    ev[2].record()
+    torch.cuda.synchronize()
+    fwd_ms = ev[0].elapsed_time(ev[1]) / reps
+    inv_ms = ev[1].elapsed_time(ev[2]) / reps
+    logn = int(np.log2(N))
+    mm = count * ((N // 2) * logn + (N // 2) * logn + N)  # fwd + inv (N^-1 scaling counted as in the convention)
+    key = eng.upload_key(*synthetic_key(p, 0x5EED))
+    rl = torch.from_numpy(rng.integers(0, p.rlwe_q, (count, 2, N), dtype=np.uint64).view(np.int64)).cuda()
+    idx = torch.arange(count, dtype=torch.int32, device="cuda") % p.lwe_n
+    eng.rlwe_by_rgsw_device(key, rl, idx)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        eng.rlwe_by_rgsw_device(key, rl, idx)
+    b.record()
+    torch.cuda.synchronize()
+    ep_ms = a.elapsed_time(b) / reps
+    key.release()
+    eng.close()
+    return {"config": f"{count} polys N={N} mod Q fwd+inv NTT; {count} RLWE x RGSW at I_2P_LB_SR (index i mod n)",
+            "ntt_fwd_ms": fwd_ms, "ntt_inv_ms": inv_ms, "ntt_roundtrip_exact": roundtrip_ok,
+            "ntt_polys_per_s": count / ((fwd_ms + inv_ms) / 1e3),
+            "ntt_modmul_per_s": mm / ((fwd_ms + inv_ms) / 1e3),
+            "ntt_hbm_gbs": 4 * count * N * 8 / ((fwd_ms + inv_ms) / 1e3) / 1e9,
+            "ext_product_ms": ep_ms, "ext_products_per_s": count / (ep_ms / 1e3),
+            "ext_product_modmul_per_s": count * 57344 / (ep_ms / 1e3)}
+
+
+def u8_job(P, op):
+    C = P.Circuit()
+    a, b = C.input_u8(), C.input_u8()
+    if op == "add":
+        C.outputs(C.u8_add(a, b))
+    elif op == "mul":
+        C.outputs(C.u8_mul(a, b))
+    elif op == "lt":
+        C.output(C.u8_cmp("lt", a, b))
+    elif op == "div_rem":
+        q, r, f = C.u8_div_rem(a, b)
+        C.outputs(q)
+        C.outputs(r)
+        C.output(f)
+    return C
+
+
+def ragged_batch(P, device, per_session=64, params=("I_2P_LB_SR", "I_4P", "I_8P"), seed=4):
+    """Ragged batch: sessions of the 2-, 4- and 8-party interactive sets in
+    one server; per session `per_session` FheUint8 ops (add, mul, div_rem,
+    lt; 20 % of the div_rem jobs with an all-zero divisor ciphertext
+    pattern) submitted at once; every step is one ragged key-switch launch
+    plus one ragged blind-rotation launch across the sessions; the launch
+    shape comes from the server's autotuner."""
+    S = P.Server(device=device, arena_bytes=4 << 30, max_items=16384)
+    keep = []
+    for i, prm in enumerate(params):
+        p = P.params(prm)
+        eng = P.Engine(prm, device=device)
+        key = eng.upload_key(*synthetic_key(p, 0x5EED + i))
+        keep.append((eng, key, S.add_session(eng, key), p))
+    tune = S.autotune(2368)
+    rng = np.random.default_rng(seed)
+    ops = ["add", "mul", "div_rem", "lt"]
+    templates = {op: u8_job(P, op) for op in ops}
+    L = keep[0][3].rlwe_n + 1
+    pool = rng.integers(0, keep[0][3].rlwe_q, (64, L), dtype=np.uint64)
+    gates = 0
+    jobs = []
+    for eng, key, sid, p in keep:
+        for k in range(per_session):
+            op = ops[k % 4]
+            C = templates[op]
+            inp = pool[rng.integers(0, 64 - 16):][:16].copy()
+            if op == "div_rem" and rng.random() < 0.2:
+                inp[8:16] = pool[0]  # one ciphertext repeated as the divisor's 8 bits
+            jobs.append(S.submit(sid, C, inp))
+            gates += C.info()["gates"]
+    t0 = time.perf_counter()
+    steps = S.run_until_idle()
+    dt = time.perf_counter() - t0
+    st = S.stats()
+    S.close()
+    for eng, key, _, _ in keep:
+        key.release()
+        eng.close()
+    return {"value": gates / dt, "unit": "gate bootstraps/s", "gates": gates, "jobs": len(jobs), "steps": steps,
+            "launches": st["launches"], "seconds": dt, "autotune": tune,
+            "config": f"sessions {list(params)}, {per_session} jobs each (add/mul/div_rem/lt), all submitted at once"}
+
+
+def serving_circuit(P, target, rng):
+    """A circuit of about `target` gates composed of FheUint8 ops chained on
+    an accumulator (single gates fill the remainder)."""
+    C = P.Circuit()
+    acc = C.input_u8()
+    sizes = [("mul", 155), ("sub", 38), ("add", 37), ("lt", 35), ("mux", 24), ("eq", 15)]
+    made = 0
+    while made < target:
+        fit = [o for o, g in sizes if g <= target - made]
+        if not fit:
+            x = C.input()
+            w = C.gate(["nand", "xor", "or"][int(rng.integers(0, 3))], acc[made % 8], x)
+            acc[made % 8] = w
+            made += 1
+            continue
+        op = fit[int(rng.integers(0, len(fit)))]
+        b = C.input_u8()
+        if op == "mul":
+            acc = C.u8_mul(acc, b)
+        elif op == "sub":
+            acc = C.u8_sub(acc, b)
+        elif op == "add":
+            acc = C.u8_add(acc, b)
+        elif op == "lt":
+            acc[0] = C.u8_cmp("lt", acc, b)
+        elif op == "mux":
+            acc = C.u8_mux(acc, b, C.input())
+        elif op == "eq":
+            acc[0] = C.u8_cmp("eq", acc, b)
+        made = C.info()["gates"]
+    C.outputs(acc)
+    return C
+
+
+def serving(P, device, sessions=64, rate=40.0, seconds=10.0, seed=8):
+    """Serving: `sessions` sessions (cycling over the 2/4/8-party interactive
+    and non-interactive sets), each with its own device-resident server key;
+    Poisson arrivals at `rate` circuits/s for `seconds`, circuit sizes
+    uniform in [1, 300] gates; admission by device bytes; continuous batching
+    (one ragged launch pair per step).  Latency = completion - arrival."""
+    S = P.Server(device=device, arena_bytes=8 << 30, max_items=16384)
+    rng = np.random.default_rng(seed)
+    host_keys = {prm: synthetic_key(P.params(prm), 0x5EED + i) for i, prm in enumerate(SERVING_PARAMS)}
+    keep, sids = [], []
+    for k in range(sessions):
+        prm = SERVING_PARAMS[k % len(SERVING_PARAMS)]
+        eng = P.Engine(prm, device=device)
+        key = eng.upload_key(*host_keys[prm])
+        keep.append((eng, key))
+        sids.append(S.add_session(eng, key))
+    del host_keys
+    tune = S.autotune(2368)
+    key_bytes = S.stats()["key_bytes"]
+    templates = [serving_circuit(P, int(rng.integers(1, 301)), rng) for _ in range(48)]
+    L = keep[0][0].L
+    pool = rng.integers(0, keep[0][0].Q, (512, L), dtype=np.uint64)
+    n_arr = int(rng.poisson(rate * seconds))
+    arrivals = np.sort(rng.uniform(0, seconds, n_arr))
+    lat, inflight, gates_done = [], {}, 0
+    idx, t0 = 0, time.perf_counter()
+    steps, max_active, step_gates = 0, 0, []
+    while idx < n_arr or inflight:
+        now = time.perf_counter() - t0
+        while idx < n_arr and arrivals[idx] <= now:
+            C = templates[int(rng.integers(0, len(templates)))]
+            ni = C.info()["inputs"]
+            off = int(rng.integers(0, 512 - ni)) if ni < 512 else 0
+            j = S.submit(sids[int(rng.integers(0, sessions))], C, pool[off:off + ni])
+            inflight[j] = (arrivals[idx], C.info()["gates"])
+            idx += 1
+        if not inflight:
+            time.sleep(max(0.0, arrivals[idx] - (time.perf_counter() - t0)))
+            continue
+        step_gates.append(S.step())
+        steps += 1
+        st = S.stats()
+        max_active = max(max_active, st["active"])
+        tdone = time.perf_counter() - t0
+        for j in list(inflight):
+            if S.status(j)["state"] == 2:
+                a, g = inflight.pop(j)
+                lat.append((tdone - a) * 1e3)
+                gates_done += g
+                S.forget(j)
+    total = time.perf_counter() - t0
+    S.close()
+    for eng, key in keep:
+        key.release()
+        eng.close()
+    lat = np.array(lat)
+    return {"value": gates_done / total, "unit": "gate bootstraps/s", "circuits": len(lat), "gates": gates_done,
+            "seconds": total, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "steps": steps, "mean_gates_per_step": float(np.mean(step_gates)), "max_active_jobs": max_active,
+            "device_key_bytes": key_bytes, "autotune": tune,
+            "config": f"{sessions} sessions over {SERVING_PARAMS}, Poisson {rate}/s for {seconds}s, "
+                      f"circuits of U[1,300] gates from FheUint8 ops, admission by device bytes"}
+
+
 def kernel_only(args):
     """One kernel on a batch of synthetic items, --warmup + --steps launches,
     printing the mean launch time (the small case profiled with ncu)."""
@@ -329,7 +541,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--mode", default="wavefront", choices=["wavefront", "br-kernel", "ks-kernel"],
+    ap.add_argument("--no-extras", action="store_true", help="skip the microbench / ragged / serving sub-results")
+    ap.add_argument("--mode", default="wavefront",
+                    choices=["wavefront", "br-kernel", "ks-kernel", "microbench", "ragged", "serving"],
                     help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
@@ -337,6 +551,13 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode in ("microbench", "ragged", "serving"):
+        import torch
+        P = pz()
+        fn = {"microbench": lambda: microbench(P, torch, 0), "ragged": lambda: ragged_batch(P, 0),
+              "serving": lambda: serving(P, 0)}[args.mode]
+        print(json.dumps({"mode": args.mode, **fn()}), flush=True)
+        return
     if args.mode != "wavefront":
         return kernel_only(args)
 
@@ -430,6 +651,12 @@ def main():
     if not args.no_plain and rank == 0:
         plain = plain_form(P, torch, local)
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["microbench"] = microbench(P, torch, local)
+        extras["ragged"] = ragged_batch(P, local)
+        extras["serving"] = serving(P, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -462,6 +689,7 @@ def main():
                          "launch_ms": br_ms, "bootstraps_per_launch": B,
                          "modmuls_per_bootstrap": modmuls / B},
             "plain": plain,
+            **extras,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
