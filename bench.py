@@ -12,7 +12,7 @@ launch; the whole circuit is one CUDA graph replayed per step.
           host->device inputs and device->host outputs inside the timed region
   plain   InteractiveLTE2Party, 128 NAND gates, one gate per launch
   roofline  blind-rotation kernel: algorithmic 32-bit multiply instructions
-          (BASELINE convention, 10 per 64-bit modmul) per second / the IMAD
+          (10 per 64-bit modmul, the roofline convention) per second / the IMAD
           rate measured on this GPU by pz_probe_imad_rate
   cpu_baseline  the CPU oracle (a C++ restatement of the reference's pbs path)
           on all host threads, bounded sample of the same gates
@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 PARAM = "NI_8P"
 N_MUL = 1024
 N_LT = 1024
-C_MM = 10  # 32-bit multiply instructions per 64-bit Shoup modmul (BASELINE.md convention)
+C_MM = 10  # 32-bit multiply instructions per 64-bit Shoup modmul (roofline convention)
 WORKLOAD_CONFIG = {
     "workload": "batched circuit wavefront: NI_8P, 1024 FheUint8 a*b + 1024 a<b, "
                 "each level one launch, whole circuit one CUDA graph",
@@ -75,7 +75,7 @@ def wavefront_circuit(P):
 
 def schedule_work(p, ks):
     """Exact counts of the blind rotation's work per ciphertext (pbs.rs:240-414)
-    from key-switched LWEs ks [count][n+1]: returns modmuls per the BASELINE
+    from key-switched LWEs ks [count][n+1]: returns modmuls by the roofline
     convention M = F (N/2) logN + I ((N/2) logN + N) + MAC."""
     br_q, n, N, g, w = p.br_q, p.lwe_n, p.rlwe_n, p.g, p.w
     dlog = np.zeros(br_q, np.int64)
@@ -489,6 +489,53 @@ def serving(P, device, sessions=64, rate=40.0, seconds=10.0, seed=8):
                       f"circuits of U[1,300] gates from FheUint8 ops, admission by device bytes"}
 
 
+def kernels_case(P, torch, device, count=296):
+    """Small profiling case: each kernel of the path once after one warm-up
+    (NI_8P, synthetic key): NTT forward/inverse, external product,
+    automorphism, batched key switch, blind rotation, and one ragged step of
+    the multi-session executor (key switch + blind rotation over 2 sessions)."""
+    prm = "NI_8P"
+    p = P.params(prm)
+    N, L = p.rlwe_n, p.rlwe_n + 1
+    eng = P.Engine(prm, device=device)
+    key = eng.upload_key(*synthetic_key(p, 0x5EED))
+    rng = np.random.default_rng(21)
+    polys = torch.from_numpy(rng.integers(0, p.rlwe_q, (count, N), dtype=np.uint64).view(np.int64)).cuda()
+    rl = torch.from_numpy(rng.integers(0, p.rlwe_q, (count, 2, N), dtype=np.uint64).view(np.int64)).cuda()
+    idx = torch.arange(count, dtype=torch.int32, device="cuda") % p.lwe_n
+    slots = torch.arange(count, dtype=torch.int32, device="cuda") % p.n_auto_keys
+    lwe = torch.from_numpy(rng.integers(0, p.lwe_q, (count, L), dtype=np.uint64).view(np.int64)).cuda()
+    ks_out = torch.empty((count, p.lwe_n + 1), dtype=torch.int32, device="cuda")
+    ks = torch.from_numpy(rng.integers(0, p.lwe_q, (count, p.lwe_n + 1), dtype=np.uint64).astype(np.uint32)
+                          .view(np.int32)).cuda()
+    tv = torch.from_numpy(rng.integers(0, 6, count).astype(np.uint8)).cuda()
+    br_out = torch.empty((count, L), dtype=torch.int64, device="cuda")
+    S = P.Server(device=device, arena_bytes=1 << 28, max_items=count)
+    eng2 = P.Engine("I_2P_LB_SR", device=device)
+    key2 = eng2.upload_key(*synthetic_key(P.params("I_2P_LB_SR"), 0x5EEE))
+    sids = [S.add_session(eng, key), S.add_session(eng2, key2)]
+    C = P.Circuit()
+    ins = [C.input() for _ in range(2 * count)]
+    for i in range(count):
+        C.output(C.gate("nand", ins[2 * i], ins[2 * i + 1]))
+    inp = rng.integers(0, p.rlwe_q, (2 * count, L), dtype=np.uint64)
+    for rep in range(2):  # warm-up, then the profiled launch of each kernel
+        eng.ntt_forward_device(polys)
+        eng.ntt_backward_device(polys)
+        eng.rlwe_by_rgsw_device(key, rl, idx)
+        eng.rlwe_auto_device(key, rl, slots)
+        eng.lwe_key_switch_device(key, lwe, ks_out)
+        eng.blind_rotate_device(key, ks, tv, br_out)
+        S.submit(sids[0], C, inp[:2 * count])
+        S.run_until_idle()
+    torch.cuda.synchronize()
+    S.close()
+    for k, e in ((key, eng), (key2, eng2)):
+        k.release()
+        e.close()
+    return {"mode": "kernels", "count": count, "param_set": prm}
+
+
 def kernel_only(args):
     """One kernel on a batch of synthetic items, --warmup + --steps launches,
     printing the mean launch time (the small case profiled with ncu)."""
@@ -543,7 +590,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the microbench / ragged / serving sub-results")
     ap.add_argument("--mode", default="wavefront",
-                    choices=["wavefront", "br-kernel", "ks-kernel", "microbench", "ragged", "serving"],
+                    choices=["wavefront", "br-kernel", "ks-kernel", "microbench", "ragged", "serving", "kernels"],
                     help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
@@ -551,11 +598,11 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.mode in ("microbench", "ragged", "serving"):
+    if args.mode in ("microbench", "ragged", "serving", "kernels"):
         import torch
         P = pz()
         fn = {"microbench": lambda: microbench(P, torch, 0), "ragged": lambda: ragged_batch(P, 0),
-              "serving": lambda: serving(P, 0)}[args.mode]
+              "serving": lambda: serving(P, 0), "kernels": lambda: kernels_case(P, torch, 0)}[args.mode]
         print(json.dumps({"mode": args.mode, **fn()}), flush=True)
         return
     if args.mode != "wavefront":

@@ -160,7 +160,9 @@ void orc_rng_uniform_mod(void *rng, uint64_t q, uint64_t *out, size_t n);
 void orc_client_keys(void *ev, int parties, int seed_base, int32_t *s, int32_t *z,
                      int32_t *s_parts, int32_t *z_parts);
 /* Server key (coefficient domain, layout of orc_key_new) under the ideal
- * secrets, errors drawn from ChaCha8(err_seed).  See DESIGN.md. */
+ * secrets, errors drawn from ChaCha8(err_seed).  Encrypting under the summed
+ * secret gives the key structure of the interactive/NI protocols' output
+ * (which only the client side produces) with less noise. */
 void orc_gen_server_key(void *ev, const int32_t *s, const int32_t *z,
                         const uint8_t err_seed[32], uint64_t *rgsw, uint64_t *autos,
                         uint64_t *ksk);

@@ -12,6 +12,7 @@
 //                 blind-rotation schedule, test vector rotation, the whole
 //                 blind rotation with the RLWE accumulator in registers,
 //                 sample extraction (pbs.rs:146-449)
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -396,17 +397,25 @@ __device__ __forceinline__ u64 operand(const u64 *base, const u32 *idx, int ct, 
 }
 
 // Key switch of ciphertexts [ct0, min(ct0 + KS_CT, count)) for the output
-// columns of this CTA (blockIdx.y).
+// columns of this CTA (blockIdx.y) over its share of the input coefficients
+// (blockIdx.z of gridDim.z).  With one share the sums are stored reduced mod
+// q_ks; with several, each CTA adds its partial sums into the zeroed output
+// with 32-bit atomics (exact: the result is taken mod q_ks, a power of two
+// <= 2^32) and the consumer reduces (value & (q_ks - 1)).
 __device__ __forceinline__ void ks_tile(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
                                         int ct0, int count, u32 *out, u32 (*dig)[KS_IC][MAX_KS_D]) {
   const int tid = threadIdx.x;
   const int col = blockIdx.y * KS_COLS + tid;
   const size_t L = (size_t)P.N + 1;
   const u32 d = P.d;
+  const u32 chunks = P.N / KS_IC, per = (chunks + gridDim.z - 1) / gridDim.z;
+  const u32 i_begin = blockIdx.z * per * KS_IC;
+  const u32 i_end = min(P.N, i_begin + per * KS_IC);
+  if (i_begin >= P.N) return;  // uniform per CTA
   u32 acc[KS_CT];
 #pragma unroll
   for (int c = 0; c < KS_CT; c++) acc[c] = 0;
-  for (u32 i0 = 0; i0 < P.N; i0 += KS_IC) {
+  for (u32 i0 = i_begin; i0 < i_end; i0 += KS_IC) {
     __syncthreads();
     for (int e = tid; e < KS_CT * KS_IC; e += KS_COLS) {
       const int c = e / KS_IC, ii = e % KS_IC;
@@ -440,11 +449,13 @@ __device__ __forceinline__ void ks_tile(const KsParams &P, const unsigned char *
       const int ct = ct0 + c;
       if (ct < count) {
         u32 v = acc[c];
-        if (col == 0) {
+        if (col == 0 && blockIdx.z == 0) {
           v += (u32)prelude_moddown(operand(c0, P.in0, ct, 0, L, P.Q), operand(c1, P.in1, ct, 0, L, P.Q),
                                     gates ? gates[ct] : 0, true, P);
         }
-        out[(size_t)ct * P.out_stride + col] = v & P.mask;
+        u32 *o = out + (size_t)ct * P.out_stride + col;
+        if (gridDim.z == 1) *o = v & P.mask;
+        else atomicAdd(o, v);
       }
     }
   }
@@ -522,7 +533,7 @@ __device__ __forceinline__ void pbs_item(const BrParams &P, int ct, const u32 *k
     for (u32 b = j; b < R; b += T) { cnt[b] = 0; fill[b] = 0; }
     __syncthreads();
     for (u32 i = j; i < n; i += T) {
-      const u32 odd = mod_switch_odd(kso[1 + i], P.q_ks_f, P.br_q_f);
+      const u32 odd = mod_switch_odd(kso[1 + i] & P.ks_mask, P.q_ks_f, P.br_q_f);
       const u32 k = P.dlog[odd];
       keys[i] = (unsigned short)k;
       atomicAdd(&cnt[k], 1u);
@@ -606,7 +617,7 @@ __device__ __forceinline__ void pbs_item(const BrParams &P, int ct, const u32 *k
     }
 
     // ---- trivial test RLWE: X^{g * odd(b)} * tv, embedded (pbs.rs:163-211)
-    const u32 odd_b = mod_switch_odd(kso[0], P.q_ks_f, P.br_q_f);
+    const u32 odd_b = mod_switch_odd(kso[0] & P.ks_mask, P.q_ks_f, P.br_q_f);
     const u32 gb = (u32)(((u64)P.g * odd_b) % P.br_q);
     u32 mexp = gb;
     bool msign = true;
@@ -801,13 +812,39 @@ cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u
   return cudaGetLastError();
 }
 
+// Shares of the input coefficients per key-switch tile: enough CTAs for
+// about four per SM (small batches), at least KS_IC coefficients per share.
+static unsigned ks_split(size_t tiles_xy, u32 N) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t target = (size_t)4 * sms, chunks = N / KS_IC;
+  unsigned z = 1;
+  while (tiles_xy * z < target && 2 * z <= chunks) z *= 2;
+  return z;
+}
+
+__global__ void ks_mask_kernel(u32 *out, size_t count, u32 stride, u32 cols, u32 mask) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count * cols; i += (size_t)gridDim.x * blockDim.x)
+    out[(i / cols) * stride + i % cols] &= mask;
+}
+
 cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
-                      size_t count, u32 *out, cudaStream_t s) {
+                      size_t count, u32 *out, cudaStream_t s, bool reduce_output) {
   if (count == 0) return cudaSuccess;
   if (P.d > (u32)MAX_KS_D) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((count + KS_CT - 1) / KS_CT), (unsigned)((P.n + 1 + KS_COLS - 1) / KS_COLS));
+  grid.z = ks_split((size_t)grid.x * grid.y, P.N);
+  cudaError_t e;
+  if (grid.z > 1 && (e = cudaMemsetAsync(out, 0, count * P.out_stride * sizeof(u32), s)) != cudaSuccess) return e;
   ks_kernel<<<grid, KS_COLS, 0, s>>>(P, gates, c0, c1, (int)count, out);
-  return cudaGetLastError();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (grid.z > 1 && reduce_output) {
+    const size_t words = count * (P.n + 1);
+    ks_mask_kernel<<<(unsigned)std::min<size_t>((words + 255) / 256, 4096), 256, 0, s>>>(out, count, P.out_stride,
+                                                                                        P.n + 1, P.mask);
+    return cudaGetLastError();
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
@@ -834,12 +871,15 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
   return cudaGetLastError();
 }
 
-cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, u32 max_n,
-                             u32 max_d, const unsigned char *gates, const u64 *wires, const u32 *in0,
-                             const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s) {
+cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,
+                             u32 max_n, u32 max_N, u32 max_d, const unsigned char *gates, const u64 *wires,
+                             const u32 *in0, const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s) {
   if (ntiles == 0) return cudaSuccess;
   if (max_d > (u32)MAX_KS_D) return cudaErrorInvalidValue;
   dim3 grid((unsigned)ntiles, (unsigned)((max_n + 1 + KS_COLS - 1) / KS_COLS));
+  grid.z = ks_split((size_t)grid.x * grid.y, max_N);
+  cudaError_t e;
+  if (grid.z > 1 && (e = cudaMemsetAsync(out, 0, count * out_stride * sizeof(u32), s)) != cudaSuccess) return e;
   ks_ragged_kernel<<<grid, KS_COLS, 0, s>>>(d_descs, d_tiles, gates, wires, in0, in1, out, out_stride);
   return cudaGetLastError();
 }

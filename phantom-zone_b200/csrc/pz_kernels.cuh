@@ -14,6 +14,7 @@ struct BrParams {
   u32 d_a, d_b, d_auto;
   u32 rgsw_rows, auto_rows;
   u32 n, br_q, w, g, emb;
+  u32 ks_mask;                     // q_ks - 1: key-switched words are read modulo q_ks
   double q_ks_f, br_q_f;           // mod_switch_odd operands (pbs.rs:416-420)
   u32 auto_k[MAX_AUTO_SLOTS];      // automorphism element mod 2N per key slot
   const unsigned short *dlog;      // [br_q]
@@ -62,8 +63,10 @@ cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, 
                                size_t count, int trivial, cudaStream_t s);
 cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *slot, size_t count,
                         int trivial, cudaStream_t s);
+// reduce_output: leave every output word reduced mod q_ks (otherwise the
+// words may carry multiples of q_ks, and consumers mask with q_ks - 1)
 cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
-                      size_t count, u32 *out, cudaStream_t s);
+                      size_t count, u32 *out, cudaStream_t s, bool reduce_output);
 cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
                        const unsigned char *gates, u64 *out, size_t count, u64 *rlwe_dbg,
                        int grid_limit, cudaStream_t s, int variant);
@@ -72,9 +75,9 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
 constexpr int PBS_VARIANTS = 3;
 // Ragged batches (several sessions / parameter sets in one launch): per-item
 // descriptors in device memory; max_* bound the sizes over the descriptors.
-cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, u32 max_n,
-                             u32 max_d, const unsigned char *gates, const u64 *wires, const u32 *in0,
-                             const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s);
+cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,
+                             u32 max_n, u32 max_N, u32 max_d, const unsigned char *gates, const u64 *wires,
+                             const u32 *in0, const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s);
 cudaError_t launch_pbs_ragged(int logn, bool d1, const BrParams *d_descs, const u32 *item_desc, u32 max_br_q,
                               u32 max_n, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out,
                               const u32 *out_idx, size_t count, int grid_limit, cudaStream_t s, int variant);

@@ -193,7 +193,7 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
   u32 *d_ks = d_ks_out ? d_ks_out : d_ks_scratch;
   const u32 ks_out_stride = d_ks_out ? c->P.lwe_n + 1 : stride;
   ks.out_stride = ks_out_stride;
-  cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s);
+  cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s, d_ks_out != nullptr);
   if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s,
@@ -306,6 +306,7 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   br.g = P.g;
   br.emb = P.embedding_factor;
   br.q_ks_f = (double)P.lwe_q;
+  br.ks_mask = (u32)(P.lwe_q - 1);
   br.br_q_f = (double)P.br_q;
   br.dlog = c->d_dlog;
   br.tv = c->d_tv;
@@ -596,7 +597,7 @@ pz_status pz_lwe_key_switch_device(pz_ctx *c, const pz_key *k, const uint64_t *d
   ks.Q_f = (double)c->P.lwe_q;
   ks.out_stride = c->P.lwe_n + 1;
   ks.raw = 1;
-  cudaError_t e = pz::launch_ks(ks, nullptr, d_in, nullptr, count, d_out, st);
+  cudaError_t e = pz::launch_ks(ks, nullptr, d_in, nullptr, count, d_out, st, true);
   if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
   return PZ_OK;
 }

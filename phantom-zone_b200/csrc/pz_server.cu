@@ -337,7 +337,8 @@ pz_status run_items(pz_server *s, const std::vector<Item> &items) {
     if ((e = cudaMemcpyAsync(d, h, lay.total, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess)
       return s->cuda("item upload", e);
     if ((e = cudaEventRecord(s->buf_free[b], s->stream)) != cudaSuccess) return s->cuda("cudaEventRecord", e);
-    e = pz::launch_ks_ragged(s->d_ksp, (const pz::KsTile *)(d + lay.tiles), ntiles, s->max_n, s->max_d,
+    e = pz::launch_ks_ragged(s->d_ksp, (const pz::KsTile *)(d + lay.tiles), ntiles, n, s->max_n,
+                             (u32)(s->L - 1), s->max_d,
                              d + lay.gate, s->d_arena, (const u32 *)(d + lay.in0), (const u32 *)(d + lay.in1),
                              s->d_ksout, s->ks_stride, s->stream);
     if (e != cudaSuccess) return s->cuda("launch_ks_ragged", e);
