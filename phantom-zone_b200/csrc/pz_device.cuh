@@ -3,8 +3,9 @@
 // Modular arithmetic mod the RLWE prime Q (< 2^62):
 //   * NTT butterflies use Shoup multiplication by precomputed twiddles
 //     (the butterflies of ntt.rs:24-104): forward values grow without
-//     reduction (below 23Q after the 11 stages of N = 2048), inverse values
-//     stay in [0, 2Q) (Harvey).
+//     reduction (below 45Q after the 11 stages of N = 2048), inverse values
+//     stay in [0, 2Q) (Harvey).  For N = 2048 the products use the special
+//     form Q = 2^54 - 77823 of that ring's prime.
 //   * The pointwise key product uses Montgomery REDC with R = 2^64.  Device
 //     keys are stored as K * N^{-1} * R mod Q, so REDC(x * K') = x * K * N^{-1}
 //     and the inverse NTT needs no final N^{-1} scaling.  Two products are
@@ -132,23 +133,50 @@ __device__ __forceinline__ int dev_index(int j, int r) {
   return (r >> 1) * (2 * NttShape<LOGN>::T) + 2 * j + (r & 1);
 }
 
-// Forward CT butterfly (the x' = x + wy, y' = x - wy of ntt.rs:31-49) without
-// Harvey's conditional subtraction: wy is a Shoup product in [0, 2q), so both
-// outputs grow by less than 2q per stage.  From inputs < q the 11 stages of
-// N = 2048 stay below 23q < 2^60 (Q < 2^55), and the Shoup product accepts
-// any 64-bit input, so no stage needs a reduction.
-__device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
-  const u64 t = shoup_mul(y, w, ws, q);
-  y = x + (q << 1) - t;
-  x = x + t;
+// The RLWE prime of every N = 2048 parameter set (parameters.rs:526-704):
+// Q = 2^54 - 77823, so q t mod 2^64 = (t << 54) - 77823 t.
+constexpr u64 Q_N2048 = 18014398509404161ull;
+__device__ __forceinline__ u64 mulq_n2048(u64 t) { return (t << 54) - t * 77823ull; }
+
+// hi64(a b) without the low partial product and without the carry out of
+// the two cross terms' low halves: returns hi64(a b) - c, c in {0, 1, 2}.
+__device__ __forceinline__ u64 umulhi_lo2(u64 a, u64 b) {
+  const u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
+  u64 t = (u64)a1 * b1;
+  t += __umulhi(a1, b0);
+  t += __umulhi(a0, b1);
+  return t;
 }
-// Harvey inverse butterfly, ntt.rs:84-104 (x, y < 2q -> x', y' < 2q)
+
+// Forward CT butterfly (the x' = x + wy, y' = x - wy of ntt.rs:31-49) without
+// Harvey's conditional subtraction: wy is a Shoup product, so both outputs
+// grow by a bounded multiple of q per stage and the Shoup product accepts any
+// 64-bit input, so no stage needs a reduction.  Generic q: wy in [0, 2q),
+// growth 2q per stage (< 23q after the 11 stages of N = 2048 from inputs
+// < q).  Q_N2048 (SPQ): the quotient from umulhi_lo2 is at most 2 short, so
+// wy in [0, 4q), growth 4q per stage (< 45q < 2^60 after 11 stages), and
+// q * quotient comes from the special form of Q.
+template <bool SPQ>
+__device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
+  if (SPQ) {
+    const u64 t = w * y - mulq_n2048(umulhi_lo2(ws, y));
+    y = x + (Q_N2048 << 2) - t;
+    x = x + t;
+  } else {
+    const u64 t = shoup_mul(y, w, ws, q);
+    y = x + (q << 1) - t;
+    x = x + t;
+  }
+}
+// Harvey inverse butterfly, ntt.rs:84-104 (x, y < 2q -> x', y' < 2q); with
+// SPQ the exact Shoup quotient times Q comes from the special form of Q.
+template <bool SPQ>
 __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
-  const u64 q2 = q << 1;
+  const u64 q2 = SPQ ? (Q_N2048 << 1) : (q << 1);
   u64 u = x + y;
   if (u >= q2) u -= q2;
-  u64 t = x + q2 - y;
-  y = shoup_mul(t, w, ws, q);
+  const u64 t = x + q2 - y;
+  y = SPQ ? w * t - mulq_n2048(umulhi(ws, t)) : shoup_mul(t, w, ws, q);
   x = u;
 }
 
@@ -186,15 +214,16 @@ __device__ __forceinline__ void tw(const u64 *t, int i, u64 &w, u64 &ws) {
 // exchange steps (y through the second N words of sm), and their butterflies
 // are independent instruction streams.  A single-polynomial call passes its
 // array as both x and y.
-template <bool TWO>
+// N = 2048 transforms run modulo Q_N2048 (the context checks it).
+template <int LOGN, bool TWO>
 __device__ __forceinline__ void fbf2(u64 (&x)[8], u64 (&y)[8], int a, int b, u64 w, u64 ws, u64 q) {
-  fbf(x[a], x[b], w, ws, q);
-  if (TWO) fbf(y[a], y[b], w, ws, q);
+  fbf<LOGN == 11>(x[a], x[b], w, ws, q);
+  if (TWO) fbf<LOGN == 11>(y[a], y[b], w, ws, q);
 }
-template <bool TWO>
+template <int LOGN, bool TWO>
 __device__ __forceinline__ void ibf2(u64 (&x)[8], u64 (&y)[8], int a, int b, u64 w, u64 ws, u64 q) {
-  ibf(x[a], x[b], w, ws, q);
-  if (TWO) ibf(y[a], y[b], w, ws, q);
+  ibf<LOGN == 11>(x[a], x[b], w, ws, q);
+  if (TWO) ibf<LOGN == 11>(y[a], y[b], w, ws, q);
 }
 
 // Forward radix-8 round k: stages with m = 8^k, 2m and 4m groups; blk is the
@@ -207,17 +236,17 @@ __device__ __forceinline__ void fwd_round8(u64 (&x)[8], u64 (&y)[8], int k, int 
   u64 w, ws;
   tw(rc.fw, m + blk, w, ws);
 #pragma unroll
-  for (int r = 0; r < 4; r++) fbf2<TWO>(x, y, r, r + 4, w, ws, q);
+  for (int r = 0; r < 4; r++) fbf2<LOGN, TWO>(x, y, r, r + 4, w, ws, q);
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     tw(rc.fw, 2 * m + 2 * blk + h, w, ws);
-    fbf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    fbf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
 #pragma unroll
   for (int h = 0; h < 4; h++) {
     tw(rc.fw, 4 * m + 4 * blk + h, w, ws);
-    fbf2<TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
+    fbf2<LOGN, TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
   }
 }
 
@@ -230,17 +259,17 @@ __device__ __forceinline__ void inv_round8(u64 (&x)[8], u64 (&y)[8], int k, int 
 #pragma unroll
   for (int h = 0; h < 4; h++) {
     tw(rc.iw, 4 * m + 4 * blk + h, w, ws);
-    ibf2<TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
+    ibf2<LOGN, TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
   }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     tw(rc.iw, 2 * m + 2 * blk + h, w, ws);
-    ibf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    ibf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    ibf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    ibf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
   tw(rc.iw, m + blk, w, ws);
 #pragma unroll
-  for (int r = 0; r < 4; r++) ibf2<TWO>(x, y, r, r + 4, w, ws, q);
+  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO>(x, y, r, r + 4, w, ws, q);
 }
 
 // Trailing 2-stage round (stages with N/4 and N/2 groups).
@@ -253,12 +282,12 @@ __device__ __forceinline__ void fwd_round4(u64 (&x)[8], u64 (&y)[8], int j, cons
   for (int h = 0; h < 2; h++) {
     const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
     tw(rc.fw, N / 4 + g, w, ws);
-    fbf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    fbf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       tw(rc.fw, N / 2 + 2 * g + e, w, ws);
-      fbf2<TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
+      fbf2<LOGN, TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
     }
   }
 }
@@ -274,11 +303,11 @@ __device__ __forceinline__ void inv_round4(u64 (&x)[8], u64 (&y)[8], int j, cons
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       tw(rc.iw, N / 2 + 2 * g + e, w, ws);
-      ibf2<TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
+      ibf2<LOGN, TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
     }
     tw(rc.iw, N / 4 + g, w, ws);
-    ibf2<TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    ibf2<TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    ibf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    ibf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
 }
 
@@ -343,7 +372,7 @@ __device__ __forceinline__ void xchg(u64 (&x)[8], u64 (&y)[8], u64 *sm, int j) {
 }
 
 // Forward negacyclic NTT (CT, ntt.rs:110-143 without reductions): coefficient
-// layout in, values < q; evaluation layout out, values < (2 log N + 1) q.
+// layout in, values < q; evaluation layout out, values < 45 q (see fbf).
 // sm: N words (2N with TWO).  The rounds run in a loop (one copy of the round
 // body); the exchanges between them are layout-specialised and picked by a
 // block-uniform switch.

@@ -240,6 +240,8 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   const u64 N = P.rlwe_n;
   c->logn = log2_exact(N);
   if (c->logn != 9 && c->logn != 11) { delete c; return PZ_ERR_NOT_SUPPORTED; }
+  // the N = 2048 kernels reduce with the special form of this ring's prime
+  if (c->logn == 11 && Q != pz::Q_N2048) { delete c; return PZ_ERR_NOT_SUPPORTED; }
   if (root == 0) root = default_root(Q, 2 * N);
   if (root == 0 || powmod(root, N, Q) != Q - 1) { delete c; return PZ_ERR_INVALID_ARGUMENT; }
   c->root = root;
