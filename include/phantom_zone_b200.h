@@ -84,6 +84,8 @@ typedef struct pz_params {
   uint32_t rgsw_rows;        /* 2 d_a + 2 d_b */
   uint32_t auto_rows;        /* 2 d_auto */
   uint32_t n_auto_keys;      /* w + 1 */
+  uint32_t ni_ks_logb, ni_ks_d; /* ui_to_s key switch decomposition of the NI sets
+                                   (parameters.rs:616-697: 1, 50); 0 otherwise */
 } pz_params;
 
 typedef struct pz_ctx pz_ctx;
@@ -235,6 +237,36 @@ pz_status pz_circuit_run(pz_ctx *ctx, const pz_key *key, pz_circuit *c, const ui
 pz_status pz_circuit_capture_graph(pz_ctx *ctx, const pz_key *key, pz_circuit *c, const uint64_t *d_inputs,
                                    uint64_t *d_outputs, void *stream);
 pz_status pz_circuit_replay_graph(pz_circuit *c, void *stream);
+
+/* ---- non-interactive input path (NI parameter sets, N = 2048) ---------------------
+ * A user of a non-interactive session sends its bools as seeded RLWEs under its own
+ * RLWE secret u_j (NonInteractiveBatchedFheBools, bool/ni_mp_api.rs:182-196); the
+ * server regenerates the a-parts, key-switches u_j -> s with that user's ui_to_s key
+ * and extracts one LWE per bool (KeySwitchWithId + extract, ni_mp_api.rs:217-236,
+ * 400-440). */
+typedef struct pz_ni_ksk pz_ni_ksk;
+/* ui_to_s key of one user: [2 ni_ks_d][N] u64 coefficient domain, rows A then B
+ * (ShoupNonInteractiveServerKeyEvaluationDomain::ui_to_s_ksk, bool/keys.rs:1083-1085,
+ * before its forward NTT) */
+pz_status pz_ni_ksk_upload(pz_ctx *ctx, const uint64_t *ksk, pz_ni_ksk **out);
+void pz_ni_ksk_release(pz_ni_ksk *ksk);
+/* NonInteractiveBatchedFheBools::from (ni_mp_api.rs:248-280): d_b [count][N] (the
+ * seeded RLWEs' b-parts) -> d_rlwe [count][2][N], a-parts from ChaCha8(seed) in batch
+ * order.  Returns when done (it checks the rejection-sampling margin). */
+pz_status pz_ni_unseed_device(pz_ctx *ctx, const uint8_t seed[32], const uint64_t *d_b, uint64_t *d_rlwe,
+                              size_t count, void *stream);
+/* rlwe_key_switch (rgsw/runtime.rs:1001-1063): d_in, d_out [count][2][N] */
+pz_status pz_ni_key_switch_device(pz_ctx *ctx, const pz_ni_ksk *ksk, const uint64_t *d_in, uint64_t *d_out,
+                                  size_t count, void *stream);
+/* BatchedFheBools::extract (ni_mp_api.rs:217-236) = sample_extract (pbs.rs:423-449):
+ * d_lwe[c] = bool d_index[c] of the batch d_rlwe [rlwe_count][2][N] (RLWE index / N,
+ * coefficient index % N); an index past the batch leaves d_lwe[c] unchanged */
+pz_status pz_sample_extract_device(pz_ctx *ctx, const uint64_t *d_rlwe, size_t rlwe_count,
+                                   const uint32_t *d_index, uint64_t *d_lwe, size_t count, void *stream);
+/* The three steps on host buffers (synchronous): b [rlwe_count][N] -> lwe_out
+ * [nbools][N + 1] for bools 0 .. nbools - 1 */
+pz_status pz_ni_ingest(pz_ctx *ctx, const pz_ni_ksk *ksk, const uint8_t seed[32], const uint64_t *b,
+                       size_t rlwe_count, uint64_t *lwe_out, size_t nbools);
 
 /* ---- multi-session executor (serving) ---------------------------------------------
  * No reference counterpart: the reference evaluates one gate at a time, in

@@ -38,6 +38,7 @@ class ParamInfo(ctypes.Structure):
         ("lwe_secret_gaussian", ctypes.c_uint32), ("variant", ctypes.c_uint32),
         ("embedding_factor", ctypes.c_uint32), ("rgsw_rows", ctypes.c_uint32),
         ("auto_rows", ctypes.c_uint32), ("n_auto_keys", ctypes.c_uint32),
+        ("ni_ks_logb", ctypes.c_uint32), ("ni_ks_d", ctypes.c_uint32),
     ]
 
 
@@ -76,6 +77,10 @@ def lib():
             "orc_not": (None, [vp, u64p]),
             "orc_gate_batch": (None, [vp, vp, u8p, u64p, u64p, u64p, ctypes.c_size_t, ctypes.c_int]),
             "orc_sample_extract": (None, [vp, u64p, u64p, ctypes.c_uint32]),
+            "orc_ni_unseed": (None, [vp, u8p, u64p, ctypes.c_size_t, u64p]),
+            "orc_ni_key_switch": (None, [vp, u64p, u64p, u64p]),
+            "orc_ni_encrypt_bools": (None, [vp, i32p, u8p, u8p, u8p, ctypes.c_size_t, u64p]),
+            "orc_ni_ksk_gen": (None, [vp, i32p, i32p, u8p, u64p]),
             "orc_u8_op": (ctypes.c_int, [vp, vp, ctypes.c_int, u64p, u64p, u64p, u64p, u64p, u64p, ctypes.POINTER(ctypes.c_int)]),
             "orc_generate_prime": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
             "orc_ntt_custom_new": (vp, [ctypes.c_uint64, ctypes.c_size_t]),
@@ -269,6 +274,45 @@ class Evaluator:
         a = np.ascontiguousarray(c, np.uint64).copy()
         lib().orc_not(self.h, _p(a))
         return a
+
+    # --- non-interactive input path (NI parameter sets) ---------------------------
+    NI_KS_D = 50  # ui_to_s key switch decomposition count (logb 1)
+
+    def ni_encrypt_bools(self, u, bits, seed, err_seed=b"\x44" * 32):
+        """Client: seeded RLWEs of `bits` under the user's RLWE secret u -> b [count][N]."""
+        bits = np.ascontiguousarray(bits, np.uint8)
+        count = (len(bits) + self.N - 1) // self.N
+        out = np.empty((count, self.N), np.uint64)
+        lib().orc_ni_encrypt_bools(self.h, _p(np.ascontiguousarray(u, np.int32), i32p),
+                                   (ctypes.c_uint8 * 32)(*bytes(seed)), (ctypes.c_uint8 * 32)(*bytes(err_seed)),
+                                   _p(bits, u8p), len(bits), _p(out))
+        return out
+
+    def ni_ksk_gen(self, u, s, err_seed=b"\x55" * 32):
+        out = np.empty((2 * self.NI_KS_D, self.N), np.uint64)
+        lib().orc_ni_ksk_gen(self.h, _p(np.ascontiguousarray(u, np.int32), i32p),
+                             _p(np.ascontiguousarray(s, np.int32), i32p), (ctypes.c_uint8 * 32)(*bytes(err_seed)),
+                             _p(out))
+        return out
+
+    def ni_unseed(self, seed, b):
+        b = np.ascontiguousarray(b, np.uint64).reshape(-1, self.N)
+        out = np.empty((len(b), 2, self.N), np.uint64)
+        lib().orc_ni_unseed(self.h, (ctypes.c_uint8 * 32)(*bytes(seed)), _p(b), len(b), _p(out))
+        return out
+
+    def ni_key_switch(self, ksk, rlwe):
+        ksk = np.ascontiguousarray(ksk, np.uint64)
+        r = np.ascontiguousarray(rlwe, np.uint64)
+        out = np.empty(2 * self.N, np.uint64)
+        lib().orc_ni_key_switch(self.h, _p(ksk), _p(r), _p(out))
+        return out.reshape(2, self.N)
+
+    def ni_ingest(self, ksk, seed, b, nbits):
+        """unseed -> key switch -> extract every bool (the server's NI input path)."""
+        rl = self.ni_unseed(seed, b)
+        ks = [self.ni_key_switch(ksk, r) for r in rl]
+        return np.stack([self.sample_extract(ks[i // self.N], i % self.N) for i in range(nbits)])
 
 
 class OracleKey:

@@ -430,6 +430,7 @@ struct Eval {
   u64 ks_mask;  // ModulusPowerOf2 mask (power_of_2.rs:95-104)
   Ntt ntt;
   Decomposer dec_lwe, dec_a, dec_b, dec_auto;
+  Decomposer dec_ni;      // non_interactive_ui_to_s_key_switch_decomposer (NI sets only)
   std::vector<u32> dlog;  // g_k_dlog_map
   u32 emb;
   std::vector<std::vector<u64>> test_vec;  // per gate
@@ -446,6 +447,8 @@ struct Eval {
     dec_a.init(Q, p.rlrg_logb, p.d_a);
     dec_b.init(Q, p.rlrg_logb, p.d_b);
     dec_auto.init(Q, p.auto_logb, p.auto_d);
+    // parameters.rs:616-697: ui_to_s key switch (logb 1, d 50) of the NI sets
+    if (p.variant == 2) dec_ni.init(Q, 1, 50);
     // evaluator.rs:664-673 dlog map over Z*_{br_q} = +-g^k
     u32 q = p.br_q;
     dlog.assign(q, 0);
@@ -900,6 +903,9 @@ int orc_param_info_get(int pid, orc_param_info *o) {
   o->embedding_factor = 2 * p.rlwe_n / p.br_q;
   o->rgsw_rows = 2 * p.d_a + 2 * p.d_b; o->auto_rows = 2 * p.auto_d;
   o->n_auto_keys = p.w + 1;
+  // parameters.rs:616-697 non_interactive_ui_to_s_key_switch_decomposer (1, 50)
+  o->ni_ks_logb = p.variant == 2 ? 1 : 0;
+  o->ni_ks_d = p.variant == 2 ? 50 : 0;
   return 0;
 }
 
@@ -1302,6 +1308,98 @@ static int decode_bool(const Eval &e, u64 m) {  // evaluator.rs:243-256
   if (v == 0) return 0;
   if (v == 1) return 1;
   return -1;
+}
+
+// ---- non-interactive input path ----------------------------------------------
+// NonInteractiveBatchedFheBools::from (ni_mp_api.rs:248-280): the a-parts of
+// the batch's RLWEs, in order, from one ChaCha8(seed) stream
+// (RandomFillUniformInModulus, random.rs:93-110); b copied.
+void orc_ni_unseed(void *ev, const uint8_t seed[32], const uint64_t *b, size_t count, uint64_t *rlwe) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N;
+  ChaCha8 prng(seed);
+  for (size_t c = 0; c < count; c++) {
+    for (size_t i = 0; i < N; i++) rlwe[c * 2 * N + i] = prng.uniform_mod(e.Q);
+    memcpy(rlwe + c * 2 * N + N, b + c * N, N * 8);
+  }
+}
+
+// rlwe_key_switch (runtime.rs:1001-1063) with the key-switching key
+// Ksk(u -> s) given in the coefficient domain ([2d][N]: rows A then B); the
+// key is sent to the evaluation domain with Shoup companions as
+// NonInteractiveServerKeyEvaluationDomain / its Shoup form do.
+void orc_ni_key_switch(void *ev, const uint64_t *ksk_coef, const uint64_t *in, uint64_t *out) {
+  Eval &e = *(Eval *)ev;
+  if (e.p.variant != 2) throw std::runtime_error("not a non-interactive parameter set");
+  const size_t N = e.N, d = e.dec_ni.d;
+  std::vector<u64> ksk(ksk_coef, ksk_coef + 2 * d * N), ksk_s(2 * d * N);
+  for (size_t r = 0; r < 2 * d; r++) e.ntt.forward(&ksk[r * N], false);
+  for (size_t i = 0; i < ksk.size(); i++) ksk_s[i] = shoup_repr(ksk[i], e.Q);
+  std::vector<u64> tmp_row(in, in + N), dec(d * N), oa(N, 0), ob(N, 0);
+  for (size_t i = 0; i < N; i++) tmp_row[i] = e.Q - tmp_row[i];  // elwise_neg_mut
+  decompose_r(e.dec_ni, tmp_row.data(), dec.data(), N);
+  for (size_t j = 0; j < d; j++) e.ntt.forward(&dec[j * N], true);  // forward_lazy
+  const u64 *ap[64] = {}, *aps[64] = {}, *bp[64] = {};
+  for (size_t j = 0; j < d; j++) { ap[j] = &ksk[j * N]; aps[j] = &ksk_s[j * N]; bp[j] = &dec[j * N]; }
+  shoup_matrix_fma(e.Q, oa.data(), ap, aps, bp, d, N);
+  for (size_t j = 0; j < d; j++) { ap[j] = &ksk[(d + j) * N]; aps[j] = &ksk_s[(d + j) * N]; }
+  shoup_matrix_fma(e.Q, ob.data(), ap, aps, bp, d, N);
+  e.ntt.backward(oa.data(), false);
+  e.ntt.backward(ob.data(), false);
+  for (size_t i = 0; i < N; i++) ob[i] = e.rmod.add(ob[i], in[N + i]);  // elwise_add_mut
+  memcpy(out, oa.data(), N * 8);
+  memcpy(out + N, ob.data(), N * 8);
+}
+
+// Client side (harness): the NI batched bool encryption of ni_mp_api.rs:302-345
+// with seeded_secret_key_encrypt_rlwe (rgsw/keygen.rs:439-481): per RLWE, a
+// from ChaCha8(seed), b = e + m + a u, m_i = true_el / false_el for the bools
+// of that RLWE and 0 beyond the last; errors from ChaCha8(err_seed).
+void orc_ni_encrypt_bools(void *ev, const int32_t *u, const uint8_t seed[32], const uint8_t err_seed[32],
+                          const uint8_t *bits, size_t nbits, uint64_t *b_out) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N, count = (nbits + N - 1) / N;
+  ChaCha8 prng(seed), rng(err_seed);
+  std::vector<u64> u_eval(N), a(N);
+  for (size_t i = 0; i < N; i++) u_eval[i] = map_from_i64(e.Q, u[i]);
+  e.ntt.forward(u_eval.data(), false);
+  for (size_t c = 0; c < count; c++) {
+    for (size_t i = 0; i < N; i++) a[i] = prng.uniform_mod(e.Q);
+    e.ntt.forward(a.data(), false);
+    for (size_t i = 0; i < N; i++) a[i] = e.rmod.mul(a[i], u_eval[i]);
+    e.ntt.backward(a.data(), false);
+    u64 *b = b_out + c * N;
+    for (size_t i = 0; i < N; i++) {
+      const size_t k = c * N + i;
+      const u64 m = k < nbits ? (bits[k] ? e.true_el : e.false_el) : 0;
+      b[i] = e.rmod.add(e.rmod.add(map_from_f64(e.Q, rng.gaussian()), m), a[i]);
+    }
+  }
+}
+
+// An ideal key-switching key Ksk(u -> s) (harness; the protocol assembles it
+// from user shares): row j of part A uniform, part B = a_j s + e_j + g_j u,
+// g_j the decomposer's gadget (decomposer.rs:13-21), coefficient domain.
+void orc_ni_ksk_gen(void *ev, const int32_t *u, const int32_t *s, const uint8_t err_seed[32], uint64_t *ksk) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N, d = e.dec_ni.d;
+  ChaCha8 rng(err_seed);
+  std::vector<u64> s_eval(N), tmp(N);
+  for (size_t i = 0; i < N; i++) s_eval[i] = map_from_i64(e.Q, s[i]);
+  e.ntt.forward(s_eval.data(), false);
+  for (size_t j = 0; j < d; j++) {
+    u64 *a = ksk + j * N, *b = ksk + (d + j) * N;
+    for (size_t i = 0; i < N; i++) a[i] = rng.uniform_mod(e.Q);
+    memcpy(tmp.data(), a, N * 8);
+    e.ntt.forward(tmp.data(), false);
+    for (size_t i = 0; i < N; i++) tmp[i] = e.rmod.mul(tmp[i], s_eval[i]);
+    e.ntt.backward(tmp.data(), false);
+    const u64 g = e.dec_ni.gadget((u32)j) % e.Q;
+    for (size_t i = 0; i < N; i++) {
+      const u64 gu = e.rmod.mul(map_from_i64(e.Q, u[i]) % e.Q, g);
+      b[i] = e.rmod.add(e.rmod.add(tmp[i], map_from_f64(e.Q, rng.gaussian())), gu);
+    }
+  }
 }
 
 int orc_decrypt_bool(void *ev, const int32_t *s, const uint64_t *lwe) {

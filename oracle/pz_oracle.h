@@ -58,6 +58,7 @@ typedef struct {
   uint32_t rgsw_rows;                /* 2 d_a + 2 d_b */
   uint32_t auto_rows;                /* 2 d_auto */
   uint32_t n_auto_keys;              /* w + 1 */
+  uint32_t ni_ks_logb, ni_ks_d;      /* ui_to_s key switch decomposition (NI sets; 0 otherwise) */
 } orc_param_info;
 
 /* Parameter set ids, in the order of src/bool/parameters.rs:526-726. */
@@ -146,6 +147,12 @@ void orc_not(void *ev, uint64_t *c0);
 void orc_gate_batch(void *ev, void *key, const uint8_t *gates, const uint64_t *c0,
                     const uint64_t *c1, uint64_t *out, size_t count, int threads);
 void orc_sample_extract(void *ev, const uint64_t *rlwe, uint64_t *lwe, uint32_t index);
+/* non-interactive input path (NI parameter sets): unseed a batch of seeded
+ * RLWEs (ni_mp_api.rs:248-280), b [count][N] -> rlwe [count][2][N]; key switch
+ * u_j -> s (runtime.rs:1001-1063) with Ksk [2 x 50][N] in the coefficient
+ * domain (rows A then B), in/out [2][N] */
+void orc_ni_unseed(void *ev, const uint8_t seed[32], const uint64_t *b, size_t count, uint64_t *rlwe);
+void orc_ni_key_switch(void *ev, const uint64_t *ksk, const uint64_t *in, uint64_t *out);
 
 /* --- client-side harness (reference runs this on clients; out of scope) -------- */
 /* ChaCha8 stream (rand_chacha 0.3 layout), for seeding */
@@ -166,6 +173,11 @@ void orc_client_keys(void *ev, int parties, int seed_base, int32_t *s, int32_t *
 void orc_gen_server_key(void *ev, const int32_t *s, const int32_t *z,
                         const uint8_t err_seed[32], uint64_t *rgsw, uint64_t *autos,
                         uint64_t *ksk);
+/* NI batched bool encryption under the user's RLWE secret u (ni_mp_api.rs:302-345):
+ * b_out [ceil(nbits / N)][N]; and an ideal Ksk(u -> s) [2 x 50][N] (coefficient domain) */
+void orc_ni_encrypt_bools(void *ev, const int32_t *u, const uint8_t seed[32], const uint8_t err_seed[32],
+                          const uint8_t *bits, size_t nbits, uint64_t *b_out);
+void orc_ni_ksk_gen(void *ev, const int32_t *u, const int32_t *s, const uint8_t err_seed[32], uint64_t *ksk);
 /* LWE_Q encryption of bool under s (lwe.rs:104-137, m = +-Q/8) */
 void orc_encrypt_bool(void *ev, void *rng, const int32_t *s, int bit, uint64_t *lwe);
 /* noisy m = b - <a, s> (lwe.rs:139-162) and the bool decode (evaluator.rs:243-256)

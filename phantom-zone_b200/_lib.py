@@ -28,6 +28,7 @@ class PzParams(ctypes.Structure):
         ("lwe_secret_gaussian", ctypes.c_uint32), ("variant", ctypes.c_uint32),
         ("embedding_factor", ctypes.c_uint32), ("rgsw_rows", ctypes.c_uint32),
         ("auto_rows", ctypes.c_uint32), ("n_auto_keys", ctypes.c_uint32),
+        ("ni_ks_logb", ctypes.c_uint32), ("ni_ks_d", ctypes.c_uint32),
     ]
 
 
@@ -70,6 +71,12 @@ SIGNATURES = {
     "pz_ctx_set_pbs_grid_limit": (st, [vp, ctypes.c_int]),
     "pz_ctx_set_pbs_variant": (st, [vp, ctypes.c_int]),
     "pz_ctx_pbs_variant": (ctypes.c_int, [vp]),
+    "pz_ni_ksk_upload": (st, [vp, u64p, ctypes.POINTER(vp)]),
+    "pz_ni_ksk_release": (None, [vp]),
+    "pz_ni_unseed_device": (st, [vp, u8p, vp, vp, ctypes.c_size_t, vp]),
+    "pz_ni_key_switch_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_sample_extract_device": (st, [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp]),
+    "pz_ni_ingest": (st, [vp, vp, u8p, u64p, ctypes.c_size_t, u64p, ctypes.c_size_t]),
     "pz_server_create": (st, [ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(vp)]),
     "pz_server_destroy": (None, [vp]),
     "pz_server_last_error": (ctypes.c_char_p, [vp]),

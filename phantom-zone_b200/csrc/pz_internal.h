@@ -51,6 +51,8 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
 pz_status fail(pz_ctx *ctx, pz_status s, const std::string &msg);
 pz_status cuda_fail(pz_ctx *ctx, const char *what, cudaError_t e);
 u32 ks_stride(const pz_params &P);
+// DefaultDecomposer parameters for (q, logb, d) (decomposer.rs:158-178)
+Decomp decomposer(u64 q, u32 logb, u32 d);
 
 // Compiled (levelized) form of a circuit, read by the multi-session executor.
 // Wire slots: inputs first (input order), then gate outputs; bit 31 = not().

@@ -1,0 +1,406 @@
+// pz_ni.cu -- the non-interactive input path on the device: the server side
+// of a NonInteractiveBatchedFheBools (ni_mp_api.rs:182-196).
+//
+//   unseed       a-parts of a batch of seeded RLWEs regenerated from the
+//                client's ChaCha8 seed (ni_mp_api.rs:248-280): the keystream
+//                is produced block-parallel, each 64-bit word passes the
+//                uniform-in-[0, Q) acceptance test of rand's UniformInt
+//                (widening multiply, rejection zone), and an exclusive scan
+//                over the accepted words places sample k of the batch at
+//                RLWE k / N, coefficient k % N -- exactly the order of the
+//                sequential stream, rejections included.
+//   key switch   rlwe_key_switch (runtime.rs:1001-1063) from the user's RLWE
+//                secret u_j to the ideal secret s: the 50 one-bit signed
+//                digits of -A are transformed two at a time and accumulated
+//                against the user's ui_to_s key rows (Montgomery form,
+//                N^{-1} folded in), then one inverse transform of both
+//                outputs and B' += B.
+//   extract      BatchedFheBools::extract (ni_mp_api.rs:217-236): bool i is
+//                sample_extract (pbs.rs:423-449) at coefficient i % N of
+//                RLWE i / N.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "pz_internal.h"
+
+using pz::u32;
+using pz::u64;
+
+struct pz_ni_ksk {
+  pz_ctx *ctx = nullptr;
+  u64 *d_ksk = nullptr;  // [2 d][N] evaluation domain, Montgomery form with N^{-1}
+  u32 d = 0;
+  size_t bytes = 0;
+};
+
+namespace {
+
+constexpr int NI_T = 256;       // threads per RLWE (8 coefficients each, N = 2048)
+constexpr int NI_LOGN = 11;
+constexpr u64 UNSEED_MARGIN = 1024;  // keystream words generated beyond the samples needed
+
+struct ChaChaKey {
+  u32 k[8];
+};
+
+__device__ __forceinline__ u32 rotl32(u32 v, int c) { return (v << c) | (v >> (32 - c)); }
+
+// ChaCha8 block `counter` in the rand_chacha 0.3 layout (constants, 8 key
+// words, 64-bit block counter, stream id 0); 16 output words.
+__device__ __forceinline__ void chacha8_block(const ChaChaKey &key, u64 counter, u32 (&out)[16]) {
+  u32 s[16], x[16];
+  s[0] = 0x61707865u; s[1] = 0x3320646eu; s[2] = 0x79622d32u; s[3] = 0x6b206574u;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s[4 + i] = key.k[i];
+  s[12] = (u32)counter; s[13] = (u32)(counter >> 32); s[14] = 0; s[15] = 0;
+#pragma unroll
+  for (int i = 0; i < 16; i++) x[i] = s[i];
+#define PZ_QR(a, b, c, d)                              \
+  x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 16);        \
+  x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 12);        \
+  x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 8);         \
+  x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 7);
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    PZ_QR(0, 4, 8, 12) PZ_QR(1, 5, 9, 13) PZ_QR(2, 6, 10, 14) PZ_QR(3, 7, 11, 15)
+    PZ_QR(0, 5, 10, 15) PZ_QR(1, 6, 11, 12) PZ_QR(2, 7, 8, 13) PZ_QR(3, 4, 9, 14)
+  }
+#undef PZ_QR
+#pragma unroll
+  for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
+}
+
+// Block b: the 8 u64 words 8b..8b+7 of the stream (two u32 words each, low
+// first), their samples (high half of v * q) and acceptance (low half <= zone).
+__global__ void unseed_candidates_kernel(ChaChaKey key, u64 nblocks, u64 q, u64 zone, u64 *samples,
+                                         unsigned char *accept, u32 *cnt) {
+  for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nblocks; b += (u64)gridDim.x * blockDim.x) {
+    u32 w[16];
+    chacha8_block(key, b, w);
+    unsigned m = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const u64 v = (u64)w[2 * i] | ((u64)w[2 * i + 1] << 32);
+      const u64 lo = v * q, hi = __umul64hi(v, q);
+      samples[8 * b + i] = hi;
+      if (lo <= zone) m |= 1u << i;
+    }
+    accept[b] = (unsigned char)m;
+    cnt[b] = __popc(m);
+  }
+}
+
+// Exclusive scan of cnt[0, n) into off (one CTA); off[n] = total.
+__global__ void __launch_bounds__(1024) unseed_scan_kernel(const u32 *cnt, u64 n, u64 *off) {
+  __shared__ u64 part[1024];
+  const u64 per = (n + blockDim.x - 1) / blockDim.x;
+  const u64 b0 = threadIdx.x * per, b1 = min(n, b0 + per);
+  u64 local = 0;
+  for (u64 b = b0; b < b1; b++) local += cnt[b];
+  part[threadIdx.x] = local;
+  __syncthreads();
+  for (unsigned o = 1; o < blockDim.x; o <<= 1) {  // inclusive Hillis-Steele scan
+    const u64 v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  u64 run = part[threadIdx.x] - local;
+  for (u64 b = b0; b < b1; b++) {
+    off[b] = run;
+    run += cnt[b];
+  }
+  if (threadIdx.x == blockDim.x - 1) off[n] = part[threadIdx.x];
+}
+
+// Accepted sample k (k < total) -> a-part of RLWE k / N, coefficient k % N.
+__global__ void unseed_place_kernel(const u64 *samples, const unsigned char *accept, const u64 *off, u64 nblocks,
+                                    u64 total, u32 N, u64 *rlwe) {
+  for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nblocks; b += (u64)gridDim.x * blockDim.x) {
+    const unsigned m = accept[b];
+    u64 pos = off[b];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if ((m >> i) & 1u) {
+        if (pos < total) rlwe[(pos / N) * 2 * N + pos % N] = samples[8 * b + i];
+        pos++;
+      }
+    }
+  }
+}
+
+// oa += REDC(x ka + y kc), ob += REDC(x kb + y kd), lazily in [0, 2q); the
+// key rows are in the device layout (register pair -> one 16-byte word).
+__device__ __forceinline__ void ni_mac(u64 (&oa)[8], u64 (&ob)[8], const u64 (&x)[8], const u64 (&y)[8],
+                                       const u64 *ka, const u64 *kb, const u64 *kc, const u64 *kd, bool two,
+                                       const pz::RingConsts &rc) {
+  const int j = threadIdx.x;
+  const u64 q = rc.q, qi = rc.qinv_neg, q2 = rc.q << 1;
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    const int di = pz::dev_index<NI_LOGN>(j, 2 * rr);
+    u64 a[2], b[2], c[2] = {0, 0}, d[2] = {0, 0};
+    pz::ld_key2(ka + di, a[0], a[1]);
+    pz::ld_key2(kb + di, b[0], b[1]);
+    if (two) {
+      pz::ld_key2(kc + di, c[0], c[1]);
+      pz::ld_key2(kd + di, d[0], d[1]);
+    }
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int r = 2 * rr + e;
+      u64 hi, lo, hi2, lo2;
+      pz::mul128(x[r], a[e], hi, lo);
+      pz::mul128(x[r], b[e], hi2, lo2);
+      if (two) {
+        pz::mac128(y[r], c[e], hi, lo);
+        pz::mac128(y[r], d[e], hi2, lo2);
+      }
+      const u64 va = oa[r] + pz::redc(hi, lo, q, qi), vb = ob[r] + pz::redc(hi2, lo2, q, qi);
+      oa[r] = va >= q2 ? va - q2 : va;
+      ob[r] = vb >= q2 ? vb - q2 : vb;
+    }
+  }
+}
+
+// One RLWE per CTA: rlwe_key_switch of in[c] with the user's key rows.
+__global__ void __launch_bounds__(NI_T, 2)
+    ni_key_switch_kernel(pz::RingConsts rc, pz::Decomp dp, u32 d, const u64 *ksk, const u64 *in, u64 *out,
+                         size_t count) {
+  constexpr int N = 1 << NI_LOGN;
+  extern __shared__ u64 sm[];  // 2N words: exchange buffer of the two-polynomial transforms
+  const int j = threadIdx.x;
+  const u64 q = rc.q;
+  for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    const u64 *p = in + c * 2 * N;
+    u64 st[8], oa[8], ob[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      st[r] = pz::decomp_init(q - p[pz::pos_coef<NI_LOGN>(j, r)], dp);  // elwise_neg_mut, then decompose
+      oa[r] = 0;
+      ob[r] = 0;
+    }
+#pragma unroll 1
+    for (u32 jd = 0; jd < d; jd += 2) {
+      const bool two = jd + 1 < d;  // uniform
+      u64 x[8], y[8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        x[r] = pz::decomp_next(st[r], dp);
+        y[r] = two ? pz::decomp_next(st[r], dp) : 0;
+      }
+      if (two) pz::ntt_fwd<NI_LOGN, true>(x, y, sm, rc);
+      else pz::ntt_fwd<NI_LOGN, false>(x, x, sm, rc);
+      ni_mac(oa, ob, x, y, ksk + (size_t)jd * N, ksk + (size_t)(d + jd) * N, ksk + (size_t)(jd + 1) * N,
+             ksk + (size_t)(d + jd + 1) * N, two, rc);
+    }
+    pz::ntt_inv<NI_LOGN, true>(oa, ob, sm, rc);
+    u64 *o = out + c * 2 * N;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int pc = pz::pos_coef<NI_LOGN>(j, r);
+      o[pc] = pz::reduce2(oa[r], q);
+      o[N + pc] = pz::add_mod(pz::reduce2(ob[r], q), p[N + pc], q);  // elwise_add_mut(B', B)
+    }
+    __syncthreads();
+  }
+}
+
+// out[c] = sample_extract(rlwe[idx[c] / N], idx[c] % N); an index past the
+// batch leaves out[c] unchanged.
+__global__ void extract_kernel(const u64 *rlwe, size_t rlwe_count, const u32 *idx, u64 *out, size_t count, u32 N,
+                               u64 q) {
+  for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    const u32 i = idx[c];
+    const size_t ct = i / N, k = i % N;
+    if (ct >= rlwe_count) continue;
+    const u64 *a = rlwe + ct * 2 * N, *b = a + N;
+    u64 *o = out + c * (size_t)(N + 1);
+    for (u32 t = threadIdx.x; t <= N; t += blockDim.x) {
+      if (t == 0) {
+        o[0] = b[k];
+      } else {
+        const size_t ii = t - 1;
+        o[t] = ii <= k ? a[k - ii] : q - a[N + k - ii];  // neg = q - x (modulus_u64.rs:147-149)
+      }
+    }
+  }
+}
+
+pz_status ni_check(pz_ctx *c) {
+  if (!c) return PZ_ERR_INVALID_ARGUMENT;
+  if (c->P.variant != 2 || c->P.ni_ks_d == 0)
+    return pz::fail(c, PZ_ERR_NOT_SUPPORTED, "not a non-interactive parameter set");
+  if (c->logn != NI_LOGN) return pz::fail(c, PZ_ERR_NOT_SUPPORTED, "ring dimension other than 2048");
+  return PZ_OK;
+}
+
+int grid_of(size_t n, int cap) { return (int)std::min<size_t>(std::max<size_t>(n, 1), (size_t)cap); }
+
+}  // namespace
+
+extern "C" {
+
+pz_status pz_ni_ksk_upload(pz_ctx *c, const uint64_t *ksk, pz_ni_ksk **out) {
+  pz_status s = ni_check(c);
+  if (s != PZ_OK) return s;
+  if (!ksk || !out) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "pz_ni_ksk_upload: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(c->mu);
+  PZ_CK(c, cudaSetDevice(c->device));
+  const size_t N = c->P.rlwe_n, polys = 2 * (size_t)c->P.ni_ks_d;
+  pz_ni_ksk *k = new pz_ni_ksk();
+  k->ctx = c;
+  k->d = c->P.ni_ks_d;
+  k->bytes = polys * N * 8;
+  u64 *stage = nullptr;
+  cudaError_t e = cudaMalloc(&k->d_ksk, k->bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&stage, k->bytes);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(stage, ksk, k->bytes, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = pz::launch_key_convert((int)c->logn, stage, k->d_ksk, polys, c->rc, c->conv_c, c->conv_cs, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(stage);
+  if (e != cudaSuccess) {
+    cudaFree(k->d_ksk);
+    delete k;
+    return pz::cuda_fail(c, "pz_ni_ksk_upload", e);
+  }
+  *out = k;
+  return PZ_OK;
+}
+
+void pz_ni_ksk_release(pz_ni_ksk *k) {
+  if (!k) return;
+  cudaSetDevice(k->ctx->device);
+  cudaFree(k->d_ksk);
+  delete k;
+}
+
+pz_status pz_ni_unseed_device(pz_ctx *c, const uint8_t seed[32], const uint64_t *d_b, uint64_t *d_rlwe, size_t count,
+                              void *stream) {
+  pz_status s = ni_check(c);
+  if (s != PZ_OK) return s;
+  if (!seed || (count && (!d_b || !d_rlwe))) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (count == 0) return PZ_OK;
+  PZ_CK(c, cudaSetDevice(c->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const u32 N = c->P.rlwe_n;
+  const u64 q = c->P.rlwe_q;
+  const u64 total = (u64)count * N;
+  const u64 nblocks = (total + UNSEED_MARGIN + 7) / 8;
+  ChaChaKey key;
+  for (int i = 0; i < 8; i++)
+    key.k[i] = (u32)seed[4 * i] | ((u32)seed[4 * i + 1] << 8) | ((u32)seed[4 * i + 2] << 16) |
+               ((u32)seed[4 * i + 3] << 24);
+  // rand 0.8 UniformInt<u64>::new_inclusive(0, q - 1): range q, zone = MAX - (2^64 - q) % q
+  const u64 zone = ~0ull - ((0ull - q) % q);
+  u64 *samples = nullptr, *off = nullptr;
+  unsigned char *acc = nullptr;
+  u32 *cnt = nullptr;
+  cudaError_t e = cudaMallocAsync(&samples, nblocks * 8 * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&off, (nblocks + 1) * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&acc, nblocks, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, nblocks * 4, st);
+  if (e == cudaSuccess) {
+    unseed_candidates_kernel<<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(key, nblocks, q, zone, samples,
+                                                                                     acc, cnt);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    unseed_scan_kernel<<<1, 1024, 0, st>>>(cnt, nblocks, off);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    unseed_place_kernel<<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(samples, acc, off, nblocks, total, N,
+                                                                               d_rlwe);
+    e = cudaGetLastError();
+  }
+  // b-parts: row 1 of every RLWE
+  if (e == cudaSuccess)
+    e = cudaMemcpy2DAsync(d_rlwe + N, 2 * N * 8, d_b, N * 8, N * 8, count, cudaMemcpyDeviceToDevice, st);
+  u64 accepted = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&accepted, off + nblocks, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFreeAsync(samples, st);
+  cudaFreeAsync(off, st);
+  cudaFreeAsync(acc, st);
+  cudaFreeAsync(cnt, st);
+  if (e != cudaSuccess) return pz::cuda_fail(c, "pz_ni_unseed_device", e);
+  if (accepted < total)  // more rejections than the margin covers (probability ~0)
+    return pz::fail(c, PZ_ERR_NOT_SUPPORTED, "unseed: rejection margin exhausted");
+  return PZ_OK;
+}
+
+pz_status pz_ni_key_switch_device(pz_ctx *c, const pz_ni_ksk *k, const uint64_t *d_in, uint64_t *d_out, size_t count,
+                                  void *stream) {
+  pz_status s = ni_check(c);
+  if (s != PZ_OK) return s;
+  if (!k || k->ctx != c) return pz::fail(c, PZ_ERR_KEY_MISMATCH, "key-switching key does not belong to this context");
+  if (count && (!d_in || !d_out)) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (count == 0) return PZ_OK;
+  PZ_CK(c, cudaSetDevice(c->device));
+  const pz::Decomp dp = pz::decomposer(c->P.rlwe_q, c->P.ni_ks_logb, c->P.ni_ks_d);
+  const size_t smem = 2 * (size_t)c->P.rlwe_n * 8;
+  ni_key_switch_kernel<<<grid_of(count, 65535), NI_T, smem, (cudaStream_t)stream>>>(c->rc, dp, k->d, k->d_ksk, d_in,
+                                                                                  d_out, count);
+  PZ_CK(c, cudaGetLastError());
+  return PZ_OK;
+}
+
+pz_status pz_sample_extract_device(pz_ctx *c, const uint64_t *d_rlwe, size_t rlwe_count, const uint32_t *d_index,
+                                   uint64_t *d_lwe, size_t count, void *stream) {
+  if (!c) return PZ_ERR_INVALID_ARGUMENT;
+  if (count && (!d_rlwe || !d_index || !d_lwe)) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (count == 0) return PZ_OK;
+  PZ_CK(c, cudaSetDevice(c->device));
+  extract_kernel<<<grid_of(count, 65535), 256, 0, (cudaStream_t)stream>>>(d_rlwe, rlwe_count, d_index, d_lwe, count,
+                                                                          c->P.rlwe_n, c->P.rlwe_q);
+  PZ_CK(c, cudaGetLastError());
+  return PZ_OK;
+}
+
+pz_status pz_ni_ingest(pz_ctx *c, const pz_ni_ksk *k, const uint8_t seed[32], const uint64_t *b, size_t rlwe_count,
+                       uint64_t *lwe_out, size_t nbools) {
+  pz_status s = ni_check(c);
+  if (s != PZ_OK) return s;
+  if (!k || k->ctx != c) return pz::fail(c, PZ_ERR_KEY_MISMATCH, "key-switching key does not belong to this context");
+  if (!seed || (rlwe_count && !b) || (nbools && !lwe_out))
+    return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
+  const size_t N = c->P.rlwe_n;
+  if (nbools > rlwe_count * N) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "more bools than the batch holds");
+  if (rlwe_count == 0) return PZ_OK;
+  std::lock_guard<std::mutex> lock(c->mu);
+  PZ_CK(c, cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+  u64 *d_b = nullptr, *d_r = nullptr, *d_k = nullptr, *d_l = nullptr;
+  u32 *d_i = nullptr;
+  std::vector<u32> idx(nbools);
+  for (size_t i = 0; i < nbools; i++) idx[i] = (u32)i;
+  cudaError_t e = cudaMallocAsync(&d_b, rlwe_count * N * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_r, rlwe_count * 2 * N * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_k, rlwe_count * 2 * N * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_l, std::max<size_t>(nbools, 1) * (N + 1) * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_i, std::max<size_t>(nbools, 1) * 4, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_b, b, rlwe_count * N * 8, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && nbools) e = cudaMemcpyAsync(d_i, idx.data(), nbools * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) {
+    s = pz_ni_unseed_device(c, seed, d_b, d_r, rlwe_count, st);
+    if (s == PZ_OK) s = pz_ni_key_switch_device(c, k, d_r, d_k, rlwe_count, st);
+    if (s == PZ_OK) s = pz_sample_extract_device(c, d_k, rlwe_count, d_i, d_l, nbools, st);
+    if (s == PZ_OK && nbools) e = cudaMemcpyAsync(lwe_out, d_l, nbools * (N + 1) * 8, cudaMemcpyDeviceToHost, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFreeAsync(d_b, st);
+  cudaFreeAsync(d_r, st);
+  cudaFreeAsync(d_k, st);
+  cudaFreeAsync(d_l, st);
+  cudaFreeAsync(d_i, st);
+  cudaStreamSynchronize(st);
+  if (s != PZ_OK) return s;
+  if (e != cudaSuccess) return pz::cuda_fail(c, "pz_ni_ingest", e);
+  return PZ_OK;
+}
+
+}  // extern "C"

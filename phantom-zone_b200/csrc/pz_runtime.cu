@@ -39,6 +39,8 @@ pz_params full_params(int id) {
   p.rgsw_rows = 2 * p.rlrg_d_a + 2 * p.rlrg_d_b;
   p.auto_rows = 2 * p.auto_d;
   p.n_auto_keys = p.w + 1;
+  p.ni_ks_logb = p.variant == 2 ? 1 : 0;  // parameters.rs:616-697
+  p.ni_ks_d = p.variant == 2 ? 50 : 0;
   return p;
 }
 
@@ -83,6 +85,8 @@ pz::Decomp make_decomp(u64 q, u32 logb, u32 d) {  // decomposer.rs:158-178
 }  // namespace
 
 namespace pz {
+Decomp decomposer(u64 q, u32 logb, u32 d) { return make_decomp(q, logb, d); }
+
 pz_status fail(pz_ctx *ctx, pz_status s, const std::string &msg) {
   if (ctx) ctx->err = msg;
   return s;

@@ -84,6 +84,32 @@ class DeviceKey:
             pass
 
 
+class NiKsk:
+    """A user's ui_to_s key-switching key resident on the engine's device."""
+
+    def __init__(self, engine, handle):
+        self.engine = engine
+        self.h = handle
+
+    def release(self):
+        if self.h:
+            lib().pz_ni_ksk_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def _seed(seed):
+    seed = bytes(seed)
+    if len(seed) != 32:
+        raise ValueError("seed must be 32 bytes")
+    return (ctypes.c_uint8 * 32)(*seed)
+
+
 class Engine:
     def __init__(self, param, device=0, ntt_root=0):
         self.param_id = param_id(param)
@@ -201,6 +227,37 @@ class Engine:
     def rlwe_auto_device(self, key, rlwe, slot, trivial=False, stream=None):
         check(lib().pz_rlwe_auto_device(self.h, key.h, _ptr(rlwe), _ptr(slot), slot.numel(), int(trivial),
                                         _stream(stream)), self.h, "pz_rlwe_auto_device")
+
+    # -- non-interactive input path ---------------------------------------------
+    def upload_ni_ksk(self, ksk):
+        """ui_to_s key of one user: [2 * ni_ks_d][N] coefficient domain (rows A then B)."""
+        ksk = np.ascontiguousarray(ksk, dtype=np.uint64)
+        if ksk.size != 2 * self.p.ni_ks_d * self.N or self.p.ni_ks_d == 0:
+            raise ValueError("ui_to_s key has the wrong size (or the set is not non-interactive)")
+        h = vp()
+        check(lib().pz_ni_ksk_upload(self.h, ksk.ctypes.data_as(u64p), ctypes.byref(h)), self.h, "pz_ni_ksk_upload")
+        return NiKsk(self, h)
+
+    def ni_unseed_device(self, seed, d_b, d_rlwe, stream=None):
+        check(lib().pz_ni_unseed_device(self.h, _seed(seed), _ptr(d_b), _ptr(d_rlwe), d_b.numel() // self.N,
+                                        _stream(stream)), self.h, "pz_ni_unseed_device")
+
+    def ni_key_switch_device(self, ksk, d_in, d_out, stream=None):
+        check(lib().pz_ni_key_switch_device(self.h, ksk.h, _ptr(d_in), _ptr(d_out), d_in.numel() // (2 * self.N),
+                                            _stream(stream)), self.h, "pz_ni_key_switch_device")
+
+    def sample_extract_device(self, d_rlwe, d_index, d_lwe, stream=None):
+        check(lib().pz_sample_extract_device(self.h, _ptr(d_rlwe), d_rlwe.numel() // (2 * self.N), _ptr(d_index),
+                                             _ptr(d_lwe), d_index.numel(), _stream(stream)), self.h,
+              "pz_sample_extract_device")
+
+    def ni_ingest(self, ksk, seed, b, nbools):
+        """Host buffers: seeded RLWE b-parts [count][N] -> LWEs [nbools][N+1] under s."""
+        b = np.ascontiguousarray(b, dtype=np.uint64).reshape(-1, self.N)
+        out = np.zeros((nbools, self.L), np.uint64)
+        check(lib().pz_ni_ingest(self.h, ksk.h, _seed(seed), b.ctypes.data_as(u64p), len(b),
+                                 out.ctypes.data_as(u64p), nbools), self.h, "pz_ni_ingest")
+        return out
 
     def lwe_key_switch_device(self, key, lwe_in, out, stream=None):
         count = lwe_in.numel() // self.L

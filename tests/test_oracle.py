@@ -241,3 +241,21 @@ def test_pbs_prelude_is_the_gate():
     for g in TRUTH:
         out, _, _, _ = key.pbs(g, combine(ev, g, c0, c1))
         assert np.array_equal(out, key.gate(g, c0, c1))
+
+
+@pytest.mark.parametrize("param", ["NI_2P", "NI_8P"])
+def test_ni_input_path_round_trip(param):
+    """Non-interactive inputs (ni_mp_api.rs:248-440): bools encrypted as seeded
+    RLWEs under a user's secret u, unseeded, key-switched u -> s with Ksk(u -> s)
+    and extracted decrypt under s; a wrong seed does not."""
+    O = oracle()
+    ev, (s, z, sp, zp), _, _ = oracle_setup(param)
+    u = sp[-1]
+    ksk = ev.ni_ksk_gen(u, s)
+    bits = np.random.default_rng(5).integers(0, 2, ev.N + 300).astype(np.uint8)  # two RLWEs, ragged
+    b = ev.ni_encrypt_bools(u, bits, b"\x07" * 32)
+    assert b.shape == (2, ev.N)
+    lwes = ev.ni_ingest(ksk, b"\x07" * 32, b, len(bits))
+    assert np.array_equal(ev.decrypt_bool(s, lwes), bits)
+    bad = ev.ni_ingest(ksk, b"\x08" * 32, b, 64)
+    assert not np.array_equal(ev.decrypt_bool(s, bad), bits[:64])
