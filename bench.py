@@ -330,6 +330,76 @@ def microbench(P, torch, device, count=4096, reps=5):
             "ext_product_modmul_per_s": count * 57344 / (ep_ms / 1e3)}
 
 
+def ni_ingest_bench(P, torch, device, count=64, reps=3):
+    """Non-interactive input path at NonInteractiveLTE8Party: `count` seeded
+    RLWEs (count x N bools) unseeded, key-switched u_j -> s and extracted,
+    device buffers, CUDA events; plus the key switch alone."""
+    prm = "NI_8P"
+    p = P.params(prm)
+    N = p.rlwe_n
+    eng = P.Engine(prm, device=device)
+    rng = np.random.default_rng(0x33)
+    ksk = eng.upload_ni_ksk(rng.integers(0, p.rlwe_q, (2 * p.ni_ks_d, N), dtype=np.uint64))
+    d_b = torch.from_numpy(rng.integers(0, p.rlwe_q, (count, N), dtype=np.uint64).view(np.int64)).cuda()
+    d_r = torch.empty((count, 2, N), dtype=torch.int64, device="cuda")
+    d_k = torch.empty_like(d_r)
+    idx = torch.arange(count * N, dtype=torch.int32, device="cuda")
+    d_l = torch.empty((count * N, N + 1), dtype=torch.int64, device="cuda")
+    seed = bytes(range(32))
+
+    def run():
+        eng.ni_unseed_device(seed, d_b, d_r)
+        eng.ni_key_switch_device(ksk, d_r, d_k)
+        eng.sample_extract_device(d_k, idx, d_l)
+
+    run()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    a.record()
+    for _ in range(reps):
+        run()
+    b.record()
+    for _ in range(reps):
+        eng.ni_key_switch_device(ksk, d_r, d_k)
+    c.record()
+    torch.cuda.synchronize()
+    all_ms = a.elapsed_time(b) / reps
+    ks_ms = b.elapsed_time(c) / reps
+    logn = int(np.log2(N))
+    mm = count * (p.ni_ks_d * (N // 2) * logn + 2 * ((N // 2) * logn + N) + 2 * p.ni_ks_d * N)
+    ksk.release()
+    eng.close()
+    del d_l
+    return {"config": f"NI_8P, {count} seeded RLWEs = {count * N} bools: unseed + rlwe_key_switch (d=50) + extract",
+            "ingest_ms": all_ms, "bools_per_s": count * N / (all_ms / 1e3), "key_switch_ms": ks_ms,
+            "rlwe_key_switches_per_s": count / (ks_ms / 1e3), "key_switch_modmul_per_s": mm / (ks_ms / 1e3)}
+
+
+def key_upload_bench(P, device):
+    """Server-key upload at NonInteractiveLTE8Party: the full expanded key from
+    the host vs the seeded form (auto-key B rows and LWE-KSK column 0 plus two
+    seeds, A parts regenerated on the device)."""
+    prm = "NI_8P"
+    p = P.params(prm)
+    rgsw, autos, ksk = synthetic_key(p, 0x5EED)
+    auto_b = np.ascontiguousarray(autos[:, p.auto_d:, :])
+    lwe_b = np.ascontiguousarray(ksk[:, 0])
+    eng = P.Engine(prm, device=device)
+    eng.upload_key(rgsw, autos, ksk).release()  # warm-up
+    t0 = time.perf_counter()
+    k1 = eng.upload_key(rgsw, autos, ksk)
+    t1 = time.perf_counter()
+    k2 = eng.upload_key_seeded(rgsw, auto_b, b"\x01" * 32, lwe_b, b"\x02" * 32)
+    t2 = time.perf_counter()
+    k1.release()
+    k2.release()
+    eng.close()
+    return {"config": "NI_8P server key, host -> device, wall clock", "full_ms": (t1 - t0) * 1e3,
+            "seeded_ms": (t2 - t1) * 1e3, "full_host_bytes": int(rgsw.nbytes + autos.nbytes + ksk.nbytes),
+            "seeded_host_bytes": int(rgsw.nbytes + auto_b.nbytes + lwe_b.nbytes + 64)}
+
+
 def u8_job(P, op):
     C = P.Circuit()
     a, b = C.input_u8(), C.input_u8()
@@ -590,7 +660,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the microbench / ragged / serving sub-results")
     ap.add_argument("--mode", default="wavefront",
-                    choices=["wavefront", "br-kernel", "ks-kernel", "microbench", "ragged", "serving", "kernels"],
+                    choices=["wavefront", "br-kernel", "ks-kernel", "microbench", "ragged", "serving", "kernels",
+                             "ni", "key-upload"],
                     help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
@@ -598,11 +669,12 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.mode in ("microbench", "ragged", "serving", "kernels"):
+    if args.mode in ("microbench", "ragged", "serving", "kernels", "ni", "key-upload"):
         import torch
         P = pz()
         fn = {"microbench": lambda: microbench(P, torch, 0), "ragged": lambda: ragged_batch(P, 0),
-              "serving": lambda: serving(P, 0), "kernels": lambda: kernels_case(P, torch, 0)}[args.mode]
+              "serving": lambda: serving(P, 0), "kernels": lambda: kernels_case(P, torch, 0),
+              "ni": lambda: ni_ingest_bench(P, torch, 0), "key-upload": lambda: key_upload_bench(P, 0)}[args.mode]
         print(json.dumps({"mode": args.mode, **fn()}), flush=True)
         return
     if args.mode != "wavefront":
@@ -703,6 +775,8 @@ def main():
         extras["microbench"] = microbench(P, torch, local)
         extras["ragged"] = ragged_batch(P, local)
         extras["serving"] = serving(P, local)
+        extras["ni_ingest"] = ni_ingest_bench(P, torch, local)
+        extras["key_upload"] = key_upload_bench(P, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

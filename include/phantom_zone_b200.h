@@ -238,6 +238,27 @@ pz_status pz_circuit_capture_graph(pz_ctx *ctx, const pz_key *key, pz_circuit *c
                                    uint64_t *d_outputs, void *stream);
 pz_status pz_circuit_replay_graph(pz_circuit *c, void *stream);
 
+/* ---- seeded server keys (device-side expansion) ------------------------------------
+ * What a server receives after key aggregation (SeededInteractiveMultiPartyServerKey,
+ * SeededNonInteractiveMultiPartyServerKey; bool/keys.rs:536-781, 851-1004): the RGSW
+ * ciphertexts in full, but only the B rows of the auto keys and column 0 of the LWE
+ * key-switching key -- their A parts come from CRS-derived ChaCha8 seeds.  The upload
+ * regenerates the A parts on the device exactly as ServerKeyEvaluationDomain::from
+ * does (keys.rs:687-781; NI: keys.rs:869-1004), then converts like pz_key_upload.
+ *   rgsw       [n][2 d_a + 2 d_b][N]  as in pz_server_key_view
+ *   auto_b     [w + 1][d_auto][N]     B rows, slots in auto_element_dlogs order
+ *                                     (parameters.rs:364-370: 0 = -g, k = g^k)
+ *   lwe_ksk_b  [d_ks N]               column 0 of the LWE KSK rows
+ *   auto_seed, lwe_ksk_seed           cr_seed.auto_keys_cts_seed(), cr_seed.lwe_ksk_cts_seed() */
+typedef struct pz_seeded_server_key_view {
+  const uint64_t *rgsw;
+  const uint64_t *auto_b;
+  const uint64_t *lwe_ksk_b;
+  uint8_t auto_seed[32];
+  uint8_t lwe_ksk_seed[32];
+} pz_seeded_server_key_view;
+pz_status pz_key_upload_seeded(pz_ctx *ctx, const pz_seeded_server_key_view *key, pz_key **out);
+
 /* ---- non-interactive input path (NI parameter sets, N = 2048) ---------------------
  * A user of a non-interactive session sends its bools as seeded RLWEs under its own
  * RLWE secret u_j (NonInteractiveBatchedFheBools, bool/ni_mp_api.rs:182-196); the
@@ -249,6 +270,10 @@ typedef struct pz_ni_ksk pz_ni_ksk;
  * (ShoupNonInteractiveServerKeyEvaluationDomain::ui_to_s_ksk, bool/keys.rs:1083-1085,
  * before its forward NTT) */
 pz_status pz_ni_ksk_upload(pz_ctx *ctx, const uint64_t *ksk, pz_ni_ksk **out);
+/* the same key from its B rows [ni_ks_d][N] and its seed
+ * (cr_seed.ui_to_s_ks_seed_for_user_i(user), keys.rs:965-1000): A rows regenerated
+ * on the device */
+pz_status pz_ni_ksk_upload_seeded(pz_ctx *ctx, const uint64_t *ksk_b, const uint8_t seed[32], pz_ni_ksk **out);
 void pz_ni_ksk_release(pz_ni_ksk *ksk);
 /* NonInteractiveBatchedFheBools::from (ni_mp_api.rs:248-280): d_b [count][N] (the
  * seeded RLWEs' b-parts) -> d_rlwe [count][2][N], a-parts from ChaCha8(seed) in batch

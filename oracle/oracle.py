@@ -81,6 +81,8 @@ def lib():
             "orc_ni_key_switch": (None, [vp, u64p, u64p, u64p]),
             "orc_ni_encrypt_bools": (None, [vp, i32p, u8p, u8p, u8p, ctypes.c_size_t, u64p]),
             "orc_ni_ksk_gen": (None, [vp, i32p, i32p, u8p, u64p]),
+            "orc_expand_seeded_key": (None, [vp, u64p, u8p, u64p, u8p, u64p, u64p]),
+            "orc_expand_ni_ksk": (None, [vp, u64p, u8p, u64p]),
             "orc_u8_op": (ctypes.c_int, [vp, vp, ctypes.c_int, u64p, u64p, u64p, u64p, u64p, u64p, ctypes.POINTER(ctypes.c_int)]),
             "orc_generate_prime": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
             "orc_ntt_custom_new": (vp, [ctypes.c_uint64, ctypes.c_size_t]),
@@ -307,6 +309,23 @@ class Evaluator:
         out = np.empty(2 * self.N, np.uint64)
         lib().orc_ni_key_switch(self.h, _p(ksk), _p(r), _p(out))
         return out.reshape(2, self.N)
+
+    def expand_seeded_key(self, auto_b, auto_seed, lwe_b, lwe_seed):
+        """Seeded server key -> coefficient-domain autos and LWE KSK (keys.rs:687-781)."""
+        i = self.info
+        autos = np.empty((i.n_auto_keys, i.auto_rows, self.N), np.uint64)
+        ksk = np.empty((i.lwe_d * self.N, self.n + 1), np.uint64)
+        lib().orc_expand_seeded_key(self.h, _p(np.ascontiguousarray(auto_b, np.uint64)),
+                                    (ctypes.c_uint8 * 32)(*bytes(auto_seed)),
+                                    _p(np.ascontiguousarray(lwe_b, np.uint64)),
+                                    (ctypes.c_uint8 * 32)(*bytes(lwe_seed)), _p(autos), _p(ksk))
+        return autos, ksk
+
+    def expand_ni_ksk(self, b, seed):
+        out = np.empty((2 * self.NI_KS_D, self.N), np.uint64)
+        lib().orc_expand_ni_ksk(self.h, _p(np.ascontiguousarray(b, np.uint64)), (ctypes.c_uint8 * 32)(*bytes(seed)),
+                                _p(out))
+        return out
 
     def ni_ingest(self, ksk, seed, b, nbits):
         """unseed -> key switch -> extract every bool (the server's NI input path)."""

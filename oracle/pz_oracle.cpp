@@ -1402,6 +1402,39 @@ void orc_ni_ksk_gen(void *ev, const int32_t *u, const int32_t *s, const uint8_t 
   }
 }
 
+// ServerKeyEvaluationDomain::from(&Seeded...ServerKey), keys.rs:687-781 and
+// (NI) 869-1004, before the forward NTT: auto keys slot by slot in
+// auto_element_dlogs order (parameters.rs:364-370), each d_auto A rows from
+// the auto stream then its B rows; LWE KSK row by row, words 1..n from the
+// ksk stream mod q_ks, word 0 = b.  Outputs in the layout of orc_key_new.
+void orc_expand_seeded_key(void *ev, const uint64_t *auto_b, const uint8_t auto_seed[32], const uint64_t *lwe_b,
+                           const uint8_t lwe_seed[32], uint64_t *autos, uint64_t *ksk) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N, n = e.n, da = e.p.auto_d;
+  ChaCha8 auto_prng(auto_seed);
+  for (size_t k = 0; k <= e.p.w; k++) {
+    u64 *key = autos + k * 2 * da * N;
+    for (size_t i = 0; i < da * N; i++) key[i] = auto_prng.uniform_mod(e.Q);
+    memcpy(key + da * N, auto_b + k * da * N, da * N * 8);
+  }
+  ChaCha8 ksk_prng(lwe_seed);
+  const size_t rows = (size_t)e.p.lwe_d * N;
+  for (size_t r = 0; r < rows; r++) {
+    u64 *row = ksk + r * (n + 1);
+    for (size_t c = 1; c <= n; c++) row[c] = ksk_prng.uniform_mod(e.p.lwe_q);
+    row[0] = lwe_b[r];
+  }
+}
+
+// ui_to_s key of one user from its B rows and seed (keys.rs:965-1000).
+void orc_expand_ni_ksk(void *ev, const uint64_t *b, const uint8_t seed[32], uint64_t *ksk) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N, d = e.dec_ni.d;
+  ChaCha8 prng(seed);
+  for (size_t i = 0; i < d * N; i++) ksk[i] = prng.uniform_mod(e.Q);
+  memcpy(ksk + d * N, b, d * N * 8);
+}
+
 int orc_decrypt_bool(void *ev, const int32_t *s, const uint64_t *lwe) {
   Eval &e = *(Eval *)ev;
   const u64 Q = e.Q;

@@ -178,6 +178,12 @@ void orc_gen_server_key(void *ev, const int32_t *s, const int32_t *z,
 void orc_ni_encrypt_bools(void *ev, const int32_t *u, const uint8_t seed[32], const uint8_t err_seed[32],
                           const uint8_t *bits, size_t nbits, uint64_t *b_out);
 void orc_ni_ksk_gen(void *ev, const int32_t *u, const int32_t *s, const uint8_t err_seed[32], uint64_t *ksk);
+/* Seeded server key expansion (keys.rs:687-781, 869-1004) before the forward NTT:
+ * auto_b [w+1][d_auto][N], lwe_b [d_ks N] -> autos [w+1][2 d_auto][N], ksk [d_ks N][n+1];
+ * and one user's ui_to_s key from its B rows [50][N] -> [100][N] */
+void orc_expand_seeded_key(void *ev, const uint64_t *auto_b, const uint8_t auto_seed[32], const uint64_t *lwe_b,
+                           const uint8_t lwe_seed[32], uint64_t *autos, uint64_t *ksk);
+void orc_expand_ni_ksk(void *ev, const uint64_t *b, const uint8_t seed[32], uint64_t *ksk);
 /* LWE_Q encryption of bool under s (lwe.rs:104-137, m = +-Q/8) */
 void orc_encrypt_bool(void *ev, void *rng, const int32_t *s, int bit, uint64_t *lwe);
 /* noisy m = b - <a, s> (lwe.rs:139-162) and the bool decode (evaluator.rs:243-256)

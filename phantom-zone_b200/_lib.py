@@ -36,6 +36,11 @@ class PzServerKeyView(ctypes.Structure):
     _fields_ = [("rgsw", u64p), ("autos", u64p), ("lwe_ksk", u64p)]
 
 
+class PzSeededServerKeyView(ctypes.Structure):
+    _fields_ = [("rgsw", u64p), ("auto_b", u64p), ("lwe_ksk_b", u64p),
+                ("auto_seed", ctypes.c_uint8 * 32), ("lwe_ksk_seed", ctypes.c_uint8 * 32)]
+
+
 class PzServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_size_t) for n in ("pending", "active", "done", "failed", "arena_slots",
                                                 "arena_slots_used", "arena_bytes", "sessions", "key_bytes")] + \
@@ -73,6 +78,8 @@ SIGNATURES = {
     "pz_ctx_pbs_variant": (ctypes.c_int, [vp]),
     "pz_ni_ksk_upload": (st, [vp, u64p, ctypes.POINTER(vp)]),
     "pz_ni_ksk_release": (None, [vp]),
+    "pz_ni_ksk_upload_seeded": (st, [vp, u64p, u8p, ctypes.POINTER(vp)]),
+    "pz_key_upload_seeded": (st, [vp, ctypes.POINTER(PzSeededServerKeyView), ctypes.POINTER(vp)]),
     "pz_ni_unseed_device": (st, [vp, u8p, vp, vp, ctypes.c_size_t, vp]),
     "pz_ni_key_switch_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_sample_extract_device": (st, [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp]),

@@ -54,6 +54,14 @@ u32 ks_stride(const pz_params &P);
 // DefaultDecomposer parameters for (q, logb, d) (decomposer.rs:158-178)
 Decomp decomposer(u64 q, u32 logb, u32 d);
 
+// RandomFillUniformInModulus (random.rs:93-110) over the ChaCha8 stream of
+// `seed`, on the device: `total` samples uniform in [0, q), sample k stored at
+// dst[(k / row_len) * row_stride + row_off + k % row_len].  Synchronous.
+pz_status seeded_fill_u64(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride,
+                          u64 row_off, u64 *dst, cudaStream_t st);
+pz_status seeded_fill_u32(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride,
+                          u64 row_off, u32 *dst, cudaStream_t st);
+
 // Compiled (levelized) form of a circuit, read by the multi-session executor.
 // Wire slots: inputs first (input order), then gate outputs; bit 31 = not().
 struct CircuitView {

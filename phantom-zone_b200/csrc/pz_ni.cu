@@ -2,13 +2,16 @@
 // of a NonInteractiveBatchedFheBools (ni_mp_api.rs:182-196).
 //
 //   unseed       a-parts of a batch of seeded RLWEs regenerated from the
-//                client's ChaCha8 seed (ni_mp_api.rs:248-280): the keystream
-//                is produced block-parallel, each 64-bit word passes the
-//                uniform-in-[0, Q) acceptance test of rand's UniformInt
-//                (widening multiply, rejection zone), and an exclusive scan
-//                over the accepted words places sample k of the batch at
-//                RLWE k / N, coefficient k % N -- exactly the order of the
-//                sequential stream, rejections included.
+//                client's ChaCha8 seed (ni_mp_api.rs:248-280) by the seeded
+//                uniform fill below.
+//   seeded fill  RandomFillUniformInModulus over one ChaCha8 stream
+//                (random.rs:93-110): the keystream is produced
+//                block-parallel, each 64-bit word passes the uniform-in-[0, q)
+//                acceptance test of rand's UniformInt (widening multiply,
+//                rejection zone), and an exclusive scan over the accepted
+//                words places sample k at its row-major destination --
+//                exactly the order of the sequential stream, rejections
+//                included.  Also used to expand seeded server keys.
 //   key switch   rlwe_key_switch (runtime.rs:1001-1063) from the user's RLWE
 //                secret u_j to the ideal secret s: the 50 one-bit signed
 //                digits of -A are transformed two at a time and accumulated
@@ -114,16 +117,17 @@ __global__ void __launch_bounds__(1024) unseed_scan_kernel(const u32 *cnt, u64 n
   if (threadIdx.x == blockDim.x - 1) off[n] = part[threadIdx.x];
 }
 
-// Accepted sample k (k < total) -> a-part of RLWE k / N, coefficient k % N.
-__global__ void unseed_place_kernel(const u64 *samples, const unsigned char *accept, const u64 *off, u64 nblocks,
-                                    u64 total, u32 N, u64 *rlwe) {
+// Accepted sample k (k < total) -> dst[(k / row_len) * row_stride + row_off + k % row_len].
+template <typename T>
+__global__ void seeded_place_kernel(const u64 *samples, const unsigned char *accept, const u64 *off, u64 nblocks,
+                                    u64 total, u64 row_len, u64 row_stride, u64 row_off, T *dst) {
   for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nblocks; b += (u64)gridDim.x * blockDim.x) {
     const unsigned m = accept[b];
     u64 pos = off[b];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       if ((m >> i) & 1u) {
-        if (pos < total) rlwe[(pos / N) * 2 * N + pos % N] = samples[8 * b + i];
+        if (pos < total) dst[(pos / row_len) * row_stride + row_off + pos % row_len] = (T)samples[8 * b + i];
         pos++;
       }
     }
@@ -238,7 +242,63 @@ pz_status ni_check(pz_ctx *c) {
 
 int grid_of(size_t n, int cap) { return (int)std::min<size_t>(std::max<size_t>(n, 1), (size_t)cap); }
 
+template <typename T>
+pz_status seeded_fill(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride, u64 row_off,
+                      T *dst, cudaStream_t st) {
+  if (total == 0) return PZ_OK;
+  const u64 nblocks = (total + UNSEED_MARGIN + 7) / 8;
+  ChaChaKey key;
+  for (int i = 0; i < 8; i++)
+    key.k[i] = (u32)seed[4 * i] | ((u32)seed[4 * i + 1] << 8) | ((u32)seed[4 * i + 2] << 16) |
+               ((u32)seed[4 * i + 3] << 24);
+  // rand 0.8 UniformInt<u64>::new_inclusive(0, q - 1): range q, zone = MAX - (2^64 - q) % q
+  const u64 zone = ~0ull - ((0ull - q) % q);
+  u64 *samples = nullptr, *off = nullptr;
+  unsigned char *acc = nullptr;
+  u32 *cnt = nullptr;
+  cudaError_t e = cudaMallocAsync(&samples, nblocks * 8 * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&off, (nblocks + 1) * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&acc, nblocks, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, nblocks * 4, st);
+  if (e == cudaSuccess) {
+    unseed_candidates_kernel<<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(key, nblocks, q, zone, samples,
+                                                                                     acc, cnt);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    unseed_scan_kernel<<<1, 1024, 0, st>>>(cnt, nblocks, off);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    seeded_place_kernel<T><<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(samples, acc, off, nblocks, total,
+                                                                                row_len, row_stride, row_off, dst);
+    e = cudaGetLastError();
+  }
+  u64 accepted = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&accepted, off + nblocks, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFreeAsync(samples, st);
+  cudaFreeAsync(off, st);
+  cudaFreeAsync(acc, st);
+  cudaFreeAsync(cnt, st);
+  if (e != cudaSuccess) return pz::cuda_fail(c, "seeded uniform fill", e);
+  if (accepted < total)  // more rejections than the margin covers (probability ~0)
+    return pz::fail(c, PZ_ERR_NOT_SUPPORTED, "seeded fill: rejection margin exhausted");
+  return PZ_OK;
+}
+
 }  // namespace
+
+namespace pz {
+pz_status seeded_fill_u64(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride,
+                          u64 row_off, u64 *dst, cudaStream_t st) {
+  return seeded_fill<u64>(c, seed, q, total, row_len, row_stride, row_off, dst, st);
+}
+pz_status seeded_fill_u32(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride,
+                          u64 row_off, u32 *dst, cudaStream_t st) {
+  return seeded_fill<u32>(c, seed, q, total, row_len, row_stride, row_off, dst, st);
+}
+}  // namespace pz
 
 extern "C" {
 
@@ -270,6 +330,38 @@ pz_status pz_ni_ksk_upload(pz_ctx *c, const uint64_t *ksk, pz_ni_ksk **out) {
   return PZ_OK;
 }
 
+pz_status pz_ni_ksk_upload_seeded(pz_ctx *c, const uint64_t *ksk_b, const uint8_t seed[32], pz_ni_ksk **out) {
+  pz_status s = ni_check(c);
+  if (s != PZ_OK) return s;
+  if (!ksk_b || !seed || !out) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "pz_ni_ksk_upload_seeded: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(c->mu);
+  PZ_CK(c, cudaSetDevice(c->device));
+  const size_t N = c->P.rlwe_n, d = c->P.ni_ks_d, polys = 2 * d;
+  pz_ni_ksk *k = new pz_ni_ksk();
+  k->ctx = c;
+  k->d = (u32)d;
+  k->bytes = polys * N * 8;
+  u64 *stage = nullptr;
+  cudaError_t e = cudaMalloc(&k->d_ksk, k->bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&stage, k->bytes);
+  // keys.rs:965-1000: d A rows from the user's stream, then the B rows
+  if (e == cudaSuccess) s = pz::seeded_fill_u64(c, seed, c->P.rlwe_q, (u64)d * N, d * N, 2 * d * N, 0, stage, c->stream);
+  if (e == cudaSuccess && s == PZ_OK)
+    e = cudaMemcpyAsync(stage + d * N, ksk_b, d * N * 8, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && s == PZ_OK)
+    e = pz::launch_key_convert((int)c->logn, stage, k->d_ksk, polys, c->rc, c->conv_c, c->conv_cs, c->stream);
+  if (e == cudaSuccess && s == PZ_OK) e = cudaStreamSynchronize(c->stream);
+  cudaFree(stage);
+  if (e != cudaSuccess || s != PZ_OK) {
+    cudaFree(k->d_ksk);
+    delete k;
+    return s != PZ_OK ? s : pz::cuda_fail(c, "pz_ni_ksk_upload_seeded", e);
+  }
+  *out = k;
+  return PZ_OK;
+}
+
 void pz_ni_ksk_release(pz_ni_ksk *k) {
   if (!k) return;
   cudaSetDevice(k->ctx->device);
@@ -286,49 +378,10 @@ pz_status pz_ni_unseed_device(pz_ctx *c, const uint8_t seed[32], const uint64_t 
   PZ_CK(c, cudaSetDevice(c->device));
   cudaStream_t st = (cudaStream_t)stream;
   const u32 N = c->P.rlwe_n;
-  const u64 q = c->P.rlwe_q;
-  const u64 total = (u64)count * N;
-  const u64 nblocks = (total + UNSEED_MARGIN + 7) / 8;
-  ChaChaKey key;
-  for (int i = 0; i < 8; i++)
-    key.k[i] = (u32)seed[4 * i] | ((u32)seed[4 * i + 1] << 8) | ((u32)seed[4 * i + 2] << 16) |
-               ((u32)seed[4 * i + 3] << 24);
-  // rand 0.8 UniformInt<u64>::new_inclusive(0, q - 1): range q, zone = MAX - (2^64 - q) % q
-  const u64 zone = ~0ull - ((0ull - q) % q);
-  u64 *samples = nullptr, *off = nullptr;
-  unsigned char *acc = nullptr;
-  u32 *cnt = nullptr;
-  cudaError_t e = cudaMallocAsync(&samples, nblocks * 8 * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&off, (nblocks + 1) * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&acc, nblocks, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, nblocks * 4, st);
-  if (e == cudaSuccess) {
-    unseed_candidates_kernel<<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(key, nblocks, q, zone, samples,
-                                                                                     acc, cnt);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) {
-    unseed_scan_kernel<<<1, 1024, 0, st>>>(cnt, nblocks, off);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) {
-    unseed_place_kernel<<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(samples, acc, off, nblocks, total, N,
-                                                                               d_rlwe);
-    e = cudaGetLastError();
-  }
-  // b-parts: row 1 of every RLWE
-  if (e == cudaSuccess)
-    e = cudaMemcpy2DAsync(d_rlwe + N, 2 * N * 8, d_b, N * 8, N * 8, count, cudaMemcpyDeviceToDevice, st);
-  u64 accepted = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&accepted, off + nblocks, 8, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFreeAsync(samples, st);
-  cudaFreeAsync(off, st);
-  cudaFreeAsync(acc, st);
-  cudaFreeAsync(cnt, st);
-  if (e != cudaSuccess) return pz::cuda_fail(c, "pz_ni_unseed_device", e);
-  if (accepted < total)  // more rejections than the margin covers (probability ~0)
-    return pz::fail(c, PZ_ERR_NOT_SUPPORTED, "unseed: rejection margin exhausted");
+  // a-parts: sample k of the stream -> RLWE k / N, coefficient k % N; b-parts: row 1
+  s = pz::seeded_fill_u64(c, seed, c->P.rlwe_q, (u64)count * N, N, 2 * N, 0, d_rlwe, st);
+  if (s != PZ_OK) return s;
+  PZ_CK(c, cudaMemcpy2DAsync(d_rlwe + N, 2 * N * 8, d_b, N * 8, N * 8, count, cudaMemcpyDeviceToDevice, st));
   return PZ_OK;
 }
 

@@ -421,6 +421,71 @@ pz_status pz_key_upload(pz_ctx *c, const pz_server_key_view *v, pz_key **out) {
   return PZ_OK;
 }
 
+pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz_key **out) {
+  if (!c || !v || !out || !v->rgsw || !v->auto_b || !v->lwe_ksk_b)
+    return fail(c, PZ_ERR_INVALID_ARGUMENT, "pz_key_upload_seeded: NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(c->mu);
+  PZ_CK(c, cudaSetDevice(c->device));
+  const pz_params &P = c->P;
+  const size_t N = P.rlwe_n;
+  const size_t rgsw_polys = (size_t)P.lwe_n * P.rgsw_rows;
+  const size_t auto_polys = (size_t)P.n_auto_keys * P.auto_rows, d_auto = P.auto_d;
+  const size_t ksk_rows = (size_t)P.lwe_d * N;
+  const u32 stride = ks_stride(P);
+  pz_key *k = new pz_key();
+  k->ctx = c;
+  u64 *d_stage = nullptr;
+  auto cleanup = [&](pz_status s, const std::string &m) {
+    cudaFree(d_stage);
+    cudaFree(k->d_rgsw); cudaFree(k->d_autos); cudaFree(k->d_ksk);
+    delete k;
+    return fail(c, s, m);
+  };
+  cudaError_t e;
+  const size_t chunk = 1024;  // polynomials per staging copy (>= the auto keys)
+  if ((e = cudaMalloc(&k->d_rgsw, rgsw_polys * N * 8)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "rgsw alloc");
+  if ((e = cudaMalloc(&k->d_autos, auto_polys * N * 8)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "auto alloc");
+  if ((e = cudaMalloc(&k->d_ksk, ksk_rows * stride * 4)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "ksk alloc");
+  if ((e = cudaMalloc(&d_stage, std::max(chunk, auto_polys) * N * 8)) != cudaSuccess)
+    return cleanup(PZ_ERR_OUT_OF_MEMORY, "staging alloc");
+  k->bytes = (rgsw_polys + auto_polys) * N * 8 + ksk_rows * stride * 4;
+  // RGSW ciphertexts: as pz_key_upload (keys.rs:738-757)
+  for (size_t p0 = 0; p0 < rgsw_polys; p0 += chunk) {
+    const size_t m = std::min(chunk, rgsw_polys - p0);
+    if ((e = cudaMemcpyAsync(d_stage, v->rgsw + p0 * N, m * N * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+        (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_rgsw + p0 * N, m, c->rc, c->conv_c, c->conv_cs,
+                                    c->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+      return cleanup(PZ_ERR_CUDA, std::string("rgsw conversion: ") + cudaGetErrorString(e));
+  }
+  // auto keys (keys.rs:702-736): per slot d_auto A rows from the auto stream, then the B rows
+  pz_status st = pz::seeded_fill_u64(c, v->auto_seed, P.rlwe_q, (u64)P.n_auto_keys * d_auto * N, d_auto * N,
+                                     2 * d_auto * N, 0, d_stage, c->stream);
+  if (st != PZ_OK) return cleanup(st, c->err);
+  if ((e = cudaMemcpy2DAsync(d_stage + d_auto * N, 2 * d_auto * N * 8, v->auto_b, d_auto * N * 8, d_auto * N * 8,
+                             P.n_auto_keys, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+      (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_autos, auto_polys, c->rc, c->conv_c, c->conv_cs,
+                                  c->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+    return cleanup(PZ_ERR_CUDA, std::string("auto key expansion: ") + cudaGetErrorString(e));
+  // LWE KSK (keys.rs:759-772): per row n A words mod q_ks from the ksk stream, word 0 = b
+  if ((e = cudaMemsetAsync(k->d_ksk, 0, ksk_rows * stride * 4, c->stream)) != cudaSuccess)
+    return cleanup(PZ_ERR_CUDA, "ksk memset");
+  st = pz::seeded_fill_u32(c, v->lwe_ksk_seed, P.lwe_q, (u64)ksk_rows * P.lwe_n, P.lwe_n, stride, 1, k->d_ksk,
+                           c->stream);
+  if (st != PZ_OK) return cleanup(st, c->err);
+  std::vector<u32> b32(ksk_rows);
+  for (size_t r = 0; r < ksk_rows; r++) b32[r] = (u32)(v->lwe_ksk_b[r] & (P.lwe_q - 1));
+  if ((e = cudaMemcpy2DAsync(k->d_ksk, stride * 4, b32.data(), 4, 4, ksk_rows, cudaMemcpyHostToDevice, c->stream)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+    return cleanup(PZ_ERR_CUDA, std::string("ksk b column: ") + cudaGetErrorString(e));
+  cudaFree(d_stage);
+  *out = k;
+  return PZ_OK;
+}
+
 void pz_key_release(pz_key *k) {
   if (!k) return;
   cudaSetDevice(k->ctx->device);

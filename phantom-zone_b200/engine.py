@@ -8,7 +8,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import PzParams, PzServerKeyView, check, lib, u8p, u64p, vp
+from ._lib import PzParams, PzSeededServerKeyView, PzServerKeyView, check, lib, u8p, u64p, vp
 
 PARAMETER_SETS = {
     "I_2P_LB_SR": 0, "I_4P": 1, "I_8P": 2, "NI_2P": 3,
@@ -167,6 +167,35 @@ class Engine:
         h = vp()
         check(lib().pz_key_upload(self.h, ctypes.byref(view), ctypes.byref(h)), self.h, "pz_key_upload")
         return DeviceKey(self, h)
+
+    def upload_key_seeded(self, rgsw, auto_b, auto_seed, lwe_ksk_b, lwe_ksk_seed):
+        """Upload a seeded server key: RGSW in full, auto-key B rows [w+1][d_auto][N]
+        and LWE-KSK column 0 [d_ks N]; the A parts are regenerated on the device
+        from the two CRS-derived seeds (keys.rs:687-781)."""
+        p = self.p
+        rgsw = np.ascontiguousarray(rgsw, dtype=np.uint64)
+        auto_b = np.ascontiguousarray(auto_b, dtype=np.uint64)
+        lwe_ksk_b = np.ascontiguousarray(lwe_ksk_b, dtype=np.uint64)
+        if rgsw.size != p.lwe_n * p.rgsw_rows * p.rlwe_n:
+            raise ValueError("rgsw has the wrong size for this parameter set")
+        if auto_b.size != p.n_auto_keys * p.auto_d * p.rlwe_n:
+            raise ValueError("auto B rows have the wrong size for this parameter set")
+        if lwe_ksk_b.size != p.lwe_d * p.rlwe_n:
+            raise ValueError("lwe ksk column has the wrong size for this parameter set")
+        v = PzSeededServerKeyView(rgsw.ctypes.data_as(u64p), auto_b.ctypes.data_as(u64p),
+                                  lwe_ksk_b.ctypes.data_as(u64p), _seed(auto_seed), _seed(lwe_ksk_seed))
+        h = vp()
+        check(lib().pz_key_upload_seeded(self.h, ctypes.byref(v), ctypes.byref(h)), self.h, "pz_key_upload_seeded")
+        return DeviceKey(self, h)
+
+    def upload_ni_ksk_seeded(self, ksk_b, seed):
+        ksk_b = np.ascontiguousarray(ksk_b, dtype=np.uint64)
+        if ksk_b.size != self.p.ni_ks_d * self.N or self.p.ni_ks_d == 0:
+            raise ValueError("ui_to_s B rows have the wrong size (or the set is not non-interactive)")
+        h = vp()
+        check(lib().pz_ni_ksk_upload_seeded(self.h, ksk_b.ctypes.data_as(u64p), _seed(seed), ctypes.byref(h)), self.h,
+              "pz_ni_ksk_upload_seeded")
+        return NiKsk(self, h)
 
     # -- gates, host memory --------------------------------------------------
     def gate_batch(self, key, gates, c0, c1):

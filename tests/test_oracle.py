@@ -259,3 +259,23 @@ def test_ni_input_path_round_trip(param):
     assert np.array_equal(ev.decrypt_bool(s, lwes), bits)
     bad = ev.ni_ingest(ksk, b"\x08" * 32, b, 64)
     assert not np.array_equal(ev.decrypt_bool(s, bad), bits[:64])
+
+
+@pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
+def test_seeded_key_expansion_stream_order(param):
+    """keys.rs:687-781: auto A rows slot by slot (auto_element_dlogs order), then
+    LWE-KSK A words row by row, each from its own ChaCha8 stream."""
+    O = oracle()
+    ev, _, coeff, _ = oracle_setup(param)
+    i = ev.info
+    d, N, n = i.auto_d, ev.N, ev.n
+    auto_b = coeff.autos[:, d:, :]
+    lwe_b = coeff.ksk[:, 0]
+    sa, sl = b"\x61" * 32, b"\x62" * 32
+    autos, ksk = ev.expand_seeded_key(auto_b, sa, lwe_b, sl)
+    a_stream = O.Rng(sa).uniform_mod(ev.Q, i.n_auto_keys * d * N).reshape(i.n_auto_keys, d, N)
+    assert np.array_equal(autos[:, :d, :], a_stream)
+    assert np.array_equal(autos[:, d:, :], auto_b)
+    k_stream = O.Rng(sl).uniform_mod(i.lwe_q, i.lwe_d * N * n).reshape(i.lwe_d * N, n)
+    assert np.array_equal(ksk[:, 1:], k_stream)
+    assert np.array_equal(ksk[:, 0], lwe_b)
