@@ -400,6 +400,38 @@ def key_upload_bench(P, device):
             "seeded_host_bytes": int(rgsw.nbytes + auto_b.nbytes + lwe_b.nbytes + 64)}
 
 
+def aggregate_bench(P, torch, device, prm="I_8P"):
+    """Interactive server-key aggregation at InteractiveLTE8Party: the RGSW step
+    for all n LWE indices and the 7 other users (n x 7 RGSW x RGSW products,
+    rgrg decomposition logb 5, 9/8 digits), synthetic ciphertexts on the device."""
+    p = P.params(prm)
+    N, n = p.rlwe_n, p.lwe_n
+    steps = 7
+    eng = P.Engine(prm, device=device)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    rows1 = 2 * (p.rgrg_d_a + p.rgrg_d_b)
+    lead = torch.randint(0, p.rlwe_q, (n, 4, N), dtype=torch.int64, device="cuda", generator=g)
+    others = torch.randint(0, p.rlwe_q, (steps, n, rows1, N), dtype=torch.int64, device="cuda", generator=g)
+    work = lead.clone()
+    eng.aggregate_rgsw_device(work, others[:1])  # warm-up: one step
+    torch.cuda.synchronize()
+    work.copy_(lead)
+    t0 = time.perf_counter()
+    eng.aggregate_rgsw_device(work, others)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    products = n * steps
+    logn = int(np.log2(N))
+    ntt = (N // 2) * logn
+    # per RGSW x RGSW: key conversion (rows1 forward NTTs) + 2 RLWE x RGSW (digit NTTs, MAC rows, 2 inverse)
+    mm = products * (rows1 * ntt + 2 * ((p.rgrg_d_a + p.rgrg_d_b) * ntt + 2 * (ntt + N) +
+                                        2 * (p.rgrg_d_a + p.rgrg_d_b) * N))
+    eng.close()
+    return {"config": f"{prm}: {n} LWE indices x {steps} other users = {products} RGSW x RGSW "
+                      f"(rgrg logb {p.rgrg_logb}, {p.rgrg_d_a}/{p.rgrg_d_b} digits), device buffers",
+            "ms": dt * 1e3, "rgsw_products_per_s": products / dt, "modmul_per_s": mm / dt}
+
+
 def u8_job(P, op):
     C = P.Circuit()
     a, b = C.input_u8(), C.input_u8()
@@ -661,7 +693,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the microbench / ragged / serving sub-results")
     ap.add_argument("--mode", default="wavefront",
                     choices=["wavefront", "br-kernel", "ks-kernel", "microbench", "ragged", "serving", "kernels",
-                             "ni", "key-upload"],
+                             "ni", "key-upload", "aggregate"],
                     help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
@@ -669,12 +701,13 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.mode in ("microbench", "ragged", "serving", "kernels", "ni", "key-upload"):
+    if args.mode in ("microbench", "ragged", "serving", "kernels", "ni", "key-upload", "aggregate"):
         import torch
         P = pz()
         fn = {"microbench": lambda: microbench(P, torch, 0), "ragged": lambda: ragged_batch(P, 0),
               "serving": lambda: serving(P, 0), "kernels": lambda: kernels_case(P, torch, 0),
-              "ni": lambda: ni_ingest_bench(P, torch, 0), "key-upload": lambda: key_upload_bench(P, 0)}[args.mode]
+              "ni": lambda: ni_ingest_bench(P, torch, 0), "key-upload": lambda: key_upload_bench(P, 0),
+              "aggregate": lambda: aggregate_bench(P, torch, 0)}[args.mode]
         print(json.dumps({"mode": args.mode, **fn()}), flush=True)
         return
     if args.mode != "wavefront":
@@ -777,6 +810,7 @@ def main():
         extras["serving"] = serving(P, local)
         extras["ni_ingest"] = ni_ingest_bench(P, torch, local)
         extras["key_upload"] = key_upload_bench(P, local)
+        extras["aggregate"] = aggregate_bench(P, torch, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -86,6 +86,8 @@ typedef struct pz_params {
   uint32_t n_auto_keys;      /* w + 1 */
   uint32_t ni_ks_logb, ni_ks_d; /* ui_to_s key switch decomposition of the NI sets
                                    (parameters.rs:616-697: 1, 50); 0 otherwise */
+  uint32_t rgrg_logb, rgrg_d_a, rgrg_d_b; /* RGSW x RGSW decomposition of key aggregation
+                                             (rgrg_decomposer_params); 0 when the set has none */
 } pz_params;
 
 typedef struct pz_ctx pz_ctx;
@@ -292,6 +294,19 @@ pz_status pz_sample_extract_device(pz_ctx *ctx, const uint64_t *d_rlwe, size_t r
  * [nbools][N + 1] for bools 0 .. nbools - 1 */
 pz_status pz_ni_ingest(pz_ctx *ctx, const pz_ni_ksk *ksk, const uint8_t seed[32], const uint64_t *b,
                        size_t rlwe_count, uint64_t *lwe_out, size_t nbools);
+
+/* ---- server-key aggregation (interactive protocol) ----------------------------------
+ * rgsw_by_rgsw_inplace (rgsw/runtime.rs:883-985), batched: d_rgsw0[c] <- d_rgsw0[c] x
+ * d_rgsw1[c].  d_rgsw0 [count][4][N]: RGSW in the rlwe x rgsw shape (d_a = d_b = 1),
+ * coefficient domain, in place; d_rgsw1 [count][2 rgrg_d_a + 2 rgrg_d_b][N]: RGSW in the
+ * rgsw x rgsw shape, coefficient domain (converted on the device).  Returns when done. */
+pz_status pz_rgsw_by_rgsw_device(pz_ctx *ctx, uint64_t *d_rgsw0, const uint64_t *d_rgsw1, size_t count,
+                                 void *stream);
+/* The RGSW step of aggregate_interactive_multi_party_server_key_shares
+ * (bool/evaluator.rs:1110-1200): d_rgsw0[c] <- d_rgsw0[c] x d_others[0][c] x ... x
+ * d_others[steps - 1][c], the other users in order; d_others [steps][count][rows][N]. */
+pz_status pz_aggregate_rgsw_device(pz_ctx *ctx, uint64_t *d_rgsw0, const uint64_t *d_others, size_t steps,
+                                   size_t count, void *stream);
 
 /* ---- multi-session executor (serving) ---------------------------------------------
  * No reference counterpart: the reference evaluates one gate at a time, in

@@ -39,6 +39,7 @@ class ParamInfo(ctypes.Structure):
         ("embedding_factor", ctypes.c_uint32), ("rgsw_rows", ctypes.c_uint32),
         ("auto_rows", ctypes.c_uint32), ("n_auto_keys", ctypes.c_uint32),
         ("ni_ks_logb", ctypes.c_uint32), ("ni_ks_d", ctypes.c_uint32),
+        ("rgrg_logb", ctypes.c_uint32), ("rgrg_d_a", ctypes.c_uint32), ("rgrg_d_b", ctypes.c_uint32),
     ]
 
 
@@ -83,6 +84,8 @@ def lib():
             "orc_ni_ksk_gen": (None, [vp, i32p, i32p, u8p, u64p]),
             "orc_expand_seeded_key": (None, [vp, u64p, u8p, u64p, u8p, u64p, u64p]),
             "orc_expand_ni_ksk": (None, [vp, u64p, u8p, u64p]),
+            "orc_rgsw_by_rgsw": (None, [vp, u64p, u64p]),
+            "orc_rgsw_encrypt": (None, [vp, i32p, u64p, ctypes.c_int, u8p, u64p]),
             "orc_u8_op": (ctypes.c_int, [vp, vp, ctypes.c_int, u64p, u64p, u64p, u64p, u64p, u64p, ctypes.POINTER(ctypes.c_int)]),
             "orc_generate_prime": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
             "orc_ntt_custom_new": (vp, [ctypes.c_uint64, ctypes.c_size_t]),
@@ -325,6 +328,22 @@ class Evaluator:
         out = np.empty((2 * self.NI_KS_D, self.N), np.uint64)
         lib().orc_expand_ni_ksk(self.h, _p(np.ascontiguousarray(b, np.uint64)), (ctypes.c_uint8 * 32)(*bytes(seed)),
                                 _p(out))
+        return out
+
+    def rgsw_rows(self, which):
+        i = self.info
+        return 2 * (i.rlrg_d_a + i.rlrg_d_b) if which == 0 else 2 * (i.rgrg_d_a + i.rgrg_d_b)
+
+    def rgsw_by_rgsw(self, rgsw0, rgsw1):
+        r0 = np.ascontiguousarray(rgsw0, np.uint64).copy()
+        lib().orc_rgsw_by_rgsw(self.h, _p(r0), _p(np.ascontiguousarray(rgsw1, np.uint64)))
+        return r0
+
+    def rgsw_encrypt(self, s, m, which, seed=b"\x71" * 32):
+        out = np.empty((self.rgsw_rows(which), self.N), np.uint64)
+        lib().orc_rgsw_encrypt(self.h, _p(np.ascontiguousarray(s, np.int32), i32p),
+                               _p(np.ascontiguousarray(m, np.uint64)), int(which),
+                               (ctypes.c_uint8 * 32)(*bytes(seed)), _p(out))
         return out
 
     def ni_ingest(self, ksk, seed, b, nbits):

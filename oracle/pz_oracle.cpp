@@ -33,26 +33,27 @@ struct Param {
   u32 g, w;
   u32 lwe_gauss;  // SecretKeyDistribution::ErrorDistribution for the LWE secret
   u32 variant;    // 0 single, 1 interactive, 2 non-interactive
+  u32 rgrg_logb, rgrg_d_a, rgrg_d_b;  // rgrg_decomposer_params (0: none)
 };
 
 const u64 Q54 = 18014398509404161ULL;
 const Param PARAMS[ORC_NUM_PARAMS] = {
     // I_2P_LB_SR  parameters.rs:526-548
-    {Q54, 1ULL << 15, 1u << 11, 1u << 11, 580, 1, 12, 17, 1, 1, 24, 1, 5, 10, 0, 1},
+    {Q54, 1ULL << 15, 1u << 11, 1u << 11, 580, 1, 12, 17, 1, 1, 24, 1, 5, 10, 0, 1, 7, 6, 5},
     // I_4P        parameters.rs:550-572
-    {Q54, 1ULL << 16, 1u << 11, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 1},
+    {Q54, 1ULL << 16, 1u << 11, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 1, 6, 7, 6},
     // I_8P        parameters.rs:574-596
-    {Q54, 1ULL << 17, 1u << 12, 1u << 11, 660, 1, 14, 17, 1, 1, 24, 1, 5, 10, 0, 1},
+    {Q54, 1ULL << 17, 1u << 12, 1u << 11, 660, 1, 14, 17, 1, 1, 24, 1, 5, 10, 0, 1, 5, 9, 8},
     // NI_2P       parameters.rs:598-623 (LWE secret from the error distribution)
-    {Q54, 1ULL << 16, 1u << 12, 1u << 11, 520, 1, 13, 17, 1, 1, 24, 1, 5, 10, 1, 2},
+    {Q54, 1ULL << 16, 1u << 12, 1u << 11, 520, 1, 13, 17, 1, 1, 24, 1, 5, 10, 1, 2, 4, 10, 9},
     // NI_4P_HB_FR parameters.rs:625-650
-    {Q54, 1ULL << 16, 1u << 11, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 2},
+    {Q54, 1ULL << 16, 1u << 11, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 2, 3, 13, 12},
     // NI_4P_LB_SR parameters.rs:652-677
-    {Q54, 1ULL << 16, 1u << 12, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 2},
+    {Q54, 1ULL << 16, 1u << 12, 1u << 11, 620, 1, 13, 17, 1, 1, 24, 1, 5, 10, 0, 2, 4, 10, 9},
     // NI_8P       parameters.rs:679-704
-    {Q54, 1ULL << 17, 1u << 12, 1u << 11, 660, 1, 14, 17, 1, 1, 24, 1, 5, 10, 0, 2},
+    {Q54, 1ULL << 17, 1u << 12, 1u << 11, 660, 1, 14, 17, 1, 1, 24, 1, 5, 10, 0, 2, 2, 20, 18},
     // SP_TEST_BOOL_PARAMS parameters.rs:706-726 (the only set with d > 1)
-    {268369921ULL, 1ULL << 16, 1u << 9, 1u << 9, 100, 4, 4, 7, 4, 4, 7, 4, 5, 5, 1, 0},
+    {268369921ULL, 1ULL << 16, 1u << 9, 1u << 9, 100, 4, 4, 7, 4, 4, 7, 4, 5, 5, 1, 0, 0, 0, 0},
 };
 
 inline int clz64(u64 v) { return v ? __builtin_clzll(v) : 64; }
@@ -431,6 +432,7 @@ struct Eval {
   Ntt ntt;
   Decomposer dec_lwe, dec_a, dec_b, dec_auto;
   Decomposer dec_ni;      // non_interactive_ui_to_s_key_switch_decomposer (NI sets only)
+  Decomposer dec_rgrg_a, dec_rgrg_b;  // rgsw_rgsw_decomposer (parameters.rs:276-298)
   std::vector<u32> dlog;  // g_k_dlog_map
   u32 emb;
   std::vector<std::vector<u64>> test_vec;  // per gate
@@ -449,6 +451,10 @@ struct Eval {
     dec_auto.init(Q, p.auto_logb, p.auto_d);
     // parameters.rs:616-697: ui_to_s key switch (logb 1, d 50) of the NI sets
     if (p.variant == 2) dec_ni.init(Q, 1, 50);
+    if (p.rgrg_logb) {
+      dec_rgrg_a.init(Q, p.rgrg_logb, p.rgrg_d_a);
+      dec_rgrg_b.init(Q, p.rgrg_logb, p.rgrg_d_b);
+    }
     // evaluator.rs:664-673 dlog map over Z*_{br_q} = +-g^k
     u32 q = p.br_q;
     dlog.assign(q, 0);
@@ -906,6 +912,7 @@ int orc_param_info_get(int pid, orc_param_info *o) {
   // parameters.rs:616-697 non_interactive_ui_to_s_key_switch_decomposer (1, 50)
   o->ni_ks_logb = p.variant == 2 ? 1 : 0;
   o->ni_ks_d = p.variant == 2 ? 50 : 0;
+  o->rgrg_logb = p.rgrg_logb; o->rgrg_d_a = p.rgrg_d_a; o->rgrg_d_b = p.rgrg_d_b;
   return 0;
 }
 
@@ -1423,6 +1430,83 @@ void orc_expand_seeded_key(void *ev, const uint64_t *auto_b, const uint8_t auto_
     u64 *row = ksk + r * (n + 1);
     for (size_t c = 1; c <= n; c++) row[c] = ksk_prng.uniform_mod(e.p.lwe_q);
     row[0] = lwe_b[r];
+  }
+}
+
+// rgsw_by_rgsw_inplace (runtime.rs:883-985): rgsw0 (rlwe x rgsw shape,
+// coefficient domain) <- rgsw0 x rgsw1, rgsw1 given in the coefficient domain
+// in the rgsw x rgsw shape (sent to the evaluation domain first, as the
+// aggregation does, evaluator.rs:1160-1163).  Every RLWE of rgsw0 -- the
+// -sm rows then the m rows -- times RGSW(m1): decompose A with the rgrg A
+// decomposer, forward NTT, poly_fma_routine (runtime.rs:363-372) against the
+// -sm rows of rgsw1; decompose B with the rgrg B decomposer against the m
+// rows; the outputs go back to the coefficient domain.
+void orc_rgsw_by_rgsw(void *ev, uint64_t *rgsw0, const uint64_t *rgsw1) {
+  Eval &e = *(Eval *)ev;
+  if (!e.p.rgrg_logb) throw std::runtime_error("parameter set without RGSW x RGSW");
+  const size_t N = e.N, da = e.p.d_a, db = e.p.d_b, ra = e.p.rgrg_d_a, rb = e.p.rgrg_d_b;
+  const size_t rows0 = 2 * da + 2 * db, rows1 = 2 * ra + 2 * rb;
+  std::vector<u64> k1(rgsw1, rgsw1 + rows1 * N);
+  for (size_t r = 0; r < rows1; r++) e.ntt.forward(&k1[r * N], false);
+  std::vector<u64> out(rows0 * N, 0), dec(std::max(ra, rb) * N);
+  auto fma = [&](u64 *o, size_t krow0, size_t rows) {
+    for (size_t j = 0; j < rows; j++) {
+      const u64 *k = &k1[(krow0 + j) * N], *x = &dec[j * N];
+      for (size_t i = 0; i < N; i++) o[i] = e.rmod.add(o[i], e.rmod.mul(x[i], k[i]));
+    }
+  };
+  auto one = [&](const u64 *a, const u64 *b, u64 *oa, u64 *ob) {
+    decompose_r(e.dec_rgrg_a, a, dec.data(), N);
+    for (size_t j = 0; j < ra; j++) e.ntt.forward(&dec[j * N], false);
+    fma(oa, 0, ra);
+    fma(ob, ra, ra);
+    decompose_r(e.dec_rgrg_b, b, dec.data(), N);
+    for (size_t j = 0; j < rb; j++) e.ntt.forward(&dec[j * N], false);
+    fma(oa, 2 * ra, rb);
+    fma(ob, 2 * ra + rb, rb);
+  };
+  for (size_t j = 0; j < da; j++)
+    one(rgsw0 + j * N, rgsw0 + (da + j) * N, &out[j * N], &out[(da + j) * N]);
+  for (size_t j = 0; j < db; j++)
+    one(rgsw0 + (2 * da + j) * N, rgsw0 + (2 * da + db + j) * N, &out[(2 * da + j) * N],
+        &out[(2 * da + db + j) * N]);
+  for (size_t r = 0; r < rows0; r++) e.ntt.backward(&out[r * N], false);
+  memcpy(rgsw0, out.data(), rows0 * N * 8);
+}
+
+// Client side (harness): RGSW(m) under s in the rlwe x rgsw shape (which = 0)
+// or the rgsw x rgsw shape (which = 1), as the key generation builds them
+// (rgsw/keygen.rs:68-160): -sm rows a += beta_j m, b = a s + e; m rows
+// b = a s + e + beta_j m.  Coefficient domain.
+void orc_rgsw_encrypt(void *ev, const int32_t *s, const uint64_t *m, int which, const uint8_t seed[32],
+                      uint64_t *out) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N;
+  const Decomposer &dpa = which ? e.dec_rgrg_a : e.dec_a, &dpb = which ? e.dec_rgrg_b : e.dec_b;
+  const size_t da = dpa.d, db = dpb.d;
+  ChaCha8 rng(seed);
+  std::vector<u64> s_eval(N), tmp(N);
+  for (size_t i = 0; i < N; i++) s_eval[i] = map_from_i64(e.Q, s[i]);
+  e.ntt.forward(s_eval.data(), false);
+  auto rlwe_zero = [&](u64 *a, u64 *b) {  // a uniform, b = a s + e
+    for (size_t i = 0; i < N; i++) a[i] = rng.uniform_mod(e.Q);
+    memcpy(tmp.data(), a, N * 8);
+    e.ntt.forward(tmp.data(), false);
+    for (size_t i = 0; i < N; i++) tmp[i] = e.rmod.mul(tmp[i], s_eval[i]);
+    e.ntt.backward(tmp.data(), false);
+    for (size_t i = 0; i < N; i++) b[i] = e.rmod.add(tmp[i], map_from_f64(e.Q, rng.gaussian()));
+  };
+  for (size_t j = 0; j < da; j++) {
+    u64 *a = out + j * N, *b = out + (da + j) * N;
+    rlwe_zero(a, b);
+    const u64 beta = dpa.gadget((u32)j) % e.Q;
+    for (size_t i = 0; i < N; i++) a[i] = e.rmod.add(a[i], e.rmod.mul(m[i] % e.Q, beta));
+  }
+  for (size_t j = 0; j < db; j++) {
+    u64 *a = out + (2 * da + j) * N, *b = out + (2 * da + db + j) * N;
+    rlwe_zero(a, b);
+    const u64 beta = dpb.gadget((u32)j) % e.Q;
+    for (size_t i = 0; i < N; i++) b[i] = e.rmod.add(b[i], e.rmod.mul(m[i] % e.Q, beta));
   }
 }
 

@@ -59,6 +59,7 @@ typedef struct {
   uint32_t auto_rows;                /* 2 d_auto */
   uint32_t n_auto_keys;              /* w + 1 */
   uint32_t ni_ks_logb, ni_ks_d;      /* ui_to_s key switch decomposition (NI sets; 0 otherwise) */
+  uint32_t rgrg_logb, rgrg_d_a, rgrg_d_b; /* RGSW x RGSW decomposition (0: none) */
 } orc_param_info;
 
 /* Parameter set ids, in the order of src/bool/parameters.rs:526-726. */
@@ -184,6 +185,12 @@ void orc_ni_ksk_gen(void *ev, const int32_t *u, const int32_t *s, const uint8_t 
 void orc_expand_seeded_key(void *ev, const uint64_t *auto_b, const uint8_t auto_seed[32], const uint64_t *lwe_b,
                            const uint8_t lwe_seed[32], uint64_t *autos, uint64_t *ksk);
 void orc_expand_ni_ksk(void *ev, const uint64_t *b, const uint8_t seed[32], uint64_t *ksk);
+/* Key aggregation: rgsw_by_rgsw_inplace (runtime.rs:883-985); rgsw0 [2 d_a + 2 d_b][N]
+ * (rlwe x rgsw shape) in place, rgsw1 [2 rgrg_d_a + 2 rgrg_d_b][N]; both coefficient domain.
+ * orc_rgsw_encrypt: RGSW(m) under s, which = 0 rlwe x rgsw shape, 1 rgsw x rgsw shape. */
+void orc_rgsw_by_rgsw(void *ev, uint64_t *rgsw0, const uint64_t *rgsw1);
+void orc_rgsw_encrypt(void *ev, const int32_t *s, const uint64_t *m, int which, const uint8_t seed[32],
+                      uint64_t *out);
 /* LWE_Q encryption of bool under s (lwe.rs:104-137, m = +-Q/8) */
 void orc_encrypt_bool(void *ev, void *rng, const int32_t *s, int bit, uint64_t *lwe);
 /* noisy m = b - <a, s> (lwe.rs:139-162) and the bool decode (evaluator.rs:243-256)

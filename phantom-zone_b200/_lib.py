@@ -29,6 +29,7 @@ class PzParams(ctypes.Structure):
         ("embedding_factor", ctypes.c_uint32), ("rgsw_rows", ctypes.c_uint32),
         ("auto_rows", ctypes.c_uint32), ("n_auto_keys", ctypes.c_uint32),
         ("ni_ks_logb", ctypes.c_uint32), ("ni_ks_d", ctypes.c_uint32),
+        ("rgrg_logb", ctypes.c_uint32), ("rgrg_d_a", ctypes.c_uint32), ("rgrg_d_b", ctypes.c_uint32),
     ]
 
 
@@ -84,6 +85,8 @@ SIGNATURES = {
     "pz_ni_key_switch_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_sample_extract_device": (st, [vp, vp, ctypes.c_size_t, vp, vp, ctypes.c_size_t, vp]),
     "pz_ni_ingest": (st, [vp, vp, u8p, u64p, ctypes.c_size_t, u64p, ctypes.c_size_t]),
+    "pz_rgsw_by_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),
+    "pz_aggregate_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp]),
     "pz_server_create": (st, [ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(vp)]),
     "pz_server_destroy": (None, [vp]),
     "pz_server_last_error": (ctypes.c_char_p, [vp]),

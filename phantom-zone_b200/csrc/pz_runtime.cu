@@ -41,6 +41,12 @@ pz_params full_params(int id) {
   p.n_auto_keys = p.w + 1;
   p.ni_ks_logb = p.variant == 2 ? 1 : 0;  // parameters.rs:616-697
   p.ni_ks_d = p.variant == 2 ? 50 : 0;
+  // rgrg_decomposer_params, parameters.rs:539-695 (none for the single-party test set)
+  static const uint32_t RGRG[PZ_NUM_PARAMS][3] = {{7, 6, 5}, {6, 7, 6}, {5, 9, 8}, {4, 10, 9},
+                                                  {3, 13, 12}, {4, 10, 9}, {2, 20, 18}, {0, 0, 0}};
+  p.rgrg_logb = RGRG[id][0];
+  p.rgrg_d_a = RGRG[id][1];
+  p.rgrg_d_b = RGRG[id][2];
   return p;
 }
 

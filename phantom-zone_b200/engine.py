@@ -288,6 +288,20 @@ class Engine:
                                  out.ctypes.data_as(u64p), nbools), self.h, "pz_ni_ingest")
         return out
 
+    # -- server-key aggregation ----------------------------------------------------
+    def rgsw_by_rgsw_device(self, rgsw0, rgsw1, stream=None):
+        """rgsw0 [count][4][N] <- rgsw0 x rgsw1 (rgsw1 [count][2 rgrg_d_a + 2 rgrg_d_b][N]), both coefficient domain."""
+        count = rgsw0.numel() // (4 * self.N)
+        check(lib().pz_rgsw_by_rgsw_device(self.h, _ptr(rgsw0), _ptr(rgsw1), count, _stream(stream)), self.h,
+              "pz_rgsw_by_rgsw_device")
+
+    def aggregate_rgsw_device(self, rgsw0, others, stream=None):
+        """rgsw0[c] <- rgsw0[c] x others[0][c] x ... (others [steps][count][rows][N])."""
+        count = rgsw0.numel() // (4 * self.N)
+        steps = others.numel() // (count * 2 * (self.p.rgrg_d_a + self.p.rgrg_d_b) * self.N) if count else 0
+        check(lib().pz_aggregate_rgsw_device(self.h, _ptr(rgsw0), _ptr(others), steps, count, _stream(stream)),
+              self.h, "pz_aggregate_rgsw_device")
+
     def lwe_key_switch_device(self, key, lwe_in, out, stream=None):
         count = lwe_in.numel() // self.L
         check(lib().pz_lwe_key_switch_device(self.h, key.h, _ptr(lwe_in), _ptr(out), count,

@@ -279,3 +279,35 @@ def test_seeded_key_expansion_stream_order(param):
     k_stream = O.Rng(sl).uniform_mod(i.lwe_q, i.lwe_d * N * n).reshape(i.lwe_d * N, n)
     assert np.array_equal(ksk[:, 1:], k_stream)
     assert np.array_equal(ksk[:, 0], lwe_b)
+
+
+@pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
+def test_rgsw_by_rgsw_decrypts_to_product(param):
+    """rgsw_by_rgsw_inplace (runtime.rs:883-985): RGSW(X^3) x RGSW(X^5) is an
+    RGSW(X^8) -- its m rows decrypt to beta X^8 and its -sm rows to -beta s X^8."""
+    O = oracle()
+    ev, (s, _, _, _), _, _ = oracle_setup(param)
+    N, Q = ev.N, ev.Q
+
+    def mono(k):
+        m = np.zeros(N, np.uint64)
+        m[k] = 1
+        return m
+
+    r0 = ev.rgsw_encrypt(s, mono(3), 0, b"\x71" * 32)
+    r1 = ev.rgsw_encrypt(s, mono(5), 1, b"\x72" * 32)
+    prod = ev.rgsw_by_rgsw(r0, r1)
+    s_mod = np.array([int(x) % Q for x in s], dtype=np.uint64)
+
+    def mul(a, b):
+        out = np.empty(N, np.uint64)
+        O.lib().orc_negacyclic_mul(Q, O._p(np.ascontiguousarray(a)), O._p(np.ascontiguousarray(b)), O._p(out), N)
+        return out
+
+    beta = 1 << (54 - ev.info.rlrg_logb)  # gadget 0 of the d = 1 rlwe x rgsw decomposer: 2^ignore_bits
+    s8 = mul(s_mod, mono(8))
+    for row_a, row_b, want in [(2, 3, mono(8)), (0, 1, (Q - s8) % Q)]:
+        noise = (mul(prod[row_a], s_mod).astype(object) * -1 + prod[row_b].astype(object)
+                 - want.astype(object) * beta) % Q
+        centred = np.array([int(v) if v < Q // 2 else int(v) - Q for v in noise])
+        assert np.max(np.abs(centred)) < (1 << 34), (row_a, np.max(np.abs(centred)))
