@@ -3,9 +3,11 @@
 // Modular arithmetic mod the RLWE prime Q (< 2^62):
 //   * NTT butterflies use Shoup multiplication by precomputed twiddles
 //     (the butterflies of ntt.rs:24-104): forward values grow without
-//     reduction (below 45Q after the 11 stages of N = 2048), inverse values
-//     stay in [0, 2Q) (Harvey).  For N = 2048 the products use the special
-//     form Q = 2^54 - 77823 of that ring's prime.
+//     reduction (below 45Q after the 11 stages of N = 2048); inverse values
+//     stay in [0, 2Q) (Harvey) for generic q, while for N = 2048 the sums
+//     grow to < 16Q inside a radix-8 round and are reduced once per round.
+//     For N = 2048 the products and reductions use the special form
+//     Q = 2^54 - 77823 of that ring's prime.
 //   * The pointwise key product uses Montgomery REDC with R = 2^64.  Device
 //     keys are stored as K * N^{-1} * R mod Q, so REDC(x * K') = x * K * N^{-1}
 //     and the inverse NTT needs no final N^{-1} scaling.  Two products are
@@ -168,16 +170,30 @@ __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
     x = x + t;
   }
 }
-// Harvey inverse butterfly, ntt.rs:84-104 (x, y < 2q -> x', y' < 2q); with
-// SPQ the exact Shoup quotient times Q comes from the special form of Q.
-template <bool SPQ>
+// Inverse GS butterfly (x' = x + y, y' = w (x - y), ntt.rs:84-104).  Generic
+// q: Harvey's form (x, y < 2q -> x', y' < 2q).  Q_N2048 (SPQ): no reduction of
+// the sum -- the rounds let sums grow to < 16 Q and reduce once per round
+// with reduce_n2048 -- and y' is an exact Shoup product in [0, 2Q); K Q must
+// bound the incoming y (the caller's stage bound).
+__device__ __forceinline__ u64 reduce_n2048(u64 v) {
+  // 2^54 = 77823 (mod Q): v = h 2^54 + l -> l + 77823 h, < 2^54 + 2^27 < 2Q
+  return (v & ((1ull << 54) - 1)) + (v >> 54) * 77823ull;
+}
+template <bool SPQ, int K>
 __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
-  const u64 q2 = SPQ ? (Q_N2048 << 1) : (q << 1);
-  u64 u = x + y;
-  if (u >= q2) u -= q2;
-  const u64 t = x + q2 - y;
-  y = SPQ ? w * t - mulq_n2048(umulhi(ws, t)) : shoup_mul(t, w, ws, q);
-  x = u;
+  if (SPQ) {
+    const u64 t = x + (u64)K * Q_N2048 - y;
+    const u64 u = x + y;
+    y = w * t - mulq_n2048(umulhi(ws, t));
+    x = u;
+  } else {
+    const u64 q2 = q << 1;
+    u64 u = x + y;
+    if (u >= q2) u -= q2;
+    const u64 t = x + q2 - y;
+    y = shoup_mul(t, w, ws, q);
+    x = u;
+  }
 }
 
 __device__ __forceinline__ u64 ldg(const u64 *p) { return __ldg(p); }
@@ -220,10 +236,21 @@ __device__ __forceinline__ void fbf2(u64 (&x)[8], u64 (&y)[8], int a, int b, u64
   fbf<LOGN == 11>(x[a], x[b], w, ws, q);
   if (TWO) fbf<LOGN == 11>(y[a], y[b], w, ws, q);
 }
-template <int LOGN, bool TWO>
+template <int LOGN, bool TWO, int K>
 __device__ __forceinline__ void ibf2(u64 (&x)[8], u64 (&y)[8], int a, int b, u64 w, u64 ws, u64 q) {
-  ibf<LOGN == 11>(x[a], x[b], w, ws, q);
-  if (TWO) ibf<LOGN == 11>(y[a], y[b], w, ws, q);
+  ibf<LOGN == 11, K>(x[a], x[b], w, ws, q);
+  if (TWO) ibf<LOGN == 11, K>(y[a], y[b], w, ws, q);
+}
+// End of an inverse round for N = 2048: every value back below 2Q.
+template <int LOGN, bool TWO>
+__device__ __forceinline__ void inv_round_reduce(u64 (&x)[8], u64 (&y)[8]) {
+  if constexpr (LOGN == 11) {
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      x[r] = reduce_n2048(x[r]);
+      if (TWO) y[r] = reduce_n2048(y[r]);
+    }
+  }
 }
 
 // Forward radix-8 round k: stages with m = 8^k, 2m and 4m groups; blk is the
@@ -256,20 +283,22 @@ __device__ __forceinline__ void inv_round8(u64 (&x)[8], u64 (&y)[8], int k, int 
   const int blk = j >> (LOGN - 3 * k - 3);
   const u64 q = rc.q;
   u64 w, ws;
+  // (N = 2048) inputs < 2Q; sums reach < 4Q, 8Q, 16Q over the three stages
 #pragma unroll
   for (int h = 0; h < 4; h++) {
     tw(rc.iw, 4 * m + 4 * blk + h, w, ws);
-    ibf2<LOGN, TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
+    ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w, ws, q);
   }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     tw(rc.iw, 2 * m + 2 * blk + h, w, ws);
-    ibf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    ibf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
   tw(rc.iw, m + blk, w, ws);
 #pragma unroll
-  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO>(x, y, r, r + 4, w, ws, q);
+  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO, 8>(x, y, r, r + 4, w, ws, q);
+  inv_round_reduce<LOGN, TWO>(x, y);
 }
 
 // Trailing 2-stage round (stages with N/4 and N/2 groups).
@@ -303,12 +332,13 @@ __device__ __forceinline__ void inv_round4(u64 (&x)[8], u64 (&y)[8], int j, cons
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       tw(rc.iw, N / 2 + 2 * g + e, w, ws);
-      ibf2<LOGN, TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
+      ibf2<LOGN, TWO, 2>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
     }
     tw(rc.iw, N / 4 + g, w, ws);
-    ibf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    ibf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
   }
+  inv_round_reduce<LOGN, TWO>(x, y);  // (N = 2048) sums < 8Q -> < 2Q
 }
 
 // Layout of full round k: thread j holds base + t r, t = N >> (3k + 3).
