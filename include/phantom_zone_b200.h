@@ -190,6 +190,10 @@ pz_status pz_ctx_set_pbs_grid_limit(pz_ctx *ctx, int grid_limit);
  * resident CTAs per SM (variant 0, 1, 2); default 0. */
 pz_status pz_ctx_set_pbs_variant(pz_ctx *ctx, int variant);
 int pz_ctx_pbs_variant(const pz_ctx *ctx);
+/* Autotuner: times every blind-rotation variant on `batch` synthetic
+ * key-switched LWEs with this key and keeps the fastest for the context
+ * (*ms: its time per launch). */
+pz_status pz_ctx_autotune(pz_ctx *ctx, const pz_key *key, size_t batch, int *variant, double *ms);
 
 /* ---- circuits ------------------------------------------------------------------
  * A circuit records gates instead of executing them (the reference executes

@@ -95,6 +95,23 @@ __device__ __forceinline__ u64 decomp_next(u64 &v, const Decomp &dp) {
   return ((0ull - c) & dp.q) + k - (c << dp.logb);
 }
 
+// One-digit decomposition (d = 1) with compile-time base 2^LOGB and IGN
+// ignored bits: decomp_init + one decomp_next, with everything after the
+// rounding shift in 32-bit arithmetic (the rounded value's digit and its next
+// bit sit in the low 32 bits).  The N = 2048 parameter sets all use
+// (LOGB, IGN) = (17, 37) for RLWE x RGSW and (24, 30) for automorphisms
+// (parameters.rs:526-704; the context checks it).
+template <int LOGB, int IGN>
+__device__ __forceinline__ u64 decompose1(u64 v, u64 q) {
+  static_assert(LOGB < 31 && IGN > 0, "digit and next bit in 32 bits");
+  if (v >= (q >> 1)) v = v - q;  // decomposer.rs:217-234 (wrapping)
+  const u32 r = (u32)(v >> IGN) + (u32)((v >> (IGN - 1)) & 1ull);
+  const u32 k = r & ((1u << LOGB) - 1u), half = 1u << (LOGB - 1);
+  const bool c = k > half || (k == half && ((r >> LOGB) & 1u));  // decomposer.rs:264-300
+  return c ? q + k - (1ull << LOGB) : (u64)k;
+}
+constexpr int RLRG_LOGB = 17, RLRG_IGN = 37, AUTO_LOGB = 24, AUTO_IGN = 30;
+
 template <int LOGN>
 struct NttShape {
   static_assert(LOGN == 9 || LOGN == 11, "ring dimension 512 or 2048");

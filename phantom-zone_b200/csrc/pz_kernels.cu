@@ -240,18 +240,27 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
     if (is_auto) {
 #pragma unroll
       for (int r = 0; r < 8; r++) {
-        u64 st = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
-        x[r] = decomp_next(st, P.dauto);
+        if constexpr (LOGN == 11) {
+          x[r] = decompose1<AUTO_LOGB, AUTO_IGN>(s_a[swz(pos_coef<LOGN>(j, r))], q);
+        } else {
+          u64 st = decomp_init(s_a[swz(pos_coef<LOGN>(j, r))], P.dauto);
+          x[r] = decomp_next(st, P.dauto);
+        }
       }
       ntt_fwd<LOGN, false>(x, x, sm, P.rc);
       mac_auto<LOGN>(x, y, K, K + N, P.rc);
     } else {
 #pragma unroll
       for (int r = 0; r < 8; r++) {
-        u64 sa = decomp_init(x[r], P.da);
-        x[r] = decomp_next(sa, P.da);
-        u64 sb = decomp_init(y[r], P.db);
-        y[r] = decomp_next(sb, P.db);
+        if constexpr (LOGN == 11) {
+          x[r] = decompose1<RLRG_LOGB, RLRG_IGN>(x[r], q);
+          y[r] = decompose1<RLRG_LOGB, RLRG_IGN>(y[r], q);
+        } else {
+          u64 sa = decomp_init(x[r], P.da);
+          x[r] = decomp_next(sa, P.da);
+          u64 sb = decomp_init(y[r], P.db);
+          y[r] = decomp_next(sb, P.db);
+        }
       }
       ntt_fwd<LOGN, true>(x, y, sm, P.rc);
       mac_pair<LOGN>(x, y, K, K + N, K + 2 * N, K + 3 * N, P.rc);

@@ -252,6 +252,13 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   if (c->logn != 9 && c->logn != 11) { delete c; return PZ_ERR_NOT_SUPPORTED; }
   // the N = 2048 kernels reduce with the special form of this ring's prime
   if (c->logn == 11 && Q != pz::Q_N2048) { delete c; return PZ_ERR_NOT_SUPPORTED; }
+  // ... and the one-digit decomposers of those sets (compile-time shapes)
+  if (c->logn == 11 && P.rlrg_d_a == 1 && P.rlrg_d_b == 1 && P.auto_d == 1 &&
+      (P.rlrg_logb != (u32)pz::RLRG_LOGB || P.auto_logb != (u32)pz::AUTO_LOGB ||
+       log2_ref(Q) - P.rlrg_logb != (u32)pz::RLRG_IGN || log2_ref(Q) - P.auto_logb != (u32)pz::AUTO_IGN)) {
+    delete c;
+    return PZ_ERR_NOT_SUPPORTED;
+  }
   if (root == 0) root = default_root(Q, 2 * N);
   if (root == 0 || powmod(root, N, Q) != Q - 1) { delete c; return PZ_ERR_INVALID_ARGUMENT; }
   c->root = root;
@@ -573,6 +580,66 @@ pz_status pz_blind_rotate_batch_device(pz_ctx *c, const pz_key *k, const uint32_
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   PZ_CK(c, pz::launch_pbs((int)c->logn, d1, br, d_ks, c->P.lwe_n + 1, d_test_vec, d_out, count, nullptr,
                           c->grid_limit, pick(c, stream), c->pbs_variant));
+  return PZ_OK;
+}
+
+pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant, double *ms) {
+  if (!c || batch == 0) return PZ_ERR_INVALID_ARGUMENT;
+  pz_status s = check_key(c, k);
+  if (s != PZ_OK) return s;
+  std::lock_guard<std::mutex> lock(c->mu);
+  PZ_CK(c, cudaSetDevice(c->device));
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  const int nv = (c->logn == 11 && d1) ? pz::PBS_VARIANTS : 1;
+  // synthetic key-switched LWEs, uniform mod q_ks, and gate codes
+  const u32 cols = c->P.lwe_n + 1;
+  std::vector<u32> ks(batch * cols);
+  std::vector<unsigned char> g(batch);
+  u64 st = 0x9E3779B97F4A7C15ull;
+  for (auto &v : ks) { st ^= st << 13; st ^= st >> 7; st ^= st << 17; v = (u32)(st % c->P.lwe_q); }
+  for (size_t i = 0; i < batch; i++) g[i] = (unsigned char)(i % 6);
+  u32 *d_ks = nullptr;
+  unsigned char *d_g = nullptr;
+  u64 *d_out = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaMalloc(&d_ks, ks.size() * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&d_g, batch);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, batch * (c->P.rlwe_n + 1) * 8);
+  if (e == cudaSuccess) e = cudaMemcpy(d_ks, ks.data(), ks.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_g, g.data(), batch, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  pz::BrParams br = c->br;
+  br.rgsw = k->d_rgsw;
+  br.autos = k->d_autos;
+  br.out_idx = nullptr;
+  double best = 1e30;
+  int bv = c->pbs_variant;
+  for (int v = 0; v < nv && e == cudaSuccess; v++) {
+    auto launch = [&]() {
+      return pz::launch_pbs((int)c->logn, d1, br, d_ks, cols, d_g, d_out, batch, nullptr, c->grid_limit, c->stream, v);
+    };
+    if ((e = launch()) != cudaSuccess) break;  // warm-up
+    if ((e = cudaEventRecord(a, c->stream)) != cudaSuccess) break;
+    for (int r = 0; r < 2 && e == cudaSuccess; r++) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(b, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float t = 0;
+    if (e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+    if (e == cudaSuccess && t / 2 < best) {
+      best = t / 2;
+      bv = v;
+    }
+  }
+  cudaFree(d_ks);
+  cudaFree(d_g);
+  cudaFree(d_out);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (e != cudaSuccess) return cuda_fail(c, "pz_ctx_autotune", e);
+  c->pbs_variant = bv;
+  if (variant) *variant = bv;
+  if (ms) *ms = best;
   return PZ_OK;
 }
 

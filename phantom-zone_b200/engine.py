@@ -149,6 +149,13 @@ class Engine:
     def pbs_variant(self, v):
         check(lib().pz_ctx_set_pbs_variant(self.h, int(v)), self.h, "set_pbs_variant")
 
+    def autotune(self, key, batch=2368):
+        """Pick the fastest blind-rotation variant for this context on `batch` gates."""
+        v, ms = ctypes.c_int(), ctypes.c_double()
+        check(lib().pz_ctx_autotune(self.h, key.h, int(batch), ctypes.byref(v), ctypes.byref(ms)), self.h,
+              "pz_ctx_autotune")
+        return {"variant": v.value, "ms": ms.value}
+
     # -- keys --------------------------------------------------------------
     def upload_key(self, rgsw, autos, lwe_ksk):
         """Upload a coefficient-domain server key (layouts of pz_server_key_view)."""

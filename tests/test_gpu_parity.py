@@ -201,3 +201,19 @@ def test_pbs_variants_bit_exact(gpu_available, param, variant):
         eng.pbs_variant = old
     want = okey.gate_batch(gates, c0, c1, threads=4)
     assert np.array_equal(got, want)
+
+
+def test_ctx_autotune_keeps_results(gpu_available):
+    """pz_ctx_autotune picks a launch variant; the gate words do not change."""
+    O = oracle()
+    ev, secrets, _, okey = oracle_setup("NI_8P")
+    eng, dkey = engine_and_key("NI_8P")
+    old = eng.pbs_variant
+    try:
+        t = eng.autotune(dkey, 296)
+        assert t["variant"] in (0, 1, 2) and t["ms"] > 0 and eng.pbs_variant == t["variant"]
+        bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, 4, 0x7F)
+        gates = np.array([O.GATES[g] for g in ["and", "nand", "xor", "nor"]], np.uint8)
+        assert np.array_equal(eng.gate_batch(dkey, gates, c0, c1), okey.gate_batch(gates, c0, c1, threads=4))
+    finally:
+        eng.pbs_variant = old
