@@ -187,8 +187,12 @@ pz_status pz_lwe_key_switch_device(pz_ctx *ctx, const pz_key *key, const uint64_
  * (the kernel then strides over the batch). */
 pz_status pz_ctx_set_pbs_grid_limit(pz_ctx *ctx, int grid_limit);
 /* Blind-rotation kernel variant for N = 2048: registers capped for 2, 3 or 4
- * resident CTAs per SM (variant 0, 1, 2); default 0. */
+ * resident CTAs per SM (variant 0, 1, 2; default 0), or 3: each ciphertext on a
+ * cluster of two CTAs (a and b on different SMs: lower latency per gate). */
 pz_status pz_ctx_set_pbs_variant(pz_ctx *ctx, int variant);
+/* Launches of at most max_gates gates use variant 3 whatever the variant set
+ * (-1, the default: half the GPU's SMs; 0: only if variant 3 is set). */
+pz_status pz_ctx_set_split_threshold(pz_ctx *ctx, int max_gates);
 int pz_ctx_pbs_variant(const pz_ctx *ctx);
 /* Autotuner: times every blind-rotation variant on `batch` synthetic
  * key-switched LWEs with this key and keeps the fastest for the context

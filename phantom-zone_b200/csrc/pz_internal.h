@@ -25,6 +25,7 @@ struct pz_ctx {
   pz::KsParams ks{};
   int grid_limit = 0;
   int pbs_variant = 0;  // blind-rotation launch shape (see pz::PBS_VARIANTS)
+  int split_below = -1;  // batches of at most this many gates use the two-CTA kernel (-1: half the SMs)
   // host-API scratch (guarded by mu)
   std::mutex mu;
   size_t cap = 0;

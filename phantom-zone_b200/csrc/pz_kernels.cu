@@ -17,6 +17,8 @@
 #include <mutex>
 #include <utility>
 
+#include <cooperative_groups.h>
+
 #include "pz_kernels.cuh"
 
 namespace pz {
@@ -27,6 +29,9 @@ namespace pz {
 // buffer of the two-polynomial transforms (region 0 alone of the
 // single-polynomial ones).
 constexpr int OP_REGIONS = 2;
+// The two-CTA blind rotation: region 0 exchanges / scatter, region 1 schedule
+// scratch / permutation of b, regions 2-3 the two digit slots read by the peer.
+constexpr int SPLIT_REGIONS = 4;
 
 // Operation codes of the blind-rotation schedule: an external product with
 // RGSW key `i` is `i`; an automorphism with key slot v (0 = -g) is
@@ -516,22 +521,41 @@ size_t pbs_smem_bytes(int logn, u32 br_q, u32 n) {
   return OP_REGIONS * N * 8 + extra;
 }
 
-// MINB: CTAs per SM the register allocation must allow (launch-shape
-// variants chosen at run time, see pz_ctx_set_pbs_variant).
-// One gate bootstrap of ciphertext ct (key-switched LWE kso, gate code
-// gcode) with the parameters and key of P; the whole CTA takes part.
-template <int LOGN, bool D1>
-__device__ __forceinline__ void pbs_item(const BrParams &P, int ct, const u32 *kso, u32 gcode, u64 *out,
-                                         u64 *rlwe_dbg, u64 *smem) {
+// Dynamic shared memory of the two-CTA kernel: 4 x N words + the schedule.
+static size_t split_smem_bytes(u32 br_q, u32 n) {
+  const size_t N = 2048, R = br_q / 2;
+  size_t extra = ((R + 1) + n + (n + R + 1)) * 2 + 4;
+  extra = (extra + 15) & ~(size_t)15;
+  return SPLIT_REGIONS * 8 * N + extra;
+}
+
+// Shared-memory arrays of the blind-rotation schedule, after `regions` x N words.
+struct SchedSmem {
+  unsigned short *start, *list, *ops;
+  u32 *nops;
+};
+template <int LOGN>
+__device__ __forceinline__ SchedSmem sched_smem(u64 *smem, int regions, u32 R, u32 n) {
+  constexpr int N = 1 << LOGN;
+  SchedSmem m;
+  m.start = (unsigned short *)(smem + regions * N);  // R + 1
+  m.list = m.start + (R + 1);                         // n
+  m.ops = m.list + n;                                 // n + R + 1
+  m.nops = (u32 *)(((size_t)(m.ops + n + R + 1) + 3) & ~(size_t)3);
+  return m;
+}
+
+// Odd mod-switch, dlog buckets (pbs.rs:147-161, stable in LWE index) and the
+// blind-rotation schedule (pbs.rs:240-414) of one key-switched LWE, built in
+// shared memory by the whole CTA (regions 0 and 1 of smem are scratch).
+template <int LOGN>
+__device__ __forceinline__ void build_schedule(const BrParams &P, const u32 *kso, u64 *smem, const SchedSmem &S) {
   constexpr int N = 1 << LOGN, T = NttShape<LOGN>::T;
-  u64 *sm = smem;
   const u32 R = P.br_q >> 1, q4 = P.br_q >> 2, n = P.n;
-  unsigned short *s_start = (unsigned short *)(smem + OP_REGIONS * N);  // R + 1
-  unsigned short *s_list = s_start + (R + 1);                           // n
-  unsigned short *s_ops = s_list + n;                                   // n + R + 1
-  u32 *s_nops = (u32 *)(((size_t)(s_ops + n + R + 1) + 3) & ~(size_t)3);
   const int j = threadIdx.x, lane = j & 31, warp = j >> 5;
-  const u64 q = P.rc.q;
+  u64 *sm = smem;
+  unsigned short *s_start = S.start, *s_list = S.list, *s_ops = S.ops;
+  u32 *s_nops = S.nops;
   {
     // ---- odd mod-switch + dlog buckets (pbs.rs:147-161), stable in LWE index
     u32 *cnt = (u32 *)sm;                                 // R counters (region 0)
@@ -624,32 +648,60 @@ __device__ __forceinline__ void pbs_item(const BrParams &P, int ct, const u32 *k
       bucket(0);  // +(g^0)
       *s_nops = no;
     }
+  }
+}
 
-    // ---- trivial test RLWE: X^{g * odd(b)} * tv, embedded (pbs.rs:163-211)
-    const u32 odd_b = mod_switch_odd(kso[0] & P.ks_mask, P.q_ks_f, P.br_q_f);
-    const u32 gb = (u32)(((u64)P.g * odd_b) % P.br_q);
-    u32 mexp = gb;
-    bool msign = true;
-    if (mexp > R) { mexp -= R; msign = false; }
-    u32 gi = gcode & 7u;
-    if (gi > 5) gi = 5;  // codes are validated on the host; never index past the 6 test vectors
-    const u64 *tv = P.tv + (size_t)gi * R;
+// Trivial test RLWE's b: X^{g * odd(b)} * tv, embedded (pbs.rs:163-211), in
+// the coefficient layout of this thread.
+template <int LOGN>
+__device__ __forceinline__ void test_rlwe_b(const BrParams &P, const u32 *kso, u32 gcode, u64 (&b)[8]) {
+  const u32 R = P.br_q >> 1;
+  const u64 q = P.rc.q;
+  const int j = threadIdx.x;
+  const u32 odd_b = mod_switch_odd(kso[0] & P.ks_mask, P.q_ks_f, P.br_q_f);
+  const u32 gb = (u32)(((u64)P.g * odd_b) % P.br_q);
+  u32 mexp = gb;
+  bool msign = true;
+  if (mexp > R) { mexp -= R; msign = false; }
+  u32 gi = gcode & 7u;
+  if (gi > 5) gi = 5;  // codes are validated on the host; never index past the 6 test vectors
+  const u64 *tv = P.tv + (size_t)gi * R;
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const u32 p = (u32)pos_coef<LOGN>(j, r);
+    u64 v = 0;
+    if (p % P.emb == 0) {
+      const u32 o = p / P.emb;
+      u32 s;
+      bool sg;
+      if (o >= mexp) { s = o - mexp; sg = msign; } else { s = o + R - mexp; sg = !msign; }
+      const u64 t = tv[s];
+      v = sg ? t : q - t;
+    }
+    b[r] = v;
+  }
+}
+
+// MINB: CTAs per SM the register allocation must allow (launch-shape
+// variants chosen at run time, see pz_ctx_set_pbs_variant).
+// One gate bootstrap of ciphertext ct (key-switched LWE kso, gate code
+// gcode) with the parameters and key of P; the whole CTA takes part.
+template <int LOGN, bool D1>
+__device__ __forceinline__ void pbs_item(const BrParams &P, int ct, const u32 *kso, u32 gcode, u64 *out,
+                                         u64 *rlwe_dbg, u64 *smem) {
+  constexpr int N = 1 << LOGN;
+  u64 *sm = smem;
+  const SchedSmem S = sched_smem<LOGN>(smem, OP_REGIONS, P.br_q >> 1, P.n);
+  unsigned short *s_ops = S.ops;
+  u32 *s_nops = S.nops;
+  const int j = threadIdx.x;
+  const u64 q = P.rc.q;
+  {
+    build_schedule<LOGN>(P, kso, smem, S);
     u64 acc[2][8];
 #pragma unroll
-    for (int r = 0; r < 8; r++) {
-      const u32 p = (u32)pos_coef<LOGN>(j, r);
-      acc[0][r] = 0;
-      u64 v = 0;
-      if (p % P.emb == 0) {
-        const u32 o = p / P.emb;
-        u32 s;
-        bool sg;
-        if (o >= mexp) { s = o - mexp; sg = msign; } else { s = o + R - mexp; sg = !msign; }
-        const u64 t = tv[s];
-        v = sg ? t : q - t;
-      }
-      acc[1][r] = v;
-    }
+    for (int r = 0; r < 8; r++) acc[0][r] = 0;
+    test_rlwe_b<LOGN>(P, kso, gcode, acc[1]);
     __syncthreads();
 
     // ---- blind rotation: one operation per schedule entry
@@ -706,6 +758,202 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
     }
     __syncthreads();
     pbs_item<LOGN, D1>(sp, ct, ks + (size_t)ct * ks_stride, gates[ct], out, nullptr, smem);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Low-latency blind rotation: one ciphertext on a cluster of two CTAs (two
+// SMs).  CTA rank 0 holds a, rank 1 holds b (same layouts and domains as the
+// one-CTA kernel: b is left in the evaluation domain ahead of non-trivial
+// automorphisms).  Per operation each CTA transforms only its own polynomial;
+// the transformed digits cross to the other CTA through distributed shared
+// memory (a two-slot buffer, alternating by operation), with exactly one
+// cluster barrier per operation on both CTAs (both build the same schedule
+// from the same input), and one more per ciphertext.  External product:
+// each CTA forms one output row pair from both digit polynomials.
+// Automorphism: rank 0 permutes, decomposes and transforms a(X^k); rank 1
+// permutes b in the evaluation domain meanwhile; after the barrier rank 0
+// multiplies by the key's A row, rank 1 by its B row and adds b(X^k).  The
+// words are those of the one-CTA kernel (every step is the same exact
+// arithmetic mod Q).  N = 2048, one-digit decompositions only.
+// ---------------------------------------------------------------------------
+namespace cg = cooperative_groups;
+
+// out = REDC(x ka + y kb), x, y in the evaluation layout, key rows in the device layout
+template <int LOGN>
+__device__ __forceinline__ void mac_two_rows(u64 (&x)[8], const u64 (&y)[8], const u64 *ka, const u64 *kb,
+                                             const RingConsts &rc) {
+  const int j = threadIdx.x;
+  const u64 q = rc.q, qi = rc.qinv_neg;
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    const int di = dev_index<LOGN>(j, 2 * rr);
+    u64 a[2], b[2];
+    ld_key2(ka + di, a[0], a[1]);
+    ld_key2(kb + di, b[0], b[1]);
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int r = 2 * rr + e;
+      u64 hi, lo;
+      mul128(x[r], a[e], hi, lo);
+      mac128(y[r], b[e], hi, lo);
+      x[r] = redc(hi, lo, q, qi);
+    }
+  }
+}
+
+template <int LOGN>
+__device__ __forceinline__ void split_op(u64 (&x)[8], u32 op, u32 t, const BrParams &P, u64 *sm, u64 *slots,
+                                         const u64 *peer_slots, unsigned rank, cg::cluster_group &cl) {
+  constexpr int N = 1 << LOGN, T = NttShape<LOGN>::T;
+  const u64 q = P.rc.q, q2 = P.rc.q << 1;
+  const int j = threadIdx.x;
+  u64 *own = slots + (t & 1) * N;
+  const u64 *peer = peer_slots + (t & 1) * N;
+  const bool keep_b = (op & OP_KEEPB) != 0;
+  if (op & OP_AUTO) {
+    const u32 k = P.auto_k[op & OP_SLOT];
+    if (op & OP_TRIVIAL) {  // runtime.rs:625-642: only b, permuted in the coefficient domain
+      if (rank == 1) {
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+          u32 tt = ((u32)pos_coef<LOGN>(j, r) * k) & (2 * N - 1);
+          const bool neg = tt >= (u32)N;
+          if (neg) tt -= N;
+          sm[swz(tt)] = neg ? q - x[r] : x[r];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 8; r++) x[r] = sm[swz(pos_coef<LOGN>(j, r))];
+      }
+      cl.sync();
+      return;
+    }
+    const u64 *K = P.autos + (size_t)(op & OP_SLOT) * P.auto_rows * N;
+    if (rank == 0) {  // a(X^k) with sign, one digit, forward transform
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        u32 tt = ((u32)pos_coef<LOGN>(j, r) * k) & (2 * N - 1);
+        const bool neg = tt >= (u32)N;
+        if (neg) tt -= N;
+        sm[swz(tt)] = neg ? q - x[r] : x[r];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < 8; r++) x[r] = decompose1<AUTO_LOGB, AUTO_IGN>(sm[swz(pos_coef<LOGN>(j, r))], q);
+      ntt_fwd<LOGN, false>(x, x, sm, P.rc);
+#pragma unroll
+      for (int r = 0; r < 8; r++) own[r * T + j] = x[r];
+    } else {  // b in the evaluation domain, permuted there
+      u64 *sb = sm + N;
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < 8; r++) sb[swz(pos_eval<LOGN>(j, r))] = x[r];
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < 8; r++) x[r] = sb[swz(auto_eval_src<LOGN>(pos_eval<LOGN>(j, r), k))];
+    }
+    cl.sync();
+    if (rank == 0) {
+      u64 z[8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) z[r] = 0;
+      mac_two_rows<LOGN>(x, z, K, K, P.rc);  // a' = d A (second product is 0)
+      ntt_inv<LOGN, false>(x, x, sm, P.rc);
+#pragma unroll
+      for (int r = 0; r < 8; r++) x[r] = reduce2(x[r], q);
+    } else {
+      u64 d[8], z[8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        d[r] = peer[r * T + j];
+        z[r] = 0;
+      }
+      mac_two_rows<LOGN>(d, z, K + N, K + N, P.rc);  // d B
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        const u64 v = d[r] + x[r];
+        x[r] = v >= q2 ? v - q2 : v;
+      }
+      if (!keep_b) {
+        ntt_inv<LOGN, false>(x, x, sm, P.rc);
+#pragma unroll
+        for (int r = 0; r < 8; r++) x[r] = reduce2(x[r], q);
+      }
+    }
+    return;
+  }
+  // external product: rows A(-sm), B(-sm), A(m), B(m) (d_a = d_b = 1)
+  const u64 *K = P.rgsw + (size_t)(op & OP_INDEX) * P.rgsw_rows * N;
+#pragma unroll
+  for (int r = 0; r < 8; r++) x[r] = decompose1<RLRG_LOGB, RLRG_IGN>(x[r], q);
+  ntt_fwd<LOGN, false>(x, x, sm, P.rc);
+#pragma unroll
+  for (int r = 0; r < 8; r++) own[r * T + j] = x[r];
+  cl.sync();
+  u64 y[8];
+#pragma unroll
+  for (int r = 0; r < 8; r++) y[r] = peer[r * T + j];
+  // rank 0: a' = da A(-sm) + db A(m); rank 1: b' = da B(-sm) + db B(m)
+  if (rank == 0) mac_two_rows<LOGN>(x, y, K, K + 2 * N, P.rc);
+  else {
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const u64 tmp = x[r];
+      x[r] = y[r];
+      y[r] = tmp;
+    }
+    mac_two_rows<LOGN>(x, y, K + N, K + 3 * N, P.rc);
+  }
+  if (rank == 0 || !keep_b) {
+    ntt_inv<LOGN, false>(x, x, sm, P.rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++) x[r] = reduce2(x[r], q);
+  }
+}
+
+template <int LOGN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttShape<LOGN>::T, 2)
+    pbs_split_kernel(BrParams P, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out, int count) {
+  constexpr int N = 1 << LOGN;
+  extern __shared__ u64 smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned rank = cl.block_rank();
+  u64 *slots = smem + 2 * N;
+  const u64 *peer_slots = cl.map_shared_rank(slots, rank ^ 1u);
+  const SchedSmem S = sched_smem<LOGN>(smem, SPLIT_REGIONS, P.br_q >> 1, P.n);
+  const int j = threadIdx.x;
+  const u64 q = P.rc.q;
+  const int ncl = gridDim.x / 2;
+  for (int ct = blockIdx.x / 2; ct < count; ct += ncl) {  // both CTAs of a cluster take the same items
+    const u32 *kso = ks + (size_t)ct * ks_stride;
+    build_schedule<LOGN>(P, kso, smem, S);
+    u64 x[8];
+    if (rank == 0) {
+#pragma unroll
+      for (int r = 0; r < 8; r++) x[r] = 0;
+    } else {
+      test_rlwe_b<LOGN>(P, kso, gates[ct], x);
+    }
+    __syncthreads();
+    const u32 nops = *S.nops;
+#pragma unroll 1
+    for (u32 t = 0; t < nops; t++) split_op<LOGN>(x, S.ops[t], t, P, smem, slots, peer_slots, rank, cl);
+    // sample extract at index 0 (pbs.rs:423-449): rank 0 the a-part, rank 1 b[0]
+    u64 *o = out + (size_t)(P.out_idx ? P.out_idx[ct] : (u32)ct) * (N + 1);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const u32 p = (u32)pos_coef<LOGN>(j, r);
+      if (rank == 0) {
+        if (p == 0) o[1] = x[r];
+        else o[1 + N - p] = q - x[r];
+      } else if (p == 0) {
+        o[0] = x[r];
+      }
+    }
+    cl.sync();  // the digit slots are reused by the next ciphertext
   }
 }
 
@@ -867,6 +1115,12 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                                    \
   if ((e = set_smem(pbs_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;                        \
   pbs_kernel<LN, DD, MB><<<grid, TH, smem, s>>>(P, ks, ks_stride, gates, out, (int)count, rlwe_dbg);
+  if (logn == 11 && d1 && variant == PBS_SPLIT && rlwe_dbg == nullptr) {
+    const size_t ssmem = split_smem_bytes(P.br_q, P.n);
+    if ((e = set_smem(pbs_split_kernel<11>, ssmem)) != cudaSuccess) return e;
+    pbs_split_kernel<11><<<2 * grid, 256, ssmem, s>>>(P, ks, ks_stride, gates, out, (int)count);
+    return cudaGetLastError();
+  }
   if (logn == 11 && d1) {
     if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
     else if (variant == 1) { PZ_LAUNCH(11, true, 3, 256) }

@@ -73,6 +73,9 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
 // launch-shape variants of the production blind rotation (registers per
 // thread capped for 2, 3 or 4 CTAs of 256 threads per SM)
 constexpr int PBS_VARIANTS = 3;
+// launch shape for small batches (N = 2048, one-digit sets): one ciphertext
+// per cluster of two CTAs, a on one SM and b on the other (lower latency)
+constexpr int PBS_SPLIT = 3;
 // Ragged batches (several sessions / parameter sets in one launch): per-item
 // descriptors in device memory; max_* bound the sizes over the descriptors.
 cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,

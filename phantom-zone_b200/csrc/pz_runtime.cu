@@ -187,6 +187,17 @@ pz_status check_gates_host(pz_ctx *c, const uint8_t *gates, size_t count, bool r
 }  // namespace
 
 namespace pz {
+int effective_variant(pz_ctx *c, size_t count) {
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  if (c->logn != 11 || !d1) return c->pbs_variant;
+  if (c->split_below < 0) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    c->split_below = sms / 2;
+  }
+  return (count <= (size_t)c->split_below) ? pz::PBS_SPLIT : c->pbs_variant;
+}
+
 pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, const u64 *d_c0, const u64 *d_c1,
                     u64 *d_out, size_t count, u32 *d_ks_out, u64 *d_rlwe, cudaStream_t s, u32 *d_ks_scratch,
                     bool raw, const u32 *in0, const u32 *in1, const u32 *out_idx) {
@@ -207,7 +218,7 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
   if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s,
-                     c->pbs_variant);
+                     effective_variant(c, count));
   if (e != cudaSuccess) return cuda_fail(c, "launch_pbs", e);
   return PZ_OK;
 }
@@ -365,8 +376,13 @@ pz_status pz_ctx_params(const pz_ctx *c, pz_params *out) {
 uint64_t pz_ctx_ntt_root(const pz_ctx *c) { return c ? c->root : 0; }
 
 pz_status pz_ctx_set_pbs_variant(pz_ctx *c, int v) {
-  if (!c || v < 0 || v >= pz::PBS_VARIANTS) return PZ_ERR_INVALID_ARGUMENT;
+  if (!c || v < 0 || v > pz::PBS_SPLIT) return PZ_ERR_INVALID_ARGUMENT;
   c->pbs_variant = v;
+  return PZ_OK;
+}
+pz_status pz_ctx_set_split_threshold(pz_ctx *c, int max_gates) {
+  if (!c || max_gates < -1) return PZ_ERR_INVALID_ARGUMENT;
+  c->split_below = max_gates;
   return PZ_OK;
 }
 int pz_ctx_pbs_variant(const pz_ctx *c) { return c ? c->pbs_variant : -1; }
@@ -579,7 +595,7 @@ pz_status pz_blind_rotate_batch_device(pz_ctx *c, const pz_key *k, const uint32_
   br.out_idx = nullptr;
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   PZ_CK(c, pz::launch_pbs((int)c->logn, d1, br, d_ks, c->P.lwe_n + 1, d_test_vec, d_out, count, nullptr,
-                          c->grid_limit, pick(c, stream), c->pbs_variant));
+                          c->grid_limit, pick(c, stream), pz::effective_variant(c, count)));
   return PZ_OK;
 }
 
@@ -590,7 +606,7 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
   std::lock_guard<std::mutex> lock(c->mu);
   PZ_CK(c, cudaSetDevice(c->device));
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
-  const int nv = (c->logn == 11 && d1) ? pz::PBS_VARIANTS : 1;
+  const int nv = (c->logn == 11 && d1) ? pz::PBS_SPLIT + 1 : 1;
   // synthetic key-switched LWEs, uniform mod q_ks, and gate codes
   const u32 cols = c->P.lwe_n + 1;
   std::vector<u32> ks(batch * cols);

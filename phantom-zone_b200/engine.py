@@ -141,6 +141,10 @@ class Engine:
     def set_pbs_grid_limit(self, g):
         check(lib().pz_ctx_set_pbs_grid_limit(self.h, int(g)), self.h, "set_pbs_grid_limit")
 
+    def set_split_threshold(self, max_gates):
+        """Launches of at most max_gates gates use the two-CTA low-latency kernel (-1: default)."""
+        check(lib().pz_ctx_set_split_threshold(self.h, int(max_gates)), self.h, "set_split_threshold")
+
     @property
     def pbs_variant(self):
         return lib().pz_ctx_pbs_variant(self.h)

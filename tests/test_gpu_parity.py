@@ -182,9 +182,10 @@ def test_gate_batch_host_api(gpu_available, param):
 
 
 @pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_pbs_variants_bit_exact(gpu_available, param, variant):
-    """Every launch-shape variant of the blind rotation gives the oracle's words."""
+    """Every launch-shape variant of the blind rotation (3: one ciphertext on a
+    cluster of two CTAs) gives the oracle's words."""
     O = oracle()
     ev, secrets, _, okey = oracle_setup(param)
     eng, dkey = engine_and_key(param)
@@ -193,12 +194,14 @@ def test_pbs_variants_bit_exact(gpu_available, param, variant):
     gates = np.array([O.GATES[g] for g in ["nand", "xor", "or", "xnor"]], np.uint8)
     old = eng.pbs_variant
     eng.pbs_variant = variant
+    eng.set_split_threshold(0)  # the variant under test, not the small-batch default
     try:
         out = to_dev(np.zeros((count, ev.L), np.uint64))
         eng.gate_batch_device(dkey, to_dev(gates), to_dev(c0), to_dev(c1), out)
         got = to_host(out)
     finally:
         eng.pbs_variant = old
+        eng.set_split_threshold(-1)
     want = okey.gate_batch(gates, c0, c1, threads=4)
     assert np.array_equal(got, want)
 
@@ -217,3 +220,32 @@ def test_ctx_autotune_keeps_results(gpu_available):
         assert np.array_equal(eng.gate_batch(dkey, gates, c0, c1), okey.gate_batch(gates, c0, c1, threads=4))
     finally:
         eng.pbs_variant = old
+
+
+def test_split_kernel_many_items_per_cluster(gpu_available):
+    """The two-CTA kernel with fewer clusters than ciphertexts (each cluster
+    bootstraps several in turn, reusing its digit slots) == the one-CTA kernel."""
+    O = oracle()
+    ev, secrets, _, okey = oracle_setup("NI_8P")
+    eng, dkey = engine_and_key("NI_8P")
+    count = 24
+    r = rng(0x7E)
+    c0 = r.uniform_mod(ev.Q, count * ev.L).reshape(count, ev.L)
+    c1 = r.uniform_mod(ev.Q, count * ev.L).reshape(count, ev.L)
+    gates = (np.arange(count) % 6).astype(np.uint8)
+    outs = []
+    old = eng.pbs_variant
+    try:
+        for v, limit in [(0, 0), (3, 5)]:
+            eng.pbs_variant = v
+            eng.set_split_threshold(0)
+            eng.set_pbs_grid_limit(limit)
+            out = to_dev(np.zeros((count, ev.L), np.uint64))
+            eng.gate_batch_device(dkey, to_dev(gates), to_dev(c0), to_dev(c1), out)
+            outs.append(to_host(out))
+    finally:
+        eng.pbs_variant = old
+        eng.set_split_threshold(-1)
+        eng.set_pbs_grid_limit(0)
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[1][:3], okey.gate_batch(gates[:3], c0[:3], c1[:3], threads=3))
