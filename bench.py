@@ -392,12 +392,17 @@ def key_upload_bench(P, device):
     t1 = time.perf_counter()
     k2 = eng.upload_key_seeded(rgsw, auto_b, b"\x01" * 32, lwe_b, b"\x02" * 32)
     t2 = time.perf_counter()
-    k1.release()
-    k2.release()
+    blob = k1.export()
+    t3 = time.perf_counter()
+    k3 = eng.import_key(blob)
+    t4 = time.perf_counter()
+    for k in (k1, k2, k3):
+        k.release()
     eng.close()
     return {"config": "NI_8P server key, host -> device, wall clock", "full_ms": (t1 - t0) * 1e3,
             "seeded_ms": (t2 - t1) * 1e3, "full_host_bytes": int(rgsw.nbytes + autos.nbytes + ksk.nbytes),
-            "seeded_host_bytes": int(rgsw.nbytes + auto_b.nbytes + lwe_b.nbytes + 64)}
+            "seeded_host_bytes": int(rgsw.nbytes + auto_b.nbytes + lwe_b.nbytes + 64),
+            "export_ms": (t3 - t2) * 1e3, "import_ms": (t4 - t3) * 1e3, "device_form_bytes": len(blob)}
 
 
 def aggregate_bench(P, torch, device, prm="I_8P"):

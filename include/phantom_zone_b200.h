@@ -248,6 +248,19 @@ pz_status pz_circuit_capture_graph(pz_ctx *ctx, const pz_key *key, pz_circuit *c
                                    uint64_t *d_outputs, void *stream);
 pz_status pz_circuit_replay_graph(pz_circuit *c, void *stream);
 
+/* ---- wire formats (no reference counterpart: the reference serialises nothing) ----
+ * Device-form server key as bytes, for checkpoint / restore and for moving a
+ * session between processes: a 64-byte header (parameter set, NTT root, sizes)
+ * and the device arrays as they are.  Import copies them back without any
+ * conversion; a blob from another parameter set or NTT root is refused.  With
+ * buf = NULL, export only writes the required *size. */
+pz_status pz_key_export(const pz_key *key, void *buf, size_t capacity, size_t *size);
+pz_status pz_key_import(pz_ctx *ctx, const void *buf, size_t size, pz_key **out);
+/* Circuits as bytes (wire handles keep their meaning); a malformed blob is
+ * rejected with PZ_ERR_INVALID_ARGUMENT. */
+pz_status pz_circuit_serialize(const pz_circuit *c, void *buf, size_t capacity, size_t *size);
+pz_status pz_circuit_deserialize(const void *buf, size_t size, pz_circuit **out);
+
 /* ---- seeded server keys (device-side expansion) ------------------------------------
  * What a server receives after key aggregation (SeededInteractiveMultiPartyServerKey,
  * SeededNonInteractiveMultiPartyServerKey; bool/keys.rs:536-781, 851-1004): the RGSW

@@ -89,6 +89,10 @@ SIGNATURES = {
     "pz_aggregate_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp]),
     "pz_ctx_autotune": (st, [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "pz_ctx_set_split_threshold": (st, [vp, ctypes.c_int]),
+    "pz_key_export": (st, [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "pz_key_import": (st, [vp, vp, ctypes.c_size_t, ctypes.POINTER(vp)]),
+    "pz_circuit_serialize": (st, [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "pz_circuit_deserialize": (st, [vp, ctypes.c_size_t, ctypes.POINTER(vp)]),
     "pz_server_create": (st, [ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(vp)]),
     "pz_server_destroy": (None, [vp]),
     "pz_server_last_error": (ctypes.c_char_p, [vp]),

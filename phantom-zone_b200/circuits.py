@@ -114,6 +114,25 @@ class Circuit:
     def u8_min(self, a, b):  # shortint/mod.rs:288-291
         return self.u8_mux(a, b, self.u8_cmp("lt", a, b))
 
+    # -- wire format -----------------------------------------------------------------
+    def serialize(self):
+        size = ctypes.c_size_t()
+        check(lib().pz_circuit_serialize(self.h, None, 0, ctypes.byref(size)), None, "pz_circuit_serialize")
+        buf = ctypes.create_string_buffer(max(size.value, 1))
+        check(lib().pz_circuit_serialize(self.h, buf, size.value, ctypes.byref(size)), None, "pz_circuit_serialize")
+        return buf.raw[:size.value]
+
+    @classmethod
+    def deserialize(cls, blob):
+        blob = bytes(blob)
+        c = cls.__new__(cls)
+        h = vp()
+        check(lib().pz_circuit_deserialize(blob, len(blob), ctypes.byref(h)), None, "pz_circuit_deserialize")
+        c.h = h
+        info = c.info()
+        c.n_inputs, c.n_outputs = info["inputs"], info["outputs"]
+        return c
+
     # -- structure -----------------------------------------------------------------
     def info(self):
         v = [ctypes.c_size_t() for _ in range(5)]

@@ -13,6 +13,7 @@
 // not() is free: it flips a bit of the wire reference, applied (q - x) when
 // the wire is read (evaluator.rs:2247-2250).
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "pz_internal.h"
@@ -483,6 +484,92 @@ pz_status pz_u8_mux(pz_circuit *c, const uint32_t *a, const uint32_t *b, uint32_
   B e{c};
   arbitrary_bit_mux(e, selector, a, b, 8, out);
   return e.ok ? PZ_OK : circ_fail(c, "pz_u8_mux failed");
+}
+
+// ---- wire format: header, wire table, gates, outputs (little-endian u32/u64)
+namespace {
+constexpr uint64_t CIRCUIT_MAGIC = 0x3130434952435a50ull;  // "PZCIRC01"
+struct CircuitHeader {
+  uint64_t magic;
+  uint32_t version, reserved;
+  uint64_t n_inputs, n_wires, n_gates, n_outputs;
+};
+}  // namespace
+
+pz_status pz_circuit_serialize(const pz_circuit *c, void *buf, size_t capacity, size_t *size) {
+  if (!c || !size) return PZ_ERR_INVALID_ARGUMENT;
+  const size_t W = c->wire_gate.size(), G = c->gates.size(), O = c->outputs.size();
+  const size_t total = sizeof(CircuitHeader) + W * 8 + G * 12 + O * 4;
+  *size = total;
+  if (!buf) return PZ_OK;
+  if (capacity < total) return PZ_ERR_INVALID_ARGUMENT;
+  CircuitHeader h{CIRCUIT_MAGIC, 1, 0, c->n_inputs, W, G, O};
+  unsigned char *p = (unsigned char *)buf;
+  memcpy(p, &h, sizeof h);
+  p += sizeof h;
+  memcpy(p, c->wire_gate.data(), W * 4);
+  memcpy(p + W * 4, c->wire_input.data(), W * 4);
+  p += W * 8;
+  for (size_t g = 0; g < G; g++) {
+    const u32 rec[3] = {c->gates[g].type, c->gates[g].a, c->gates[g].b};
+    memcpy(p + g * 12, rec, 12);
+  }
+  p += G * 12;
+  memcpy(p, c->outputs.data(), O * 4);
+  return PZ_OK;
+}
+
+// Rebuilds a circuit from a blob, checking every index (a malformed blob is
+// rejected, never read out of bounds).
+pz_status pz_circuit_deserialize(const void *buf, size_t size, pz_circuit **out) {
+  if (!buf || !out) return PZ_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  CircuitHeader h;
+  if (size < sizeof h) return PZ_ERR_INVALID_ARGUMENT;
+  memcpy(&h, buf, sizeof h);
+  if (h.magic != CIRCUIT_MAGIC || h.version != 1) return PZ_ERR_INVALID_ARGUMENT;
+  const uint64_t W = h.n_wires, G = h.n_gates, O = h.n_outputs;
+  if (W > (1ull << 31) || G > W || O > (1ull << 31) || h.n_inputs > W) return PZ_ERR_INVALID_ARGUMENT;
+  if (size != sizeof h + W * 8 + G * 12 + O * 4) return PZ_ERR_INVALID_ARGUMENT;
+  const unsigned char *p = (const unsigned char *)buf + sizeof h;
+  std::vector<u32> wg(W), wi(W), outs(O);
+  memcpy(wg.data(), p, W * 4);
+  memcpy(wi.data(), p + W * 4, W * 4);
+  p += W * 8;
+  pz_circuit *c = new pz_circuit();
+  // replay the creation order: inputs and gates interleaved as recorded
+  uint64_t next_gate = 0, next_input = 0;
+  bool ok = true;
+  for (uint64_t w = 0; w < W && ok; w++) {
+    if (wg[w] == NONE) {
+      ok = wi[w] == next_input;
+      if (ok) { c->input(); next_input++; }
+    } else {
+      ok = wg[w] == next_gate && next_gate < G;
+      if (ok) {
+        u32 rec[3];
+        memcpy(rec, p + next_gate * 12, 12);
+        // operands must be earlier wires (valid() checks the range)
+        ok = rec[0] <= 5 && (rec[1] & pz::WIRE_MASK) < w && (rec[2] & pz::WIRE_MASK) < w &&
+             c->gate((int)rec[0], rec[1], rec[2]) == (u32)w;
+        next_gate++;
+      }
+    }
+  }
+  ok = ok && next_gate == G && next_input == h.n_inputs;
+  if (ok) {
+    memcpy(outs.data(), p + G * 12, O * 4);
+    for (uint64_t i = 0; i < O && ok; i++) {
+      ok = c->valid(outs[i]);
+      if (ok) c->outputs.push_back(outs[i]);
+    }
+  }
+  if (!ok) {
+    delete c;
+    return PZ_ERR_INVALID_ARGUMENT;
+  }
+  *out = c;
+  return PZ_OK;
 }
 
 pz_status pz_circuit_run_device(pz_ctx *ctx, const pz_key *k, pz_circuit *c, const uint64_t *d_inputs,

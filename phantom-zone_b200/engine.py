@@ -72,6 +72,14 @@ class DeviceKey:
     def device_bytes(self):
         return lib().pz_key_device_bytes(self.h)
 
+    def export(self):
+        """Device-form key as bytes (checkpoint / hand-over between processes)."""
+        size = ctypes.c_size_t()
+        check(lib().pz_key_export(self.h, None, 0, ctypes.byref(size)), self.engine.h, "pz_key_export")
+        buf = ctypes.create_string_buffer(size.value)
+        check(lib().pz_key_export(self.h, buf, size.value, ctypes.byref(size)), self.engine.h, "pz_key_export")
+        return buf.raw
+
     def release(self):
         if self.h:
             lib().pz_key_release(self.h)
@@ -177,6 +185,13 @@ class Engine:
                                lwe_ksk.ctypes.data_as(u64p))
         h = vp()
         check(lib().pz_key_upload(self.h, ctypes.byref(view), ctypes.byref(h)), self.h, "pz_key_upload")
+        return DeviceKey(self, h)
+
+    def import_key(self, blob):
+        """A key exported by DeviceKey.export() under the same parameter set and NTT root."""
+        blob = bytes(blob)
+        h = vp()
+        check(lib().pz_key_import(self.h, blob, len(blob), ctypes.byref(h)), self.h, "pz_key_import")
         return DeviceKey(self, h)
 
     def upload_key_seeded(self, rgsw, auto_b, auto_seed, lwe_ksk_b, lwe_ksk_seed):
