@@ -272,7 +272,8 @@ pz_status pz_circuit_deserialize(const void *buf, size_t size, pz_circuit **out)
  *   auto_b     [w + 1][d_auto][N]     B rows, slots in auto_element_dlogs order
  *                                     (parameters.rs:364-370: 0 = -g, k = g^k)
  *   lwe_ksk_b  [d_ks N]               column 0 of the LWE KSK rows
- *   auto_seed, lwe_ksk_seed           cr_seed.auto_keys_cts_seed(), cr_seed.lwe_ksk_cts_seed() */
+ *   auto_seed, lwe_ksk_seed           cr_seed.auto_keys_cts_seed(), cr_seed.lwe_ksk_cts_seed()
+ * The arrays may be in host or device memory. */
 typedef struct pz_seeded_server_key_view {
   const uint64_t *rgsw;
   const uint64_t *auto_b;
@@ -295,7 +296,7 @@ typedef struct pz_ni_ksk pz_ni_ksk;
 pz_status pz_ni_ksk_upload(pz_ctx *ctx, const uint64_t *ksk, pz_ni_ksk **out);
 /* the same key from its B rows [ni_ks_d][N] and its seed
  * (cr_seed.ui_to_s_ks_seed_for_user_i(user), keys.rs:965-1000): A rows regenerated
- * on the device */
+ * on the device; ksk_b in host or device memory */
 pz_status pz_ni_ksk_upload_seeded(pz_ctx *ctx, const uint64_t *ksk_b, const uint8_t seed[32], pz_ni_ksk **out);
 void pz_ni_ksk_release(pz_ni_ksk *ksk);
 /* NonInteractiveBatchedFheBools::from (ni_mp_api.rs:248-280): d_b [count][N] (the
@@ -328,6 +329,54 @@ pz_status pz_rgsw_by_rgsw_device(pz_ctx *ctx, uint64_t *d_rgsw0, const uint64_t 
  * d_others[steps - 1][c], the other users in order; d_others [steps][count][rows][N]. */
 pz_status pz_aggregate_rgsw_device(pz_ctx *ctx, uint64_t *d_rgsw0, const uint64_t *d_others, size_t steps,
                                    size_t count, void *stream);
+
+/* ---- server-key aggregation (non-interactive protocol) ------------------------------
+ * aggregate_non_interactive_multi_party_server_key_shares (bool/evaluator.rs:1222-1622).
+ * One user's share (CommonReferenceSeededNonInteractiveMultiPartyServerKeyShare,
+ * bool/keys.rs:1240-1290), every array u64, coefficient domain, DEVICE memory:
+ *   ui_to_s_ksk        [ni_ks_d][N]       (a_k s_j + e + beta u_j), a_k from the user's seed
+ *   ksk_zero_encs      [users - 1][ni_ks_d][N]  zero encryptions for user l at l (l < own id)
+ *                                         or l - 1 (ui_to_s_ksk_zero_encs_for_user_i)
+ *   self_leader_cts    [segment][max(rlrg_d_a, rlrg_d_b)][N]  NI RGSW rows of the indices
+ *                                         the user leads (multi_party_user_id_lwe_segment)
+ *   not_leader_cts     [lwe_n - segment][max(rgrg_d_a, rgrg_d_b)][N]  the other indices,
+ *                                         in index order
+ *   rgsw_zero_encs     [lwe_n][rgrg_d_a][N]
+ *   auto_keys          [w + 1][d_auto][N] B rows, auto_element_dlogs order
+ *   lwe_ksk            [d_ks N]           (mod lwe q)
+ * Entries are canonical (< the modulus), as the reference's additions assume. */
+typedef struct pz_ni_server_key_share_view {
+  const uint64_t *ui_to_s_ksk;
+  const uint64_t *ksk_zero_encs;
+  const uint64_t *self_leader_cts;
+  const uint64_t *not_leader_cts;
+  const uint64_t *rgsw_zero_encs;
+  const uint64_t *auto_keys;
+  const uint64_t *lwe_ksk;
+} pz_ni_server_key_share_view;
+/* NonInteractiveMultiPartyCrs (bool/evaluator.rs:115-172) seeds from the common
+ * reference seed: what = 0 auto keys, 1 LWE KSK, 2 ui_to_s KSK of user `index`,
+ * 3 NI RGSW of LWE index `index`.  Host only. */
+#define PZ_CRS_AUTO_KEYS 0
+#define PZ_CRS_LWE_KSK 1
+#define PZ_CRS_UI_TO_S_KSK 2
+#define PZ_CRS_NI_RGSW 3
+pz_status pz_ni_crs_seed(const uint8_t crs_seed[32], int what, size_t index, uint8_t out[32]);
+/* The aggregation, outputs in DEVICE memory in the form the reference returns
+ * (SeededNonInteractiveMultiPartyServerKey, coefficient domain):
+ *   d_ksk_b   [users][ni_ks_d][N]  per-user Ksk(u_j -> s) B rows
+ *   d_rgsw    [lwe_n][4][N]        RGSW(X^{z[l]}) in the rlwe x rgsw shape
+ *   d_auto_b  [w + 1][d_auto][N]   summed auto key B rows
+ *   d_lwe_b   [d_ks N]             summed LWE KSK column 0
+ * shares[j] is user j's.  Returns when done. */
+pz_status pz_ni_aggregate_device(pz_ctx *ctx, const uint8_t crs_seed[32], const pz_ni_server_key_share_view *shares,
+                                 size_t users, uint64_t *d_ksk_b, uint64_t *d_rgsw, uint64_t *d_auto_b,
+                                 uint64_t *d_lwe_b, void *stream);
+/* Aggregation followed by the expansion to the evaluation form (keys.rs:869-1004):
+ * the server key and every user's ui_to_s key (ksks_out[users]). */
+pz_status pz_ni_aggregate_server_key(pz_ctx *ctx, const uint8_t crs_seed[32],
+                                     const pz_ni_server_key_share_view *shares, size_t users, pz_key **key_out,
+                                     pz_ni_ksk **ksks_out);
 
 /* ---- multi-session executor (serving) ---------------------------------------------
  * No reference counterpart: the reference evaluates one gate at a time, in

@@ -86,6 +86,12 @@ def lib():
             "orc_expand_ni_ksk": (None, [vp, u64p, u8p, u64p]),
             "orc_rgsw_by_rgsw": (None, [vp, u64p, u64p]),
             "orc_rgsw_encrypt": (None, [vp, i32p, u64p, ctypes.c_int, u8p, u64p]),
+            "orc_ni_crs_seed": (None, [u8p, ctypes.c_int, ctypes.c_size_t, u8p]),
+            "orc_ni_aggregate": (None, [vp, u8p, ctypes.c_int] + [ctypes.POINTER(u64p)] * 7 +
+                                 [ctypes.c_size_t, ctypes.c_size_t, u64p, u64p, u64p, u64p]),
+            "orc_gen_seeded_auto_lwe": (None, [vp, i32p, i32p, u8p, u8p, u8p, u64p, u64p]),
+            "orc_ni_gen_share": (None, [vp, u8p, ctypes.c_int, ctypes.c_int, i32p, i32p, i32p, u8p, u64p, u64p,
+                                        u64p, u64p, u64p]),
             "orc_u8_op": (ctypes.c_int, [vp, vp, ctypes.c_int, u64p, u64p, u64p, u64p, u64p, u64p, ctypes.POINTER(ctypes.c_int)]),
             "orc_generate_prime": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
             "orc_ntt_custom_new": (vp, [ctypes.c_uint64, ctypes.c_size_t]),
@@ -117,6 +123,14 @@ def lib():
 
 def _p(a, t=u64p):
     return a.ctypes.data_as(t)
+
+
+def ni_crs_seed(crs, what, index=0):
+    """NonInteractiveMultiPartyCrs seed (evaluator.rs:115-172): what 0 auto keys, 1 LWE KSK,
+    2 ui_to_s KSK of user `index`, 3 NI RGSW of LWE index `index`."""
+    out = (ctypes.c_uint8 * 32)()
+    lib().orc_ni_crs_seed((ctypes.c_uint8 * 32)(*bytes(crs)), int(what), int(index), out)
+    return bytes(out)
 
 
 def param_info(name_or_id):
@@ -345,6 +359,90 @@ class Evaluator:
                                _p(np.ascontiguousarray(m, np.uint64)), int(which),
                                (ctypes.c_uint8 * 32)(*bytes(seed)), _p(out))
         return out
+
+    def lwe_segment(self, user, users):
+        """multi_party_user_id_lwe_segment (evaluator.rs:613-626)."""
+        per = -(-self.n // users)
+        b, e = per * user, min(per * (user + 1), self.n)
+        return b, max(b, e)
+
+    def ni_gen_share(self, crs, user, users, s, u, z, err_seed):
+        """RGSW / KSK parts of one user's NI server key share (evaluator.rs:1624-1975)
+        -> dict of arrays (coefficient domain)."""
+        N, n, d = self.N, self.n, self.NI_KS_D
+        info = param_info(self.pid)
+        ra, rb = info.rgrg_d_a, info.rgrg_d_b
+        mx, ml = max(ra, rb), max(info.rlrg_d_a, info.rlrg_d_b)
+        b, e = self.lwe_segment(user, users)
+        out = dict(ui_to_s_ksk=np.empty((d, N), np.uint64),
+                   ksk_zero_encs=np.empty((max(users - 1, 1), d, N), np.uint64),
+                   self_leader=np.empty((max(e - b, 1), ml, N), np.uint64),
+                   not_leader=np.empty((max(n - (e - b), 1), mx, N), np.uint64),
+                   zero_encs=np.empty((n, ra, N), np.uint64))
+        lib().orc_ni_gen_share(self.h, (ctypes.c_uint8 * 32)(*bytes(crs)), int(user), int(users),
+                               _p(np.ascontiguousarray(s, np.int32), i32p), _p(np.ascontiguousarray(u, np.int32), i32p),
+                               _p(np.ascontiguousarray(z, np.int32), i32p), (ctypes.c_uint8 * 32)(*bytes(err_seed)),
+                               *[_p(out[k]) for k in ("ui_to_s_ksk", "ksk_zero_encs", "self_leader", "not_leader",
+                                                      "zero_encs")])
+        out["self_leader"] = out["self_leader"][:e - b]
+        out["not_leader"] = out["not_leader"][:n - (e - b)]
+        out["ksk_zero_encs"] = out["ksk_zero_encs"][:users - 1]
+        return out
+
+    def gen_seeded_auto_lwe(self, s, z, auto_seed, lwe_seed, err_seed=b"\x44" * 32):
+        """Auto-key B rows [w+1][d_auto][N] and LWE-KSK column 0 [d_ks N] under (s, z), A parts
+        from the two seeds' streams (the seeded server key's form)."""
+        info = self.info
+        auto_b = np.empty((info.w + 1, info.auto_d, self.N), np.uint64)
+        lwe_b = np.empty(info.lwe_d * self.N, np.uint64)
+        lib().orc_gen_seeded_auto_lwe(self.h, _p(np.ascontiguousarray(s, np.int32), i32p),
+                                      _p(np.ascontiguousarray(z, np.int32), i32p),
+                                      (ctypes.c_uint8 * 32)(*bytes(auto_seed)), (ctypes.c_uint8 * 32)(*bytes(lwe_seed)),
+                                      (ctypes.c_uint8 * 32)(*bytes(err_seed)), _p(auto_b), _p(lwe_b))
+        return auto_b, lwe_b
+
+    def ni_aggregate(self, crs, shares, i0=0, i1=None, threads=1):
+        """aggregate_non_interactive_multi_party_server_key_shares (evaluator.rs:1222-1622).
+        shares: list (user id order) of dicts with ui_to_s_ksk, ksk_zero_encs, self_leader,
+        not_leader, zero_encs, auto_keys [w+1][d_auto][N], lwe_ksk [lwe_d N].
+        -> (ksk_b [users][50][N], rgsw [i1-i0][rows][N], auto [w+1][d_auto][N], lwe [lwe_d N])."""
+        info = param_info(self.pid)
+        i1 = self.n if i1 is None else i1
+        users, N = len(shares), self.N
+        keep = []
+
+        def ptrs(key):
+            arrs = [np.ascontiguousarray(sh[key], np.uint64) for sh in shares]
+            keep.extend(arrs)
+            return (u64p * users)(*[_p(a) for a in arrs])
+
+        fields = [ptrs(k) for k in ("ui_to_s_ksk", "ksk_zero_encs", "self_leader", "not_leader", "zero_encs",
+                                    "auto_keys", "lwe_ksk")]
+        rows = 2 * info.rlrg_d_a + 2 * info.rlrg_d_b
+        ksk = np.empty((users, self.NI_KS_D, N), np.uint64)
+        rgsw = np.empty((max(i1 - i0, 1), rows, N), np.uint64)
+        auto = np.empty((info.w + 1, info.auto_d, N), np.uint64)
+        lwe = np.empty(info.lwe_d * N, np.uint64)
+        cs = (ctypes.c_uint8 * 32)(*bytes(crs))
+        if threads <= 1 or i1 - i0 < 2:
+            lib().orc_ni_aggregate(self.h, cs, users, *fields, i0, i1, _p(ksk), _p(rgsw), _p(auto), _p(lwe))
+            return ksk, rgsw[:i1 - i0], auto, lwe
+        from concurrent.futures import ThreadPoolExecutor  # ctypes calls run without the GIL
+
+        step = -(-(i1 - i0) // threads)
+        parts = [(a, min(a + step, i1)) for a in range(i0, i1, step)]
+
+        def run(ab):
+            a, b = ab
+            k2, a2, l2 = np.empty_like(ksk), np.empty_like(auto), np.empty_like(lwe)
+            view = rgsw[a - i0:b - i0]
+            lib().orc_ni_aggregate(self.h, cs, users, *fields, a, b, _p(k2), _p(view), _p(a2), _p(l2))
+            return k2, a2, l2
+
+        with ThreadPoolExecutor(len(parts)) as ex:
+            res = list(ex.map(run, parts))
+        ksk[:], auto[:], lwe[:] = res[0]
+        return ksk, rgsw[:i1 - i0], auto, lwe
 
     def ni_ingest(self, ksk, seed, b, nbits):
         """unseed -> key switch -> extract every bool (the server's NI input path)."""

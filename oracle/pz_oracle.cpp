@@ -1474,6 +1474,334 @@ void orc_rgsw_by_rgsw(void *ev, uint64_t *rgsw0, const uint64_t *rgsw1) {
   memcpy(rgsw0, out.data(), rows0 * N * 8);
 }
 
+// puncture_p_rng (utils.rs:219-228) with RandomFill<[u8; 32]> (random.rs:
+// 162-175): `times` successive 32-byte fills of ChaCha8(seed), the last one
+// kept; a byte is Uniform::new_inclusive(0, 255), i.e. the low byte of one
+// u32 word of the stream.
+void crs_puncture(const uint8_t seed[32], size_t times, uint8_t out[32]) {
+  ChaCha8 r(seed);
+  for (size_t t = 0; t < times; t++)
+    for (int i = 0; i < 32; i++) out[i] = (uint8_t)r.next_u32();
+}
+
+// NonInteractiveMultiPartyCrs (evaluator.rs:115-172): what = 0 auto keys,
+// 1 LWE KSK, 2 ui_to_s KSK of user `index`, 3 NI RGSW of LWE index `index`.
+void orc_ni_crs_seed(const uint8_t crs[32], int what, size_t index, uint8_t out[32]) {
+  uint8_t key[32], t[32];
+  crs_puncture(crs, 1, key);  // key_seed
+  switch (what) {
+    case 0: crs_puncture(key, 2, out); break;
+    case 1: crs_puncture(key, 3, out); break;
+    case 2: crs_puncture(crs, 2, t); crs_puncture(t, index + 1, out); break;  // ui_to_s_ks_seed
+    default: crs_puncture(key, 1, t); crs_puncture(t, index + 1, out); break;  // ni_rgsw_cts_main_seed
+  }
+}
+
+// multi_party_user_id_lwe_segment (evaluator.rs:613-626); an empty segment
+// when the start passes lwe_n.
+void lwe_segment(size_t user, size_t users, size_t n, size_t *b, size_t *e) {
+  const size_t per = (n + users - 1) / users;
+  *b = per * user;
+  *e = std::min(per * (user + 1), n);
+  if (*e < *b) *e = *b;
+}
+
+struct NiDigits {  // one value to key-switch: its 50 one-bit digits, forward NTT
+  std::vector<u64> d;
+};
+
+// The key switch of produce_rgsw_ciphertext_from_ni_rgsw (evaluator.rs:
+// 542-553 / 581-591) given the value's transformed digits: a = sum_j A_j c_j,
+// b = sum_j B_j c_j (elwise_fma_mut), back to the coefficient domain.
+void ni_ks_rows(const Eval &e, const u64 *ksk_eval, const u64 *dig, u64 *oa, u64 *ob) {
+  const size_t N = e.N, d = e.dec_ni.d;
+  std::fill(oa, oa + N, 0);
+  std::fill(ob, ob + N, 0);
+  for (size_t j = 0; j < d; j++) {
+    const u64 *c = dig + j * N, *pa = ksk_eval + j * N, *pb = ksk_eval + (d + j) * N;
+    for (size_t i = 0; i < N; i++) {
+      ob[i] = e.rmod.add(ob[i], e.rmod.mul(pb[i], c[i]));
+      oa[i] = e.rmod.add(oa[i], e.rmod.mul(pa[i], c[i]));
+    }
+  }
+  e.ntt.backward(oa, false);
+  e.ntt.backward(ob, false);
+}
+
+// The RGSW step of aggregate_non_interactive_multi_party_server_key_shares
+// (evaluator.rs:1310-1560) for LWE indices [i0, i1): a_l rows from the
+// index's stream (d_max - d_b punctured rows, then d_b rows, negated), zero
+// encryptions summed over the users, every value decomposed (50 one-bit
+// digits) and transformed once; the leader's RGSW in the rlwe x rgsw shape
+// from the last rlrg rows (produce_rgsw_ciphertext_from_ni_rgsw,
+// :480-608), then times every other user's RGSW in the rgsw x rgsw shape in
+// increasing user id.  ksk_eval [users][2 50][N]: Ksk(u_j -> s) in the
+// evaluation domain, A rows (from the user's stream) then aggregated B rows.
+// out [i1 - i0][2 d_a + 2 d_b][N], coefficient domain.
+void ni_aggregate_rgsw(Eval &e, const uint8_t crs[32], size_t users, const u64 *ksk_eval,
+                       const uint64_t *const *self_leader, const uint64_t *const *not_leader,
+                       const uint64_t *const *zero_encs, size_t i0, size_t i1, u64 *out) {
+  const size_t N = e.N, n = e.n, d = e.dec_ni.d;
+  const size_t ra = e.p.rgrg_d_a, rb = e.p.rgrg_d_b, max_d = std::max(ra, rb);
+  const size_t la = e.p.d_a, lb = e.p.d_b, max_l = std::max(la, lb), rows0 = 2 * la + 2 * lb;
+  const size_t rows1 = 2 * ra + 2 * rb, R = ra + rb;
+  std::vector<u64> dig(R * d * N), val(N), other(rows1 * N);
+  for (size_t li = i0; li < i1; li++) {
+    uint8_t seed[32];
+    orc_ni_crs_seed(crs, 3, li, seed);
+    ChaCha8 a_prng(seed);
+    for (size_t r = 0; r < max_d - rb; r++)  // puncture
+      for (size_t i = 0; i < N; i++) a_prng.uniform_mod(e.Q);
+    for (size_t v = 0; v < R; v++) {
+      if (v < ra) {  // sum_k zero_enc_k row v
+        std::fill(val.begin(), val.end(), 0);
+        for (size_t k = 0; k < users; k++) {
+          const u64 *z = zero_encs[k] + (li * ra + v) * N;
+          for (size_t i = 0; i < N; i++) val[i] = e.rmod.add(val[i], z[i]);
+        }
+      } else {  // -a row (elwise_neg_mut: q - x)
+        for (size_t i = 0; i < N; i++) val[i] = e.Q - a_prng.uniform_mod(e.Q);
+      }
+      u64 *dv = &dig[v * d * N];
+      decompose_r(e.dec_ni, val.data(), dv, N);
+      for (size_t j = 0; j < d; j++) e.ntt.forward(dv + j * N, false);
+    }
+    size_t leader = 0;
+    for (size_t k = 0; k < users; k++) {
+      size_t b, en;
+      lwe_segment(k, users, n, &b, &en);
+      if (li >= b && li < en) leader = k;
+    }
+    // leader: values ra - la .. ra (zero encs) and R - lb .. R (-a), its ct rows
+    u64 *o = out + (li - i0) * rows0 * N;
+    {
+      size_t b, en;
+      lwe_segment(leader, users, n, &b, &en);
+      const u64 *ct = self_leader[leader] + (li - b) * max_l * N;
+      const u64 *ke = ksk_eval + leader * 2 * d * N;
+      for (size_t r = 0; r < la; r++) {
+        u64 *oa = o + r * N, *ob = o + (la + r) * N;
+        ni_ks_rows(e, ke, &dig[(ra - la + r) * d * N], oa, ob);
+        const u64 *c = ct + (max_l - la + r) * N;
+        for (size_t i = 0; i < N; i++) oa[i] = e.rmod.add(oa[i], c[i]);
+      }
+      for (size_t r = 0; r < lb; r++) {
+        u64 *oa = o + (2 * la + r) * N, *ob = o + (2 * la + lb + r) * N;
+        ni_ks_rows(e, ke, &dig[(R - lb + r) * d * N], oa, ob);
+        const u64 *c = ct + (max_l - lb + r) * N;
+        for (size_t i = 0; i < N; i++) ob[i] = e.rmod.add(ob[i], c[i]);
+      }
+    }
+    for (size_t k = 0; k < users; k++) {
+      if (k == leader) continue;
+      size_t b, en;
+      lwe_segment(k, users, n, &b, &en);
+      const size_t pos = li < b ? li : li - (en - b);
+      const u64 *ct = not_leader[k] + pos * max_d * N;
+      const u64 *ke = ksk_eval + k * 2 * d * N;
+      for (size_t r = 0; r < ra; r++) {
+        u64 *oa = &other[r * N], *ob = &other[(ra + r) * N];
+        ni_ks_rows(e, ke, &dig[r * d * N], oa, ob);
+        const u64 *c = ct + (max_d - ra + r) * N;
+        for (size_t i = 0; i < N; i++) oa[i] = e.rmod.add(oa[i], c[i]);
+      }
+      for (size_t r = 0; r < rb; r++) {
+        u64 *oa = &other[(2 * ra + r) * N], *ob = &other[(2 * ra + rb + r) * N];
+        ni_ks_rows(e, ke, &dig[(ra + r) * d * N], oa, ob);
+        const u64 *c = ct + (max_d - rb + r) * N;
+        for (size_t i = 0; i < N; i++) ob[i] = e.rmod.add(ob[i], c[i]);
+      }
+      orc_rgsw_by_rgsw(&e, o, other.data());
+    }
+  }
+}
+
+// aggregate_non_interactive_multi_party_server_key_shares (evaluator.rs:
+// 1222-1622) on shares given field by field (arrays of per-user pointers,
+// user id order): Ksk(u_j -> s) B rows = own ui_to_s_ksk + the other users'
+// zero encryptions for j (evaluator.rs:1269-1294), coefficient domain; auto
+// keys and LWE KSK summed (:1563-1605); RGSWs of LWE indices [i0, i1).
+// ksk_out [users][50][N], rgsw_out [i1 - i0][rows][N], auto_out
+// [w + 1][d_auto][N], lwe_out [lwe_d N].
+void orc_ni_aggregate(void *ev, const uint8_t crs[32], int users_, const uint64_t *const *ui_to_s_ksk,
+                      const uint64_t *const *ksk_zero_encs, const uint64_t *const *self_leader,
+                      const uint64_t *const *not_leader, const uint64_t *const *zero_encs,
+                      const uint64_t *const *auto_keys, const uint64_t *const *lwe_ksk, size_t i0, size_t i1,
+                      uint64_t *ksk_out, uint64_t *rgsw_out, uint64_t *auto_out, uint64_t *lwe_out) {
+  Eval &e = *(Eval *)ev;
+  if (e.p.variant != 2 || !e.p.rgrg_logb) throw std::runtime_error("not a non-interactive parameter set");
+  const size_t users = (size_t)users_, N = e.N, d = e.dec_ni.d;
+  for (size_t j = 0; j < users; j++) {
+    u64 *o = ksk_out + j * d * N;
+    memcpy(o, ui_to_s_ksk[j], d * N * 8);
+    for (size_t k = 0; k < users; k++) {
+      if (k == j) continue;
+      const u64 *z = ksk_zero_encs[k] + (j < k ? j : j - 1) * d * N;
+      for (size_t i = 0; i < d * N; i++) o[i] = e.rmod.add(o[i], z[i]);
+    }
+  }
+  const size_t na = (e.p.w + 1) * e.p.auto_d * N;
+  std::fill(auto_out, auto_out + na, 0);
+  for (size_t k = 0; k < users; k++)
+    for (size_t i = 0; i < na; i++) auto_out[i] = e.rmod.add(auto_out[i], auto_keys[k][i]);
+  const size_t nl = (size_t)e.p.lwe_d * N;
+  const u64 ql = e.p.lwe_q;
+  std::fill(lwe_out, lwe_out + nl, 0);
+  for (size_t k = 0; k < users; k++)
+    for (size_t i = 0; i < nl; i++) {
+      const u64 v = lwe_out[i] + lwe_ksk[k][i];
+      lwe_out[i] = v >= ql ? v - ql : v;
+    }
+  if (i1 <= i0) return;
+  std::vector<u64> keval(users * 2 * d * N);
+  for (size_t j = 0; j < users; j++) {
+    uint8_t seed[32];
+    orc_ni_crs_seed(crs, 2, j, seed);
+    ChaCha8 prng(seed);
+    u64 *k = &keval[j * 2 * d * N];
+    for (size_t i = 0; i < d * N; i++) k[i] = prng.uniform_mod(e.Q);
+    memcpy(k + d * N, ksk_out + j * d * N, d * N * 8);
+    for (size_t r = 0; r < 2 * d; r++) e.ntt.forward(k + r * N, false);
+  }
+  ni_aggregate_rgsw(e, crs, users, keval.data(), self_leader, not_leader, zero_encs, i0, i1, rgsw_out);
+}
+
+// Client side (harness): the auto-key and LWE-KSK B parts under (s, z) with
+// their A parts from the CRS streams, as the multi-party share routines
+// build them (evaluator.rs:1981-2043 -> seeded_auto_key_gen, rgsw/keygen.rs:
+// 306-363; seeded_lwe_ksk_keygen, lwe.rs:46-101): the same encryptions as
+// orc_gen_server_key, A rows drawn in the order orc_expand_seeded_key
+// regenerates them.  auto_b [w + 1][d_auto][N]; lwe_b [d_ks N].
+void orc_gen_seeded_auto_lwe(void *ev, const int32_t *s, const int32_t *z, const uint8_t auto_seed[32],
+                             const uint8_t lwe_seed[32], const uint8_t err_seed[32], uint64_t *auto_b,
+                             uint64_t *lwe_b) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N, n = e.n, dauto = e.p.auto_d;
+  const u64 Q = e.Q;
+  ChaCha8 rng(err_seed), ap(auto_seed), lp(lwe_seed);
+  std::vector<u64> s_eval(N), tmp(N), a(N), neg_s_auto(N), sm(N);
+  for (size_t i = 0; i < N; i++) s_eval[i] = map_from_i64(Q, s[i]);
+  e.ntt.forward(s_eval.data(), false);
+  for (size_t i = 0; i < N; i++) sm[i] = map_from_i64(Q, s[i]);
+  for (size_t kk = 0; kk <= e.p.w; kk++) {
+    const auto &idx = e.auto_idx[kk];
+    const auto &sg = e.auto_sign[kk];
+    for (size_t i = 0; i < N; i++) neg_s_auto[idx[i]] = sg[i] ? e.rmod.neg(sm[i]) : sm[i];
+    for (size_t j = 0; j < dauto; j++) {
+      for (size_t i = 0; i < N; i++) a[i] = ap.uniform_mod(Q);
+      memcpy(tmp.data(), a.data(), N * 8);
+      e.ntt.forward(tmp.data(), false);
+      for (size_t i = 0; i < N; i++) tmp[i] = e.rmod.mul(tmp[i], s_eval[i]);
+      e.ntt.backward(tmp.data(), false);
+      u64 *b = auto_b + (kk * dauto + j) * N;
+      const u64 beta = e.dec_auto.gadget((u32)j) % Q;
+      for (size_t i = 0; i < N; i++) {
+        b[i] = e.rmod.add(map_from_f64(Q, rng.gaussian()), tmp[i]);
+        b[i] = e.rmod.add(b[i], e.rmod.mul(neg_s_auto[i] % Q, beta));
+      }
+    }
+  }
+  const u64 qk = e.p.lwe_q, mask = qk - 1;
+  const size_t d = e.p.lwe_d;
+  std::vector<u64> zm(n);
+  for (size_t i = 0; i < n; i++) zm[i] = map_from_i64(qk, z[i]) & mask;
+  for (size_t i = 0; i < N; i++) {
+    const u64 neg_si = (0 - map_from_i64(qk, s[i])) & mask;
+    for (size_t j = 0; j < d; j++) {
+      u64 az = 0;
+      for (size_t c = 0; c < n; c++) az = (az + lp.uniform_mod(qk) * zm[c]) & mask;
+      const u64 beta = e.dec_lwe.gadget((u32)j) & mask;
+      u64 b = (az + beta * neg_si) & mask;
+      lwe_b[i * d + j] = (b + map_from_f64(qk, rng.gaussian())) & mask;
+    }
+  }
+}
+
+// Client side (harness): the NI server key share of gen_non_interactive_
+// multi_party_key_share (evaluator.rs:1624-1975) for the RGSW and KSK parts,
+// with non_interactive_ksk_gen / _zero_encryptions_for_other_party_i
+// (multi_party.rs:186-286): s, u RLWE secrets, z the LWE secret of the user;
+// errors from ChaCha8(err_seed).  Outputs: ksk [50][N]; ksk_zero [users-1][50][N];
+// self_leader [segment][max(rlrg)][N]; not_leader [n - segment][max(rgrg)][N];
+// zero [n][rgrg_d_a][N].
+void orc_ni_gen_share(void *ev, const uint8_t crs[32], int user, int users, const int32_t *s, const int32_t *u,
+                      const int32_t *z, const uint8_t err_seed[32], uint64_t *ksk, uint64_t *ksk_zero,
+                      uint64_t *self_leader, uint64_t *not_leader, uint64_t *zero) {
+  Eval &e = *(Eval *)ev;
+  const size_t N = e.N, n = e.n, d = e.dec_ni.d, Q = e.Q;
+  const size_t ra = e.p.rgrg_d_a, rb = e.p.rgrg_d_b, max_d = std::max(ra, rb);
+  const size_t max_l = std::max(e.p.d_a, e.p.d_b);
+  const Decomposer &dmax = ra >= rb ? e.dec_rgrg_a : e.dec_rgrg_b;
+  const Decomposer &lmax = e.p.d_a >= e.p.d_b ? e.dec_a : e.dec_b;
+  ChaCha8 rng(err_seed);
+  std::vector<u64> s_eval(N), u_eval(N), tmp(N), m(N);
+  for (size_t i = 0; i < N; i++) s_eval[i] = map_from_i64(Q, s[i]);
+  for (size_t i = 0; i < N; i++) u_eval[i] = map_from_i64(Q, u[i]);
+  e.ntt.forward(s_eval.data(), false);
+  e.ntt.forward(u_eval.data(), false);
+  auto mul_add_err = [&](u64 *row, const std::vector<u64> &sec) {  // row <- row * sec + e
+    e.ntt.forward(row, false);
+    for (size_t i = 0; i < N; i++) row[i] = e.rmod.mul(row[i], sec[i]);
+    e.ntt.backward(row, false);
+    for (size_t i = 0; i < N; i++) row[i] = e.rmod.add(row[i], map_from_f64(Q, rng.gaussian()));
+  };
+  uint8_t seed[32];
+  orc_ni_crs_seed(crs, 2, (size_t)user, seed);
+  {  // ui_to_s ksk: a s + e + beta u
+    ChaCha8 p(seed);
+    for (size_t j = 0; j < d; j++) {
+      u64 *row = ksk + j * N;
+      for (size_t i = 0; i < N; i++) row[i] = p.uniform_mod(Q);
+      mul_add_err(row, s_eval);
+      const u64 beta = e.dec_ni.gadget((u32)j) % Q;
+      for (size_t i = 0; i < N; i++) row[i] = e.rmod.add(row[i], e.rmod.mul(map_from_i64(Q, u[i]), beta));
+    }
+  }
+  size_t t = 0;
+  for (int o = 0; o < users; o++) {  // zero encryptions with the other users' a
+    if (o == user) continue;
+    orc_ni_crs_seed(crs, 2, (size_t)o, seed);
+    ChaCha8 p(seed);
+    for (size_t j = 0; j < d; j++) {
+      u64 *row = ksk_zero + (t * d + j) * N;
+      for (size_t i = 0; i < N; i++) row[i] = p.uniform_mod(Q);
+      mul_add_err(row, s_eval);
+    }
+    t++;
+  }
+  size_t sb, se;
+  lwe_segment((size_t)user, (size_t)users, n, &sb, &se);
+  for (size_t li = 0; li < n; li++) {
+    orc_ni_crs_seed(crs, 3, li, seed);
+    {  // zero encryptions a s + e, after d_max - d_a punctured rows
+      ChaCha8 p(seed);
+      for (size_t r = 0; r < (max_d - ra) * N; r++) p.uniform_mod(Q);
+      for (size_t r = 0; r < ra; r++) {
+        u64 *row = zero + (li * ra + r) * N;
+        for (size_t i = 0; i < N; i++) row[i] = p.uniform_mod(Q);
+        mul_add_err(row, s_eval);
+      }
+    }
+    // X^{emb z_l} (utils.rs:195-217)
+    std::fill(m.begin(), m.end(), 0);
+    const int64_t si = (int64_t)z[li] * (int64_t)e.emb;
+    if (si < 0) m[N - (size_t)(-si)] = Q - 1; else m[(size_t)si] = 1;
+    const bool lead = li >= sb && li < se;
+    const size_t rows = lead ? max_l : max_d;
+    const Decomposer &g = lead ? lmax : dmax;
+    u64 *ct = lead ? self_leader + (li - sb) * max_l * N : not_leader + (li < sb ? li : li - (se - sb)) * max_d * N;
+    ChaCha8 p(seed);
+    for (size_t r = 0; r < (max_d - rows) * N; r++) p.uniform_mod(Q);
+    for (size_t r = 0; r < rows; r++) {  // u a + e + beta m
+      u64 *row = ct + r * N;
+      for (size_t i = 0; i < N; i++) row[i] = p.uniform_mod(Q);
+      mul_add_err(row, u_eval);
+      const u64 beta = g.gadget((u32)r) % Q;
+      for (size_t i = 0; i < N; i++) row[i] = e.rmod.add(row[i], e.rmod.mul(m[i], beta));
+    }
+  }
+}
+
 // Client side (harness): RGSW(m) under s in the rlwe x rgsw shape (which = 0)
 // or the rgsw x rgsw shape (which = 1), as the key generation builds them
 // (rgsw/keygen.rs:68-160): -sm rows a += beta_j m, b = a s + e; m rows

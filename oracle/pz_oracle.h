@@ -191,6 +191,24 @@ void orc_expand_ni_ksk(void *ev, const uint64_t *b, const uint8_t seed[32], uint
 void orc_rgsw_by_rgsw(void *ev, uint64_t *rgsw0, const uint64_t *rgsw1);
 void orc_rgsw_encrypt(void *ev, const int32_t *s, const uint64_t *m, int which, const uint8_t seed[32],
                       uint64_t *out);
+/* NonInteractiveMultiPartyCrs seeds (evaluator.rs:115-172): what 0 auto keys, 1 LWE KSK,
+ * 2 ui_to_s KSK of user `index`, 3 NI RGSW of LWE index `index` */
+void orc_ni_crs_seed(const uint8_t crs[32], int what, size_t index, uint8_t out[32]);
+/* aggregate_non_interactive_multi_party_server_key_shares (evaluator.rs:1222-1622); per-user
+ * pointer arrays in user id order; RGSWs for LWE indices [i0, i1) */
+void orc_ni_aggregate(void *ev, const uint8_t crs[32], int users, const uint64_t *const *ui_to_s_ksk,
+                      const uint64_t *const *ksk_zero_encs, const uint64_t *const *self_leader,
+                      const uint64_t *const *not_leader, const uint64_t *const *zero_encs,
+                      const uint64_t *const *auto_keys, const uint64_t *const *lwe_ksk, size_t i0, size_t i1,
+                      uint64_t *ksk_out, uint64_t *rgsw_out, uint64_t *auto_out, uint64_t *lwe_out);
+/* harness: auto-key / LWE-KSK B parts under (s, z) with CRS-stream A parts */
+void orc_gen_seeded_auto_lwe(void *ev, const int32_t *s, const int32_t *z, const uint8_t auto_seed[32],
+                             const uint8_t lwe_seed[32], const uint8_t err_seed[32], uint64_t *auto_b,
+                             uint64_t *lwe_b);
+/* harness: RGSW / KSK parts of one user's NI server key share (evaluator.rs:1624-1975) */
+void orc_ni_gen_share(void *ev, const uint8_t crs[32], int user, int users, const int32_t *s, const int32_t *u,
+                      const int32_t *z, const uint8_t err_seed[32], uint64_t *ksk, uint64_t *ksk_zero,
+                      uint64_t *self_leader, uint64_t *not_leader, uint64_t *zero);
 /* LWE_Q encryption of bool under s (lwe.rs:104-137, m = +-Q/8) */
 void orc_encrypt_bool(void *ev, void *rng, const int32_t *s, int bit, uint64_t *lwe);
 /* noisy m = b - <a, s> (lwe.rs:139-162) and the bool decode (evaluator.rs:243-256)

@@ -42,6 +42,11 @@ class PzSeededServerKeyView(ctypes.Structure):
                 ("auto_seed", ctypes.c_uint8 * 32), ("lwe_ksk_seed", ctypes.c_uint8 * 32)]
 
 
+class PzNiShareView(ctypes.Structure):
+    _fields_ = [(n, vp) for n in ("ui_to_s_ksk", "ksk_zero_encs", "self_leader_cts", "not_leader_cts",
+                                  "rgsw_zero_encs", "auto_keys", "lwe_ksk")]
+
+
 class PzServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_size_t) for n in ("pending", "active", "done", "failed", "arena_slots",
                                                 "arena_slots_used", "arena_bytes", "sessions", "key_bytes")] + \
@@ -87,6 +92,10 @@ SIGNATURES = {
     "pz_ni_ingest": (st, [vp, vp, u8p, u64p, ctypes.c_size_t, u64p, ctypes.c_size_t]),
     "pz_rgsw_by_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_aggregate_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp]),
+    "pz_ni_crs_seed": (st, [u8p, ctypes.c_int, ctypes.c_size_t, u8p]),
+    "pz_ni_aggregate_device": (st, [vp, u8p, ctypes.POINTER(PzNiShareView), ctypes.c_size_t, vp, vp, vp, vp, vp]),
+    "pz_ni_aggregate_server_key": (st, [vp, u8p, ctypes.POINTER(PzNiShareView), ctypes.c_size_t,
+                                        ctypes.POINTER(vp), ctypes.POINTER(vp)]),
     "pz_ctx_autotune": (st, [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]),
     "pz_ctx_set_split_threshold": (st, [vp, ctypes.c_int]),
     "pz_key_export": (st, [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),

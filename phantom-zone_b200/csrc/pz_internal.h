@@ -42,6 +42,12 @@ struct pz_key {
   size_t bytes = 0;
 };
 
+struct pz_ni_ksk {
+  pz_ctx *ctx = nullptr;
+  pz::u64 *d_ksk = nullptr;  // [2 d][N] evaluation domain, Montgomery form with N^{-1}
+  pz::u32 d = 0;
+  size_t bytes = 0;
+};
 
 namespace pz {
 // Launch sequence of one batch of gate bootstraps (ks kernel -> pbs kernel).
@@ -62,6 +68,10 @@ pz_status seeded_fill_u64(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u
                           u64 row_off, u64 *dst, cudaStream_t st);
 pz_status seeded_fill_u32(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride,
                           u64 row_off, u32 *dst, cudaStream_t st);
+// `streams` streams at once (seeds[i] -> dst + i * stream_stride, `total`
+// samples each, contiguous).  Synchronous.
+pz_status seeded_fill_batch_u64(pz_ctx *c, const uint8_t (*seeds)[32], size_t streams, u64 q, u64 total, u64 *dst,
+                                u64 stream_stride, cudaStream_t st);
 
 // Compiled (levelized) form of a circuit, read by the multi-session executor.
 // Wire slots: inputs first (input order), then gate outputs; bit 31 = not().

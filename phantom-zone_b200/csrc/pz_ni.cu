@@ -26,58 +26,27 @@
 #include <vector>
 
 #include "pz_internal.h"
+#include "pz_ni.cuh"
 
 using pz::u32;
 using pz::u64;
 
-struct pz_ni_ksk {
-  pz_ctx *ctx = nullptr;
-  u64 *d_ksk = nullptr;  // [2 d][N] evaluation domain, Montgomery form with N^{-1}
-  u32 d = 0;
-  size_t bytes = 0;
-};
-
 namespace {
 
-constexpr int NI_T = 256;       // threads per RLWE (8 coefficients each, N = 2048)
-constexpr int NI_LOGN = 11;
+using pz::ni::ChaChaKey;
+using pz::ni::chacha8_block;
+using pz::ni::ni_mac;
+using pz::ni::NI_LOGN;
+using pz::ni::NI_T;
 constexpr u64 UNSEED_MARGIN = 1024;  // keystream words generated beyond the samples needed
 
-struct ChaChaKey {
-  u32 k[8];
-};
-
-__device__ __forceinline__ u32 rotl32(u32 v, int c) { return (v << c) | (v >> (32 - c)); }
-
-// ChaCha8 block `counter` in the rand_chacha 0.3 layout (constants, 8 key
-// words, 64-bit block counter, stream id 0); 16 output words.
-__device__ __forceinline__ void chacha8_block(const ChaChaKey &key, u64 counter, u32 (&out)[16]) {
-  u32 s[16], x[16];
-  s[0] = 0x61707865u; s[1] = 0x3320646eu; s[2] = 0x79622d32u; s[3] = 0x6b206574u;
-#pragma unroll
-  for (int i = 0; i < 8; i++) s[4 + i] = key.k[i];
-  s[12] = (u32)counter; s[13] = (u32)(counter >> 32); s[14] = 0; s[15] = 0;
-#pragma unroll
-  for (int i = 0; i < 16; i++) x[i] = s[i];
-#define PZ_QR(a, b, c, d)                              \
-  x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 16);        \
-  x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 12);        \
-  x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 8);         \
-  x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 7);
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-    PZ_QR(0, 4, 8, 12) PZ_QR(1, 5, 9, 13) PZ_QR(2, 6, 10, 14) PZ_QR(3, 7, 11, 15)
-    PZ_QR(0, 5, 10, 15) PZ_QR(1, 6, 11, 12) PZ_QR(2, 7, 8, 13) PZ_QR(3, 4, 9, 14)
-  }
-#undef PZ_QR
-#pragma unroll
-  for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
-}
-
-// Block b: the 8 u64 words 8b..8b+7 of the stream (two u32 words each, low
-// first), their samples (high half of v * q) and acceptance (low half <= zone).
-__global__ void unseed_candidates_kernel(ChaChaKey key, u64 nblocks, u64 q, u64 zone, u64 *samples,
+// Block b of stream blockIdx.y: the 8 u64 words 8b..8b+7 of the stream (two
+// u32 words each, low first), their samples (high half of v * q) and
+// acceptance (low half <= zone).
+__global__ void unseed_candidates_kernel(const ChaChaKey *keys, u64 nblocks, u64 q, u64 zone, u64 *samples,
                                          unsigned char *accept, u32 *cnt) {
+  const ChaChaKey key = keys[blockIdx.y];
+  const u64 base = blockIdx.y * nblocks;
   for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nblocks; b += (u64)gridDim.x * blockDim.x) {
     u32 w[16];
     chacha8_block(key, b, w);
@@ -86,19 +55,22 @@ __global__ void unseed_candidates_kernel(ChaChaKey key, u64 nblocks, u64 q, u64 
     for (int i = 0; i < 8; i++) {
       const u64 v = (u64)w[2 * i] | ((u64)w[2 * i + 1] << 32);
       const u64 lo = v * q, hi = __umul64hi(v, q);
-      samples[8 * b + i] = hi;
+      samples[8 * (base + b) + i] = hi;
       if (lo <= zone) m |= 1u << i;
     }
-    accept[b] = (unsigned char)m;
-    cnt[b] = __popc(m);
+    accept[base + b] = (unsigned char)m;
+    cnt[base + b] = __popc(m);
   }
 }
 
-// Exclusive scan of cnt[0, n) into off (one CTA); off[n] = total.
+// Exclusive scan of stream blockIdx.x's cnt[0, n) into its off (one CTA per
+// stream); off[n] = the stream's accepted total.
 __global__ void __launch_bounds__(1024) unseed_scan_kernel(const u32 *cnt, u64 n, u64 *off) {
   __shared__ u64 part[1024];
+  cnt += blockIdx.x * n;
+  off += blockIdx.x * (n + 1);
   const u64 per = (n + blockDim.x - 1) / blockDim.x;
-  const u64 b0 = threadIdx.x * per, b1 = min(n, b0 + per);
+  const u64 b0 = min(n, threadIdx.x * per), b1 = min(n, b0 + per);
   u64 local = 0;
   for (u64 b = b0; b < b1; b++) local += cnt[b];
   part[threadIdx.x] = local;
@@ -117,10 +89,16 @@ __global__ void __launch_bounds__(1024) unseed_scan_kernel(const u32 *cnt, u64 n
   if (threadIdx.x == blockDim.x - 1) off[n] = part[threadIdx.x];
 }
 
-// Accepted sample k (k < total) -> dst[(k / row_len) * row_stride + row_off + k % row_len].
+// Accepted sample k (k < total) of stream blockIdx.y ->
+// dst[y * stream_stride + (k / row_len) * row_stride + row_off + k % row_len].
 template <typename T>
 __global__ void seeded_place_kernel(const u64 *samples, const unsigned char *accept, const u64 *off, u64 nblocks,
-                                    u64 total, u64 row_len, u64 row_stride, u64 row_off, T *dst) {
+                                    u64 total, u64 row_len, u64 row_stride, u64 row_off, T *dst, u64 stream_stride) {
+  const u64 y = blockIdx.y;
+  samples += y * 8 * nblocks;
+  accept += y * nblocks;
+  off += y * (nblocks + 1);
+  dst += y * stream_stride;
   for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nblocks; b += (u64)gridDim.x * blockDim.x) {
     const unsigned m = accept[b];
     u64 pos = off[b];
@@ -130,40 +108,6 @@ __global__ void seeded_place_kernel(const u64 *samples, const unsigned char *acc
         if (pos < total) dst[(pos / row_len) * row_stride + row_off + pos % row_len] = (T)samples[8 * b + i];
         pos++;
       }
-    }
-  }
-}
-
-// oa += REDC(x ka + y kc), ob += REDC(x kb + y kd), lazily in [0, 2q); the
-// key rows are in the device layout (register pair -> one 16-byte word).
-__device__ __forceinline__ void ni_mac(u64 (&oa)[8], u64 (&ob)[8], const u64 (&x)[8], const u64 (&y)[8],
-                                       const u64 *ka, const u64 *kb, const u64 *kc, const u64 *kd, bool two,
-                                       const pz::RingConsts &rc) {
-  const int j = threadIdx.x;
-  const u64 q = rc.q, qi = rc.qinv_neg, q2 = rc.q << 1;
-#pragma unroll
-  for (int rr = 0; rr < 4; rr++) {
-    const int di = pz::dev_index<NI_LOGN>(j, 2 * rr);
-    u64 a[2], b[2], c[2] = {0, 0}, d[2] = {0, 0};
-    pz::ld_key2(ka + di, a[0], a[1]);
-    pz::ld_key2(kb + di, b[0], b[1]);
-    if (two) {
-      pz::ld_key2(kc + di, c[0], c[1]);
-      pz::ld_key2(kd + di, d[0], d[1]);
-    }
-#pragma unroll
-    for (int e = 0; e < 2; e++) {
-      const int r = 2 * rr + e;
-      u64 hi, lo, hi2, lo2;
-      pz::mul128(x[r], a[e], hi, lo);
-      pz::mul128(x[r], b[e], hi2, lo2);
-      if (two) {
-        pz::mac128(y[r], c[e], hi, lo);
-        pz::mac128(y[r], d[e], hi2, lo2);
-      }
-      const u64 va = oa[r] + pz::redc(hi, lo, q, qi), vb = ob[r] + pz::redc(hi2, lo2, q, qi);
-      oa[r] = va >= q2 ? va - q2 : va;
-      ob[r] = vb >= q2 ? vb - q2 : vb;
     }
   }
 }
@@ -242,48 +186,57 @@ pz_status ni_check(pz_ctx *c) {
 
 int grid_of(size_t n, int cap) { return (int)std::min<size_t>(std::max<size_t>(n, 1), (size_t)cap); }
 
+// `streams` independent ChaCha8 streams (seeds[i]), `total` samples each,
+// stream i written from dst + i * stream_stride.  Synchronous.
 template <typename T>
-pz_status seeded_fill(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride, u64 row_off,
-                      T *dst, cudaStream_t st) {
-  if (total == 0) return PZ_OK;
+pz_status seeded_fill(pz_ctx *c, const uint8_t (*seeds)[32], size_t streams, u64 q, u64 total, u64 row_len,
+                      u64 row_stride, u64 row_off, T *dst, u64 stream_stride, cudaStream_t st) {
+  if (total == 0 || streams == 0) return PZ_OK;
+  if (streams > 65535) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "seeded fill: more than 65535 streams");
   const u64 nblocks = (total + UNSEED_MARGIN + 7) / 8;
-  ChaChaKey key;
-  for (int i = 0; i < 8; i++)
-    key.k[i] = (u32)seed[4 * i] | ((u32)seed[4 * i + 1] << 8) | ((u32)seed[4 * i + 2] << 16) |
-               ((u32)seed[4 * i + 3] << 24);
+  std::vector<ChaChaKey> keys(streams);
+  for (size_t i = 0; i < streams; i++) keys[i] = pz::ni::chacha_key(seeds[i]);
   // rand 0.8 UniformInt<u64>::new_inclusive(0, q - 1): range q, zone = MAX - (2^64 - q) % q
   const u64 zone = ~0ull - ((0ull - q) % q);
   u64 *samples = nullptr, *off = nullptr;
   unsigned char *acc = nullptr;
   u32 *cnt = nullptr;
-  cudaError_t e = cudaMallocAsync(&samples, nblocks * 8 * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&off, (nblocks + 1) * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&acc, nblocks, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, nblocks * 4, st);
+  ChaChaKey *d_keys = nullptr;
+  std::vector<u64> accepted(streams, 0);
+  cudaError_t e = cudaMallocAsync(&samples, streams * nblocks * 8 * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&off, streams * (nblocks + 1) * 8, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&acc, streams * nblocks, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, streams * nblocks * 4, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_keys, streams * sizeof(ChaChaKey), st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_keys, keys.data(), streams * sizeof(ChaChaKey), cudaMemcpyHostToDevice, st);
+  const dim3 grid((unsigned)grid_of((nblocks + 255) / 256, 65535), (unsigned)streams);
   if (e == cudaSuccess) {
-    unseed_candidates_kernel<<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(key, nblocks, q, zone, samples,
-                                                                                     acc, cnt);
+    unseed_candidates_kernel<<<grid, 256, 0, st>>>(d_keys, nblocks, q, zone, samples, acc, cnt);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
-    unseed_scan_kernel<<<1, 1024, 0, st>>>(cnt, nblocks, off);
+    unseed_scan_kernel<<<(unsigned)streams, 1024, 0, st>>>(cnt, nblocks, off);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
-    seeded_place_kernel<T><<<grid_of((nblocks + 255) / 256, 65535), 256, 0, st>>>(samples, acc, off, nblocks, total,
-                                                                                row_len, row_stride, row_off, dst);
+    seeded_place_kernel<T><<<grid, 256, 0, st>>>(samples, acc, off, nblocks, total, row_len, row_stride, row_off, dst,
+                                                 stream_stride);
     e = cudaGetLastError();
   }
-  u64 accepted = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&accepted, off + nblocks, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)  // off[n] of every stream
+    e = cudaMemcpy2DAsync(accepted.data(), 8, off + nblocks, (nblocks + 1) * 8, 8, streams, cudaMemcpyDeviceToHost,
+                          st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   cudaFreeAsync(samples, st);
   cudaFreeAsync(off, st);
   cudaFreeAsync(acc, st);
   cudaFreeAsync(cnt, st);
+  cudaFreeAsync(d_keys, st);
   if (e != cudaSuccess) return pz::cuda_fail(c, "seeded uniform fill", e);
-  if (accepted < total)  // more rejections than the margin covers (probability ~0)
-    return pz::fail(c, PZ_ERR_NOT_SUPPORTED, "seeded fill: rejection margin exhausted");
+  for (size_t i = 0; i < streams; i++)
+    if (accepted[i] < total)  // more rejections than the margin covers (probability ~0)
+      return pz::fail(c, PZ_ERR_NOT_SUPPORTED, "seeded fill: rejection margin exhausted");
   return PZ_OK;
 }
 
@@ -292,11 +245,15 @@ pz_status seeded_fill(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 r
 namespace pz {
 pz_status seeded_fill_u64(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride,
                           u64 row_off, u64 *dst, cudaStream_t st) {
-  return seeded_fill<u64>(c, seed, q, total, row_len, row_stride, row_off, dst, st);
+  return seeded_fill<u64>(c, (const uint8_t(*)[32])seed, 1, q, total, row_len, row_stride, row_off, dst, 0, st);
 }
 pz_status seeded_fill_u32(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u64 row_len, u64 row_stride,
                           u64 row_off, u32 *dst, cudaStream_t st) {
-  return seeded_fill<u32>(c, seed, q, total, row_len, row_stride, row_off, dst, st);
+  return seeded_fill<u32>(c, (const uint8_t(*)[32])seed, 1, q, total, row_len, row_stride, row_off, dst, 0, st);
+}
+pz_status seeded_fill_batch_u64(pz_ctx *c, const uint8_t (*seeds)[32], size_t streams, u64 q, u64 total, u64 *dst,
+                                u64 stream_stride, cudaStream_t st) {
+  return seeded_fill<u64>(c, seeds, streams, q, total, total, total, 0, dst, stream_stride, st);
 }
 }  // namespace pz
 
@@ -348,7 +305,7 @@ pz_status pz_ni_ksk_upload_seeded(pz_ctx *c, const uint64_t *ksk_b, const uint8_
   // keys.rs:965-1000: d A rows from the user's stream, then the B rows
   if (e == cudaSuccess) s = pz::seeded_fill_u64(c, seed, c->P.rlwe_q, (u64)d * N, d * N, 2 * d * N, 0, stage, c->stream);
   if (e == cudaSuccess && s == PZ_OK)
-    e = cudaMemcpyAsync(stage + d * N, ksk_b, d * N * 8, cudaMemcpyHostToDevice, c->stream);
+    e = cudaMemcpyAsync(stage + d * N, ksk_b, d * N * 8, cudaMemcpyDefault, c->stream);
   if (e == cudaSuccess && s == PZ_OK)
     e = pz::launch_key_convert((int)c->logn, stage, k->d_ksk, polys, c->rc, c->conv_c, c->conv_cs, c->stream);
   if (e == cudaSuccess && s == PZ_OK) e = cudaStreamSynchronize(c->stream);

@@ -482,7 +482,7 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
   // RGSW ciphertexts: as pz_key_upload (keys.rs:738-757)
   for (size_t p0 = 0; p0 < rgsw_polys; p0 += chunk) {
     const size_t m = std::min(chunk, rgsw_polys - p0);
-    if ((e = cudaMemcpyAsync(d_stage, v->rgsw + p0 * N, m * N * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+    if ((e = cudaMemcpyAsync(d_stage, v->rgsw + p0 * N, m * N * 8, cudaMemcpyDefault, c->stream)) != cudaSuccess ||
         (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_rgsw + p0 * N, m, c->rc, c->conv_c, c->conv_cs,
                                     c->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
@@ -493,7 +493,7 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
                                      2 * d_auto * N, 0, d_stage, c->stream);
   if (st != PZ_OK) return cleanup(st, c->err);
   if ((e = cudaMemcpy2DAsync(d_stage + d_auto * N, 2 * d_auto * N * 8, v->auto_b, d_auto * N * 8, d_auto * N * 8,
-                             P.n_auto_keys, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+                             P.n_auto_keys, cudaMemcpyDefault, c->stream)) != cudaSuccess ||
       (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_autos, auto_polys, c->rc, c->conv_c, c->conv_cs,
                                   c->stream)) != cudaSuccess ||
       (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
@@ -504,8 +504,11 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
   st = pz::seeded_fill_u32(c, v->lwe_ksk_seed, P.lwe_q, (u64)ksk_rows * P.lwe_n, P.lwe_n, stride, 1, k->d_ksk,
                            c->stream);
   if (st != PZ_OK) return cleanup(st, c->err);
+  std::vector<u64> b64(ksk_rows);  // host or device source
+  if ((e = cudaMemcpy(b64.data(), v->lwe_ksk_b, ksk_rows * 8, cudaMemcpyDefault)) != cudaSuccess)
+    return cleanup(PZ_ERR_CUDA, std::string("ksk b column: ") + cudaGetErrorString(e));
   std::vector<u32> b32(ksk_rows);
-  for (size_t r = 0; r < ksk_rows; r++) b32[r] = (u32)(v->lwe_ksk_b[r] & (P.lwe_q - 1));
+  for (size_t r = 0; r < ksk_rows; r++) b32[r] = (u32)(b64[r] & (P.lwe_q - 1));
   if ((e = cudaMemcpy2DAsync(k->d_ksk, stride * 4, b32.data(), 4, 4, ksk_rows, cudaMemcpyHostToDevice, c->stream)) !=
           cudaSuccess ||
       (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)

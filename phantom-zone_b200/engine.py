@@ -8,7 +8,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import PzParams, PzSeededServerKeyView, PzServerKeyView, check, lib, u8p, u64p, vp
+from ._lib import PzNiShareView, PzParams, PzSeededServerKeyView, PzServerKeyView, check, lib, u8p, u64p, vp
 
 PARAMETER_SETS = {
     "I_2P_LB_SR": 0, "I_4P": 1, "I_8P": 2, "NI_2P": 3,
@@ -109,6 +109,18 @@ class NiKsk:
             self.release()
         except Exception:
             pass
+
+
+CRS_AUTO_KEYS, CRS_LWE_KSK, CRS_UI_TO_S_KSK, CRS_NI_RGSW = 0, 1, 2, 3
+NI_SHARE_FIELDS = ("ui_to_s_ksk", "ksk_zero_encs", "self_leader_cts", "not_leader_cts", "rgsw_zero_encs",
+                   "auto_keys", "lwe_ksk")
+
+
+def ni_crs_seed(crs, what, index=0):
+    """NonInteractiveMultiPartyCrs seed (bool/evaluator.rs:115-172), host only."""
+    out = (ctypes.c_uint8 * 32)()
+    check(lib().pz_ni_crs_seed(_seed(crs), int(what), int(index), out), None, "pz_ni_crs_seed")
+    return bytes(out)
 
 
 def _seed(seed):
@@ -327,6 +339,32 @@ class Engine:
         steps = others.numel() // (count * 2 * (self.p.rgrg_d_a + self.p.rgrg_d_b) * self.N) if count else 0
         check(lib().pz_aggregate_rgsw_device(self.h, _ptr(rgsw0), _ptr(others), steps, count, _stream(stream)),
               self.h, "pz_aggregate_rgsw_device")
+
+    def _ni_share_views(self, shares):
+        """shares: list (user id order) of dicts NI_SHARE_FIELDS -> device tensors (u64 as int64)."""
+        views = (PzNiShareView * len(shares))()
+        for v, sh in zip(views, shares):
+            for f in NI_SHARE_FIELDS:
+                t = sh.get(f)
+                setattr(v, f, t.data_ptr() if t is not None and t.numel() else None)
+        return views
+
+    def ni_aggregate_device(self, crs, shares, ksk_b, rgsw, auto_b, lwe_b, stream=None):
+        """aggregate_non_interactive_multi_party_server_key_shares (bool/evaluator.rs:1222-1622)
+        on device shares; outputs (device tensors) in the seeded server key's coefficient form."""
+        views = self._ni_share_views(shares)
+        check(lib().pz_ni_aggregate_device(self.h, _seed(crs), views, len(shares), _ptr(ksk_b), _ptr(rgsw),
+                                           _ptr(auto_b), _ptr(lwe_b), _stream(stream)), self.h,
+              "pz_ni_aggregate_device")
+
+    def ni_aggregate_server_key(self, crs, shares):
+        """Aggregation + expansion: -> (DeviceKey, [NiKsk per user]); shares on the device."""
+        views = self._ni_share_views(shares)
+        kh = vp()
+        ks = (vp * len(shares))()
+        check(lib().pz_ni_aggregate_server_key(self.h, _seed(crs), views, len(shares), ctypes.byref(kh), ks),
+              self.h, "pz_ni_aggregate_server_key")
+        return DeviceKey(self, kh), [NiKsk(self, vp(h)) for h in ks]
 
     def lwe_key_switch_device(self, key, lwe_in, out, stream=None):
         count = lwe_in.numel() // self.L

@@ -53,3 +53,14 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.pz_ctx_create(99, 0, ctypes.byref(h)) == 1  # PZ_ERR_INVALID_ARGUMENT
     assert L.pz_param_get(-1, None) == 1
     assert L.pz_status_string(0) == b"ok"
+
+
+def test_ni_crs_seeds_host_matches_oracle():
+    """pz_ni_crs_seed (host code, block-indexed ChaCha8) == the oracle's
+    sequential puncturing (evaluator.rs:115-172), every kind of seed."""
+    from conftest import oracle
+    O = oracle()
+    eng = pz().engine
+    crs = bytes(range(3, 35))
+    for what, idx in [(0, 0), (1, 0), (2, 0), (2, 7), (3, 0), (3, 1), (3, 659)]:
+        assert eng.ni_crs_seed(crs, what, idx) == O.ni_crs_seed(crs, what, idx)

@@ -311,3 +311,137 @@ def test_rgsw_by_rgsw_decrypts_to_product(param):
                  - want.astype(object) * beta) % Q
         centred = np.array([int(v) if v < Q // 2 else int(v) - Q for v in noise])
         assert np.max(np.abs(centred)) < (1 << 34), (row_a, np.max(np.abs(centred)))
+
+
+def test_ni_crs_seeds_are_punctured_streams():
+    """NonInteractiveMultiPartyCrs (evaluator.rs:115-172): every seed is the
+    t-th 32-byte fill of a ChaCha8 stream (puncture_p_rng, utils.rs:219-228),
+    a byte being the low byte of one u32 word (random.rs:162-175)."""
+    O = oracle()
+
+    def puncture(seed, times):
+        r = O.Rng(seed)
+        out = b""
+        for _ in range(times):
+            out = b""
+            for _ in range(16):  # two u32 words per next_u64, low word first
+                v = int(O.lib().orc_rng_next_u64(r.h))
+                out += bytes([v & 0xFF, (v >> 32) & 0xFF])
+        return out
+
+    crs = bytes(range(7, 39))
+    key = puncture(crs, 1)
+    assert O.ni_crs_seed(crs, 0) == puncture(key, 2)
+    assert O.ni_crs_seed(crs, 1) == puncture(key, 3)
+    ks = puncture(crs, 2)
+    for j in (0, 3):
+        assert O.ni_crs_seed(crs, 2, j) == puncture(ks, j + 1)
+    main = puncture(key, 1)
+    for i in (0, 1, 9):
+        assert O.ni_crs_seed(crs, 3, i) == puncture(main, i + 1)
+
+
+def _ni_shares(ev, crs, users, seed_base=0):
+    """Client-side NI key shares (evaluator.rs:1624-1975) for `users` users, with
+    random auto / LWE KSK rows (the aggregation only sums those)."""
+    s, z, sp, zp = ev.client_keys(users, seed_base=seed_base)
+    up = ev.client_keys(users, seed_base=seed_base + 7)[2]
+    info = ev.info
+    g = np.random.default_rng(31 + seed_base)
+    shares = []
+    for j in range(users):
+        sh = ev.ni_gen_share(crs, j, users, sp[j], up[j], zp[j], bytes([j + 1]) * 32)
+        sh["auto_keys"] = g.integers(0, ev.Q, (info.w + 1, info.auto_d, ev.N), dtype=np.uint64)
+        sh["lwe_ksk"] = g.integers(0, info.lwe_q, info.lwe_d * ev.N, dtype=np.uint64)
+        shares.append(sh)
+    return s, z, up, shares
+
+
+def test_ni_aggregation_decrypts():
+    """aggregate_non_interactive_multi_party_server_key_shares (evaluator.rs:
+    1222-1622) restated: the aggregated RGSW of LWE index l encrypts
+    X^{emb z[l]} (z the ideal LWE secret) under the ideal RLWE secret s -- its
+    m rows decrypt to beta X^{emb z[l]}, its -sm rows to -beta s X^{emb z[l]} --
+    for indices led by each user; each user's Ksk(u_j -> s) decrypts to its
+    gadget multiples of u_j; the auto / LWE KSK parts are the sums."""
+    O = oracle()
+    ev = O.Evaluator("NI_2P")
+    N, Q, users = ev.N, ev.Q, 2
+    crs = b"\x5a" * 32
+    s, z, up, shares = _ni_shares(ev, crs, users)
+    emb = 2 * N // ev.info.br_q
+    s_mod = np.array([int(x) % Q for x in s], dtype=np.uint64)
+
+    def mul(a, b):
+        out = np.empty(N, np.uint64)
+        O.lib().orc_negacyclic_mul(Q, O._p(np.ascontiguousarray(a)), O._p(np.ascontiguousarray(b)), O._p(out), N)
+        return out
+
+    def centred_max(v):
+        v = np.asarray(v).astype(object) % Q
+        return max(abs(int(x) if x < Q // 2 else int(x) - Q) for x in v)
+
+    beta = 1 << (54 - ev.info.rlrg_logb)
+    for i0 in (0, ev.n - 2):  # user 0 leads the first, user 1 the last indices
+        ksk, rgsw, auto, lwe = ev.ni_aggregate(crs, shares, i0, i0 + 2)
+        for k in range(2):
+            li = i0 + k
+            m = np.zeros(N, np.uint64)
+            e = int(z[li]) * emb
+            if e < 0:
+                m[N + e] = Q - 1
+            else:
+                m[e] = 1
+            sm = mul(s_mod, m)
+            r = rgsw[k]
+            for row_a, row_b, want in [(2, 3, m), (0, 1, (Q - sm) % Q)]:
+                noise = (r[row_b].astype(object) - mul(r[row_a], s_mod).astype(object)
+                         - want.astype(object) * beta)
+                assert centred_max(noise) < (1 << 34), (li, row_a, centred_max(noise))
+    assert np.array_equal(auto, sum(sh["auto_keys"].astype(object) for sh in shares) % Q)
+    assert np.array_equal(lwe, sum(sh["lwe_ksk"].astype(object) for sh in shares) % ev.info.lwe_q)
+    for j in range(users):  # B - A s = e + beta_i u_j, A from the user's CRS stream
+        a_rows = O.Rng(O.ni_crs_seed(crs, 2, j)).uniform_mod(Q, 50 * N).reshape(50, N)
+        u_mod = np.array([int(x) % Q for x in up[j]], dtype=np.uint64)
+        for i in (0, 25, 49):
+            g = 1 << (4 + i)  # one-bit digits over the top 50 of the 54 bits: beta_i = 2^(4 + i)
+            noise = (ksk[j, i].astype(object) - mul(a_rows[i], s_mod).astype(object)
+                     - u_mod.astype(object) * g)
+            assert centred_max(noise) < (1 << 12), (j, i)
+
+
+def test_ni_protocol_end_to_end():
+    """The whole non-interactive server side on the oracle: genuine shares of
+    two users (auto / LWE-KSK parts seeded from the CRS) -> aggregation of all
+    LWE indices -> seeded expansion (keys.rs:869-1004) -> each user's bools
+    ingested with its aggregated ui_to_s key -> NAND gates across the two
+    users' inputs decrypt correctly under the ideal secret."""
+    O = oracle()
+    ev = O.Evaluator("NI_2P")
+    users = 2
+    crs = b"\x5a" * 32
+    s, z, sp, zp = ev.client_keys(users)
+    up = ev.client_keys(users, seed_base=7)[2]
+    auto_b, lwe_b = ev.gen_seeded_auto_lwe(s, z, O.ni_crs_seed(crs, 0), O.ni_crs_seed(crs, 1))
+    shares = []
+    for j in range(users):
+        sh = ev.ni_gen_share(crs, j, users, sp[j], up[j], zp[j], bytes([j + 1]) * 32)
+        sh["auto_keys"] = auto_b if j == 0 else np.zeros_like(auto_b)
+        sh["lwe_ksk"] = lwe_b if j == 0 else np.zeros_like(lwe_b)
+        shares.append(sh)
+    ksk_b, rgsw, auto, lwe = ev.ni_aggregate(crs, shares, threads=8)
+    autos, ksk = ev.expand_seeded_key(auto, O.ni_crs_seed(crs, 0), lwe, O.ni_crs_seed(crs, 1))
+    key = ev.key(O.ServerKeyCoeff(rgsw, autos, ksk))
+    g = np.random.default_rng(12)
+    k = 6
+    ins = []
+    for j in range(users):
+        bits = g.integers(0, 2, k).astype(np.uint8)
+        seed = bytes([0x30 + j]) * 32
+        b = ev.ni_encrypt_bools(up[j], bits, seed)
+        lw = ev.ni_ingest(ev.expand_ni_ksk(ksk_b[j], O.ni_crs_seed(crs, 2, j)), seed, b, k)
+        assert np.array_equal(ev.decrypt_bool(s, lw), bits)
+        ins.append((bits, lw))
+    (b0, l0), (b1, l1) = ins
+    out = key.gate_batch(np.full(k, O.GATES["nand"], np.uint8), l0, l1, threads=4)
+    assert np.array_equal(ev.decrypt_bool(s, out), 1 - (b0 & b1))
