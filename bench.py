@@ -437,6 +437,51 @@ def aggregate_bench(P, torch, device, prm="I_8P"):
             "ms": dt * 1e3, "rgsw_products_per_s": products / dt, "modmul_per_s": mm / dt}
 
 
+def ni_aggregate_bench(P, torch, device, prm="NI_8P", users=8):
+    """Non-interactive server-key aggregation at NonInteractiveLTE8Party with 8
+    users: ui_to_s keys, auto / LWE KSK sums and the RGSWs of all n LWE indices
+    (per index 38 values x 50 digits transformed once, 38 x 7 + 2 key-switch
+    MACs, 7 RGSW x RGSW products), synthetic canonical shares on the device."""
+    p = P.params(prm)
+    N, n, Q = p.rlwe_n, p.lwe_n, p.rlwe_q
+    ra, rb = p.rgrg_d_a, p.rgrg_d_b
+    mx, ml = max(ra, rb), max(p.rlrg_d_a, p.rlrg_d_b)
+    eng = P.Engine(prm, device=device)
+    g = torch.Generator(device="cuda").manual_seed(9)
+
+    def U(*shape, q=Q):
+        return torch.randint(0, q, shape, dtype=torch.int64, device="cuda", generator=g)
+
+    per = -(-n // users)
+    shares = []
+    for j in range(users):
+        b, e = min(per * j, n), min(per * (j + 1), n)
+        shares.append(dict(ui_to_s_ksk=U(50, N), ksk_zero_encs=U(users - 1, 50, N), self_leader_cts=U(e - b, ml, N),
+                           not_leader_cts=U(n - (e - b), mx, N), rgsw_zero_encs=U(n, ra, N),
+                           auto_keys=U(p.n_auto_keys, p.auto_d, N), lwe_ksk=U(p.lwe_d * N, q=p.lwe_q)))
+    ksk = torch.empty((users, 50, N), dtype=torch.int64, device="cuda")
+    rgsw = torch.empty((n, 4, N), dtype=torch.int64, device="cuda")
+    auto = torch.empty((p.n_auto_keys, p.auto_d, N), dtype=torch.int64, device="cuda")
+    lwe = torch.empty(p.lwe_d * N, dtype=torch.int64, device="cuda")
+    crs = bytes(range(32))
+    eng.ni_aggregate_device(crs, shares, ksk, rgsw, auto, lwe)  # warm-up (allocator, module load)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.ni_aggregate_device(crs, shares, ksk, rgsw, auto, lwe)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    R = ra + rb
+    ntt = (N // 2) * int(np.log2(N))
+    ks_macs = n * (R * (users - 1) + 2)
+    products = n * (users - 1)
+    share_bytes = sum(int(t.numel()) * 8 for sh in shares for t in sh.values())
+    eng.close()
+    return {"config": f"{prm}, {users} users: {n} LWE indices, {n * R} values x 50 digits, {ks_macs} key-switch "
+                      f"MACs, {products} RGSW x RGSW (rgrg logb {p.rgrg_logb}, {ra}/{rb} digits), device shares",
+            "ms": dt * 1e3, "share_bytes": share_bytes, "digit_ntts_per_s": n * R * 50 / dt,
+            "ks_macs_per_s": ks_macs / dt, "butterflies_per_s": (n * R * 50 + ks_macs * 2) * ntt / dt}
+
+
 def u8_job(P, op):
     C = P.Circuit()
     a, b = C.input_u8(), C.input_u8()
@@ -698,7 +743,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the microbench / ragged / serving sub-results")
     ap.add_argument("--mode", default="wavefront",
                     choices=["wavefront", "br-kernel", "ks-kernel", "microbench", "ragged", "serving", "kernels",
-                             "ni", "key-upload", "aggregate"],
+                             "ni", "key-upload", "aggregate", "ni-aggregate"],
                     help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
@@ -706,13 +751,14 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.mode in ("microbench", "ragged", "serving", "kernels", "ni", "key-upload", "aggregate"):
+    if args.mode in ("microbench", "ragged", "serving", "kernels", "ni", "key-upload", "aggregate", "ni-aggregate"):
         import torch
         P = pz()
         fn = {"microbench": lambda: microbench(P, torch, 0), "ragged": lambda: ragged_batch(P, 0),
               "serving": lambda: serving(P, 0), "kernels": lambda: kernels_case(P, torch, 0),
               "ni": lambda: ni_ingest_bench(P, torch, 0), "key-upload": lambda: key_upload_bench(P, 0),
-              "aggregate": lambda: aggregate_bench(P, torch, 0)}[args.mode]
+              "aggregate": lambda: aggregate_bench(P, torch, 0),
+              "ni-aggregate": lambda: ni_aggregate_bench(P, torch, 0)}[args.mode]
         print(json.dumps({"mode": args.mode, **fn()}), flush=True)
         return
     if args.mode != "wavefront":
@@ -817,6 +863,7 @@ def main():
         extras["ni_ingest"] = ni_ingest_bench(P, torch, local)
         extras["key_upload"] = key_upload_bench(P, local)
         extras["aggregate"] = aggregate_bench(P, torch, local)
+        extras["ni_aggregate"] = ni_aggregate_bench(P, torch, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
