@@ -190,8 +190,10 @@ __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
 // Inverse GS butterfly (x' = x + y, y' = w (x - y), ntt.rs:84-104).  Generic
 // q: Harvey's form (x, y < 2q -> x', y' < 2q).  Q_N2048 (SPQ): no reduction of
 // the sum -- the rounds let sums grow to < 16 Q and reduce once per round
-// with reduce_n2048 -- and y' is an exact Shoup product in [0, 2Q); K Q must
-// bound the incoming y (the caller's stage bound).
+// with reduce_n2048 -- and y' is a Shoup product whose quotient comes from
+// umulhi_lo2 (at most 2 short beyond Shoup's own 1), so y' in [0, 4Q); K Q
+// must bound the incoming y (the caller's stage bound: inputs < 2Q, then
+// outputs < 4Q after one stage and < 8Q after two, hence K = 2, 4, 8).
 __device__ __forceinline__ u64 reduce_n2048(u64 v) {
   // 2^54 = 77823 (mod Q): v = h 2^54 + l -> l + 77823 h, < 2^54 + 2^27 < 2Q
   return (v & ((1ull << 54) - 1)) + (v >> 54) * 77823ull;
@@ -201,7 +203,7 @@ __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
   if (SPQ) {
     const u64 t = x + (u64)K * Q_N2048 - y;
     const u64 u = x + y;
-    y = w * t - mulq_n2048(umulhi(ws, t));
+    y = w * t - mulq_n2048(umulhi_lo2(ws, t));
     x = u;
   } else {
     const u64 q2 = q << 1;
