@@ -43,9 +43,14 @@ constexpr u64 UNSEED_MARGIN = 1024;  // keystream words generated beyond the sam
 // Block b of stream blockIdx.y: the 8 u64 words 8b..8b+7 of the stream (two
 // u32 words each, low first), their samples (high half of v * q) and
 // acceptance (low half <= zone).
-__global__ void unseed_candidates_kernel(const ChaChaKey *keys, u64 nblocks, u64 q, u64 zone, u64 *samples,
-                                         unsigned char *accept, u32 *cnt) {
-  const ChaChaKey key = keys[blockIdx.y];
+constexpr int FILL_STREAMS = 64;  // streams per launch (their keys travel as a kernel parameter)
+struct ChaChaKeys {
+  ChaChaKey k[FILL_STREAMS];
+};
+
+__global__ void unseed_candidates_kernel(const __grid_constant__ ChaChaKeys keys, u64 nblocks, u64 q, u64 zone,
+                                         u64 *samples, unsigned char *accept, u32 *cnt) {
+  const ChaChaKey key = keys.k[blockIdx.y];
   const u64 base = blockIdx.y * nblocks;
   for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nblocks; b += (u64)gridDim.x * blockDim.x) {
     u32 w[16];
@@ -64,8 +69,8 @@ __global__ void unseed_candidates_kernel(const ChaChaKey *keys, u64 nblocks, u64
 }
 
 // Exclusive scan of stream blockIdx.x's cnt[0, n) into its off (one CTA per
-// stream); off[n] = the stream's accepted total.
-__global__ void __launch_bounds__(1024) unseed_scan_kernel(const u32 *cnt, u64 n, u64 *off) {
+// stream); off[n] and totals[stream] = the stream's accepted total.
+__global__ void __launch_bounds__(1024) unseed_scan_kernel(const u32 *cnt, u64 n, u64 *off, u64 *totals) {
   __shared__ u64 part[1024];
   cnt += blockIdx.x * n;
   off += blockIdx.x * (n + 1);
@@ -86,7 +91,10 @@ __global__ void __launch_bounds__(1024) unseed_scan_kernel(const u32 *cnt, u64 n
     off[b] = run;
     run += cnt[b];
   }
-  if (threadIdx.x == blockDim.x - 1) off[n] = part[threadIdx.x];
+  if (threadIdx.x == blockDim.x - 1) {
+    off[n] = part[threadIdx.x];
+    totals[blockIdx.x] = part[threadIdx.x];
+  }
 }
 
 // Accepted sample k (k < total) of stream blockIdx.y ->
@@ -192,47 +200,39 @@ template <typename T>
 pz_status seeded_fill(pz_ctx *c, const uint8_t (*seeds)[32], size_t streams, u64 q, u64 total, u64 row_len,
                       u64 row_stride, u64 row_off, T *dst, u64 stream_stride, cudaStream_t st) {
   if (total == 0 || streams == 0) return PZ_OK;
-  if (streams > 65535) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "seeded fill: more than 65535 streams");
   const u64 nblocks = (total + UNSEED_MARGIN + 7) / 8;
-  std::vector<ChaChaKey> keys(streams);
-  for (size_t i = 0; i < streams; i++) keys[i] = pz::ni::chacha_key(seeds[i]);
+  const size_t group = std::min<size_t>(streams, FILL_STREAMS);
   // rand 0.8 UniformInt<u64>::new_inclusive(0, q - 1): range q, zone = MAX - (2^64 - q) % q
   const u64 zone = ~0ull - ((0ull - q) % q);
-  u64 *samples = nullptr, *off = nullptr;
-  unsigned char *acc = nullptr;
-  u32 *cnt = nullptr;
-  ChaChaKey *d_keys = nullptr;
+  // one scratch allocation: samples | off | totals | cnt | accept
+  const size_t b_samples = group * nblocks * 64, b_off = group * (nblocks + 1) * 8, b_tot = group * 8,
+               b_cnt = group * nblocks * 4, b_acc = group * nblocks;
+  unsigned char *scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, b_samples + b_off + b_tot + b_cnt + b_acc, st);
+  u64 *samples = (u64 *)scratch, *off = (u64 *)(scratch + b_samples), *tot = (u64 *)(scratch + b_samples + b_off);
+  u32 *cnt = (u32 *)(scratch + b_samples + b_off + b_tot);
+  unsigned char *acc = scratch + b_samples + b_off + b_tot + b_cnt;
   std::vector<u64> accepted(streams, 0);
-  cudaError_t e = cudaMallocAsync(&samples, streams * nblocks * 8 * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&off, streams * (nblocks + 1) * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&acc, streams * nblocks, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, streams * nblocks * 4, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&d_keys, streams * sizeof(ChaChaKey), st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_keys, keys.data(), streams * sizeof(ChaChaKey), cudaMemcpyHostToDevice, st);
-  const dim3 grid((unsigned)grid_of((nblocks + 255) / 256, 65535), (unsigned)streams);
-  if (e == cudaSuccess) {
-    unseed_candidates_kernel<<<grid, 256, 0, st>>>(d_keys, nblocks, q, zone, samples, acc, cnt);
+  for (size_t s0 = 0; s0 < streams && e == cudaSuccess; s0 += group) {
+    const size_t m = std::min(group, streams - s0);
+    ChaChaKeys keys{};
+    for (size_t i = 0; i < m; i++) keys.k[i] = pz::ni::chacha_key(seeds[s0 + i]);
+    const dim3 grid((unsigned)grid_of((nblocks + 255) / 256, 65535), (unsigned)m);
+    unseed_candidates_kernel<<<grid, 256, 0, st>>>(keys, nblocks, q, zone, samples, acc, cnt);
     e = cudaGetLastError();
+    if (e == cudaSuccess) {
+      unseed_scan_kernel<<<(unsigned)m, 1024, 0, st>>>(cnt, nblocks, off, tot);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+      seeded_place_kernel<T><<<grid, 256, 0, st>>>(samples, acc, off, nblocks, total, row_len, row_stride, row_off,
+                                                   dst + s0 * stream_stride, stream_stride);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&accepted[s0], tot, m * 8, cudaMemcpyDeviceToHost, st);
   }
-  if (e == cudaSuccess) {
-    unseed_scan_kernel<<<(unsigned)streams, 1024, 0, st>>>(cnt, nblocks, off);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) {
-    seeded_place_kernel<T><<<grid, 256, 0, st>>>(samples, acc, off, nblocks, total, row_len, row_stride, row_off, dst,
-                                                 stream_stride);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess)  // off[n] of every stream
-    e = cudaMemcpy2DAsync(accepted.data(), 8, off + nblocks, (nblocks + 1) * 8, 8, streams, cudaMemcpyDeviceToHost,
-                          st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFreeAsync(samples, st);
-  cudaFreeAsync(off, st);
-  cudaFreeAsync(acc, st);
-  cudaFreeAsync(cnt, st);
-  cudaFreeAsync(d_keys, st);
+  cudaFreeAsync(scratch, st);
   if (e != cudaSuccess) return pz::cuda_fail(c, "seeded uniform fill", e);
   for (size_t i = 0; i < streams; i++)
     if (accepted[i] < total)  // more rejections than the margin covers (probability ~0)
