@@ -321,8 +321,10 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
   }
 }
 
+// One-digit (D1) forms are register-capped to 3 CTAs per SM, the shape the
+// blind-rotation autotuner picks for the same operation body.
 template <int LOGN, bool D1>
-__global__ void __launch_bounds__(NttShape<LOGN>::T)
+__global__ void __launch_bounds__(NttShape<LOGN>::T, D1 ? 3 : 1)
     ext_product_kernel(BrParams P, u64 *rlwe, const u32 *idx, size_t count, int trivial) {
   constexpr int N = 1 << LOGN;
   extern __shared__ u64 smem[];
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
 }
 
 template <int LOGN, bool D1>
-__global__ void __launch_bounds__(NttShape<LOGN>::T)
+__global__ void __launch_bounds__(NttShape<LOGN>::T, D1 ? 3 : 1)
     auto_kernel(BrParams P, u64 *rlwe, const u32 *slot, size_t count, int trivial) {
   constexpr int N = 1 << LOGN;
   extern __shared__ u64 smem[];
