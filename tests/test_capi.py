@@ -53,6 +53,12 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.pz_ctx_create(99, 0, ctypes.byref(h)) == 1  # PZ_ERR_INVALID_ARGUMENT
     assert L.pz_param_get(-1, None) == 1
     assert L.pz_status_string(0) == b"ok"
+    # NULL context / seed / share arguments are refused before any device work
+    assert L.pz_ni_aggregate_device(None, None, None, 0, None, None, None, None, None) == 1
+    assert L.pz_ni_aggregate_server_key(None, None, None, 0, None, None) == 1
+    out = (ctypes.c_uint8 * 32)()
+    assert L.pz_ni_crs_seed(None, 0, 0, out) == 1
+    assert L.pz_ni_crs_seed((ctypes.c_uint8 * 32)(), 4, 0, out) == 1  # unknown seed kind
 
 
 def test_ni_crs_seeds_host_matches_oracle():
