@@ -249,7 +249,7 @@ def run_reference(args):
 
 
 def plain_form(P, torch, device, seed=7):
-    """InteractiveLTE2Party, 128 NAND bootstraps, one gate per launch."""
+    """Plain form at InteractiveLTE2Party: 128 NAND bootstraps, one gate per launch."""
     p = P.params("I_2P_LB_SR")
     eng = P.Engine("I_2P_LB_SR", device=device)
     key = eng.upload_key(*synthetic_key(p, seed))
