@@ -748,6 +748,7 @@ def main():
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
     ap.add_argument("--variant", type=int, default=None, help="blind-rotation launch-shape variant")
+    ap.add_argument("--users", type=int, default=8, help="users of the ni-aggregate mode")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -758,7 +759,7 @@ def main():
               "serving": lambda: serving(P, 0), "kernels": lambda: kernels_case(P, torch, 0),
               "ni": lambda: ni_ingest_bench(P, torch, 0), "key-upload": lambda: key_upload_bench(P, 0),
               "aggregate": lambda: aggregate_bench(P, torch, 0),
-              "ni-aggregate": lambda: ni_aggregate_bench(P, torch, 0)}[args.mode]
+              "ni-aggregate": lambda: ni_aggregate_bench(P, torch, 0, prm=args.param, users=args.users)}[args.mode]
         print(json.dumps({"mode": args.mode, **fn()}), flush=True)
         return
     if args.mode != "wavefront":
