@@ -163,6 +163,101 @@ __global__ void __launch_bounds__(NI_T, 2)
   }
 }
 
+// Small batches: the digits of one RLWE split over gridDim.y CTAs.  CTA
+// (c, s) runs the decomposition through digit pair `pend` of its share (the
+// signed digits carry from low to high, so every share walks the digits
+// before its own) and transforms and accumulates only pairs [pbeg, pend);
+// its partial (A, B) sums, evaluation domain in [0, 2q), go to
+// part[c][s][2][N] in the thread-major order ni_ks_finish_kernel reads.
+__global__ void __launch_bounds__(NI_T, 2)
+    ni_ks_partial_kernel(pz::RingConsts rc, pz::Decomp dp, u32 d, const u64 *ksk, const u64 *in, u64 *part,
+                         size_t count) {
+  constexpr int N = 1 << NI_LOGN;
+  extern __shared__ u64 sm[];
+  const int j = threadIdx.x;
+  const u64 q = rc.q;
+  const u32 pairs = (d + 1) / 2, share = (pairs + gridDim.y - 1) / gridDim.y;
+  const u32 pbeg = blockIdx.y * share, pend = min(pairs, pbeg + share);
+  for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    const u64 *p = in + c * 2 * N;
+    u64 st[8], oa[8], ob[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      st[r] = pz::decomp_init(q - p[pz::pos_coef<NI_LOGN>(j, r)], dp);  // elwise_neg_mut, then decompose
+      oa[r] = 0;
+      ob[r] = 0;
+    }
+#pragma unroll 1
+    for (u32 pi = 0; pi < pbeg; pi++) {  // digits of the earlier shares: carries only
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        pz::decomp_next(st[r], dp);
+        if (2 * pi + 1 < d) pz::decomp_next(st[r], dp);
+      }
+    }
+#pragma unroll 1
+    for (u32 pi = pbeg; pi < pend; pi++) {
+      const u32 jd = 2 * pi;
+      const bool two = jd + 1 < d;  // uniform
+      u64 x[8], y[8];
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        x[r] = pz::decomp_next(st[r], dp);
+        y[r] = two ? pz::decomp_next(st[r], dp) : 0;
+      }
+      if (two) pz::ntt_fwd<NI_LOGN, true>(x, y, sm, rc);
+      else pz::ntt_fwd<NI_LOGN, false>(x, x, sm, rc);
+      ni_mac(oa, ob, x, y, ksk + (size_t)jd * N, ksk + (size_t)(d + jd) * N, ksk + (size_t)(jd + 1) * N,
+             ksk + (size_t)(d + jd + 1) * N, two, rc);
+    }
+    u64 *o = part + (c * gridDim.y + blockIdx.y) * 2 * N;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      o[r * NI_T + j] = oa[r];
+      o[N + r * NI_T + j] = ob[r];
+    }
+    __syncthreads();
+  }
+}
+
+// Sum of the `shares` partials (each < 2q, so the sum is reduced with the
+// special form of Q once), one inverse transform of both outputs, B' += B.
+__global__ void __launch_bounds__(NI_T, 2)
+    ni_ks_finish_kernel(pz::RingConsts rc, const u64 *part, u32 shares, const u64 *in, u64 *out, size_t count) {
+  constexpr int N = 1 << NI_LOGN;
+  extern __shared__ u64 sm[];
+  const int j = threadIdx.x;
+  const u64 q = rc.q;
+  for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    u64 oa[8], ob[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) oa[r] = ob[r] = 0;
+    for (u32 sh = 0; sh < shares; sh++) {
+      const u64 *src = part + (c * shares + sh) * 2 * N;
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        oa[r] += src[r * NI_T + j];
+        ob[r] += src[N + r * NI_T + j];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      oa[r] = pz::reduce_n2048(oa[r]);
+      ob[r] = pz::reduce_n2048(ob[r]);
+    }
+    pz::ntt_inv<NI_LOGN, true>(oa, ob, sm, rc);
+    const u64 *p = in + c * 2 * N;
+    u64 *o = out + c * 2 * N;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int pc = pz::pos_coef<NI_LOGN>(j, r);
+      o[pc] = pz::reduce2(oa[r], q);
+      o[N + pc] = pz::add_mod(pz::reduce2(ob[r], q), p[N + pc], q);  // elwise_add_mut(B', B)
+    }
+    __syncthreads();
+  }
+}
+
 // out[c] = sample_extract(rlwe[idx[c] / N], idx[c] % N); an index past the
 // batch leaves out[c] unchanged.
 __global__ void extract_kernel(const u64 *rlwe, size_t rlwe_count, const u32 *idx, u64 *out, size_t count, u32 N,
@@ -352,9 +447,28 @@ pz_status pz_ni_key_switch_device(pz_ctx *c, const pz_ni_ksk *k, const uint64_t 
   PZ_CK(c, cudaSetDevice(c->device));
   const pz::Decomp dp = pz::decomposer(c->P.rlwe_q, c->P.ni_ks_logb, c->P.ni_ks_d);
   const size_t smem = 2 * (size_t)c->P.rlwe_n * 8;
-  ni_key_switch_kernel<<<grid_of(count, 65535), NI_T, smem, (cudaStream_t)stream>>>(c->rc, dp, k->d, k->d_ksk, d_in,
-                                                                                  d_out, count);
-  PZ_CK(c, cudaGetLastError());
+  cudaStream_t st = (cudaStream_t)stream;
+  // fewer RLWEs than two per SM: split each one's digit pairs over CTAs
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  const u32 pairs = (k->d + 1) / 2;
+  const size_t shares = std::min<size_t>(std::min<size_t>(8, pairs), (2 * (size_t)sms + count - 1) / count);
+  if (shares <= 1) {
+    ni_key_switch_kernel<<<grid_of(count, 65535), NI_T, smem, st>>>(c->rc, dp, k->d, k->d_ksk, d_in, d_out, count);
+    PZ_CK(c, cudaGetLastError());
+    return PZ_OK;
+  }
+  u64 *part = nullptr;
+  PZ_CK(c, cudaMallocAsync(&part, count * shares * 2 * c->P.rlwe_n * 8, st));
+  ni_ks_partial_kernel<<<dim3((unsigned)count, (unsigned)shares), NI_T, smem, st>>>(c->rc, dp, k->d, k->d_ksk, d_in,
+                                                                                   part, count);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    ni_ks_finish_kernel<<<grid_of(count, 65535), NI_T, smem, st>>>(c->rc, part, (u32)shares, d_in, d_out, count);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(part, st);
+  if (e != cudaSuccess) return pz::cuda_fail(c, "pz_ni_key_switch_device", e);
   return PZ_OK;
 }
 

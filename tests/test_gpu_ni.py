@@ -34,13 +34,14 @@ def test_unseed_matches_oracle(gpu_available, param):
     assert np.array_equal(to_host(d_r).reshape(3, 2, ev.N), want)
 
 
-@pytest.mark.parametrize("param", NI)
-def test_ni_key_switch_matches_oracle(gpu_available, param):
+@pytest.mark.parametrize("param,count", [("NI_2P", 6), ("NI_8P", 6), ("NI_8P", 1), ("NI_8P", 300)])
+def test_ni_key_switch_matches_oracle(gpu_available, param, count):
+    """Small batches split each RLWE's digits over CTAs (1, 6 RLWEs); large
+    ones run one CTA per RLWE (300)."""
     ev, s, u, ksk, _, eng, dksk, _ = setup_ni(param)
-    count = 6
     rl = np.random.default_rng(4).integers(0, ev.Q, (count, 2, ev.N), dtype=np.uint64)
-    rl[1, 0, :9] = 0  # -0 = q in the reference's elwise_neg_mut
-    rl[2, 0, :] = 0
+    rl[0, 0, :9] = 0  # -0 = q in the reference's elwise_neg_mut
+    rl[-1, 0, :] = 0
     want = np.stack([ev.ni_key_switch(ksk, r) for r in rl])
     d_out = to_dev(np.zeros_like(rl))
     eng.ni_key_switch_device(dksk, to_dev(rl), d_out)
