@@ -427,6 +427,16 @@ pz_status pz_server_set_launch(pz_server *s, int pbs_variant, int grid_limit);
  * on `batch` synthetic gates spread over the sessions and keeps the fastest.
  * Needs an idle server (no admitted job). */
 pz_status pz_server_autotune(pz_server *s, size_t batch, int *variant, int *grid_limit, double *ms);
+/* Which jobs advance a level at each step.  ALL_READY (default): every
+ * admitted job.  CRITICAL_PATH: the jobs with the most levels left always
+ * advance; the others fill the step only up to the launch-time tier those
+ * already pay for (one CTA per SM, two, ..., then whole waves), deepest
+ * first -- a batch of jobs submitted together ends after the same number of
+ * steps with fewer partly-filled launches; a short job may wait behind a
+ * deep one, so serving keeps ALL_READY.  Results are the same under both. */
+#define PZ_SCHEDULE_ALL_READY 0
+#define PZ_SCHEDULE_CRITICAL_PATH 1
+pz_status pz_server_set_schedule(pz_server *s, int policy);
 
 #ifdef __cplusplus
 }

@@ -92,6 +92,7 @@ SIGNATURES = {
     "pz_ni_ingest": (st, [vp, vp, u8p, u64p, ctypes.c_size_t, u64p, ctypes.c_size_t]),
     "pz_rgsw_by_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_aggregate_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp]),
+    "pz_server_set_schedule": (st, [vp, ctypes.c_int]),
     "pz_ni_crs_seed": (st, [u8p, ctypes.c_int, ctypes.c_size_t, u8p]),
     "pz_ni_aggregate_device": (st, [vp, u8p, ctypes.POINTER(PzNiShareView), ctypes.c_size_t, vp, vp, vp, vp, vp]),
     "pz_ni_aggregate_server_key": (st, [vp, u8p, ctypes.POINTER(PzNiShareView), ctypes.c_size_t,

@@ -82,6 +82,8 @@ struct pz_server {
   size_t outref_cap = 0;
 
   int pbs_variant = 0, grid_limit = 0;
+  int schedule = PZ_SCHEDULE_ALL_READY;
+  int sm_count = 148;  // the device's SMs (148 on B200; the dry-run server keeps this)
 
   struct Job {
     u64 id = 0;
@@ -351,6 +353,54 @@ pz_status run_items(pz_server *s, const std::vector<Item> &items) {
   return PZ_OK;
 }
 
+// The jobs that advance one level this step.  PZ_SCHEDULE_ALL_READY: every
+// admitted job with a level left.  PZ_SCHEDULE_CRITICAL_PATH: the jobs with
+// the most levels left always advance (they set the number of steps the
+// batch needs); the others, most levels left first, fill the step only up to
+// the launch-time tier the mandatory gates already pay for -- one CTA per SM,
+// two, ... up to the variant's CTAs per SM, then whole waves -- so work with
+// slack moves into steps that would otherwise leave SMs idle.  A job waits
+// at most until its remaining depth is the largest, so the batch still ends
+// after (deepest circuit) steps.
+size_t level_width(const pz_server::Job *j) { return j->v.level_off[j->level + 1] - j->v.level_off[j->level]; }
+
+void select_jobs(pz_server *s, std::vector<pz_server::Job *> &run) {
+  run.clear();
+  if (s->schedule != PZ_SCHEDULE_CRITICAL_PATH) {
+    for (auto *j : s->active)
+      if (j->level < j->v.levels) run.push_back(j);
+    return;
+  }
+  size_t depth = 0;
+  for (auto *j : s->active)
+    if (j->level < j->v.levels) depth = std::max(depth, j->v.levels - j->level);
+  std::vector<pz_server::Job *> opt;
+  size_t g = 0;
+  for (auto *j : s->active) {
+    if (j->level >= j->v.levels) continue;
+    if (j->v.levels - j->level == depth) {
+      run.push_back(j);
+      g += level_width(j);
+    } else {
+      opt.push_back(j);
+    }
+  }
+  const size_t sms = (size_t)std::max(1, s->sm_count);
+  const size_t cps = s->pbs_variant == 0 ? 2 : s->pbs_variant == 2 ? 4 : 3;
+  const size_t wave = sms * cps;
+  const size_t cap = g <= wave ? std::max<size_t>(1, (g + sms - 1) / sms) * sms : (g + wave - 1) / wave * wave;
+  std::stable_sort(opt.begin(), opt.end(), [](const pz_server::Job *a, const pz_server::Job *b) {
+    return a->v.levels - a->level > b->v.levels - b->level;
+  });
+  for (auto *j : opt) {
+    const size_t w = level_width(j);
+    if (g + w <= cap) {
+      run.push_back(j);
+      g += w;
+    }
+  }
+}
+
 // Gather the outputs of finished jobs (on the stream; copies complete at the
 // step's final synchronisation).
 pz_status finish_outputs(pz_server *s, const std::vector<pz_server::Job *> &fin) {
@@ -413,6 +463,7 @@ pz_status pz_server_create(int device, size_t arena_bytes, size_t max_items, pz_
   pz_server *s = new pz_server();
   s->dry = device == PZ_SERVER_DRY_RUN;
   s->device = s->dry ? 0 : device;
+  if (!s->dry) cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device);
   s->max_items = max_items;
   s->arena_slots = 0;
   s->arena_bytes_req = arena_bytes;  // slots are sized by the first session's ring (L words)
@@ -502,15 +553,15 @@ pz_status pz_server_step(pz_server *s, size_t *gates_run) {
   if (!s->dry) cudaSetDevice(s->device);
   pz_status st = admit(s);
   if (st != PZ_OK) return st;
-  // next level of every admitted job, sorted by session (counting sort)
+  std::vector<pz_server::Job *> run;
+  select_jobs(s, run);
+  // next level of every selected job, sorted by session (counting sort)
   std::vector<size_t> per(s->sessions.size() + 1, 0);
-  for (auto *j : s->active)
-    if (j->level < j->v.levels) per[j->session + 1] += j->v.level_off[j->level + 1] - j->v.level_off[j->level];
+  for (auto *j : run) per[j->session + 1] += j->v.level_off[j->level + 1] - j->v.level_off[j->level];
   for (size_t i = 1; i < per.size(); i++) per[i] += per[i - 1];
   const size_t total = per.back();
   std::vector<Item> items(total);
-  for (auto *j : s->active) {
-    if (j->level >= j->v.levels) continue;
+  for (auto *j : run) {
     const size_t a = j->v.level_off[j->level], b = j->v.level_off[j->level + 1];
     size_t &pos = per[j->session];
     for (size_t g = a; g < b; g++) {
@@ -590,6 +641,14 @@ pz_status pz_server_set_launch(pz_server *s, int pbs_variant, int grid_limit) {
   if (!s || pbs_variant < 0 || pbs_variant >= pz::PBS_VARIANTS || grid_limit < 0) return PZ_ERR_INVALID_ARGUMENT;
   s->pbs_variant = pbs_variant;
   s->grid_limit = grid_limit;
+  return PZ_OK;
+}
+
+pz_status pz_server_set_schedule(pz_server *s, int policy) {
+  if (!s) return PZ_ERR_INVALID_ARGUMENT;
+  if (policy != PZ_SCHEDULE_ALL_READY && policy != PZ_SCHEDULE_CRITICAL_PATH)
+    return s->fail(PZ_ERR_INVALID_ARGUMENT, "pz_server_set_schedule: unknown policy");
+  s->schedule = policy;
   return PZ_OK;
 }
 

@@ -20,6 +20,9 @@ DRY_RUN = -1
 PENDING, RUNNING, DONE, FAILED = 0, 1, 2, 3
 
 
+SCHEDULE_ALL_READY, SCHEDULE_CRITICAL_PATH = 0, 1
+
+
 class Server:
     def __init__(self, device=0, arena_bytes=1 << 30, max_items=8192):
         h = vp()
@@ -118,6 +121,10 @@ class Server:
 
     def set_launch(self, pbs_variant, grid_limit=0):
         self._chk(lib().pz_server_set_launch(self.h, int(pbs_variant), int(grid_limit)), "set_launch")
+
+    def set_schedule(self, policy):
+        """ALL_READY (0, default) or CRITICAL_PATH (1): see pz_server_set_schedule."""
+        self._chk(lib().pz_server_set_schedule(self.h, int(policy)), "set_schedule")
 
     def autotune(self, batch):
         v, g, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()

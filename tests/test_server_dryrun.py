@@ -120,3 +120,51 @@ def test_mixed_ring_rejected():
     S.add_virtual_session(P.param_id("NI_8P"))
     with pytest.raises(RuntimeError):
         S.add_virtual_session(P.param_id("SP_TEST"))  # N = 512: another ring
+
+
+def _ragged_mix(S, sids, per_op):
+    ops = ["add", "mul", "div_rem", "lt"]
+    circs = {op: u8_circuit(op) for op in ops}
+    for sid in sids:
+        for k in range(4 * per_op):
+            S.submit(sid, circs[ops[k % 4]])
+    return circs
+
+
+def _run_counts(S):
+    counts = []
+    while S.stats()["active"] or S.stats()["pending"]:
+        counts.append(S.step())
+    return counts
+
+
+def test_critical_path_schedule_keeps_depth_and_fills_tiers():
+    """CRITICAL_PATH: the batch still ends after (deepest circuit) steps and
+    runs every gate once; the wide first levels of the short jobs are spread
+    over steps the deep jobs leave part-empty, so fewer waves are launched
+    (tiers: 148 SMs, 3 CTAs per SM at the default launch variant)."""
+    P = pz()
+    waves = {}
+    for policy in (P.server.SCHEDULE_ALL_READY, P.server.SCHEDULE_CRITICAL_PATH):
+        S, sids = make_server(1 << 22, params=("I_2P_LB_SR", "I_4P", "I_8P"), max_items=16384)
+        S.set_launch(1)
+        S.set_schedule(policy)
+        circs = _ragged_mix(S, sids, 16)
+        counts = _run_counts(S)
+        depth = max(c.info()["levels"] for c in circs.values())
+        assert len(counts) == depth
+        assert sum(counts) == sum(c.info()["gates"] for c in circs.values()) * 16 * len(sids)
+        assert S.stats()["done"] == 4 * 16 * len(sids)
+        # launch-time model: partial waves by their SM tier, whole waves of 444
+        w = 0.0
+        for g in counts:
+            full, rem = divmod(g, 444)
+            w += full + (0 if rem == 0 else (1 / 3 if rem <= 148 else 2 / 3 if rem <= 296 else 1))
+        waves[policy] = w
+    assert waves[P.server.SCHEDULE_CRITICAL_PATH] < 0.85 * waves[P.server.SCHEDULE_ALL_READY]
+
+
+def test_schedule_policy_rejects_unknown():
+    S, _ = make_server(1 << 16)
+    with pytest.raises(Exception):
+        S.set_schedule(7)
