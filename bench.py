@@ -630,6 +630,19 @@ def serving(P, device, sessions=64, rate=40.0, seconds=10.0, seed=8):
                 gates_done += g
                 S.forget(j)
     total = time.perf_counter() - t0
+    # one client alone: an FheUint8 add (37 gates over its levels) on an idle server, five times
+    Ca = P.Circuit()
+    a_in, b_in = Ca.input_u8(), Ca.input_u8()
+    Ca.outputs(Ca.u8_add(a_in, b_in))
+    alone = []
+    for r in range(6):
+        ta = time.perf_counter()
+        ja = S.submit(sids[0], Ca, pool[r:r + 16])
+        while S.status(ja)["state"] != 2:
+            S.step()
+        if r:
+            alone.append((time.perf_counter() - ta) * 1e3)
+        S.forget(ja)
     S.close()
     for eng, key in keep:
         key.release()
@@ -639,6 +652,7 @@ def serving(P, device, sessions=64, rate=40.0, seconds=10.0, seed=8):
             "seconds": total, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "steps": steps, "mean_gates_per_step": float(np.mean(step_gates)), "max_active_jobs": max_active,
             "device_key_bytes": key_bytes, "autotune": tune,
+            "alone_add_ms": float(np.median(alone)), "alone_add_levels": Ca.info()["levels"],
             "config": f"{sessions} sessions over {SERVING_PARAMS}, Poisson {rate}/s for {seconds}s, "
                       f"circuits of U[1,300] gates from FheUint8 ops, admission by device bytes"}
 

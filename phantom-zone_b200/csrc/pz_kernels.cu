@@ -959,6 +959,56 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttShape<LOGN>::T, 2
   }
 }
 
+// The two-CTA kernel over a ragged batch: item ct uses the parameter set and
+// key of descriptor item_desc[ct] (both CTAs of its cluster load the same
+// descriptor) and scatters its output to out_idx[ct]; the schedule arrays are
+// laid out for the item's own (br_q, n) inside the launch's maximum.
+template <int LOGN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttShape<LOGN>::T, 2)
+    pbs_split_ragged_kernel(const BrParams *descs, const u32 *item_desc, const u32 *ks, u32 ks_stride,
+                            const unsigned char *gates, u64 *out, const u32 *out_idx, int count) {
+  constexpr int N = 1 << LOGN;
+  extern __shared__ u64 smem[];
+  __shared__ BrParams sp;
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned rank = cl.block_rank();
+  u64 *slots = smem + 2 * N;
+  const u64 *peer_slots = cl.map_shared_rank(slots, rank ^ 1u);
+  const int j = threadIdx.x;
+  const int ncl = gridDim.x / 2;
+  for (int ct = blockIdx.x / 2; ct < count; ct += ncl) {  // both CTAs of a cluster take the same items
+    if (threadIdx.x == 0) sp = descs[item_desc[ct]];
+    __syncthreads();
+    const SchedSmem S = sched_smem<LOGN>(smem, SPLIT_REGIONS, sp.br_q >> 1, sp.n);
+    const u64 q = sp.rc.q;
+    const u32 *kso = ks + (size_t)ct * ks_stride;
+    build_schedule<LOGN>(sp, kso, smem, S);
+    u64 x[8];
+    if (rank == 0) {
+#pragma unroll
+      for (int r = 0; r < 8; r++) x[r] = 0;
+    } else {
+      test_rlwe_b<LOGN>(sp, kso, gates[ct], x);
+    }
+    __syncthreads();
+    const u32 nops = *S.nops;
+#pragma unroll 1
+    for (u32 t = 0; t < nops; t++) split_op<LOGN>(x, S.ops[t], t, sp, smem, slots, peer_slots, rank, cl);
+    u64 *o = out + (size_t)out_idx[ct] * (N + 1);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const u32 p = (u32)pos_coef<LOGN>(j, r);
+      if (rank == 0) {
+        if (p == 0) o[1] = x[r];
+        else o[1 + N - p] = q - x[r];
+      } else if (p == 0) {
+        o[0] = x[r];
+      }
+    }
+    cl.sync();  // the digit slots and sp are reused by the next ciphertext
+  }
+}
+
 // Throughput probe for the roofline denominator: 8 independent chains of
 // 32-bit multiply-adds per thread (mad.lo.u32, the IMAD the 64-bit modular
 // multiplications are built from).  `sink` keeps the chains live.
@@ -1157,6 +1207,13 @@ cudaError_t launch_pbs_ragged(int logn, bool d1, const BrParams *d_descs, const 
   int grid = (int)count;
   if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
   cudaError_t e;
+  if (logn == 11 && d1 && variant == PBS_SPLIT) {
+    const size_t ssmem = split_smem_bytes(max_br_q, max_n);
+    if ((e = set_smem(pbs_split_ragged_kernel<11>, ssmem)) != cudaSuccess) return e;
+    pbs_split_ragged_kernel<11><<<2 * grid, 256, ssmem, s>>>(d_descs, item_desc, ks, ks_stride, gates, out, out_idx,
+                                                             (int)count);
+    return cudaGetLastError();
+  }
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                                    \
   if ((e = set_smem(pbs_ragged_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;                 \
   pbs_ragged_kernel<LN, DD, MB><<<grid, TH, smem, s>>>(d_descs, item_desc, ks, ks_stride, gates, out, out_idx, \

@@ -344,9 +344,11 @@ pz_status run_items(pz_server *s, const std::vector<Item> &items) {
                              d + lay.gate, s->d_arena, (const u32 *)(d + lay.in0), (const u32 *)(d + lay.in1),
                              s->d_ksout, s->ks_stride, s->stream);
     if (e != cudaSuccess) return s->cuda("launch_ks_ragged", e);
+    // a step of at most half the SMs' gates: one cluster of two CTAs per gate (the latency form)
+    const int variant = (s->logn == 11 && s->d1 && n <= (size_t)s->sm_count / 2) ? pz::PBS_SPLIT : s->pbs_variant;
     e = pz::launch_pbs_ragged(s->logn, s->d1, s->d_br, (const u32 *)(d + lay.desc), s->max_br_q, s->max_n,
                               s->d_ksout, s->ks_stride, d + lay.gate, s->d_arena, (const u32 *)(d + lay.out), n,
-                              s->grid_limit, s->stream, s->pbs_variant);
+                              s->grid_limit, s->stream, variant);
     if (e != cudaSuccess) return s->cuda("launch_pbs_ragged", e);
     s->launches += 2;
   }
