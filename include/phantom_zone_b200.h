@@ -329,6 +329,35 @@ pz_status pz_rgsw_by_rgsw_device(pz_ctx *ctx, uint64_t *d_rgsw0, const uint64_t 
  * d_others[steps - 1][c], the other users in order; d_others [steps][count][rows][N]. */
 pz_status pz_aggregate_rgsw_device(pz_ctx *ctx, uint64_t *d_rgsw0, const uint64_t *d_others, size_t steps,
                                    size_t count, void *stream);
+/* The whole aggregate_interactive_multi_party_server_key_shares (bool/evaluator.rs:1050-
+ * 1200) on one user's share per entry (CommonReferenceSeededInteractiveMultiPartyServer-
+ * KeyShare, bool/keys.rs:334-360), u64, coefficient domain, DEVICE memory:
+ *   self_leader_rgsws      [segment][2 rlrg_d_a + 2 rlrg_d_b][N]  RGSWs of the LWE indices
+ *                          the user leads (multi_party_user_id_lwe_segment)
+ *   not_self_leader_rgsws  [lwe_n - segment][2 rgrg_d_a + 2 rgrg_d_b][N]  the other
+ *                          indices, in index order
+ *   auto_keys              [w + 1][d_auto][N] B rows, auto_element_dlogs order
+ *   lwe_ksk                [d_ks N]
+ * shares[j] is user j's.  Outputs (DEVICE memory, the SeededInteractiveMultiPartyServerKey
+ * form): d_rgsw [lwe_n][4][N], d_auto_b [w + 1][d_auto][N], d_lwe_b [d_ks N].  Returns
+ * when done. */
+typedef struct pz_server_key_share_view {
+  const uint64_t *self_leader_rgsws;
+  const uint64_t *not_self_leader_rgsws;
+  const uint64_t *auto_keys;
+  const uint64_t *lwe_ksk;
+} pz_server_key_share_view;
+pz_status pz_aggregate_device(pz_ctx *ctx, const pz_server_key_share_view *shares, size_t users,
+                              uint64_t *d_rgsw, uint64_t *d_auto_b, uint64_t *d_lwe_b, void *stream);
+/* InteractiveMultiPartyCrs (bool/evaluator.rs:78-100) seeds: what = 0 public-key share,
+ * 1 auto keys, 2 LWE KSK.  Host only. */
+#define PZ_ICRS_PUBLIC_KEY 0
+#define PZ_ICRS_AUTO_KEYS 1
+#define PZ_ICRS_LWE_KSK 2
+pz_status pz_interactive_crs_seed(const uint8_t crs_seed[32], int what, uint8_t out[32]);
+/* Aggregation followed by the seeded expansion (keys.rs:687-781): the server key. */
+pz_status pz_aggregate_server_key(pz_ctx *ctx, const uint8_t crs_seed[32], const pz_server_key_share_view *shares,
+                                  size_t users, pz_key **key_out);
 
 /* ---- server-key aggregation (non-interactive protocol) ------------------------------
  * aggregate_non_interactive_multi_party_server_key_shares (bool/evaluator.rs:1222-1622).

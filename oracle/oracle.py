@@ -87,6 +87,7 @@ def lib():
             "orc_rgsw_by_rgsw": (None, [vp, u64p, u64p]),
             "orc_rgsw_encrypt": (None, [vp, i32p, u64p, ctypes.c_int, u8p, u64p]),
             "orc_ni_crs_seed": (None, [u8p, ctypes.c_int, ctypes.c_size_t, u8p]),
+            "orc_interactive_crs_seed": (None, [u8p, ctypes.c_int, u8p]),
             "orc_ni_aggregate": (None, [vp, u8p, ctypes.c_int] + [ctypes.POINTER(u64p)] * 7 +
                                  [ctypes.c_size_t, ctypes.c_size_t, u64p, u64p, u64p, u64p]),
             "orc_gen_seeded_auto_lwe": (None, [vp, i32p, i32p, u8p, u8p, u8p, u64p, u64p]),
@@ -130,6 +131,13 @@ def ni_crs_seed(crs, what, index=0):
     2 ui_to_s KSK of user `index`, 3 NI RGSW of LWE index `index`."""
     out = (ctypes.c_uint8 * 32)()
     lib().orc_ni_crs_seed((ctypes.c_uint8 * 32)(*bytes(crs)), int(what), int(index), out)
+    return bytes(out)
+
+
+def interactive_crs_seed(crs, what):
+    """InteractiveMultiPartyCrs seed (evaluator.rs:78-100): what 0 public-key share, 1 auto keys, 2 LWE KSK."""
+    out = (ctypes.c_uint8 * 32)()
+    lib().orc_interactive_crs_seed((ctypes.c_uint8 * 32)(*bytes(crs)), int(what), out)
     return bytes(out)
 
 
@@ -400,6 +408,35 @@ class Evaluator:
                                       (ctypes.c_uint8 * 32)(*bytes(auto_seed)), (ctypes.c_uint8 * 32)(*bytes(lwe_seed)),
                                       (ctypes.c_uint8 * 32)(*bytes(err_seed)), _p(auto_b), _p(lwe_b))
         return auto_b, lwe_b
+
+    def aggregate(self, shares, i0=0, i1=None):
+        """aggregate_interactive_multi_party_server_key_shares (evaluator.rs:1050-1200) composed from
+        the restated pieces: auto-key and LWE-KSK sums, and per LWE index l the leader's RGSW
+        (rlwe x rgsw shape) times every other user's RGSW (rgsw x rgsw shape) in increasing id
+        (rgsw_by_rgsw_inplace).  shares: dicts self_leader [segment][rows0][N], not_leader
+        [n - segment][rows1][N], auto_keys [w+1][d_auto][N], lwe_ksk [d_ks N] (user id order).
+        -> (rgsw [i1-i0][rows0][N], auto, lwe)."""
+        info = self.info
+        users = len(shares)
+        i1 = self.n if i1 is None else i1
+        auto = np.zeros_like(shares[0]["auto_keys"], dtype=object)
+        lwe = np.zeros_like(shares[0]["lwe_ksk"], dtype=object)
+        for sh in shares:
+            auto = (auto + sh["auto_keys"].astype(object)) % self.Q
+            lwe = (lwe + sh["lwe_ksk"].astype(object)) % info.lwe_q
+        segs = [self.lwe_segment(u, users) for u in range(users)]
+        out = []
+        for li in range(i0, i1):
+            lead = next(u for u, (b, e) in enumerate(segs) if b <= li < e)
+            r = shares[lead]["self_leader"][li - segs[lead][0]].copy()
+            for o in range(users):
+                if o == lead:
+                    continue
+                b, e = segs[o]
+                pos = li if li < b else li - (e - b)
+                r = self.rgsw_by_rgsw(r, shares[o]["not_leader"][pos])
+            out.append(r)
+        return np.stack(out), auto.astype(np.uint64), lwe.astype(np.uint64)
 
     def ni_aggregate(self, crs, shares, i0=0, i1=None, threads=1):
         """aggregate_non_interactive_multi_party_server_key_shares (evaluator.rs:1222-1622).

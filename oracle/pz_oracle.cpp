@@ -1497,6 +1497,18 @@ void orc_ni_crs_seed(const uint8_t crs[32], int what, size_t index, uint8_t out[
   }
 }
 
+// InteractiveMultiPartyCrs (evaluator.rs:78-100): what = 0 public-key share,
+// 1 auto keys, 2 LWE KSK.
+void orc_interactive_crs_seed(const uint8_t crs[32], int what, uint8_t out[32]) {
+  uint8_t key[32];
+  if (what == 0) {
+    crs_puncture(crs, 1, out);
+    return;
+  }
+  crs_puncture(crs, 2, key);  // key_seed
+  crs_puncture(key, what == 1 ? 1 : 2, out);
+}
+
 // multi_party_user_id_lwe_segment (evaluator.rs:613-626); an empty segment
 // when the start passes lwe_n.
 void lwe_segment(size_t user, size_t users, size_t n, size_t *b, size_t *e) {

@@ -194,6 +194,8 @@ void orc_rgsw_encrypt(void *ev, const int32_t *s, const uint64_t *m, int which, 
 /* NonInteractiveMultiPartyCrs seeds (evaluator.rs:115-172): what 0 auto keys, 1 LWE KSK,
  * 2 ui_to_s KSK of user `index`, 3 NI RGSW of LWE index `index` */
 void orc_ni_crs_seed(const uint8_t crs[32], int what, size_t index, uint8_t out[32]);
+/* InteractiveMultiPartyCrs seeds (evaluator.rs:78-100): what 0 public-key share, 1 auto keys, 2 LWE KSK */
+void orc_interactive_crs_seed(const uint8_t crs[32], int what, uint8_t out[32]);
 /* aggregate_non_interactive_multi_party_server_key_shares (evaluator.rs:1222-1622); per-user
  * pointer arrays in user id order; RGSWs for LWE indices [i0, i1) */
 void orc_ni_aggregate(void *ev, const uint8_t crs[32], int users, const uint64_t *const *ui_to_s_ksk,

@@ -47,6 +47,10 @@ class PzNiShareView(ctypes.Structure):
                                   "rgsw_zero_encs", "auto_keys", "lwe_ksk")]
 
 
+class PzServerKeyShareView(ctypes.Structure):
+    _fields_ = [(n, vp) for n in ("self_leader_rgsws", "not_self_leader_rgsws", "auto_keys", "lwe_ksk")]
+
+
 class PzServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_size_t) for n in ("pending", "active", "done", "failed", "arena_slots",
                                                 "arena_slots_used", "arena_bytes", "sessions", "key_bytes")] + \
@@ -93,6 +97,10 @@ SIGNATURES = {
     "pz_rgsw_by_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_aggregate_rgsw_device": (st, [vp, vp, vp, ctypes.c_size_t, ctypes.c_size_t, vp]),
     "pz_server_set_schedule": (st, [vp, ctypes.c_int]),
+    "pz_interactive_crs_seed": (st, [u8p, ctypes.c_int, u8p]),
+    "pz_aggregate_device": (st, [vp, ctypes.POINTER(PzServerKeyShareView), ctypes.c_size_t, vp, vp, vp, vp]),
+    "pz_aggregate_server_key": (st, [vp, u8p, ctypes.POINTER(PzServerKeyShareView), ctypes.c_size_t,
+                                     ctypes.POINTER(vp)]),
     "pz_ni_crs_seed": (st, [u8p, ctypes.c_int, ctypes.c_size_t, u8p]),
     "pz_ni_aggregate_device": (st, [vp, u8p, ctypes.POINTER(PzNiShareView), ctypes.c_size_t, vp, vp, vp, vp, vp]),
     "pz_ni_aggregate_server_key": (st, [vp, u8p, ctypes.POINTER(PzNiShareView), ctypes.c_size_t,

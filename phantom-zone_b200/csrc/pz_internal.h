@@ -73,6 +73,11 @@ pz_status seeded_fill_u32(pz_ctx *c, const uint8_t seed[32], u64 q, u64 total, u
 pz_status seeded_fill_batch_u64(pz_ctx *c, const uint8_t (*seeds)[32], size_t streams, u64 q, u64 total, u64 *dst,
                                 u64 stream_stride, cudaStream_t st);
 
+// puncture_p_rng over ChaCha8(seed): the `times`-th 32-byte fill (host)
+void crs_puncture(const uint8_t seed[32], size_t times, uint8_t out[32]);
+// out[i] = sum_t d_src[t][i] mod q over k device rows of len words (canonical inputs)
+cudaError_t launch_sum_mod(const u64 *const *d_src, u32 k, size_t len, u64 q, u64 *out, cudaStream_t st);
+
 // Compiled (levelized) form of a circuit, read by the multi-session executor.
 // Wire slots: inputs first (input order), then gate outputs; bit 31 = not().
 struct CircuitView {

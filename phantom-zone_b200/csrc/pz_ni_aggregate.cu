@@ -193,18 +193,7 @@ __global__ void __launch_bounds__(NI_T, 2)
 
 int grid_cap(size_t n, int cap) { return (int)std::min<size_t>(std::max<size_t>(n, 1), (size_t)cap); }
 
-// puncture_p_rng (utils.rs:219-228) with RandomFill<[u8; 32]> (random.rs:
-// 162-175): the `times`-th 32-byte fill of ChaCha8(seed); each byte is the
-// low byte of one u32 word, so fill t is words 32 (t - 1) .. 32 t - 1, i.e.
-// blocks 2 (t - 1) and 2 (t - 1) + 1.
-void puncture(const uint8_t seed[32], size_t times, uint8_t out[32]) {
-  const pz::ni::ChaChaKey key = pz::ni::chacha_key(seed);
-  for (int h = 0; h < 2; h++) {
-    u32 w[16];
-    pz::ni::chacha8_block(key, 2 * (u64)(times - 1) + h, w);
-    for (int i = 0; i < 16; i++) out[16 * h + i] = (uint8_t)w[i];
-  }
-}
+void puncture(const uint8_t seed[32], size_t times, uint8_t out[32]) { pz::crs_puncture(seed, times, out); }
 
 void segment(size_t user, size_t users, size_t n, u32 *b, u32 *e) {  // evaluator.rs:613-626
   const size_t per = (n + users - 1) / users;
@@ -215,7 +204,39 @@ void segment(size_t user, size_t users, size_t n, u32 *b, u32 *e) {  // evaluato
 
 }  // namespace
 
+namespace pz {
+// puncture_p_rng (utils.rs:219-228) with RandomFill<[u8; 32]> (random.rs:
+// 162-175): the `times`-th 32-byte fill of ChaCha8(seed); each byte is the
+// low byte of one u32 word, so fill t is words 32 (t - 1) .. 32 t - 1, i.e.
+// blocks 2 (t - 1) and 2 (t - 1) + 1.
+void crs_puncture(const uint8_t seed[32], size_t times, uint8_t out[32]) {
+  const ni::ChaChaKey key = ni::chacha_key(seed);
+  for (int h = 0; h < 2; h++) {
+    u32 w[16];
+    ni::chacha8_block(key, 2 * (u64)(times - 1) + h, w);
+    for (int i = 0; i < 16; i++) out[16 * h + i] = (uint8_t)w[i];
+  }
+}
+cudaError_t launch_sum_mod(const u64 *const *d_src, u32 k, size_t len, u64 q, u64 *out, cudaStream_t st) {
+  if (len == 0) return cudaSuccess;
+  sum_mod_kernel<<<grid_cap(len / 256, 1184), 256, 0, st>>>(d_src, k, len, q, out);
+  return cudaGetLastError();
+}
+}  // namespace pz
+
 extern "C" {
+
+pz_status pz_interactive_crs_seed(const uint8_t crs[32], int what, uint8_t out[32]) {
+  if (!crs || !out || what < 0 || what > 2) return PZ_ERR_INVALID_ARGUMENT;
+  if (what == PZ_ICRS_PUBLIC_KEY) {
+    pz::crs_puncture(crs, 1, out);
+    return PZ_OK;
+  }
+  uint8_t key[32];
+  pz::crs_puncture(crs, 2, key);  // key_seed
+  pz::crs_puncture(key, what == PZ_ICRS_AUTO_KEYS ? 1 : 2, out);
+  return PZ_OK;
+}
 
 pz_status pz_ni_crs_seed(const uint8_t crs[32], int what, size_t index, uint8_t out[32]) {
   if (!crs || !out || what < 0 || what > 3) return PZ_ERR_INVALID_ARGUMENT;

@@ -8,7 +8,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import PzNiShareView, PzParams, PzSeededServerKeyView, PzServerKeyView, check, lib, u8p, u64p, vp
+from ._lib import PzNiShareView, PzParams, PzServerKeyShareView, PzSeededServerKeyView, PzServerKeyView, check, lib, u8p, u64p, vp
 
 PARAMETER_SETS = {
     "I_2P_LB_SR": 0, "I_4P": 1, "I_8P": 2, "NI_2P": 3,
@@ -120,6 +120,17 @@ def ni_crs_seed(crs, what, index=0):
     """NonInteractiveMultiPartyCrs seed (bool/evaluator.rs:115-172), host only."""
     out = (ctypes.c_uint8 * 32)()
     check(lib().pz_ni_crs_seed(_seed(crs), int(what), int(index), out), None, "pz_ni_crs_seed")
+    return bytes(out)
+
+
+ICRS_PUBLIC_KEY, ICRS_AUTO_KEYS, ICRS_LWE_KSK = 0, 1, 2
+SHARE_FIELDS = ("self_leader_rgsws", "not_self_leader_rgsws", "auto_keys", "lwe_ksk")
+
+
+def interactive_crs_seed(crs, what):
+    """InteractiveMultiPartyCrs seed (bool/evaluator.rs:78-100), host only."""
+    out = (ctypes.c_uint8 * 32)()
+    check(lib().pz_interactive_crs_seed(_seed(crs), int(what), out), None, "pz_interactive_crs_seed")
     return bytes(out)
 
 
@@ -339,6 +350,28 @@ class Engine:
         steps = others.numel() // (count * 2 * (self.p.rgrg_d_a + self.p.rgrg_d_b) * self.N) if count else 0
         check(lib().pz_aggregate_rgsw_device(self.h, _ptr(rgsw0), _ptr(others), steps, count, _stream(stream)),
               self.h, "pz_aggregate_rgsw_device")
+
+    def _share_views(self, shares):
+        """shares: list (user id order) of dicts SHARE_FIELDS -> device tensors (u64 as int64)."""
+        views = (PzServerKeyShareView * len(shares))()
+        for v, sh in zip(views, shares):
+            for f in SHARE_FIELDS:
+                t = sh.get(f)
+                setattr(v, f, t.data_ptr() if t is not None and t.numel() else None)
+        return views
+
+    def aggregate_device(self, shares, rgsw, auto_b, lwe_b, stream=None):
+        """aggregate_interactive_multi_party_server_key_shares (bool/evaluator.rs:1050-1200) on
+        device shares; outputs (device tensors) in the seeded server key's coefficient form."""
+        check(lib().pz_aggregate_device(self.h, self._share_views(shares), len(shares), _ptr(rgsw), _ptr(auto_b),
+                                        _ptr(lwe_b), _stream(stream)), self.h, "pz_aggregate_device")
+
+    def aggregate_server_key(self, crs, shares):
+        """Aggregation + seeded expansion -> DeviceKey; shares on the device."""
+        kh = vp()
+        check(lib().pz_aggregate_server_key(self.h, _seed(crs), self._share_views(shares), len(shares),
+                                            ctypes.byref(kh)), self.h, "pz_aggregate_server_key")
+        return DeviceKey(self, kh)
 
     def _ni_share_views(self, shares):
         """shares: list (user id order) of dicts NI_SHARE_FIELDS -> device tensors (u64 as int64)."""

@@ -59,6 +59,9 @@ def test_invalid_arguments_rejected_without_gpu():
     out = (ctypes.c_uint8 * 32)()
     assert L.pz_ni_crs_seed(None, 0, 0, out) == 1
     assert L.pz_ni_crs_seed((ctypes.c_uint8 * 32)(), 4, 0, out) == 1  # unknown seed kind
+    assert L.pz_aggregate_device(None, None, 0, None, None, None, None) == 1
+    assert L.pz_aggregate_server_key(None, None, None, 0, None) == 1
+    assert L.pz_interactive_crs_seed((ctypes.c_uint8 * 32)(), 3, out) == 1
 
 
 def test_ni_crs_seeds_host_matches_oracle():
@@ -70,3 +73,12 @@ def test_ni_crs_seeds_host_matches_oracle():
     crs = bytes(range(3, 35))
     for what, idx in [(0, 0), (1, 0), (2, 0), (2, 7), (3, 0), (3, 1), (3, 659)]:
         assert eng.ni_crs_seed(crs, what, idx) == O.ni_crs_seed(crs, what, idx)
+
+
+def test_interactive_crs_seeds_host_matches_oracle():
+    """pz_interactive_crs_seed == the oracle's InteractiveMultiPartyCrs (evaluator.rs:78-100)."""
+    from conftest import oracle
+    O = oracle()
+    crs = bytes(range(5, 37))
+    for what in range(3):
+        assert pz().engine.interactive_crs_seed(crs, what) == O.interactive_crs_seed(crs, what)

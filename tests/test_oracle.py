@@ -339,6 +339,11 @@ def test_ni_crs_seeds_are_punctured_streams():
     main = puncture(key, 1)
     for i in (0, 1, 9):
         assert O.ni_crs_seed(crs, 3, i) == puncture(main, i + 1)
+    # InteractiveMultiPartyCrs (evaluator.rs:78-100): public key 1, key seed 2 -> auto 1, lwe 2
+    assert O.interactive_crs_seed(crs, 0) == puncture(crs, 1)
+    ikey = puncture(crs, 2)
+    assert O.interactive_crs_seed(crs, 1) == puncture(ikey, 1)
+    assert O.interactive_crs_seed(crs, 2) == puncture(ikey, 2)
 
 
 def _ni_shares(ev, crs, users, seed_base=0):
@@ -445,3 +450,55 @@ def test_ni_protocol_end_to_end():
     (b0, l0), (b1, l1) = ins
     out = key.gate_batch(np.full(k, O.GATES["nand"], np.uint8), l0, l1, threads=4)
     assert np.array_equal(ev.decrypt_bool(s, out), 1 - (b0 & b1))
+
+
+def interactive_shares(ev, crs, users, seed_base=0):
+    """Interactive server key shares (keys.rs:334-360) built from RGSW encryptions of
+    X^{emb z_j[l]} under the ideal secret (what the collective public key encrypts to):
+    the leader's in the rlwe x rgsw shape, the others' in the rgsw x rgsw shape; auto /
+    LWE-KSK B parts under (s, z) with CRS-seeded A parts, all in user 0's share."""
+    O = oracle()
+    s, z, sp, zp = ev.client_keys(users, seed_base=seed_base)
+    N, Q = ev.N, ev.Q
+    emb = 2 * N // ev.info.br_q
+    auto_b, lwe_b = ev.gen_seeded_auto_lwe(s, z, O.interactive_crs_seed(crs, 1), O.interactive_crs_seed(crs, 2))
+
+    def mono(v):
+        m = np.zeros(N, np.uint64)
+        e = int(v) * emb
+        if e < 0:
+            m[N + e] = Q - 1
+        else:
+            m[e] = 1
+        return m
+
+    shares = []
+    for j in range(users):
+        b, e = ev.lwe_segment(j, users)
+        lead = [ev.rgsw_encrypt(s, mono(zp[j][li]), 0, bytes([j, li % 256, li // 256]) + b"\x01" * 29)
+                for li in range(b, e)]
+        other = [ev.rgsw_encrypt(s, mono(zp[j][li]), 1, bytes([j, li % 256, li // 256]) + b"\x02" * 29)
+                 for li in list(range(0, b)) + list(range(e, ev.n))]
+        shares.append(dict(self_leader=np.stack(lead) if lead else np.zeros((0, 4, N), np.uint64),
+                           not_leader=np.stack(other) if other else np.zeros((0, ev.rgsw_rows(1), N), np.uint64),
+                           auto_keys=auto_b if j == 0 else np.zeros_like(auto_b),
+                           lwe_ksk=lwe_b if j == 0 else np.zeros_like(lwe_b)))
+    return s, shares
+
+
+def test_interactive_aggregation_end_to_end():
+    """aggregate_interactive_multi_party_server_key_shares (evaluator.rs:1050-1200) on the
+    oracle: two users' shares -> aggregated RGSWs (leader x other) + summed auto / LWE
+    KSK -> seeded expansion with the interactive CRS seeds -> gates decrypt correctly."""
+    O = oracle()
+    ev = O.Evaluator("I_2P_LB_SR")
+    crs = b"\x2a" * 32
+    s, shares = interactive_shares(ev, crs, 2)
+    rgsw, auto, lwe = ev.aggregate(shares)
+    autos, ksk = ev.expand_seeded_key(auto, O.interactive_crs_seed(crs, 1), lwe, O.interactive_crs_seed(crs, 2))
+    key = ev.key(O.ServerKeyCoeff(rgsw, autos, ksk))
+    r = O.Rng(b"\x07" * 32)
+    bits0, bits1 = np.array([0, 1, 1, 0, 1, 0]), np.array([0, 0, 1, 1, 1, 1])
+    c0, c1 = ev.encrypt_bool(r, s, bits0), ev.encrypt_bool(r, s, bits1)
+    out = key.gate_batch(np.full(6, O.GATES["nand"], np.uint8), c0, c1, threads=4)
+    assert np.array_equal(ev.decrypt_bool(s, out), 1 - (bits0 & bits1))
