@@ -426,6 +426,29 @@ def aggregate_bench(P, torch, device, prm="I_8P"):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     products = n * steps
+    # the whole aggregation from 8 parties' shares (pz_aggregate_device: RGSW placement and gathers
+    # per leader segment, the same products, auto / LWE-KSK sums)
+    users, per = steps + 1, -(-n // (steps + 1))
+    shares = []
+    for u in range(users):
+        seg = min(per * (u + 1), n) - min(per * u, n)
+        shares.append(dict(
+            self_leader_rgsws=torch.randint(0, p.rlwe_q, (seg, 4, N), dtype=torch.int64, device="cuda", generator=g),
+            not_self_leader_rgsws=torch.randint(0, p.rlwe_q, (n - seg, rows1, N), dtype=torch.int64, device="cuda",
+                                                generator=g),
+            auto_keys=torch.randint(0, p.rlwe_q, (p.n_auto_keys, p.auto_d, N), dtype=torch.int64, device="cuda",
+                                    generator=g),
+            lwe_ksk=torch.randint(0, p.lwe_q, (p.lwe_d * N,), dtype=torch.int64, device="cuda", generator=g)))
+    o_rgsw = torch.empty((n, 4, N), dtype=torch.int64, device="cuda")
+    o_auto = torch.empty((p.n_auto_keys, p.auto_d, N), dtype=torch.int64, device="cuda")
+    o_lwe = torch.empty((p.lwe_d * N,), dtype=torch.int64, device="cuda")
+    eng.aggregate_device(shares, o_rgsw, o_auto, o_lwe)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    eng.aggregate_device(shares, o_rgsw, o_auto, o_lwe)
+    torch.cuda.synchronize()
+    whole_ms = (time.perf_counter() - t1) * 1e3
+    del shares
     logn = int(np.log2(N))
     ntt = (N // 2) * logn
     # per RGSW x RGSW: key conversion (rows1 forward NTTs) + 2 RLWE x RGSW (digit NTTs, MAC rows, 2 inverse)
@@ -434,7 +457,8 @@ def aggregate_bench(P, torch, device, prm="I_8P"):
     eng.close()
     return {"config": f"{prm}: {n} LWE indices x {steps} other users = {products} RGSW x RGSW "
                       f"(rgrg logb {p.rgrg_logb}, {p.rgrg_d_a}/{p.rgrg_d_b} digits), device buffers",
-            "ms": dt * 1e3, "rgsw_products_per_s": products / dt, "modmul_per_s": mm / dt}
+            "ms": dt * 1e3, "rgsw_products_per_s": products / dt, "modmul_per_s": mm / dt,
+            "whole_aggregation_ms": whole_ms}
 
 
 def ni_aggregate_bench(P, torch, device, prm="NI_8P", users=8):
