@@ -178,3 +178,24 @@ def test_wavefront_mul_lt_graph_replay(gpu_available, param):
     a_ct, b_ct = inp[0:8], inp[8:16]
     assert np.array_equal(lts[0], okey.u8_op("lt", a_ct, b_ct)[0][0])
     assert np.array_equal(muls[0], okey.u8_op("mul", a_ct, b_ct)[0])
+
+
+@pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
+def test_mul_and_lt_multi_party_decryption(gpu_available, param):
+    """FheUint8 a*b and a<b on the GPU, each output bit decrypted by the
+    parties' decryption shares and their aggregation (multi-party decryption,
+    mp_api.rs:491-660) with the 2 / 8 parties of the parameter set."""
+    O = oracle()
+    ev, (s, _, sp, _), _, _ = oracle_setup(param)
+    eng, key = eng_key(param)
+    C = pz().Circuit()
+    a, b = C.input_u8(), C.input_u8()
+    C.outputs(C.u8_mul(a, b))
+    C.output(C.u8_cmp("lt", a, b))
+    r = O.Rng(b"\x05" * 32)
+    for x, y in [(201, 77), (13, 250), (0, 0)]:
+        inp = np.concatenate([enc_u8(ev, r, s, [x])[0], enc_u8(ev, r, s, [y])[0]])
+        out = C.run(eng, key, inp)
+        bits = ev.mp_decrypt_bool(r, sp, out)
+        assert sum(int(v) << i for i, v in enumerate(bits[:8])) == (x * y) % 256
+        assert int(bits[8]) == int(x < y)
