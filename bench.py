@@ -41,6 +41,9 @@ PARAM = "NI_8P"
 N_MUL = 1024
 N_LT = 1024
 C_MM = 10  # 32-bit multiply instructions per 64-bit Shoup modmul (roofline convention)
+GATE_NAMES = ["and", "nand", "or", "nor", "xor", "xnor"]
+REF_STEP_SECONDS = 10.0  # wall time of one timed step of the CPU reference arm
+ROOFLINE_WAVES = 8  # whole waves of the blind-rotation launch timed for the roofline
 WORKLOAD_CONFIG = {
     "workload": "batched circuit wavefront: NI_8P, 1024 FheUint8 a*b + 1024 a<b, "
                 "each level one launch, whole circuit one CUDA graph",
@@ -121,6 +124,57 @@ def schedule_work(p, ks):
     return total
 
 
+def traffic_record(P, variant, B):
+    """DRAM bytes per launch of B bootstraps from the committed ncu capture
+    (profiles/pbs_kernel_traffic.json, bytes per bootstrap of a warm launch),
+    used only when it was taken on the blind-rotation revision this library
+    reports and on the same launch shape; None otherwise."""
+    path = os.path.join(ROOT, "profiles", "pbs_kernel_traffic.json")
+    rev = P.kernel_revision()
+    try:
+        rec = json.load(open(path))
+    except (OSError, ValueError):
+        return None, "no ncu capture on record"
+    if rec.get("kernel_revision") != rev or rec.get("variant") != variant:
+        return None, (f"ncu capture on record is of {rec.get('kernel_revision')} variant {rec.get('variant')}, "
+                      f"not {rev} variant {variant}")
+    return int(rec["bytes_per_bootstrap"] * B), (f"ncu capture of {rev} variant {variant}: "
+                                                  f"{rec['bytes_per_bootstrap']} B per bootstrap x {B}")
+
+
+def wavefront_parity_check(p, okey, h_in, h_out, d_out, mul_ids=(0,), lt_ids=(N_MUL, N_MUL + N_LT - 1)):
+    """The measured wavefront checked after the timed region: the graph
+    replay's outputs equal the host-buffer run's word for word, and the
+    outputs of a few circuits equal the oracle's sequential gate-by-gate
+    evaluation of the same FheUint8 ops (shortint/ops.rs) on the same inputs
+    and synthetic key, word for word."""
+    from concurrent.futures import ThreadPoolExecutor
+    L = p.rlwe_n + 1
+    replay = d_out.cpu().numpy().view(np.uint64)
+    host = h_out.numpy().view(np.uint64)
+    same_paths = bool(np.array_equal(replay, host))
+    inp = h_in.numpy().view(np.uint64)
+
+    def job(kind_i):
+        kind, i = kind_i
+        a, b = inp[16 * i:16 * i + 8], inp[16 * i + 8:16 * i + 16]
+        if kind == "mul":
+            return kind, i, okey.u8_op("mul", a, b)[0], replay[8 * i:8 * i + 8]
+        return kind, i, okey.u8_op("lt", a, b)[0], replay[8 * N_MUL + (i - N_MUL)][None, :]
+
+    jobs = [("mul", i) for i in mul_ids] + [("lt", i) for i in lt_ids]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        res = list(ex.map(job, jobs))
+    ok = same_paths and all(np.array_equal(want.reshape(-1, L), got.reshape(-1, L)) for _, _, want, got in res)
+    return {"parity_checked": bool(ok), "replay_equals_host_run": same_paths,
+            "circuits_checked": [f"{k} #{i}" for k, i, _, _ in res],
+            "ciphertexts_checked": int(sum(g.size // L for _, _, _, g in res)),
+            "oracle_seconds": time.perf_counter() - t0,
+            "what": "every output of the graph replay == the C-ABI host-buffer run; the listed circuits' outputs == "
+                    "the oracle's sequential evaluation, word for word"}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -198,49 +252,109 @@ def max_over_ranks(dist, x, device=None):
 
 
 # ---------------------------------------------------------------------------
-def cpu_gate_sample(p, key_arrays, threads, gates_per_thread, seed=11):
-    """Time the oracle (CPU restatement of the reference) on independent gates."""
+def host_cores():
+    """Logical CPUs this process may run on, and the physical cores behind them
+    (distinct (package, core) pairs in the sysfs topology)."""
+    cpus = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else list(range(os.cpu_count() or 1))
+    phys = set()
+    for c in cpus:
+        base = f"/sys/devices/system/cpu/cpu{c}/topology/"
+        try:
+            phys.add((open(base + "physical_package_id").read().strip(), open(base + "core_id").read().strip()))
+        except OSError:
+            phys.add(("?", str(c)))
+    return len(cpus), len(phys)
+
+
+def wavefront_gate_mix(ev):
+    """Gate codes (and, nand, or, nor, xor, xnor) of the wavefront -- 1024
+    FheUint8 a*b and 1024 a<b -- tallied from the oracle's own restatement of
+    the reference's circuits (a dry run, nothing bootstrapped)."""
+    return N_MUL * ev.u8_gate_mix("mul") + N_LT * ev.u8_gate_mix("lt")
+
+
+def mix_gates(mix, count, rng):
+    """`count` gate codes in the proportions of `mix` (largest remainder), shuffled."""
+    mix = np.asarray(mix, np.float64)
+    want = mix / mix.sum() * count
+    n = np.floor(want).astype(np.int64)
+    for i in np.argsort(-(want - n))[:count - int(n.sum())]:
+        n[i] += 1
+    codes = np.repeat(np.arange(6, dtype=np.uint8), n)
+    rng.shuffle(codes)
+    return codes
+
+
+def cpu_gate_sample(p, key_arrays, threads, count, mix, seed=11, okey=None):
+    """Time the oracle (CPU restatement of the reference's gate path) on `count`
+    independent gates of the gate mix `mix`, spread over `threads` threads."""
     from oracle import oracle as O
-    ev = O.Evaluator(PARAM)
-    key = ev.key(O.ServerKeyCoeff(*key_arrays))
+    if okey is None:
+        okey = O.Evaluator(PARAM).key(O.ServerKeyCoeff(*key_arrays))
     rng = np.random.default_rng(seed)
-    count = threads * gates_per_thread
     c0 = rng.integers(0, p.rlwe_q, (count, p.rlwe_n + 1), dtype=np.uint64)
     c1 = rng.integers(0, p.rlwe_q, (count, p.rlwe_n + 1), dtype=np.uint64)
-    gates = rng.integers(0, 6, count).astype(np.uint8)
+    gates = mix_gates(mix, count, rng)
     t0 = time.perf_counter()
-    key.gate_batch(gates, c0, c1, threads=threads)
+    okey.gate_batch(gates, c0, c1, threads=threads)
     dt = time.perf_counter() - t0
     return count / dt, count, dt
 
 
+def cpu_reference_setup(key_arrays=None):
+    """The oracle side of the workload: parameter record, synthetic key (the
+    same words the GPU arm uploads, unless given), oracle key and the
+    wavefront's gate mix.  Uses the oracle only -- the product library is not
+    loaded."""
+    from oracle import oracle as O
+    p = O.param_info(PARAM)
+    if key_arrays is None:
+        key_arrays = synthetic_key(p, 0x5EED)
+    ev = O.Evaluator(PARAM)
+    okey = ev.key(O.ServerKeyCoeff(*key_arrays))
+    return p, key_arrays, okey, wavefront_gate_mix(ev)
+
+
+def cpu_calibrated_sample(p, key_arrays, okey, mix, threads, seconds):
+    """Gates per sample sized to about `seconds` of wall time on `threads`
+    threads (calibrated on two gates per thread)."""
+    rate0, _, _ = cpu_gate_sample(p, key_arrays, threads, 2 * threads, mix, seed=10, okey=okey)
+    return max(threads, int(round(seconds * rate0 / threads)) * threads)
+
+
 def run_reference(args):
-    """--impl reference: the CPU restatement of the reference path on host cores."""
+    """--impl reference: the CPU restatement of the reference's gate path (the
+    oracle, a port: the Rust crate cannot be built here) on all host threads,
+    on independent gates in the wavefront's gate mix.  Rank 0 alone under
+    torchrun; the product library is never loaded on this arm."""
     dist, rank, world, _ = dist_setup(args)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
-    P = pz()
-    p = P.params(PARAM)
-    threads = os.cpu_count() or 1
-    key_arrays = synthetic_key(p, 0x5EED)
+    threads, physical = host_cores()
+    p, key_arrays, okey, mix = cpu_reference_setup()
+    count = cpu_calibrated_sample(p, key_arrays, okey, mix, threads, args.ref_step_seconds)
     per_step = []
-    gates_per_thread = 2
     for s in range(args.warmup + args.steps):
-        rate, count, dt = cpu_gate_sample(p, key_arrays, threads, gates_per_thread, seed=100 + s)
+        # warm-up steps: one gate per thread; timed steps: the calibrated sample
+        n = threads if s < args.warmup else count
+        _, _, dt = cpu_gate_sample(p, key_arrays, threads, n, mix, seed=100 + s, okey=okey)
         if s >= args.warmup:
             per_step.append(dt)
-    value = threads * gates_per_thread * len(per_step) / sum(per_step)
+    value = count * len(per_step) / sum(per_step)
+    mix_s = ", ".join(f"{g} {int(c)}" for g, c in zip(GATE_NAMES, mix) if c)
+    sample = (f"{count} independent NI_8P gates per step in the wavefront's gate mix ({mix_s} per 1024 a*b + "
+              f"1024 a<b), {threads} threads on {physical} physical cores, "
+              f"{sum(per_step) / len(per_step):.1f} s wall per step")
     line = {
         "impl": "reference", "metric": "gate bootstraps/sec", "value": value, "unit": "gate bootstraps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(per_step) / len(per_step), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": dict(WORKLOAD_CONFIG, sample=f"{threads * gates_per_thread} gates of the wavefront's "
-                                               f"gate mix per step on {threads} host threads"),
-        "cpu_baseline": {"value": value, "unit": "gate bootstraps/s", "cores": threads, "kind": "port",
-                         "sample": f"{threads * gates_per_thread} independent gates per step on {threads} threads"},
+        "config": dict(WORKLOAD_CONFIG, sample=sample),
+        "cpu_baseline": {"value": value, "unit": "gate bootstraps/s", "cores": threads, "physical_cores": physical,
+                         "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "gate bootstraps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -526,10 +640,10 @@ def u8_job(P, op):
 def ragged_batch(P, device, per_session=64, params=("I_2P_LB_SR", "I_4P", "I_8P"), seed=4):
     """Ragged batch: sessions of the 2-, 4- and 8-party interactive sets in
     one server; per session `per_session` FheUint8 ops (add, mul, div_rem,
-    lt; 20 % of the div_rem jobs with an all-zero divisor ciphertext
-    pattern) submitted at once; every step is one ragged key-switch launch
+    lt; 20 % of the div_rem jobs with divisor 0) submitted at once; every step is one ragged key-switch launch
     plus one ragged blind-rotation launch across the sessions; the launch
-    shape comes from the server's autotuner."""
+    shape comes from the server's autotuner.  The zero divisors are trivial
+    encryptions of 0 (every bit a = 0, b = -Q/8), valid under every key."""
     S = P.Server(device=device, arena_bytes=4 << 30, max_items=16384)
     keep = []
     for i, prm in enumerate(params):
@@ -552,7 +666,10 @@ def ragged_batch(P, device, per_session=64, params=("I_2P_LB_SR", "I_4P", "I_8P"
             C = templates[op]
             inp = pool[rng.integers(0, 64 - 16):][:16].copy()
             if op == "div_rem" and rng.random() < 0.2:
-                inp[8:16] = pool[0]  # one ciphertext repeated as the divisor's 8 bits
+                # divisor 0: every bit a noiseless encryption of false under any
+                # key -- a = 0, b = -Q/8 (false_el, evaluator.rs:239-242)
+                inp[8:16] = 0
+                inp[8:16, 0] = keep[0][3].rlwe_q - (keep[0][3].rlwe_q >> 3)
             jobs.append(S.submit(sid, C, inp))
             gates += C.info()["gates"]
     t0 = time.perf_counter()
@@ -779,6 +896,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity-check", action="store_true",
+                    help="skip the oracle check of the measured wavefront's outputs")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the microbench / ragged / serving sub-results")
     ap.add_argument("--mode", default="wavefront",
@@ -789,6 +908,8 @@ def main():
     ap.add_argument("--param", default=PARAM)
     ap.add_argument("--variant", type=int, default=None, help="blind-rotation launch-shape variant")
     ap.add_argument("--users", type=int, default=8, help="users of the ni-aggregate mode")
+    ap.add_argument("--ref-step-seconds", type=float, default=REF_STEP_SECONDS,
+                    help="wall time of one timed step of the CPU reference arm")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -866,8 +987,9 @@ def main():
     e2e_total = max_over_ranks(dist, sum(e2e_ms), "cuda")
     e2e_value = world * gates_per_step * args.steps / (e2e_total / 1e3)
 
-    # dominant kernel: blind rotation alone on 2368 key-switched LWEs (4 waves of 592)
-    B = 2368
+    # dominant kernel: blind rotation alone on whole waves of the autotuned
+    # launch shape (ROOFLINE_WAVES x the items resident at once)
+    B = ROOFLINE_WAVES * eng.pbs_slots()
     ks = rng.integers(0, p.lwe_q, (B, p.lwe_n + 1), dtype=np.uint64).astype(np.uint32)
     d_ks = torch.from_numpy(ks.view(np.int32)).cuda()
     d_tv = torch.from_numpy(rng.integers(0, 6, B).astype(np.uint8)).cuda()
@@ -885,12 +1007,7 @@ def main():
     modmuls = schedule_work(p, ks)
     achieved = modmuls * C_MM / (br_ms / 1e3) / 1e12  # T IMAD/s
     peak = P.probe_imad_rate(local) / 1e12
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "pbs_kernel_traffic_ni8p_2368.md")
-    if os.path.exists(prof):
-        for ln in open(prof):
-            if ln.startswith("traffic_bytes_per_bootstrap:"):
-                traffic = int(ln.split(":")[1]) * B  # ncu dram read+write, warm launch of B items
+    traffic, traffic_source = traffic_record(P, tune["variant"], B)
 
     plain = None
     if not args.no_plain and rank == 0:
@@ -906,15 +1023,20 @@ def main():
         extras["aggregate"] = aggregate_bench(P, torch, local)
         extras["ni_aggregate"] = ni_aggregate_bench(P, torch, local)
 
-    cpu = None
+    cpu, parity = None, None
+    okey_c = mix = None
+    if rank == 0 and (not args.no_cpu_baseline or not args.no_parity_check):
+        _, _, okey_c, mix = cpu_reference_setup(key_arrays)
+    if rank == 0 and not args.no_parity_check:
+        parity = wavefront_parity_check(p, okey_c, h_in, h_out, d_out)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        # calibrate on one gate per thread, then size the sample to ~12 s of CPU work
-        rate0, _, _ = cpu_gate_sample(p, key_arrays, threads, 1, seed=10)
-        per_thread = int(min(max(12.0 * rate0 / threads, 2), 256))
-        rate, count, dt = cpu_gate_sample(p, key_arrays, threads, per_thread)
-        cpu = {"value": rate, "unit": "gate bootstraps/s", "cores": threads, "kind": "port",
-               "sample": f"{count} independent NI_8P gates ({threads} threads x {per_thread}) in {dt:.1f} s"}
+        threads, physical = host_cores()
+        count = cpu_calibrated_sample(p, key_arrays, okey_c, mix, threads, 12.0)
+        rate, count, dt = cpu_gate_sample(p, key_arrays, threads, count, mix, okey=okey_c)
+        cpu = {"value": rate, "unit": "gate bootstraps/s", "cores": threads, "physical_cores": physical,
+               "kind": "port",
+               "sample": f"{count} independent NI_8P gates in the wavefront's gate mix, {threads} threads on "
+                         f"{physical} physical cores, {dt:.1f} s"}
 
     if rank == 0:
         launches_per_step = 2 * info["levels"] + 1
@@ -935,10 +1057,12 @@ def main():
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "int", "kernel": "pbs_kernel (blind rotation)", "achieved": achieved,
                          "peak": peak, "unit": "TIMAD/s", "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": traffic_source,
                          "peak_source": "pz_probe_imad_rate on this GPU (MEASURED_PEAKS.json has no integer peak)",
                          "launch_ms": br_ms, "bootstraps_per_launch": B,
                          "modmuls_per_bootstrap": modmuls / B},
             "plain": plain,
+            "parity": parity,
             **extras,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

@@ -141,7 +141,10 @@ pz_status pz_gate_batch_device(pz_ctx *ctx, const pz_key *key, const uint8_t *d_
  * (stride = n + 1 rounded up to 32; 4096 gates at NI_8P) and larger batches
  * are rejected with PZ_ERR_INVALID_ARGUMENT.  The first call on a device
  * looks up the array's device address and should come before any stream
- * capture.  Every call shares the array: calls whose work overlaps on the
+ * capture; creating a context on the device makes the next call look it up
+ * again.  A cudaDeviceReset in the process destroys every device object of
+ * this library: release contexts and keys before it and create new ones
+ * after it.  Every call shares the array: calls whose work overlaps on the
  * GPU race and must be serialized by the caller. */
 #define PZ_NOALLOC_KS_WORDS (4096u * 672u)
 pz_status pz_gate_batch_device_noalloc(pz_ctx *ctx, const pz_key *key, const uint8_t *d_gates,
@@ -194,9 +197,19 @@ pz_status pz_ctx_set_pbs_variant(pz_ctx *ctx, int variant);
  * (-1, the default: half the GPU's SMs; 0: only if variant 3 is set). */
 pz_status pz_ctx_set_split_threshold(pz_ctx *ctx, int max_gates);
 int pz_ctx_pbs_variant(const pz_ctx *ctx);
-/* Autotuner: times every blind-rotation variant on `batch` synthetic
- * key-switched LWEs with this key and keeps the fastest for the context
- * (*ms: its time per launch). */
+/* Ciphertexts a blind-rotation launch of shape `variant` (-1: the context's
+ * current one) holds resident on the device at once: a batch that is a
+ * multiple of it runs in whole waves.  No reference counterpart (the
+ * reference runs one bootstrap per call, pbs.rs:104-233). */
+pz_status pz_ctx_pbs_slots(pz_ctx *ctx, int variant, size_t *slots);
+/* Revision tag of the blind-rotation kernels in this library (changes with
+ * their code; a profile applies to the revision it was taken on).  No
+ * reference counterpart. */
+const char *pz_kernel_revision(void);
+/* Autotuner: times every blind-rotation variant on synthetic key-switched
+ * LWEs with this key -- `batch` of them, or, from one wave up, the largest
+ * whole number of that variant's waves not above `batch` -- and keeps the
+ * fastest per ciphertext for the context (*ms: its time for `batch`). */
 pz_status pz_ctx_autotune(pz_ctx *ctx, const pz_key *key, size_t batch, int *variant, double *ms);
 
 /* ---- circuits ------------------------------------------------------------------
@@ -282,6 +295,18 @@ typedef struct pz_seeded_server_key_view {
   uint8_t lwe_ksk_seed[32];
 } pz_seeded_server_key_view;
 pz_status pz_key_upload_seeded(pz_ctx *ctx, const pz_seeded_server_key_view *key, pz_key **out);
+
+/* Seed-expansion primitives, exposed so their words can be checked against
+ * published known answers.  The reference expands seeds with rand_chacha
+ * 0.3.1's ChaCha8Rng and samples with rand 0.8.5's
+ * Uniform::new_inclusive(0, q - 1) (random.rs:93-110); the seeded key upload
+ * and the NI unseed use these same functions on the device.
+ * pz_chacha_block: the ChaCha block function (rounds 8, 12 or 20) on a full
+ * 16-word input state; out = rounds(state) + state.
+ * pz_uniform_mod_word: one 64-bit word through the uniform sampler: accepted
+ * when lo64(word q) <= 2^64 - 1 - (2^64 - q) mod q, sample = hi64(word q). */
+pz_status pz_chacha_block(const uint32_t state[16], int rounds, uint32_t out[16]);
+pz_status pz_uniform_mod_word(uint64_t q, uint64_t word, uint64_t *sample, int *accepted);
 
 /* ---- non-interactive input path (NI parameter sets, N = 2048) ---------------------
  * A user of a non-interactive session sends its bools as seeded RLWEs under its own

@@ -94,6 +94,7 @@ def lib():
             "orc_ni_gen_share": (None, [vp, u8p, ctypes.c_int, ctypes.c_int, i32p, i32p, i32p, u8p, u64p, u64p,
                                         u64p, u64p, u64p]),
             "orc_u8_op": (ctypes.c_int, [vp, vp, ctypes.c_int, u64p, u64p, u64p, u64p, u64p, u64p, ctypes.POINTER(ctypes.c_int)]),
+            "orc_u8_gate_mix": (ctypes.c_int, [vp, ctypes.c_int, u64p]),
             "orc_generate_prime": (ctypes.c_uint64, [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
             "orc_ntt_custom_new": (vp, [ctypes.c_uint64, ctypes.c_size_t]),
             "orc_ntt_custom_free": (None, [vp]),
@@ -103,6 +104,8 @@ def lib():
             "orc_decompose_custom": (ctypes.c_uint32, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, u64p]),
             "orc_round_value": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_uint32]),
             "orc_recompose": (ctypes.c_uint64, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, u64p]),
+            "orc_chacha_block": (None, [u32p, ctypes.c_int, u32p]),
+            "orc_uniform_mod_word": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, u64p]),
             "orc_rng_new": (vp, [u8p]),
             "orc_rng_free": (None, [vp]),
             "orc_rng_next_u64": (ctypes.c_uint64, [vp]),
@@ -147,6 +150,21 @@ def param_info(name_or_id):
     if lib().orc_param_info_get(pid, ctypes.byref(info)) != 0:
         raise ValueError(f"unknown parameter set {name_or_id}")
     return info
+
+
+def chacha_block(state, rounds):
+    """The ChaCha block function on a 16-word input state (out = rounds(state) + state)."""
+    s = np.ascontiguousarray(state, np.uint32)
+    out = np.zeros(16, np.uint32)
+    lib().orc_chacha_block(_p(s, u32p), int(rounds), _p(out, u32p))
+    return out
+
+
+def uniform_mod_word(q, word):
+    """rand 0.8's uniform sampler for [0, q) on one 64-bit word: (accepted, sample)."""
+    v = ctypes.c_uint64()
+    ok = lib().orc_uniform_mod_word(int(q), int(word), ctypes.byref(v))
+    return bool(ok), v.value
 
 
 class Rng:
@@ -273,6 +291,13 @@ class Evaluator:
             row = out[k]
             lib().orc_encrypt_bool(self.h, rng.h, sp, int(b), _p(row))
         return out
+
+    def u8_gate_mix(self, op):
+        """Gates the FheUint8 operation `op` issues, by gate code (and, nand,
+        or, nor, xor, xnor), from a dry run of the sequential restatement."""
+        counts = np.zeros(6, np.uint64)
+        assert lib().orc_u8_gate_mix(self.h, OracleKey.U8_OPS[op], _p(counts)) == 0
+        return counts.astype(np.int64)
 
     def decrypt_bool(self, s, cts):
         cts = np.atleast_2d(np.ascontiguousarray(cts, np.uint64))

@@ -145,6 +145,35 @@ void shoup_matrix_fma(u64 q, u64 *out, const u64 *const *a, const u64 *const *a_
 // from the published ChaCha algorithm; agreement with the Rust crate's words
 // is unpinned here (no Rust toolchain).
 // ---------------------------------------------------------------------------
+// The ChaCha block function with `rounds` rounds (RFC 8439 section 2.3 for
+// 20) on a full 16-word input state: out = rounds(s) + s.
+static inline u32 rotl32(u32 v, int c) { return (v << c) | (v >> (32 - c)); }
+void chacha_core(const u32 s[16], int rounds, u32 out[16]) {
+  u32 x[16];
+  memcpy(x, s, sizeof x);
+#define QR(a, b, c, d)                           \
+  x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 16);  \
+  x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 12);  \
+  x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 8);   \
+  x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 7);
+  for (int r = 0; r < rounds / 2; r++) {
+    QR(0, 4, 8, 12) QR(1, 5, 9, 13) QR(2, 6, 10, 14) QR(3, 7, 11, 15)
+    QR(0, 5, 10, 15) QR(1, 6, 11, 12) QR(2, 7, 8, 13) QR(3, 4, 9, 14)
+  }
+#undef QR
+  for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
+}
+
+// rand 0.8 UniformInt<u64>::new_inclusive(0, q-1) + sample (random.rs:93-110):
+// one word v, accepted when lo64(v q) <= zone = MAX - (2^64 - q) mod q; the
+// sample is hi64(v q).
+inline bool uniform_word(u64 v, u64 q, u64 &sample) {
+  const u64 zone = UINT64_MAX - ((0ull - q) % q);
+  const u128 m = (u128)v * q;
+  sample = (u64)(m >> 64);
+  return (u64)m <= zone;
+}
+
 struct ChaCha8 {
   u32 key[8];
   u64 counter = 0;
@@ -155,24 +184,12 @@ struct ChaCha8 {
       key[i] = (u32)seed[4 * i] | ((u32)seed[4 * i + 1] << 8) | ((u32)seed[4 * i + 2] << 16) |
                ((u32)seed[4 * i + 3] << 24);
   }
-  static inline u32 rotl(u32 v, int c) { return (v << c) | (v >> (32 - c)); }
   void block() {
-    u32 x[16], s[16];
+    u32 s[16];
     s[0] = 0x61707865u; s[1] = 0x3320646eu; s[2] = 0x79622d32u; s[3] = 0x6b206574u;
     for (int i = 0; i < 8; i++) s[4 + i] = key[i];
     s[12] = (u32)counter; s[13] = (u32)(counter >> 32); s[14] = 0; s[15] = 0;
-    memcpy(x, s, sizeof x);
-#define QR(a, b, c, d)                         \
-  x[a] += x[b]; x[d] = rotl(x[d] ^ x[a], 16);  \
-  x[c] += x[d]; x[b] = rotl(x[b] ^ x[c], 12);  \
-  x[a] += x[b]; x[d] = rotl(x[d] ^ x[a], 8);   \
-  x[c] += x[d]; x[b] = rotl(x[b] ^ x[c], 7);
-    for (int r = 0; r < 4; r++) {
-      QR(0, 4, 8, 12) QR(1, 5, 9, 13) QR(2, 6, 10, 14) QR(3, 7, 11, 15)
-      QR(0, 5, 10, 15) QR(1, 6, 11, 12) QR(2, 7, 8, 13) QR(3, 4, 9, 14)
-    }
-#undef QR
-    for (int i = 0; i < 16; i++) buf[i] = x[i] + s[i];
+    chacha_core(s, 8, buf);
     counter++;
     idx = 0;
   }
@@ -188,14 +205,9 @@ struct ChaCha8 {
   // rand 0.8 UniformInt<u64>::new_inclusive(0, q-1) + sample (widening
   // multiply with rejection zone), random.rs:93-110.
   u64 uniform_mod(u64 q) {
-    u64 range = q;
-    u64 ints_to_reject = (UINT64_MAX - range + 1) % range;
-    u64 zone = UINT64_MAX - ints_to_reject;
     for (;;) {
-      u64 v = next_u64();
-      u128 m = (u128)v * range;
-      u64 hi = (u64)(m >> 64), lo = (u64)m;
-      if (lo <= zone) return hi;
+      u64 sample;
+      if (uniform_word(next_u64(), q, sample)) return sample;
     }
   }
   // Uniform::new(0, m) for usize (exclusive upper bound).
@@ -745,12 +757,14 @@ void gate(const Eval &e, const Key &k, Scratch &sc, int g, u64 *c0, const u64 *c
 typedef std::vector<u64> Ct;
 struct SEval {
   const Eval &e;
-  const Key &k;
+  const Key *k;  // null: a dry run that only tallies the gates (no bootstrap)
   Scratch sc;
-  SEval(const Eval &e_, const Key &k_) : e(e_), k(k_), sc(e_) {}
+  uint64_t *tally = nullptr;  // gates issued, by gate code
+  SEval(const Eval &e_, const Key *k_) : e(e_), k(k_), sc(e_) {}
   Ct g(int t, const Ct &a, const Ct &b) {  // gate(a, b): BooleanGates::* (evaluator.rs:2252-2316)
+    if (tally) tally[t]++;
     Ct out = a;
-    gate(e, k, sc, t, out.data(), b.data());
+    if (k) gate(e, *k, sc, t, out.data(), b.data());
     return out;
   }
   Ct not_(const Ct &a) {  // evaluator.rs:2318-2322
@@ -1048,10 +1062,9 @@ void orc_sample_extract(void *ev, const uint64_t *rlwe, uint64_t *lwe, uint32_t 
 // 12 overflowing_sub.  out: [8][N+1] or, for comparisons, [1][N+1]; out2:
 // remainder (div_rem) or overflow flag.  flag (div_rem): in/out division by
 // zero flag; *flag_set says whether it holds a ciphertext.
-int orc_u8_op(void *ev, void *key, int op, const uint64_t *a, const uint64_t *b, const uint64_t *sel,
-              uint64_t *out, uint64_t *out2, uint64_t *flag, int *flag_set) {
-  Eval &e = *(Eval *)ev;
-  SEval s(e, *(Key *)key);
+static int u8_op(SEval &s, int op, const uint64_t *a, const uint64_t *b, const uint64_t *sel, uint64_t *out,
+                 uint64_t *out2, uint64_t *flag, int *flag_set) {
+  const Eval &e = s.e;
   const size_t L = e.N + 1;
   std::vector<Ct> A(8), Bv(8);
   for (int i = 0; i < 8; i++) {
@@ -1107,6 +1120,25 @@ int orc_u8_op(void *ev, void *key, int op, const uint64_t *a, const uint64_t *b,
     }
   }
   return -1;
+}
+
+int orc_u8_op(void *ev, void *key, int op, const uint64_t *a, const uint64_t *b, const uint64_t *sel,
+              uint64_t *out, uint64_t *out2, uint64_t *flag, int *flag_set) {
+  SEval s(*(Eval *)ev, (const Key *)key);
+  return u8_op(s, op, a, b, sel, out, out2, flag, flag_set);
+}
+
+// Gates one FheUint8 operation issues, by gate code (and, nand, or, nor, xor,
+// xnor): the operation run dry on zero ciphertexts, nothing bootstrapped.
+int orc_u8_gate_mix(void *ev, int op, uint64_t counts[6]) {
+  const Eval &e = *(Eval *)ev;
+  const size_t L = e.N + 1;
+  std::vector<uint64_t> a(8 * L, 0), b(8 * L, 0), sel(L, 0), out(8 * L), out2(8 * L), flag(L, 0);
+  for (int t = 0; t < 6; t++) counts[t] = 0;
+  SEval s(e, nullptr);
+  s.tally = counts;
+  int fs = 0;
+  return u8_op(s, op, a.data(), b.data(), sel.data(), out.data(), out2.data(), flag.data(), &fs);
 }
 
 // ---- generic pins (reference unit tests at their own sizes) -----------------
@@ -1171,6 +1203,8 @@ uint64_t orc_recompose(uint64_t q, uint32_t logb, uint32_t d, const uint64_t *li
 }
 
 // ---- client harness --------------------------------------------------------
+void orc_chacha_block(const uint32_t state[16], int rounds, uint32_t out[16]) { chacha_core(state, rounds, out); }
+int orc_uniform_mod_word(uint64_t q, uint64_t word, uint64_t *sample) { return uniform_word(word, q, *sample); }
 void *orc_rng_new(const uint8_t seed[32]) { return new ChaCha8(seed); }
 void orc_rng_free(void *r) { delete (ChaCha8 *)r; }
 uint64_t orc_rng_next_u64(void *r) { return ((ChaCha8 *)r)->next_u64(); }

@@ -105,6 +105,9 @@ void orc_negacyclic_mul(uint64_t q, const uint64_t *a, const uint64_t *b,
  * 12 overflowing_sub.  a, b, out, out2: [8][N+1]; comparisons write [1][N+1]. */
 int orc_u8_op(void *ev, void *key, int op, const uint64_t *a, const uint64_t *b, const uint64_t *sel,
               uint64_t *out, uint64_t *out2, uint64_t *flag, int *flag_set);
+/* The gates operation `op` issues, tallied by gate code (and, nand, or, nor,
+ * xor, xnor) without bootstrapping anything (a dry run on zero ciphertexts). */
+int orc_u8_gate_mix(void *ev, int op, uint64_t counts[6]);
 
 /* generic pins: the reference's unit tests at their own sizes */
 uint64_t orc_generate_prime(uint32_t num_bits, uint64_t modulo, uint64_t upper_bound);
@@ -157,6 +160,11 @@ void orc_ni_key_switch(void *ev, const uint64_t *ksk, const uint64_t *in, uint64
 
 /* --- client-side harness (reference runs this on clients; out of scope) -------- */
 /* ChaCha8 stream (rand_chacha 0.3 layout), for seeding */
+/* ChaCha block function with `rounds` rounds on a full 16-word input state
+ * (out = rounds(state) + state), and one word through rand 0.8's uniform
+ * sampler for [0, q) (returns 1 when accepted; *sample = hi64(word q)). */
+void orc_chacha_block(const uint32_t state[16], int rounds, uint32_t out[16]);
+int orc_uniform_mod_word(uint64_t q, uint64_t word, uint64_t *sample);
 void *orc_rng_new(const uint8_t seed[32]);
 void orc_rng_free(void *rng);
 uint64_t orc_rng_next_u64(void *rng);

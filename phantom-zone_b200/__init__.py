@@ -7,8 +7,10 @@ declared in include/phantom_zone_b200.h; this package is the Python host side
 interface.  Import it with ``importlib.import_module("phantom-zone_b200")``.
 """
 from . import _lib
-from .engine import GATES, PARAMETER_SETS, SELECTORS, DeviceKey, Engine, param_id, params, probe_imad_rate
+from .engine import (GATES, PARAMETER_SETS, SELECTORS, DeviceKey, Engine, kernel_revision, param_id, params,
+                     probe_imad_rate)
 from .circuits import Circuit
 from .server import DRY_RUN, Server
 
-__all__ = ["Circuit", "Server", "DRY_RUN", "Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "param_id", "params", "probe_imad_rate", "_lib"]
+__all__ = ["Circuit", "Server", "DRY_RUN", "Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "kernel_revision", "param_id", "params",
+           "probe_imad_rate", "_lib"]

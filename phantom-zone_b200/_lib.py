@@ -86,6 +86,11 @@ SIGNATURES = {
     "pz_ctx_set_pbs_grid_limit": (st, [vp, ctypes.c_int]),
     "pz_ctx_set_pbs_variant": (st, [vp, ctypes.c_int]),
     "pz_ctx_pbs_variant": (ctypes.c_int, [vp]),
+    "pz_ctx_pbs_slots": (st, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "pz_kernel_revision": (ctypes.c_char_p, []),
+    "pz_chacha_block": (st, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),
+    "pz_uniform_mod_word": (st, [ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                 ctypes.POINTER(ctypes.c_int)]),
     "pz_ni_ksk_upload": (st, [vp, u64p, ctypes.POINTER(vp)]),
     "pz_ni_ksk_release": (None, [vp]),
     "pz_ni_ksk_upload_seeded": (st, [vp, u64p, u8p, ctypes.POINTER(vp)]),

@@ -39,6 +39,9 @@ struct pz_circuit {
   std::string err;
   // compiled schedule (host)
   bool compiled = false;
+  // structure version: bumped by every added input, gate or output; the
+  // device buffers and a captured graph belong to bound_version
+  uint64_t version = 0, bound_version = ~0ull;
   std::vector<size_t> level_off;  // levels + 1 offsets into the per-gate arrays
   std::vector<unsigned char> h_type;
   std::vector<u32> h_in0, h_in1, h_out, h_outref;
@@ -55,8 +58,12 @@ struct pz_circuit {
   u32 new_wire(u32 gate, u32 input) {
     wire_gate.push_back(gate);
     wire_input.push_back(input);
-    compiled = false;
+    touch();
     return (u32)(wire_gate.size() - 1);
+  }
+  void touch() {
+    compiled = false;
+    version++;
   }
   bool valid(u32 ref) const { return ref != NONE && (ref & pz::WIRE_MASK) < wire_gate.size(); }
   u32 input() { return new_wire(NONE, (u32)n_inputs++); }
@@ -75,6 +82,7 @@ struct pz_circuit {
     d_wires = nullptr; d_type = nullptr; d_in0 = d_in1 = d_out = d_outref = d_ks = nullptr;
     wire_cap = 0;
     dev_ctx = nullptr;
+    bound_version = ~0ull;
   }
   ~pz_circuit() { free_device(); }
 };
@@ -307,9 +315,12 @@ __global__ void gather_kernel(const u64 *wires, const u32 *refs, u64 *out, size_
   }
 }
 
+// Device buffers sized for the circuit as it is now.  A circuit that gained
+// inputs, gates or outputs since it was bound is re-uploaded (its old buffers
+// and any captured graph are released).
 pz_status bind_device(pz_ctx *ctx, pz_circuit *c) {
   compile(c);
-  if (c->dev_ctx == ctx && c->d_type) return PZ_OK;
+  if (c->dev_ctx == ctx && c->d_type && c->bound_version == c->version) return PZ_OK;
   c->free_device();
   const size_t G = c->gates.size(), L = (size_t)ctx->P.rlwe_n + 1;
   const size_t W = c->n_inputs + G;
@@ -330,6 +341,7 @@ pz_status bind_device(pz_ctx *ctx, pz_circuit *c) {
     PZ_CK(ctx, cudaMemcpy(c->d_outref, c->h_outref.data(), c->outputs.size() * 4, cudaMemcpyHostToDevice));
   c->wire_cap = W;
   c->dev_ctx = ctx;
+  c->bound_version = c->version;
   return PZ_OK;
 }
 
@@ -396,7 +408,7 @@ uint32_t pz_circuit_not(pz_circuit *c, uint32_t a) { return (c && c->valid(a)) ?
 pz_status pz_circuit_output(pz_circuit *c, uint32_t w) {
   if (!c || !c->valid(w)) return circ_fail(c, "invalid wire");
   c->outputs.push_back(w);
-  c->compiled = false;
+  c->touch();
   return PZ_OK;
 }
 
@@ -578,6 +590,7 @@ pz_status pz_circuit_run_device(pz_ctx *ctx, const pz_key *k, pz_circuit *c, con
   if (!k || k->ctx != ctx) return pz::fail(ctx, PZ_ERR_KEY_MISMATCH, "key does not belong to this context");
   if ((c->n_inputs && !d_inputs) || (!c->outputs.empty() && !d_outputs))
     return pz::fail(ctx, PZ_ERR_INVALID_ARGUMENT, "NULL circuit buffer");
+  std::lock_guard<std::mutex> lock(ctx->mu);
   PZ_CK(ctx, cudaSetDevice(ctx->device));
   pz_status s = bind_device(ctx, c);
   if (s != PZ_OK) return s;
@@ -614,6 +627,7 @@ pz_status pz_circuit_capture_graph(pz_ctx *ctx, const pz_key *k, pz_circuit *c, 
                                    uint64_t *d_outputs, void *stream) {
   if (!ctx || !c) return PZ_ERR_INVALID_ARGUMENT;
   if (!k || k->ctx != ctx) return pz::fail(ctx, PZ_ERR_KEY_MISMATCH, "key does not belong to this context");
+  std::lock_guard<std::mutex> lock(ctx->mu);
   PZ_CK(ctx, cudaSetDevice(ctx->device));
   pz_status s = bind_device(ctx, c);
   if (s != PZ_OK) return s;
@@ -642,6 +656,7 @@ pz_status pz_circuit_capture_graph(pz_ctx *ctx, const pz_key *k, pz_circuit *c, 
 
 pz_status pz_circuit_replay_graph(pz_circuit *c, void *stream) {
   if (!c || !c->graph_exec || !c->dev_ctx) return circ_fail(c, "no captured graph");
+  if (c->bound_version != c->version) return circ_fail(c, "circuit changed since its graph was captured");
   cudaError_t e = cudaGraphLaunch(c->graph_exec, (cudaStream_t)stream);
   if (e != cudaSuccess) return pz::cuda_fail(c->dev_ctx, "cudaGraphLaunch", e);
   return PZ_OK;

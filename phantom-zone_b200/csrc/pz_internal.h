@@ -56,6 +56,8 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
                     u64 *d_out, size_t count, u32 *d_ks_out, u64 *d_rlwe, cudaStream_t s, u32 *d_ks_scratch,
                     bool raw, const u32 *in0 = nullptr, const u32 *in1 = nullptr, const u32 *out_idx = nullptr);
 pz_status fail(pz_ctx *ctx, pz_status s, const std::string &msg);
+// forget the no-alloc scratch address cached for a device (pz_noalloc.cu)
+void noalloc_forget_device(int device);
 pz_status cuda_fail(pz_ctx *ctx, const char *what, cudaError_t e);
 u32 ks_stride(const pz_params &P);
 // DefaultDecomposer parameters for (q, logb, d) (decomposer.rs:158-178)

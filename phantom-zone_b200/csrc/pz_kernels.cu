@@ -1186,6 +1186,37 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
   return cudaGetLastError();
 }
 
+// Items a blind-rotation launch holds resident at once on the current device
+// with launch shape `variant` (CTAs per SM from the occupancy calculator x
+// SMs; one item per two-CTA cluster for the split shape).  A batch that is a
+// multiple of this runs in whole waves.
+cudaError_t pbs_slots(int logn, bool d1, u32 br_q, u32 n, int variant, size_t *slots) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const size_t smem = pbs_smem_bytes(logn, br_q, n);
+  size_t div = 1;
+#define PZ_OCC(K, TH, SM)                                                                 \
+  if ((e = set_smem(K, SM)) != cudaSuccess) return e;                                      \
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, K, TH, SM);
+  if (logn == 11 && d1 && variant == PBS_SPLIT) {
+    PZ_OCC(pbs_split_kernel<11>, 256, split_smem_bytes(br_q, n))
+    div = 2;
+  } else if (logn == 11 && d1) {
+    if (variant == 0) { PZ_OCC((pbs_kernel<11, true, 2>), 256, smem) }
+    else if (variant == 1) { PZ_OCC((pbs_kernel<11, true, 3>), 256, smem) }
+    else { PZ_OCC((pbs_kernel<11, true, 4>), 256, smem) }
+  } else if (logn == 11) { PZ_OCC((pbs_kernel<11, false, 1>), 256, smem) }
+  else if (logn == 9 && d1) { PZ_OCC((pbs_kernel<9, true, 1>), 64, smem) }
+  else if (logn == 9) { PZ_OCC((pbs_kernel<9, false, 1>), 64, smem) }
+  else return cudaErrorInvalidValue;
+#undef PZ_OCC
+  if (e != cudaSuccess) return e;
+  *slots = std::max<size_t>((size_t)per_sm * sms / div, 1);
+  return cudaSuccess;
+}
+
 cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,
                              u32 max_n, u32 max_N, u32 max_d, const unsigned char *gates, const u64 *wires,
                              const u32 *in0, const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s) {

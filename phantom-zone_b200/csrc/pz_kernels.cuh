@@ -5,6 +5,9 @@
 namespace pz {
 
 constexpr int MAX_KS_D = 16;   // key-switch decomposition count bound
+// Revision of the blind-rotation kernels: bumped with every change to their
+// code, so that a profile taken on one revision is not reported for another.
+constexpr const char *BR_KERNEL_REVISION = "br-v8";
 constexpr int MAX_AUTO_SLOTS = 16;
 
 // Everything the blind rotation needs for one parameter set + server key.
@@ -88,5 +91,7 @@ cudaError_t launch_not(const u64 *in, u64 *out, size_t words, u64 q, cudaStream_
 cudaError_t launch_imad_probe(int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s);
 // per launch: blocks * threads * iters * 16 * 8 multiply-adds
 size_t pbs_smem_bytes(int logn, u32 br_q, u32 n);
+// blind-rotation items resident at once for a launch shape (whole-wave size)
+cudaError_t pbs_slots(int logn, bool d1, u32 br_q, u32 n, int variant, size_t *slots);
 
 }  // namespace pz

@@ -35,6 +35,7 @@ namespace {
 
 using pz::ni::ChaChaKey;
 using pz::ni::chacha8_block;
+using pz::ni::uniform_from_word;
 using pz::ni::ni_mac;
 using pz::ni::NI_LOGN;
 using pz::ni::NI_T;
@@ -59,9 +60,9 @@ __global__ void unseed_candidates_kernel(const __grid_constant__ ChaChaKeys keys
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const u64 v = (u64)w[2 * i] | ((u64)w[2 * i + 1] << 32);
-      const u64 lo = v * q, hi = __umul64hi(v, q);
-      samples[8 * (base + b) + i] = hi;
-      if (lo <= zone) m |= 1u << i;
+      u64 sample;
+      if (uniform_from_word(v, q, zone, sample)) m |= 1u << i;
+      samples[8 * (base + b) + i] = sample;
     }
     accept[base + b] = (unsigned char)m;
     cnt[base + b] = __popc(m);
@@ -297,8 +298,7 @@ pz_status seeded_fill(pz_ctx *c, const uint8_t (*seeds)[32], size_t streams, u64
   if (total == 0 || streams == 0) return PZ_OK;
   const u64 nblocks = (total + UNSEED_MARGIN + 7) / 8;
   const size_t group = std::min<size_t>(streams, FILL_STREAMS);
-  // rand 0.8 UniformInt<u64>::new_inclusive(0, q - 1): range q, zone = MAX - (2^64 - q) % q
-  const u64 zone = ~0ull - ((0ull - q) % q);
+  const u64 zone = pz::ni::uniform_zone(q);  // rand 0.8 UniformInt::new_inclusive(0, q - 1)
   // one scratch allocation: samples | off | totals | cnt | accept
   const size_t b_samples = group * nblocks * 64, b_off = group * (nblocks + 1) * 8, b_tot = group * 8,
                b_cnt = group * nblocks * 4, b_acc = group * nblocks;
@@ -353,6 +353,28 @@ pz_status seeded_fill_batch_u64(pz_ctx *c, const uint8_t (*seeds)[32], size_t st
 }  // namespace pz
 
 extern "C" {
+
+pz_status pz_chacha_block(const uint32_t state[16], int rounds, uint32_t out[16]) {
+  if (!state || !out) return PZ_ERR_INVALID_ARGUMENT;
+  u32 s[16], o[16];
+  for (int i = 0; i < 16; i++) s[i] = state[i];
+  switch (rounds) {
+    case 8: pz::ni::chacha_core<8>(s, o); break;
+    case 12: pz::ni::chacha_core<12>(s, o); break;
+    case 20: pz::ni::chacha_core<20>(s, o); break;
+    default: return PZ_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < 16; i++) out[i] = o[i];
+  return PZ_OK;
+}
+
+pz_status pz_uniform_mod_word(uint64_t q, uint64_t word, uint64_t *sample, int *accepted) {
+  if (q == 0 || !sample || !accepted) return PZ_ERR_INVALID_ARGUMENT;
+  u64 v = 0;
+  *accepted = pz::ni::uniform_from_word(word, q, pz::ni::uniform_zone(q), v) ? 1 : 0;
+  *sample = v;
+  return PZ_OK;
+}
 
 pz_status pz_ni_ksk_upload(pz_ctx *c, const uint64_t *ksk, pz_ni_ksk **out) {
   pz_status s = ni_check(c);

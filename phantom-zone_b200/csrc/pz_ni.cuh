@@ -30,14 +30,13 @@ inline ChaChaKey chacha_key(const uint8_t seed[32]) {
 
 __host__ __device__ __forceinline__ u32 rotl32(u32 v, int c) { return (v << c) | (v >> (32 - c)); }
 
-// ChaCha8 block `counter` in the rand_chacha 0.3 layout (constants, 8 key
-// words, 64-bit block counter, stream id 0); 16 output words.
-__host__ __device__ __forceinline__ void chacha8_block(const ChaChaKey &key, u64 counter, u32 (&out)[16]) {
-  u32 s[16], x[16];
-  s[0] = 0x61707865u; s[1] = 0x3320646eu; s[2] = 0x79622d32u; s[3] = 0x6b206574u;
-PZ_HD_UNROLL
-  for (int i = 0; i < 8; i++) s[4 + i] = key.k[i];
-  s[12] = (u32)counter; s[13] = (u32)(counter >> 32); s[14] = 0; s[15] = 0;
+// The ChaCha block function (the published algorithm, as RFC 8439 section
+// 2.3 states it for 20 rounds) on a full 16-word input state: ROUNDS / 2
+// double rounds, then the input added word by word.
+template <int ROUNDS>
+__host__ __device__ __forceinline__ void chacha_core(const u32 (&s)[16], u32 (&out)[16]) {
+  static_assert(ROUNDS % 2 == 0, "double rounds");
+  u32 x[16];
 PZ_HD_UNROLL
   for (int i = 0; i < 16; i++) x[i] = s[i];
 #define PZ_QR(a, b, c, d)                              \
@@ -46,13 +45,38 @@ PZ_HD_UNROLL
   x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 8);         \
   x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 7);
 PZ_HD_UNROLL
-  for (int r = 0; r < 4; r++) {
+  for (int r = 0; r < ROUNDS / 2; r++) {
     PZ_QR(0, 4, 8, 12) PZ_QR(1, 5, 9, 13) PZ_QR(2, 6, 10, 14) PZ_QR(3, 7, 11, 15)
     PZ_QR(0, 5, 10, 15) PZ_QR(1, 6, 11, 12) PZ_QR(2, 7, 8, 13) PZ_QR(3, 4, 9, 14)
   }
 #undef PZ_QR
 PZ_HD_UNROLL
   for (int i = 0; i < 16; i++) out[i] = x[i] + s[i];
+}
+
+// ChaCha8 block `counter` in the rand_chacha 0.3 layout (constants, 8 key
+// words, 64-bit block counter in words 12-13, stream id 0 in words 14-15);
+// 16 output words, consumed low word first by rand_core's BlockRng.
+__host__ __device__ __forceinline__ void chacha8_block(const ChaChaKey &key, u64 counter, u32 (&out)[16]) {
+  u32 s[16];
+  s[0] = 0x61707865u; s[1] = 0x3320646eu; s[2] = 0x79622d32u; s[3] = 0x6b206574u;
+PZ_HD_UNROLL
+  for (int i = 0; i < 8; i++) s[4 + i] = key.k[i];
+  s[12] = (u32)counter; s[13] = (u32)(counter >> 32); s[14] = 0; s[15] = 0;
+  chacha_core<8>(s, out);
+}
+
+// rand 0.8's UniformInt<u64> built by new_inclusive(0, q - 1) and sampled
+// (the fill of random.rs:93-110): zone = MAX - (2^64 - q) mod q; a 64-bit
+// word v is accepted when lo64(v q) <= zone, and the sample is hi64(v q).
+__host__ __device__ __forceinline__ u64 uniform_zone(u64 q) { return ~0ull - ((0ull - q) % q); }
+__host__ __device__ __forceinline__ bool uniform_from_word(u64 v, u64 q, u64 zone, u64 &sample) {
+#ifdef __CUDA_ARCH__
+  sample = __umul64hi(v, q);
+#else
+  sample = (u64)(((unsigned __int128)v * q) >> 64);
+#endif
+  return v * q <= zone;
 }
 
 // oa += REDC(x ka + y kc), ob += REDC(x kb + y kd), lazily in [0, 2q); the

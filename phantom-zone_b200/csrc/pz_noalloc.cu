@@ -30,6 +30,19 @@ std::mutex g_mu;
 pz::u32 *g_addr[MAX_DEVICES] = {};
 }  // namespace
 
+namespace pz {
+// Drop the cached device address of the array on `device`; the next
+// no-alloc call there looks it up again.  Called whenever a context is
+// created: a cudaDeviceReset destroys every device object of this library
+// (contexts and keys included), and a context created afterwards must not
+// reuse an address resolved in the old CUDA context.
+void noalloc_forget_device(int device) {
+  if (device < 0 || device >= MAX_DEVICES) return;
+  std::lock_guard<std::mutex> lock(g_mu);
+  g_addr[device] = nullptr;
+}
+}  // namespace pz
+
 extern "C" pz_status pz_gate_batch_device_noalloc(pz_ctx *c, const pz_key *k, const uint8_t *d_gates,
                                                   const uint64_t *d_c0, const uint64_t *d_c1, uint64_t *d_out,
                                                   size_t count, void *stream) {
@@ -48,8 +61,9 @@ extern "C" pz_status pz_gate_batch_device_noalloc(pz_ctx *c, const pz_key *k, co
   PZ_CK(c, cudaSetDevice(c->device));
   pz::u32 *scratch = nullptr;
   {
-    // First call on a device: resolve the array's device address with that
-    // device current (the host-side symbol is not a device address).
+    // First call on a device (since the last context creation there):
+    // resolve the array's device address with that device current (the
+    // host-side symbol is not a device address).
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_addr[c->device]) {
       void *p = nullptr;

@@ -252,6 +252,7 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   if (!out) return PZ_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   if (id < 0 || id >= PZ_NUM_PARAMS) return PZ_ERR_INVALID_ARGUMENT;
+  pz::noalloc_forget_device(device);
   pz_ctx *c = new pz_ctx();
   c->param_id = id;
   c->device = device;
@@ -635,8 +636,14 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
   double best = 1e30;
   int bv = c->pbs_variant;
   for (int v = 0; v < nv && e == cudaSuccess; v++) {
+    // a batch of at least one wave is timed in whole waves of this shape (a
+    // partial last wave would charge the shape for the batch's remainder):
+    // the largest multiple of the shape's resident items not above the batch
+    size_t slots = 1, items = batch;
+    if ((e = pz::pbs_slots((int)c->logn, d1, c->P.br_q, c->P.lwe_n, v, &slots)) != cudaSuccess) break;
+    if (batch >= slots) items = batch / slots * slots;
     auto launch = [&]() {
-      return pz::launch_pbs((int)c->logn, d1, br, d_ks, cols, d_g, d_out, batch, nullptr, c->grid_limit, c->stream, v);
+      return pz::launch_pbs((int)c->logn, d1, br, d_ks, cols, d_g, d_out, items, nullptr, c->grid_limit, c->stream, v);
     };
     if ((e = launch()) != cudaSuccess) break;  // warm-up
     if ((e = cudaEventRecord(a, c->stream)) != cudaSuccess) break;
@@ -645,8 +652,9 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
     if (e == cudaSuccess) e = cudaEventSynchronize(b);
     float t = 0;
     if (e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
-    if (e == cudaSuccess && t / 2 < best) {
-      best = t / 2;
+    const double per_batch = t / 2.0 / (double)items * (double)batch;
+    if (e == cudaSuccess && per_batch < best) {
+      best = per_batch;
       bv = v;
     }
   }
@@ -659,6 +667,18 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
   c->pbs_variant = bv;
   if (variant) *variant = bv;
   if (ms) *ms = best;
+  return PZ_OK;
+}
+
+const char *pz_kernel_revision(void) { return pz::BR_KERNEL_REVISION; }
+
+pz_status pz_ctx_pbs_slots(pz_ctx *c, int variant, size_t *slots) {
+  if (!c || !slots) return PZ_ERR_INVALID_ARGUMENT;
+  if (variant < 0) variant = c->pbs_variant;
+  if (variant > pz::PBS_SPLIT) return fail(c, PZ_ERR_INVALID_ARGUMENT, "unknown launch shape");
+  PZ_CK(c, cudaSetDevice(c->device));
+  const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
+  PZ_CK(c, pz::pbs_slots((int)c->logn, d1, c->P.br_q, c->P.lwe_n, variant, slots));
   return PZ_OK;
 }
 

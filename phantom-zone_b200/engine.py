@@ -48,6 +48,12 @@ def probe_imad_rate(device=0):
     return v.value
 
 
+def kernel_revision():
+    """Revision tag of the blind-rotation kernel in the loaded library (a
+    profile on record applies only to the revision it was taken on)."""
+    return lib().pz_kernel_revision().decode()
+
+
 def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
@@ -183,6 +189,13 @@ class Engine:
     @pbs_variant.setter
     def pbs_variant(self, v):
         check(lib().pz_ctx_set_pbs_variant(self.h, int(v)), self.h, "set_pbs_variant")
+
+    def pbs_slots(self, variant=-1):
+        """Ciphertexts a blind-rotation launch of shape `variant` (-1: the
+        current one) holds resident at once; multiples run in whole waves."""
+        n = ctypes.c_size_t()
+        check(lib().pz_ctx_pbs_slots(self.h, int(variant), ctypes.byref(n)), self.h, "pz_ctx_pbs_slots")
+        return n.value
 
     def autotune(self, key, batch=2368):
         """Pick the fastest blind-rotation variant for this context on `batch` gates."""

@@ -199,3 +199,51 @@ def test_mul_and_lt_multi_party_decryption(gpu_available, param):
         bits = ev.mp_decrypt_bool(r, sp, out)
         assert sum(int(v) << i for i, v in enumerate(bits[:8])) == (x * y) % 256
         assert int(bits[8]) == int(x < y)
+
+
+def test_circuit_grown_after_a_run_is_rebound(gpu_available):
+    """A circuit that gains inputs, gates and outputs after it ran (and after
+    its graph was captured) is re-uploaded on its next run: the stale graph is
+    refused, and every output of the grown circuit equals the oracle's gate
+    evaluation, word for word."""
+    import torch
+    param = "SP_TEST"
+    ev, (s, _, _, _), _, okey = oracle_setup(param)
+    eng, key = eng_key(param)
+    r = oracle().Rng(b"\x0b" * 32)
+    bits = [1, 0, 1, 1, 0]
+    cts = ev.encrypt_bool(r, s, bits)
+    C = pz().Circuit()
+    a, b = C.input(), C.input()
+    w0 = C.gate("nand", a, b)
+    C.output(w0)
+    first = C.run(eng, key, cts[:2])
+    assert np.array_equal(first[0], okey.gate("nand", cts[0], cts[1]))
+    d_in = to_dev(cts[:2])
+    d_out = to_dev(np.zeros((1, ev.L), np.uint64))
+    C.capture_graph(eng, key, d_in, d_out)
+    # grow: three more inputs, gates reading old and new wires, two more outputs
+    c, d, e = C.input(), C.input(), C.input()
+    w1 = C.gate("xor", w0, c)
+    w2 = C.gate("or", C.not_(w1), d)
+    w3 = C.gate("and", w2, e)
+    C.output(w1)
+    C.output(w3)
+    with pytest.raises(RuntimeError):
+        C.replay_graph()
+    got = C.run(eng, key, cts)
+    v0 = okey.gate("nand", cts[0], cts[1])
+    v1 = okey.gate("xor", v0, cts[2])
+    v2 = okey.gate("or", ev.not_(v1), cts[3])
+    v3 = okey.gate("and", v2, cts[4])
+    assert np.array_equal(got, np.stack([v0, v1, v3]))
+    # the device path binds the grown circuit too
+    d_in = to_dev(cts)
+    d_out = to_dev(np.zeros((3, ev.L), np.uint64))
+    C.run_device(eng, key, d_in, d_out)
+    torch.cuda.synchronize()
+    assert np.array_equal(to_host(d_out).reshape(3, ev.L), got)
+    truth = [1 - (bits[0] & bits[1])]
+    truth.append(truth[0] ^ bits[2])
+    truth.append(((1 - truth[1]) | bits[3]) & bits[4])
+    assert list(ev.decrypt_bool(s, got)) == truth

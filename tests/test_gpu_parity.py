@@ -249,3 +249,24 @@ def test_split_kernel_many_items_per_cluster(gpu_available):
         eng.set_pbs_grid_limit(0)
     assert np.array_equal(outs[0], outs[1])
     assert np.array_equal(outs[1][:3], okey.gate_batch(gates[:3], c0[:3], c1[:3], threads=3))
+
+
+def test_pbs_slots_whole_waves(gpu_available):
+    """pz_ctx_pbs_slots: every launch shape reports its resident ciphertexts
+    (a multiple of the SM count for the one-CTA shapes, more CTAs per SM for
+    tighter register caps), and the autotuner times whole waves of them."""
+    import torch
+    eng, dkey = engine_and_key("NI_8P")
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    slots = [eng.pbs_slots(v) for v in range(4)]
+    assert all(s > 0 for s in slots)
+    for v in range(3):
+        assert slots[v] % sms == 0
+    assert slots[0] <= slots[1] <= slots[2]
+    assert eng.pbs_slots(-1) == slots[eng.pbs_variant]
+    old = eng.pbs_variant
+    try:
+        t = eng.autotune(dkey, 2 * slots[2])
+        assert t["variant"] in (0, 1, 2, 3) and t["ms"] > 0
+    finally:
+        eng.pbs_variant = old

@@ -81,13 +81,14 @@ def expect(op, ev, s, out, x, y):
 
 @pytest.mark.parametrize("policy", [0, 1])
 def test_ragged_mixed_parameter_sets(gpu_available, policy):
-    """One step mixes I_2P, I_4P and NI_8P sessions (n = 580/620/660, d_ks =
-    12/13/14, br_q = 2^11/2^11/2^12) running add, lt and div_rem (divisor 0
-    in one job); every output equals the job run alone and decrypts right,
-    under both step schedules (all ready levels; critical path first)."""
+    """One step mixes I_2P, I_4P, I_8P and NI_8P sessions (n = 580/620/660/660,
+    d_ks = 12/13/14/14, br_q = 2^11/2^11/2^12/2^12) running add, lt and
+    div_rem (divisor 0 in one job); every output equals the job run alone and
+    decrypts right, under both step schedules (all ready levels; critical path
+    first)."""
     P = pz()
-    params = ["I_2P_LB_SR", "I_4P", "NI_8P"]
-    S = P.Server(device=0, arena_bytes=1 << 28, max_items=4096)
+    params = ["I_2P_LB_SR", "I_4P", "I_8P", "NI_8P"]
+    S = P.Server(device=0, arena_bytes=1 << 29, max_items=4096)
     S.set_schedule(policy)
     sids = {p: S.add_session(*session(p)[:2]) for p in params}
     rng = np.random.default_rng(3)

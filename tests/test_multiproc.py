@@ -54,7 +54,7 @@ def test_reference_arm_under_torchrun_two_ranks():
     env = dict(os.environ, OMP_NUM_THREADS="1")
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), os.path.join(ROOT, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--ref-step-seconds", "0.5"]
     out = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
@@ -62,3 +62,28 @@ def test_reference_arm_under_torchrun_two_ranks():
     rec = json.loads(lines[0])
     assert rec["impl"] == "reference" and rec["n_gpus"] == 2 and rec["value"] > 0
     assert rec["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_reference_arm_never_loads_the_product():
+    """The reference arm times the oracle only: after a run, neither the
+    product package nor its shared library is in the process, and the line
+    names the gate mix, the threads and the physical cores."""
+    code = (
+        "import sys, json, argparse, io, contextlib\n"
+        f"sys.path.insert(0, {ROOT!r})\n"
+        "import bench\n"
+        "buf = io.StringIO()\n"
+        "args = argparse.Namespace(impl='reference', gpus=1, steps=1, warmup=1, ref_step_seconds=0.5)\n"
+        "with contextlib.redirect_stdout(buf):\n"
+        "    bench.run_reference(args)\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'line': json.loads(buf.getvalue().strip().splitlines()[-1]),\n"
+        "                  'lib': 'libpz_b200' in maps, 'oracle': 'liboracle_pz' in maps,\n"
+        "                  'pkg': any(m.startswith('phantom-zone_b200') for m in sys.modules)}))\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    rec = json.loads(out.stdout.strip().splitlines()[-1])
+    assert not rec["lib"] and not rec["pkg"] and rec["oracle"]
+    cb = rec["line"]["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["physical_cores"] >= 1
+    assert "gate mix" in cb["sample"] and "and " in cb["sample"]
