@@ -115,6 +115,12 @@ pz_status pz_ctx_create(int param_id, int device, pz_ctx **out);
 pz_status pz_ctx_create_ex(int param_id, int device, uint64_t ntt_root, pz_ctx **out);
 void pz_ctx_destroy(pz_ctx *ctx);
 const char *pz_last_error(const pz_ctx *ctx);
+/* Error bits kernels of this context set on the device instead of trapping
+ * (bit 0: a bounded wait for a bulk copy into shared memory ran out; the
+ * kernel returned and its outputs are not valid).  Synchronizes the device,
+ * returns the bits in *bits and clears them.  No reference counterpart (the
+ * reference panics on the CPU). */
+pz_status pz_ctx_device_error(pz_ctx *ctx, uint32_t *bits);
 pz_status pz_ctx_params(const pz_ctx *ctx, pz_params *out);
 uint64_t pz_ctx_ntt_root(const pz_ctx *ctx);
 
@@ -439,8 +445,9 @@ pz_status pz_ni_aggregate_server_key(pz_ctx *ctx, const uint8_t crs_seed[32],
  * (context, device key) pair of any parameter set sharing the server's ring
  * (all production sets: N = 2048, the same Q); a job is a circuit submitted
  * to a session.  pz_server_step admits pending jobs in arrival order while
- * their wires fit the device arena (admission by device bytes; keys are
- * resident already), then advances every admitted job by one circuit level:
+ * their wires fit the device arena and their session's key is resident or
+ * can be made resident (admission by ciphertext + key bytes; see managed
+ * sessions below), then advances every admitted job by one circuit level:
  * the gates of all sessions run as one ragged key-switch launch and one
  * ragged blind-rotation launch per max_items gates, each gate with its own
  * session's parameters and key.  A job admitted while others are mid-circuit
@@ -453,6 +460,8 @@ typedef struct {
   size_t arena_slots, arena_slots_used, arena_bytes;
   size_t sessions, key_bytes;
   uint64_t steps, gates, launches;
+  size_t resident_key_bytes, key_budget; /* key_budget 0: no limit */
+  uint64_t key_imports, key_evictions;
 } pz_server_stats;
 #define PZ_SERVER_DRY_RUN (-1) /* device id of a host-only server: bookkeeping, no GPU work */
 /* arena_bytes: device bytes for job wires ((n_inputs + n_gates) x (N + 1) x 8 per job);
@@ -463,6 +472,22 @@ const char *pz_server_last_error(const pz_server *s);
 pz_status pz_server_add_session(pz_server *s, pz_ctx *ctx, const pz_key *key, uint32_t *session);
 /* dry-run servers only: a session of parameter set param_id without a key */
 pz_status pz_server_add_virtual_session(pz_server *s, int param_id, uint32_t *session);
+/* Managed session: the server keeps a copy of the key's device-form blob
+ * (pz_key_export) and holds the device key only while it is needed.  A job of
+ * a managed session is admitted when its key is resident or fits the key
+ * budget after evicting the least recently used resident managed keys of
+ * sessions with no job in flight (import: a plain host-to-device copy of the
+ * blob); otherwise it waits, in arrival order.  A job whose key alone exceeds
+ * the budget fails (state 3).  No reference counterpart (the reference holds
+ * one server key per process, bool/mp_api.rs:128-146). */
+pz_status pz_server_add_managed_session(pz_server *s, pz_ctx *ctx, const void *key_blob, size_t blob_bytes,
+                                        uint32_t *session);
+/* dry-run servers only: a managed session of param_id (residency bookkeeping only) */
+pz_status pz_server_add_virtual_managed_session(pz_server *s, int param_id, uint32_t *session);
+/* Device bytes resident managed keys may hold (0: no limit, the default). */
+pz_status pz_server_set_key_budget(pz_server *s, size_t bytes);
+/* *resident = 1 when the session's key is on the device now. */
+pz_status pz_server_session_resident(pz_server *s, uint32_t session, int *resident);
 /* inputs [n_inputs][N + 1], outputs [n_outputs][N + 1]; device_io = 1: device pointers */
 pz_status pz_server_submit(pz_server *s, uint32_t session, pz_circuit *c, const uint64_t *inputs,
                            uint64_t *outputs, int device_io, uint64_t *job);

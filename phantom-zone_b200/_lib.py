@@ -54,7 +54,9 @@ class PzServerKeyShareView(ctypes.Structure):
 class PzServerStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_size_t) for n in ("pending", "active", "done", "failed", "arena_slots",
                                                 "arena_slots_used", "arena_bytes", "sessions", "key_bytes")] + \
-               [(n, ctypes.c_uint64) for n in ("steps", "gates", "launches")]
+               [(n, ctypes.c_uint64) for n in ("steps", "gates", "launches")] + \
+               [(n, ctypes.c_size_t) for n in ("resident_key_bytes", "key_budget")] + \
+               [(n, ctypes.c_uint64) for n in ("key_imports", "key_evictions")]
 
 
 # name -> (restype, argtypes); every symbol declared in the public header
@@ -88,6 +90,7 @@ SIGNATURES = {
     "pz_ctx_pbs_variant": (ctypes.c_int, [vp]),
     "pz_ctx_pbs_slots": (st, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "pz_kernel_revision": (ctypes.c_char_p, []),
+    "pz_ctx_device_error": (st, [vp, ctypes.POINTER(ctypes.c_uint32)]),
     "pz_chacha_block": (st, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),
     "pz_uniform_mod_word": (st, [ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
                                  ctypes.POINTER(ctypes.c_int)]),
@@ -121,6 +124,10 @@ SIGNATURES = {
     "pz_server_last_error": (ctypes.c_char_p, [vp]),
     "pz_server_add_session": (st, [vp, vp, vp, u32p]),
     "pz_server_add_virtual_session": (st, [vp, ctypes.c_int, u32p]),
+    "pz_server_add_managed_session": (st, [vp, vp, ctypes.c_void_p, ctypes.c_size_t, u32p]),
+    "pz_server_add_virtual_managed_session": (st, [vp, ctypes.c_int, u32p]),
+    "pz_server_set_key_budget": (st, [vp, ctypes.c_size_t]),
+    "pz_server_session_resident": (st, [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int)]),
     "pz_server_submit": (st, [vp, ctypes.c_uint32, vp, vp, vp, ctypes.c_int, u64p]),
     "pz_server_step": (st, [vp, ctypes.POINTER(ctypes.c_size_t)]),
     "pz_server_job_status": (st, [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),

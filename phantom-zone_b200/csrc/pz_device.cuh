@@ -38,6 +38,7 @@ struct RingConsts {
   u64 qinv_neg;  // -Q^{-1} mod 2^64
   u64 n_inv, n_inv_s;  // N^{-1} mod Q and its Shoup companion
   u64 one_s;            // Shoup companion of 1: reduce_any(v) = v mod Q for any v
+  u64 iw1n, iw1n_s;     // psi^{-bitrev(1)} N^{-1} (the last inverse stage's twiddle with N^{-1}) + Shoup
   const u64 *fw;  // forward twiddles: pairs (psi^{bitrev(i)}, Shoup companion)
   const u64 *iw;  // inverse twiddles: pairs (psi^{-bitrev(i)}, Shoup companion)
 };
@@ -445,13 +446,15 @@ __device__ __forceinline__ void ntt_fwd(u64 (&x)[8], u64 (&y)[8], u64 *sm, const
 // Inverse negacyclic NTT (GS, ntt.rs:187-230 without the N^{-1} factor):
 // evaluation layout in, values < 2q; coefficient layout out, values < 2q.
 // sm: N words (2N with TWO).
-template <int LOGN, bool TWO>
+// LEAD_SYNC = false: the caller has just passed a block barrier after its
+// last use of sm.
+template <int LOGN, bool TWO, bool LEAD_SYNC = true>
 __device__ __forceinline__ void ntt_inv(u64 (&x)[8], u64 (&y)[8], u64 *sm, const RingConsts &rc) {
   typedef NttShape<LOGN> S;
   const int j = tid_opaque();
   // The first exchange below is warp-local, but the previous user of sm may
   // have read it across warps (a transform's last exchange): full barrier.
-  __syncthreads();
+  if (LEAD_SYNC) __syncthreads();
   if constexpr (S::PARTIAL) {
     inv_round4<LOGN, TWO>(x, y, j, rc);
     xchg<LOGN, 3, 2, TWO>(x, y, sm, j);
@@ -509,5 +512,47 @@ __device__ __forceinline__ void load_key_row(const u64 *row, u64 (&k)[8]) {
 #pragma unroll
   for (int rr = 0; rr < 4; rr++) ld_key2(row + dev_index<LOGN>(j, 2 * rr), k[2 * rr], k[2 * rr + 1]);
 }
+
+// ---------------------------------------------------------------------------
+// Bulk copies into shared memory (cp.async.bulk, completion counted on an
+// mbarrier in bytes).  Sources are this GPU's global memory; no multicast.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(u64 *bar, u32 count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// make initialised mbarriers visible to the bulk-copy unit (then a block barrier)
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// order this thread's earlier shared-memory accesses before later bulk copies
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// One thread: `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global src to shared dst; completes one phase of *bar (initialised with one
+// arrival).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, u32 bytes, u64 *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// Wait for the phase of *bar with the given parity to complete, for at most
+// about `limit` SM clock cycles; false when the limit ran out.
+constexpr long long MBAR_WAIT_LIMIT = 1ll << 31;  // ~1.1 s at 1965 MHz
+__device__ __forceinline__ bool mbar_wait(u64 *bar, u32 parity, long long limit = MBAR_WAIT_LIMIT) {
+  const u32 a = smem_addr(bar);
+  const long long t0 = clock64();
+  for (;;) {
+    u32 done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit) return false;
+  }
+}
+// Error bits a kernel sets in the context's device error word.
+constexpr u32 DEVERR_MBAR_TIMEOUT = 1u;
 
 }  // namespace pz

@@ -23,6 +23,7 @@ struct pz_ctx {
   pz::u64 conv_c = 0, conv_cs = 0;
   pz::BrParams br{};
   pz::KsParams ks{};
+  pz::u32 *d_err = nullptr;  // device error word: DEVERR_* bits set by kernels whose bounded waits ran out
   int grid_limit = 0;
   int pbs_variant = 0;  // blind-rotation launch shape (see pz::PBS_VARIANTS)
   int split_below = -1;  // batches of at most this many gates use the two-CTA kernel (-1: half the SMs)

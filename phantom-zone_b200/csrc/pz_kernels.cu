@@ -106,6 +106,150 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
 }
 
 // ---------------------------------------------------------------------------
+// Batched NTT for N = 2048 (the kernel microbench and the pz_ntt_* entry
+// points): persistent CTAs, two polynomials per iteration transformed
+// together (shared twiddles and barriers, independent butterfly streams).
+// The next pair's 32 KB come into the other half of a double-buffered
+// shared-memory stage by one bulk copy (cp.async.bulk + mbarrier) while the
+// current pair is transformed, so the loads never stall the transform.
+// Outputs go from registers to global memory: the forward in the evaluation
+// order (each thread holds two runs of four consecutive words: 32-byte
+// stores), the inverse in the coefficient order (warp-contiguous stores).
+// The inverse folds N^{-1} into its last stage (x' = N^{-1}(x + y),
+// y' = w N^{-1}(x - y)): 1024 products instead of the 2048 of a separate
+// scaling.  Every mbarrier wait is bounded; a wait that runs out sets
+// DEVERR_MBAR_TIMEOUT in *err and the CTA returns after a bounded wait for
+// its other copy in flight.
+// ---------------------------------------------------------------------------
+constexpr int NTTB_N = 2048;
+constexpr size_t NTTB_SMEM = (size_t)6 * NTTB_N * 8 + 16;  // exchange 2N | 2 stages of 2N | 2 mbarriers
+
+// Last inverse round (k = 0) with N^{-1} folded into its final stage; values
+// leave in [0, 4Q).
+template <bool TWO>
+__device__ __forceinline__ void inv_round8_last_scaled(u64 (&x)[8], u64 (&y)[8], const RingConsts &rc) {
+  constexpr int LOGN = 11;
+  const u64 q = rc.q;
+  u64 w, ws;
+#pragma unroll
+  for (int h = 0; h < 4; h++) {
+    tw(rc.iw, 4 + h, w, ws);
+    ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w, ws, q);
+  }
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    tw(rc.iw, 2 + h, w, ws);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+  }
+  auto last = [&](u64 &a, u64 &b) {  // sums < 16Q, b < 8Q here
+    const u64 u = a + b, t = a + 8 * Q_N2048 - b;
+    a = rc.n_inv * u - mulq_n2048(umulhi_lo2(rc.n_inv_s, u));
+    b = rc.iw1n * t - mulq_n2048(umulhi_lo2(rc.iw1n_s, t));
+  };
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    last(x[r], x[r + 4]);
+    if (TWO) last(y[r], y[r + 4]);
+  }
+}
+
+// Inverse transform of the batch kernel: rounds unrolled (the last one scaled).
+template <bool TWO>
+__device__ __forceinline__ void ntt_inv_scaled(u64 (&x)[8], u64 (&y)[8], u64 *sm, const RingConsts &rc) {
+  constexpr int LOGN = 11;
+  const int j = tid_opaque();
+  __syncthreads();
+  inv_round4<LOGN, TWO>(x, y, j, rc);
+  xchg<LOGN, 3, 2, TWO>(x, y, sm, j);
+  inv_round8<LOGN, TWO>(x, y, 2, j, rc);
+  xchg<LOGN, 2, 1, TWO>(x, y, sm, j);
+  inv_round8<LOGN, TWO>(x, y, 1, j, rc);
+  xchg<LOGN, 1, 0, TWO>(x, y, sm, j);
+  inv_round8_last_scaled<TWO>(x, y, rc);
+}
+
+__device__ __forceinline__ void st_global_v4(u64 *p, u64 a, u64 b, u64 c, u64 d) {
+  asm volatile("st.global.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(a), "l"(b), "l"(c), "l"(d) : "memory");
+}
+__device__ __forceinline__ void lds2(const u64 *p, u64 &a, u64 &b) {
+  asm volatile("ld.shared.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"(smem_addr(p)));
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t count, RingConsts rc, u32 *err) {
+  constexpr int N = NTTB_N, LOGN = 11;
+  extern __shared__ __align__(128) u64 smem[];
+  u64 *xs = smem, *stage = smem + 2 * N, *bar = smem + 6 * N;
+  const int j = threadIdx.x;
+  const size_t pairs = (count + 1) / 2;
+  auto issue = [&](size_t p, int b) {  // one thread: pair p -> stage b
+    const size_t first = 2 * p;
+    const u32 bytes = (u32)((count - first >= 2 ? 2 : 1) * N * 8);
+    fence_proxy_async_smem();
+    bulk_load(stage + (size_t)b * 2 * N, polys + first * N, bytes, bar + b);
+  };
+  if (j == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  size_t p = blockIdx.x;
+  if (j == 0 && p < pairs) issue(p, 0);
+  for (u32 it = 0; p < pairs; it++, p += gridDim.x) {
+    const int b = it & 1;
+    const bool more = p + gridDim.x < pairs;
+    // stage b^1 was read in the previous iteration, before that transform's barriers
+    if (j == 0 && more) issue(p + gridDim.x, b ^ 1);
+    if (!__syncthreads_and(mbar_wait(bar + b, (it >> 1) & 1))) {
+      if (j == 0) {
+        atomicOr(err, DEVERR_MBAR_TIMEOUT);
+        if (more) mbar_wait(bar + (b ^ 1), ((it + 1) >> 1) & 1);  // bounded: the copy issued above
+      }
+      return;
+    }
+    const u64 *sx = stage + (size_t)b * 2 * N, *sy = sx + N;
+    const bool two = 2 * p + 1 < count;
+    u64 *ox = polys + 2 * p * N, *oy = ox + N;
+    u64 x[8], y[8];
+    if (!INV) {
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        x[r] = sx[pos_coef<LOGN>(j, r)];
+        y[r] = sy[pos_coef<LOGN>(j, r)];
+      }
+      ntt_fwd<LOGN, true>(x, y, xs, rc);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {  // registers 4h..4h+3: four consecutive evaluation positions
+        const int o = pos_eval<LOGN>(j, 4 * h);
+        st_global_v4(ox + o, reduce2(reduce_n2048(x[4 * h]), Q_N2048), reduce2(reduce_n2048(x[4 * h + 1]), Q_N2048),
+                     reduce2(reduce_n2048(x[4 * h + 2]), Q_N2048), reduce2(reduce_n2048(x[4 * h + 3]), Q_N2048));
+        if (two)
+          st_global_v4(oy + o, reduce2(reduce_n2048(y[4 * h]), Q_N2048),
+                       reduce2(reduce_n2048(y[4 * h + 1]), Q_N2048), reduce2(reduce_n2048(y[4 * h + 2]), Q_N2048),
+                       reduce2(reduce_n2048(y[4 * h + 3]), Q_N2048));
+      }
+    } else {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int o = pos_eval<LOGN>(j, 4 * h);
+        lds2(sx + o, x[4 * h], x[4 * h + 1]);
+        lds2(sx + o + 2, x[4 * h + 2], x[4 * h + 3]);
+        lds2(sy + o, y[4 * h], y[4 * h + 1]);
+        lds2(sy + o + 2, y[4 * h + 2], y[4 * h + 3]);
+      }
+      ntt_inv_scaled<true>(x, y, xs, rc);
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+        ox[pos_coef<LOGN>(j, r)] = reduce4(x[r], Q_N2048);
+        if (two) oy[pos_coef<LOGN>(j, r)] = reduce4(y[r], Q_N2048);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // One blind-rotation operation on the accumulator acc = (a, b):
 //   op = RGSW index i:  acc <- acc x RGSW_i        (rlwe_by_rgsw_shoup, runtime.rs:754-855)
 //   op = OP_AUTO | v:   acc <- auto_{k_v}(acc)      (rlwe_auto_shoup, runtime.rs:530-643)
@@ -764,6 +908,234 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
 }
 
 // ---------------------------------------------------------------------------
+// Blind rotation with the keys streamed into shared memory (launch shape
+// PBS_BULK, N = 2048, one-digit decompositions).  Each CTA keeps a 64 KB key
+// stage.  Right after an operation's multiply-accumulate has read the stage,
+// one thread issues the bulk copy (cp.async.bulk + mbarrier, from this GPU's
+// memory, no multicast) of the next operation's key rows -- the 4 RGSW rows
+// (64 KB) or the 2 automorphism-key rows (32 KB), contiguous in the device
+// layout -- which lands while the CTA runs this operation's inverse
+// transform and the next one's decomposition and forward transform.  The
+// multiply-accumulate then reads its key from shared memory, not from L2.
+// Two CTAs per SM (the stage); the register cap is 128.  Every wait is
+// bounded: one that runs out sets DEVERR_MBAR_TIMEOUT and the CTA returns.
+// ---------------------------------------------------------------------------
+constexpr int BULK_REGIONS = 6;  // 2N words exchange / permutations, 4N words key stage
+
+static size_t bulk_sched_bytes(u32 br_q, u32 n) {
+  const size_t R = br_q / 2;
+  size_t extra = ((R + 1) + n + (n + R + 1)) * 2 + 4;
+  return (extra + 15) & ~(size_t)15;
+}
+static size_t bulk_smem_bytes(u32 br_q, u32 n) {
+  return (size_t)BULK_REGIONS * 8 * 2048 + bulk_sched_bytes(br_q, n) + 16;  // + the mbarrier
+}
+__device__ __forceinline__ u64 *bulk_bar(u64 *smem, u32 br_q, u32 n) {
+  const u32 R = br_q / 2;
+  u32 extra = ((R + 1) + n + (n + R + 1)) * 2 + 4;
+  extra = (extra + 15) & ~15u;
+  return (u64 *)((char *)smem + (size_t)BULK_REGIONS * 8 * 2048 + extra);
+}
+
+// Key rows of a keyed operation (not a trivial automorphism): source and bytes.
+__device__ __forceinline__ void op_key_rows(const BrParams &P, u32 op, const u64 *&src, u32 &bytes) {
+  constexpr size_t N = 2048;
+  if (op & OP_AUTO) {
+    src = P.autos + (size_t)(op & OP_SLOT) * P.auto_rows * N;
+    bytes = P.auto_rows * (u32)N * 8;
+  } else {
+    src = P.rgsw + (size_t)(op & OP_INDEX) * P.rgsw_rows * N;
+    bytes = P.rgsw_rows * (u32)N * 8;
+  }
+}
+__device__ __forceinline__ bool op_keyed(u32 op) { return !((op & OP_AUTO) && (op & OP_TRIVIAL)); }
+
+// mac_pair / mac_auto with the key rows in shared memory (device layout,
+// row r at ks + r N).
+__device__ __forceinline__ void mac_pair_staged(u64 (&x)[8], u64 (&y)[8], const u64 *ks, const RingConsts &rc) {
+  constexpr int LOGN = 11, N = 2048;
+  const int j = threadIdx.x;
+  const u64 q = rc.q, qi = rc.qinv_neg;
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    const int di = dev_index<LOGN>(j, 2 * rr);
+    u64 a[2], b[2], c[2], d[2];
+    lds2(ks + di, a[0], a[1]);
+    lds2(ks + N + di, b[0], b[1]);
+    lds2(ks + 2 * N + di, c[0], c[1]);
+    lds2(ks + 3 * N + di, d[0], d[1]);
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int r = 2 * rr + e;
+      const u64 xv = x[r], yv = y[r];
+      u64 hi, lo, hi2, lo2;
+      mul128(xv, a[e], hi, lo);
+      mul128(xv, b[e], hi2, lo2);
+      mac128(yv, c[e], hi, lo);
+      mac128(yv, d[e], hi2, lo2);
+      x[r] = redc(hi, lo, q, qi);
+      y[r] = redc(hi2, lo2, q, qi);
+    }
+  }
+}
+__device__ __forceinline__ void mac_auto_staged(u64 (&x)[8], u64 (&y)[8], const u64 *ks, const RingConsts &rc) {
+  constexpr int LOGN = 11, N = 2048;
+  const int j = threadIdx.x;
+  const u64 q = rc.q, qi = rc.qinv_neg, q2 = rc.q << 1;
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    const int di = dev_index<LOGN>(j, 2 * rr);
+    u64 a[2], b[2];
+    lds2(ks + di, a[0], a[1]);
+    lds2(ks + N + di, b[0], b[1]);
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const int r = 2 * rr + e;
+      u64 hi, lo, hi2, lo2;
+      mul128(x[r], a[e], hi, lo);
+      mul128(x[r], b[e], hi2, lo2);
+      x[r] = redc(hi, lo, q, qi);
+      const u64 v = redc(hi2, lo2, q, qi) + y[r];
+      y[r] = v >= q2 ? v - q2 : v;
+    }
+  }
+}
+
+// One keyed operation of the staged blind rotation: bootstrap_op's one-digit
+// path with the key from the stage (its copy completes phase `parity` of
+// *bar); after the multiply-accumulate the copy of the next operation's key
+// (next_src, next_bytes; none when next_src is null) is issued into the same
+// stage.  False (uniformly over the CTA) when the wait ran out.
+__device__ __forceinline__ bool bootstrap_op_staged(u64 (&acc)[2][8], u32 op, const BrParams &P, u64 *sm,
+                                                    u64 *stage, u64 *bar, u32 parity, const u64 *next_src,
+                                                    u32 next_bytes) {
+  constexpr int LOGN = 11, N = 2048;
+  const u64 q = P.rc.q;
+  const int j = threadIdx.x;
+  u64(&x)[8] = acc[0];
+  u64(&y)[8] = acc[1];
+  const bool is_auto = (op & OP_AUTO) != 0;
+  const bool keep_b = (op & OP_KEEPB) != 0;
+  u64 *s_a = sm, *s_b = sm + N;
+  if (is_auto) {  // non-trivial: a(X^k) with sign, b permuted in the evaluation domain
+    const u32 k = P.auto_k[op & OP_SLOT];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      u32 t = ((u32)pos_coef<LOGN>(j, r) * k) & (2 * N - 1);
+      const bool neg = t >= (u32)N;
+      if (neg) t -= N;
+      s_a[swz(t)] = neg ? q - x[r] : x[r];
+      s_b[swz(pos_eval<LOGN>(j, r))] = y[r];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; r++) y[r] = s_b[swz(auto_eval_src<LOGN>(pos_eval<LOGN>(j, r), k))];
+#pragma unroll
+    for (int r = 0; r < 8; r++) x[r] = decompose1<AUTO_LOGB, AUTO_IGN>(s_a[swz(pos_coef<LOGN>(j, r))], q);
+    ntt_fwd<LOGN, false>(x, x, sm, P.rc);
+  } else {
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      x[r] = decompose1<RLRG_LOGB, RLRG_IGN>(x[r], q);
+      y[r] = decompose1<RLRG_LOGB, RLRG_IGN>(y[r], q);
+    }
+    ntt_fwd<LOGN, true>(x, y, sm, P.rc);
+  }
+  if (!__syncthreads_and(mbar_wait(bar, parity))) {
+    if (j == 0) {
+      atomicOr(P.err, DEVERR_MBAR_TIMEOUT);
+      mbar_wait(bar, parity);  // bounded: the copy this CTA still has in flight
+    }
+    return false;
+  }
+  if (is_auto) mac_auto_staged(x, y, stage, P.rc);
+  else mac_pair_staged(x, y, stage, P.rc);
+  __syncthreads();  // every thread has read the stage (also the exchange barrier of the inverse)
+  if (j == 0 && next_src) {
+    fence_proxy_async_smem();
+    bulk_load(stage, next_src, next_bytes, bar);
+  }
+  if (keep_b) {
+    ntt_inv<LOGN, false, false>(x, x, sm, P.rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++) x[r] = reduce2(x[r], q);
+  } else {
+    ntt_inv<LOGN, true, false>(x, y, sm, P.rc);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      x[r] = reduce2(x[r], q);
+      y[r] = reduce2(y[r], q);
+    }
+  }
+  return true;
+}
+
+// One gate bootstrap with staged keys; `phase` counts this CTA's completed
+// waits (the mbarrier's phase parity).  False when a wait ran out.
+__device__ __forceinline__ bool pbs_item_staged(const BrParams &P, int ct, const u32 *kso, u32 gcode, u64 *out,
+                                                u64 *smem, u64 *bar, u32 &phase) {
+  constexpr int LOGN = 11, N = 2048;
+  u64 *sm = smem, *stage = smem + 2 * N;
+  const SchedSmem S = sched_smem<LOGN>(smem, BULK_REGIONS, P.br_q >> 1, P.n);
+  const int j = threadIdx.x;
+  const u64 q = P.rc.q;
+  build_schedule<LOGN>(P, kso, smem, S);
+  u64 acc[2][8];
+#pragma unroll
+  for (int r = 0; r < 8; r++) acc[0][r] = 0;
+  test_rlwe_b<LOGN>(P, kso, gcode, acc[1]);
+  __syncthreads();
+  const u32 nops = *S.nops;
+  u32 t = 0;
+  // trivial automorphisms (only before the first external product) need no key
+#pragma unroll 1
+  for (; t < nops && !op_keyed(S.ops[t]); t++) bootstrap_op<LOGN, true>(acc, S.ops[t], P, sm);
+  if (j == 0 && t < nops) {
+    const u64 *src;
+    u32 bytes;
+    op_key_rows(P, S.ops[t], src, bytes);
+    fence_proxy_async_smem();
+    bulk_load(stage, src, bytes, bar);
+  }
+#pragma unroll 1
+  for (; t < nops; t++) {
+    const u64 *nsrc = nullptr;
+    u32 nbytes = 0;
+    if (t + 1 < nops) op_key_rows(P, S.ops[t + 1], nsrc, nbytes);
+    if (!bootstrap_op_staged(acc, S.ops[t], P, sm, stage, bar, phase & 1u, nsrc, nbytes)) return false;
+    phase++;
+  }
+  // ---- sample extract at index 0 (pbs.rs:423-449)
+  u64 *o = out + (size_t)(P.out_idx ? P.out_idx[ct] : (u32)ct) * (N + 1);
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const u32 p = (u32)pos_coef<LOGN>(j, r);
+    if (p == 0) {
+      o[0] = acc[1][r];
+      o[1] = acc[0][r];
+    } else {
+      o[1 + N - p] = q - acc[0][r];
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(256, 2)
+    pbs_bulk_kernel(BrParams P, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out, int count) {
+  extern __shared__ __align__(128) u64 smem[];
+  u64 *bar = bulk_bar(smem, P.br_q, P.n);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  u32 phase = 0;
+  for (int ct = blockIdx.x; ct < count; ct += gridDim.x)
+    if (!pbs_item_staged(P, ct, ks + (size_t)ct * ks_stride, gates[ct], out, smem, bar, phase)) return;
+}
+
+// ---------------------------------------------------------------------------
 // Low-latency blind rotation: one ciphertext on a cluster of two CTAs (two
 // SMs).  CTA rank 0 holds a, rank 1 holds b (same layouts and domains as the
 // one-CTA kernel: b is left in the evaluation domain ahead of non-trivial
@@ -1054,19 +1426,42 @@ cudaError_t launch_key_convert(int logn, const u64 *in, u64 *out, size_t npolys,
   return cudaGetLastError();
 }
 
-cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s) {
+template <typename K>
+static cudaError_t set_smem(K kernel, size_t bytes);
+
+// Persistent grid of the batched NTT: two CTAs per SM, no more CTAs than pairs.
+static int ntt_batch_grid(size_t count) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t pairs = (count + 1) / 2;
+  return (int)std::min<size_t>(pairs, (size_t)2 * sms);
+}
+
+cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s) {
   if (count == 0) return cudaSuccess;
-  if (logn == 11) ntt_fwd_kernel<11><<<grid_for(count), 256, 0, s>>>(polys, count, rc);
-  else if (logn == 9) ntt_fwd_kernel<9><<<grid_for(count), 64, 0, s>>>(polys, count, rc);
-  else return cudaErrorInvalidValue;
+  if (logn == 11) {
+    cudaError_t e = set_smem(ntt_batch_kernel<false>, NTTB_SMEM);
+    if (e != cudaSuccess) return e;
+    ntt_batch_kernel<false><<<ntt_batch_grid(count), 256, NTTB_SMEM, s>>>(polys, count, rc, err);
+  } else if (logn == 9) {
+    ntt_fwd_kernel<9><<<grid_for(count), 64, 0, s>>>(polys, count, rc);
+  } else {
+    return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s) {
+cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s) {
   if (count == 0) return cudaSuccess;
-  if (logn == 11) ntt_inv_kernel<11><<<grid_for(count), 256, 0, s>>>(polys, count, rc);
-  else if (logn == 9) ntt_inv_kernel<9><<<grid_for(count), 64, 0, s>>>(polys, count, rc);
-  else return cudaErrorInvalidValue;
+  if (logn == 11) {
+    cudaError_t e = set_smem(ntt_batch_kernel<true>, NTTB_SMEM);
+    if (e != cudaSuccess) return e;
+    ntt_batch_kernel<true><<<ntt_batch_grid(count), 256, NTTB_SMEM, s>>>(polys, count, rc, err);
+  } else if (logn == 9) {
+    ntt_inv_kernel<9><<<grid_for(count), 64, 0, s>>>(polys, count, rc);
+  } else {
+    return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -1173,6 +1568,13 @@ cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 
     pbs_split_kernel<11><<<2 * grid, 256, ssmem, s>>>(P, ks, ks_stride, gates, out, (int)count);
     return cudaGetLastError();
   }
+  if (logn == 11 && d1 && variant == PBS_BULK && rlwe_dbg == nullptr) {
+    const size_t bsmem = bulk_smem_bytes(P.br_q, P.n);
+    if ((e = set_smem(pbs_bulk_kernel, bsmem)) != cudaSuccess) return e;
+    pbs_bulk_kernel<<<grid, 256, bsmem, s>>>(P, ks, ks_stride, gates, out, (int)count);
+    return cudaGetLastError();
+  }
+  if (variant > 2) variant = 0;  // shapes without a debug-output form
   if (logn == 11 && d1) {
     if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
     else if (variant == 1) { PZ_LAUNCH(11, true, 3, 256) }
@@ -1203,6 +1605,8 @@ cudaError_t pbs_slots(int logn, bool d1, u32 br_q, u32 n, int variant, size_t *s
   if (logn == 11 && d1 && variant == PBS_SPLIT) {
     PZ_OCC(pbs_split_kernel<11>, 256, split_smem_bytes(br_q, n))
     div = 2;
+  } else if (logn == 11 && d1 && variant == PBS_BULK) {
+    PZ_OCC(pbs_bulk_kernel, 256, bulk_smem_bytes(br_q, n))
   } else if (logn == 11 && d1) {
     if (variant == 0) { PZ_OCC((pbs_kernel<11, true, 2>), 256, smem) }
     else if (variant == 1) { PZ_OCC((pbs_kernel<11, true, 3>), 256, smem) }

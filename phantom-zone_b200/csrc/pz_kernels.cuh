@@ -25,6 +25,7 @@ struct BrParams {
   const u64 *rgsw;                 // [n][rgsw_rows][N] device layout, Montgomery form
   const u64 *autos;                // [w+1][auto_rows][N]
   const u32 *out_idx;              // optional scatter: output of gate ct -> LWE out_idx[ct]
+  u32 *err;                        // the context's device error word (DEVERR_* bits)
 };
 
 // Gate prelude + mod-down + LWE key switch.
@@ -60,8 +61,9 @@ constexpr unsigned char GATE_RAW = 0x80;
 
 cudaError_t launch_key_convert(int logn, const u64 *in, u64 *out, size_t npolys, const RingConsts &rc,
                                u64 c, u64 cs, cudaStream_t s);
-cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s);
-cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts &rc, cudaStream_t s);
+// err: the context's device error word (DEVERR_* bits)
+cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s);
+cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s);
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
                                size_t count, int trivial, cudaStream_t s);
 cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *slot, size_t count,
@@ -79,6 +81,10 @@ constexpr int PBS_VARIANTS = 3;
 // launch shape for small batches (N = 2048, one-digit sets): one ciphertext
 // per cluster of two CTAs, a on one SM and b on the other (lower latency)
 constexpr int PBS_SPLIT = 3;
+// launch shape with every operation's key rows streamed into a shared-memory
+// stage by bulk copies (N = 2048, one-digit sets; two CTAs per SM)
+constexpr int PBS_BULK = 4;
+constexpr int PBS_MAX_VARIANT = PBS_BULK;
 // Ragged batches (several sessions / parameter sets in one launch): per-item
 // descriptors in device memory; max_* bound the sizes over the descriptors.
 cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,

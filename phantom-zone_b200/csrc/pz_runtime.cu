@@ -304,6 +304,8 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   CK_CREATE(cudaMemcpy(c->d_tw, tw.data(), 4 * N * 8, cudaMemcpyHostToDevice));
   CK_CREATE(cudaMalloc(&c->d_dlog, dlog.size() * 2));
   CK_CREATE(cudaMemcpy(c->d_dlog, dlog.data(), dlog.size() * 2, cudaMemcpyHostToDevice));
+  CK_CREATE(cudaMalloc(&c->d_err, sizeof(u32)));
+  CK_CREATE(cudaMemset(c->d_err, 0, sizeof(u32)));
   CK_CREATE(cudaMalloc(&c->d_tv, tv.size() * 8));
   CK_CREATE(cudaMemcpy(c->d_tv, tv.data(), tv.size() * 8, cudaMemcpyHostToDevice));
 #undef CK_CREATE
@@ -316,6 +318,8 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   rc.n_inv = invmod(N, Q);
   rc.n_inv_s = shoup(rc.n_inv, Q);
   rc.one_s = shoup(1, Q);
+  rc.iw1n = mulmod(tw[2 * N + 2], rc.n_inv, Q);  // psi^{-bitrev(1)} N^{-1}
+  rc.iw1n_s = shoup(rc.iw1n, Q);
   rc.fw = c->d_tw;
   rc.iw = c->d_tw + 2 * N;
   const u64 r64 = (u64)(((u128)1 << 64) % Q);
@@ -323,6 +327,7 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   c->conv_cs = shoup(c->conv_c, Q);
   pz::BrParams &br = c->br;
   br.rc = rc;
+  br.err = c->d_err;
   br.da = make_decomp(Q, P.rlrg_logb, P.rlrg_d_a);
   br.db = make_decomp(Q, P.rlrg_logb, P.rlrg_d_b);
   br.dauto = make_decomp(Q, P.auto_logb, P.auto_d);
@@ -361,13 +366,24 @@ void pz_ctx_destroy(pz_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  cudaFree(c->d_tw); cudaFree(c->d_dlog); cudaFree(c->d_tv);
+  cudaFree(c->d_tw); cudaFree(c->d_dlog); cudaFree(c->d_tv); cudaFree(c->d_err);
   cudaFree(c->d_c0); cudaFree(c->d_c1); cudaFree(c->d_out); cudaFree(c->d_gates); cudaFree(c->d_ks);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
 
 const char *pz_last_error(const pz_ctx *c) { return c ? c->err.c_str() : "no context"; }
+
+pz_status pz_ctx_device_error(pz_ctx *c, uint32_t *bits) {
+  if (!c || !bits) return PZ_ERR_INVALID_ARGUMENT;
+  PZ_CK(c, cudaSetDevice(c->device));
+  PZ_CK(c, cudaDeviceSynchronize());
+  u32 v = 0;
+  PZ_CK(c, cudaMemcpy(&v, c->d_err, sizeof v, cudaMemcpyDeviceToHost));
+  if (v) PZ_CK(c, cudaMemset(c->d_err, 0, sizeof v));
+  *bits = v;
+  return PZ_OK;
+}
 
 pz_status pz_ctx_params(const pz_ctx *c, pz_params *out) {
   if (!c || !out) return PZ_ERR_INVALID_ARGUMENT;
@@ -377,7 +393,7 @@ pz_status pz_ctx_params(const pz_ctx *c, pz_params *out) {
 uint64_t pz_ctx_ntt_root(const pz_ctx *c) { return c ? c->root : 0; }
 
 pz_status pz_ctx_set_pbs_variant(pz_ctx *c, int v) {
-  if (!c || v < 0 || v > pz::PBS_SPLIT) return PZ_ERR_INVALID_ARGUMENT;
+  if (!c || v < 0 || v > pz::PBS_MAX_VARIANT) return PZ_ERR_INVALID_ARGUMENT;
   c->pbs_variant = v;
   return PZ_OK;
 }
@@ -610,7 +626,7 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
   std::lock_guard<std::mutex> lock(c->mu);
   PZ_CK(c, cudaSetDevice(c->device));
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
-  const int nv = (c->logn == 11 && d1) ? pz::PBS_SPLIT + 1 : 1;
+  const int nv = (c->logn == 11 && d1) ? pz::PBS_MAX_VARIANT + 1 : 1;
   // synthetic key-switched LWEs, uniform mod q_ks, and gate codes
   const u32 cols = c->P.lwe_n + 1;
   std::vector<u32> ks(batch * cols);
@@ -675,7 +691,7 @@ const char *pz_kernel_revision(void) { return pz::BR_KERNEL_REVISION; }
 pz_status pz_ctx_pbs_slots(pz_ctx *c, int variant, size_t *slots) {
   if (!c || !slots) return PZ_ERR_INVALID_ARGUMENT;
   if (variant < 0) variant = c->pbs_variant;
-  if (variant > pz::PBS_SPLIT) return fail(c, PZ_ERR_INVALID_ARGUMENT, "unknown launch shape");
+  if (variant > pz::PBS_MAX_VARIANT) return fail(c, PZ_ERR_INVALID_ARGUMENT, "unknown launch shape");
   PZ_CK(c, cudaSetDevice(c->device));
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   PZ_CK(c, pz::pbs_slots((int)c->logn, d1, c->P.br_q, c->P.lwe_n, variant, slots));
@@ -725,14 +741,14 @@ pz_status pz_not_batch_device(pz_ctx *c, const uint64_t *d_in, uint64_t *d_out, 
 pz_status pz_ntt_forward_device(pz_ctx *c, uint64_t *d, size_t count, void *stream) {
   if (!c || (count && !d)) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
   PZ_CK(c, cudaSetDevice(c->device));
-  PZ_CK(c, pz::launch_ntt_fwd((int)c->logn, d, count, c->rc, pick(c, stream)));
+  PZ_CK(c, pz::launch_ntt_fwd((int)c->logn, d, count, c->rc, c->d_err, pick(c, stream)));
   return PZ_OK;
 }
 
 pz_status pz_ntt_backward_device(pz_ctx *c, uint64_t *d, size_t count, void *stream) {
   if (!c || (count && !d)) return fail(c, PZ_ERR_INVALID_ARGUMENT, "NULL argument");
   PZ_CK(c, cudaSetDevice(c->device));
-  PZ_CK(c, pz::launch_ntt_inv((int)c->logn, d, count, c->rc, pick(c, stream)));
+  PZ_CK(c, pz::launch_ntt_inv((int)c->logn, d, count, c->rc, c->d_err, pick(c, stream)));
   return PZ_OK;
 }
 

@@ -8,7 +8,11 @@
 // circuit is a job bound to a session (a context + a device-resident server
 // key).  A step
 //   1. admits pending jobs in arrival order while their wires fit the device
-//      arena (admission by device bytes; keys are already resident),
+//      arena and their session's server key is resident or can be made
+//      resident within the key budget (admission by ciphertext + key bytes):
+//      a managed session's key is imported from its device-form blob on
+//      demand, evicting the keys of the least recently used sessions that
+//      have no job in flight,
 //   2. collects the next level of every admitted job, sorts the gates by
 //      session and runs them as ONE ragged key-switch launch (tiles of one
 //      session each) plus ONE ragged blind-rotation launch (each CTA loads
@@ -49,11 +53,23 @@ struct pz_server {
 
   struct Session {
     pz_ctx *ctx = nullptr;
-    const pz_key *key = nullptr;
+    const pz_key *key = nullptr;  // the device key while resident (null: not resident)
     int param_id = 0;
     size_t key_bytes = 0;
+    // managed: the server owns the device key, imported from `blob` (the
+    // pz_key_export form) when a job needs it and released on eviction
+    bool managed = false;
+    std::vector<unsigned char> blob;
+    pz_key *owned = nullptr;
+    bool virt_resident = false;  // dry run: residency without a device key
+    size_t jobs_in_flight = 0;   // admitted, unfinished jobs: they pin the key
+    u64 last_use = 0;            // LRU clock of the last admission / step that used the key
   };
   std::vector<Session> sessions;
+  // device bytes resident managed keys may hold (SIZE_MAX: no limit)
+  size_t key_budget = SIZE_MAX, managed_bytes = 0;
+  u64 use_clock = 0, key_imports = 0, key_evictions = 0;
+  bool descs_dirty = false;
   int logn = -1;
   bool d1 = true;
   size_t L = 0;
@@ -167,11 +183,15 @@ struct pz_server {
     return l;
   }
 
+  bool resident(const Session &se) const { return !se.managed || se.owned || se.virt_resident; }
+
   ~pz_server() {
     for (auto &kv : jobs) delete kv.second;
     if (!dry) {
       cudaSetDevice(device);
       if (stream) cudaStreamSynchronize(stream);
+      for (auto &se : sessions)
+        if (se.owned) pz_key_release(se.owned);
       for (int b = 0; b < 2; b++) {
         if (h_buf[b]) cudaFreeHost(h_buf[b]);
         if (d_buf[b]) cudaFree(d_buf[b]);
@@ -205,13 +225,14 @@ pz_status upload_descs(pz_server *s) {
   std::vector<pz::KsParams> ks(s->sessions.size());
   for (size_t i = 0; i < s->sessions.size(); i++) {
     const auto &se = s->sessions[i];
-    br[i] = se.ctx->br;
-    br[i].rgsw = se.key->d_rgsw;
-    br[i].autos = se.key->d_autos;
+    br[i] = se.ctx->br;  // a session without a resident key gets no items: null key pointers
+    br[i].rgsw = se.key ? se.key->d_rgsw : nullptr;
+    br[i].autos = se.key ? se.key->d_autos : nullptr;
     br[i].out_idx = nullptr;
     ks[i] = se.ctx->ks;
-    ks[i].ksk = se.key->d_ksk;
+    ks[i].ksk = se.key ? se.key->d_ksk : nullptr;
   }
+  s->descs_dirty = false;
   cudaFree(s->d_br);
   cudaFree(s->d_ksp);
   s->d_br = nullptr;
@@ -225,7 +246,8 @@ pz_status upload_descs(pz_server *s) {
   return PZ_OK;
 }
 
-pz_status add_session_common(pz_server *s, int param_id, pz_ctx *ctx, const pz_key *key, uint32_t *session) {
+pz_status add_session_common(pz_server *s, int param_id, pz_ctx *ctx, const pz_key *key, uint32_t *session,
+                             const void *blob = nullptr, size_t blob_bytes = 0, bool managed = false) {
   pz_params P;
   if (pz_param_get(param_id, &P) != PZ_OK) return s->fail(PZ_ERR_INVALID_ARGUMENT, "bad parameter set");
   const int logn = (int)__builtin_ctzll(P.rlwe_n);
@@ -243,7 +265,9 @@ pz_status add_session_common(pz_server *s, int param_id, pz_ctx *ctx, const pz_k
   se.key = key;
   se.param_id = param_id;
   se.key_bytes = key ? key->bytes : key_bytes_of(P);
-  s->sessions.push_back(se);
+  se.managed = managed;
+  if (blob) se.blob.assign((const unsigned char *)blob, (const unsigned char *)blob + blob_bytes);
+  s->sessions.push_back(std::move(se));
   s->max_n = std::max(s->max_n, P.lwe_n);
   s->max_br_q = std::max(s->max_br_q, P.br_q);
   s->max_d = std::max(s->max_d, P.lwe_d);
@@ -272,20 +296,93 @@ pz_status ensure_arena(pz_server *s, size_t arena_bytes) {
   return PZ_OK;
 }
 
-// Admit pending jobs in arrival order while their wires fit.
+void evict(pz_server *s, pz_server::Session &se) {
+  if (se.owned) pz_key_release(se.owned);
+  se.owned = nullptr;
+  se.key = nullptr;
+  se.virt_resident = false;
+  s->managed_bytes -= se.key_bytes;
+  s->key_evictions++;
+  s->descs_dirty = true;
+}
+
+// Make the key of session `sid` resident: evict the least recently used
+// resident managed keys of sessions without jobs in flight until it fits the
+// budget, then import it.  *fits = false: not now (the keys in the way are
+// pinned by running jobs); a CUDA or blob error is returned as such.
+pz_status make_resident(pz_server *s, u32 sid, bool *fits) {
+  pz_server::Session &se = s->sessions[sid];
+  *fits = true;
+  if (s->resident(se)) return PZ_OK;
+  while (s->managed_bytes + se.key_bytes > s->key_budget) {
+    pz_server::Session *victim = nullptr;
+    for (auto &o : s->sessions)
+      if (&o != &se && o.managed && s->resident(o) && o.jobs_in_flight == 0 &&
+          (!victim || o.last_use < victim->last_use))
+        victim = &o;
+    if (!victim) {
+      *fits = false;
+      return PZ_OK;
+    }
+    evict(s, *victim);
+  }
+  if (s->dry) {
+    se.virt_resident = true;
+  } else {
+    pz_key *k = nullptr;
+    pz_status st = pz_key_import(se.ctx, se.blob.data(), se.blob.size(), &k);
+    if (st != PZ_OK) return s->fail(st, std::string("managed session key import: ") + pz_last_error(se.ctx));
+    se.owned = k;
+    se.key = k;
+  }
+  s->managed_bytes += se.key_bytes;
+  s->key_imports++;
+  s->descs_dirty = true;
+  return PZ_OK;
+}
+
+void fail_job(pz_server *s, pz_server::Job *j) {
+  j->state = 3;
+  j->t_done = now_ms();
+  s->n_failed++;
+  s->pending.pop_front();
+}
+
+// The wire arena and the key-switch scratch for the widest session so far.
+pz_status ensure_device_buffers(pz_server *s) {
+  pz_status st = ensure_arena(s, s->arena_bytes_req);
+  if (st != PZ_OK) return st;
+  if (s->ks_stride > s->ksout_stride) {
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->d_ksout);
+    s->d_ksout = nullptr;
+    s->ksout_stride = 0;
+    cudaError_t e = cudaMalloc(&s->d_ksout, s->max_items * (size_t)s->ks_stride * 4);
+    if (e != cudaSuccess) return s->cuda("cudaMalloc", e);
+    s->ksout_stride = s->ks_stride;
+  }
+  return PZ_OK;
+}
+
+// Admit pending jobs in arrival order while their wires fit the arena and
+// their session's key is (or can be made) resident.
 pz_status admit(pz_server *s) {
   while (!s->pending.empty()) {
     pz_server::Job *j = s->pending.front();
     const size_t need = j->v.n_inputs + j->v.n_gates;
-    if (need > s->arena_slots) {  // can never fit
-      j->state = 3;
-      j->t_done = now_ms();
-      s->n_failed++;
-      s->pending.pop_front();
+    pz_server::Session &se = s->sessions[j->session];
+    if (need > s->arena_slots || (se.managed && se.key_bytes > s->key_budget)) {  // can never fit
+      fail_job(s, j);
       continue;
     }
+    bool fits = true;
+    pz_status st = make_resident(s, j->session, &fits);
+    if (st != PZ_OK) return st;
+    if (!fits) break;
     size_t base;
     if (!s->alloc(std::max<size_t>(need, 1), &base)) break;
+    se.jobs_in_flight++;
+    se.last_use = ++s->use_clock;
     j->base = base;
     j->slots = std::max<size_t>(need, 1);
     j->level = 0;
@@ -299,7 +396,7 @@ pz_status admit(pz_server *s) {
     s->pending.pop_front();
     s->active.push_back(j);
   }
-  return PZ_OK;
+  return s->descs_dirty ? upload_descs(s) : PZ_OK;
 }
 
 struct Item {
@@ -501,17 +598,40 @@ pz_status pz_server_add_session(pz_server *s, pz_ctx *ctx, const pz_key *key, ui
   cudaSetDevice(s->device);
   pz_status st = add_session_common(s, ctx->param_id, ctx, key, session);
   if (st != PZ_OK) return st;
-  st = ensure_arena(s, s->arena_bytes_req);
+  return ensure_device_buffers(s);
+}
+
+pz_status pz_server_add_managed_session(pz_server *s, pz_ctx *ctx, const void *key_blob, size_t blob_bytes,
+                                        uint32_t *session) {
+  if (!s || !ctx || !key_blob || !blob_bytes) return PZ_ERR_INVALID_ARGUMENT;
+  if (s->dry) return s->fail(PZ_ERR_INVALID_ARGUMENT, "dry-run server: use pz_server_add_virtual_managed_session");
+  if (ctx->device != s->device) return s->fail(PZ_ERR_INVALID_ARGUMENT, "context is on another device");
+  if (blob_bytes != 64 + key_bytes_of(ctx->P))
+    return s->fail(PZ_ERR_INVALID_ARGUMENT, "managed session: blob size does not match the parameter set");
+  cudaSetDevice(s->device);
+  pz_status st = add_session_common(s, ctx->param_id, ctx, nullptr, session, key_blob, blob_bytes, true);
   if (st != PZ_OK) return st;
-  if (s->ks_stride > s->ksout_stride) {  // key-switch scratch for the widest session
-    cudaStreamSynchronize(s->stream);
-    cudaFree(s->d_ksout);
-    s->d_ksout = nullptr;
-    s->ksout_stride = 0;
-    cudaError_t e = cudaMalloc(&s->d_ksout, s->max_items * (size_t)s->ks_stride * 4);
-    if (e != cudaSuccess) return s->cuda("cudaMalloc", e);
-    s->ksout_stride = s->ks_stride;
-  }
+  return ensure_device_buffers(s);
+}
+
+pz_status pz_server_add_virtual_managed_session(pz_server *s, int param_id, uint32_t *session) {
+  if (!s) return PZ_ERR_INVALID_ARGUMENT;
+  if (!s->dry) return s->fail(PZ_ERR_INVALID_ARGUMENT, "virtual sessions exist only on a dry-run server");
+  pz_status st = add_session_common(s, param_id, nullptr, nullptr, session, nullptr, 0, true);
+  if (st != PZ_OK) return st;
+  return ensure_arena(s, s->arena_bytes_req);
+}
+
+pz_status pz_server_set_key_budget(pz_server *s, size_t bytes) {
+  if (!s) return PZ_ERR_INVALID_ARGUMENT;
+  s->key_budget = bytes ? bytes : SIZE_MAX;
+  return PZ_OK;
+}
+
+pz_status pz_server_session_resident(pz_server *s, uint32_t session, int *resident) {
+  if (!s || !resident) return PZ_ERR_INVALID_ARGUMENT;
+  if (session >= s->sessions.size()) return s->fail(PZ_ERR_INVALID_ARGUMENT, "unknown session");
+  *resident = s->resident(s->sessions[session]) ? 1 : 0;
   return PZ_OK;
 }
 
@@ -564,6 +684,7 @@ pz_status pz_server_step(pz_server *s, size_t *gates_run) {
   const size_t total = per.back();
   std::vector<Item> items(total);
   for (auto *j : run) {
+    s->sessions[j->session].last_use = ++s->use_clock;
     const size_t a = j->v.level_off[j->level], b = j->v.level_off[j->level + 1];
     size_t &pos = per[j->session];
     for (size_t g = a; g < b; g++) {
@@ -591,6 +712,7 @@ pz_status pz_server_step(pz_server *s, size_t *gates_run) {
     j->state = 2;
     j->t_done = t;
     s->release(j->base, j->slots);
+    s->sessions[j->session].jobs_in_flight--;
     s->n_done++;
   }
   s->active.swap(still);
@@ -632,7 +754,13 @@ pz_status pz_server_stats_get(pz_server *s, pz_server_stats *out) {
   out->arena_slots_used = s->slots_used;
   out->arena_bytes = s->arena_slots * s->L * 8;
   out->sessions = s->sessions.size();
-  for (auto &se : s->sessions) out->key_bytes += se.key_bytes;
+  for (auto &se : s->sessions) {
+    out->key_bytes += se.key_bytes;
+    if (s->resident(se)) out->resident_key_bytes += se.key_bytes;
+  }
+  out->key_budget = s->key_budget == SIZE_MAX ? 0 : s->key_budget;
+  out->key_imports = s->key_imports;
+  out->key_evictions = s->key_evictions;
   out->steps = s->steps;
   out->gates = s->gates;
   out->launches = s->launches;
@@ -666,8 +794,12 @@ pz_status pz_server_autotune(pz_server *s, size_t batch, int *variant, int *grid
   std::mt19937_64 rng(0x7A11u);
   std::vector<u32> ks((size_t)batch * s->ks_stride, 0), desc(batch), outi(batch);
   std::vector<unsigned char> g(batch);
+  std::vector<u32> live;  // sessions whose key is on the device now
+  for (u32 i = 0; i < (u32)s->sessions.size(); i++)
+    if (s->sessions[i].key) live.push_back(i);
+  if (live.empty()) return s->fail(PZ_ERR_INVALID_ARGUMENT, "autotune needs a session with a resident key");
   for (size_t i = 0; i < batch; i++) {
-    desc[i] = (u32)(i % s->sessions.size());
+    desc[i] = live[i % live.size()];
     const pz_params &P = s->sessions[desc[i]].ctx->P;
     for (u32 c = 0; c <= P.lwe_n; c++) ks[i * s->ks_stride + c] = (u32)(rng() % P.lwe_q);
     g[i] = (unsigned char)(rng() % 6);

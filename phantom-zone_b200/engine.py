@@ -190,6 +190,13 @@ class Engine:
     def pbs_variant(self, v):
         check(lib().pz_ctx_set_pbs_variant(self.h, int(v)), self.h, "set_pbs_variant")
 
+    def device_error(self):
+        """Error bits set by this context's kernels on the device (bounded waits
+        that ran out); synchronizes the device and clears them."""
+        v = ctypes.c_uint32()
+        check(lib().pz_ctx_device_error(self.h, ctypes.byref(v)), self.h, "pz_ctx_device_error")
+        return v.value
+
     def pbs_slots(self, variant=-1):
         """Ciphertexts a blind-rotation launch of shape `variant` (-1: the
         current one) holds resident at once; multiples run in whole waves."""

@@ -55,6 +55,33 @@ class Server:
         self.L = engine.L
         return sid.value
 
+    def add_managed_session(self, engine, key_blob):
+        """A session whose device key the server imports from `key_blob` (the
+        bytes of DeviceKey.export()) when a job needs it and evicts when the
+        key budget calls for room (least recently used, no job in flight)."""
+        sid = ctypes.c_uint32()
+        blob = bytes(key_blob)  # the server keeps its own copy
+        self._chk(lib().pz_server_add_managed_session(self.h, engine.h, blob, len(blob), ctypes.byref(sid)),
+                  "add_managed_session")
+        self.L = engine.L
+        return sid.value
+
+    def add_virtual_managed_session(self, param_id):
+        """Dry-run servers: a managed session (residency bookkeeping only)."""
+        sid = ctypes.c_uint32()
+        self._chk(lib().pz_server_add_virtual_managed_session(self.h, int(param_id), ctypes.byref(sid)),
+                  "add_virtual_managed_session")
+        return sid.value
+
+    def set_key_budget(self, nbytes):
+        """Device bytes resident managed keys may hold (0: no limit)."""
+        self._chk(lib().pz_server_set_key_budget(self.h, int(nbytes)), "set_key_budget")
+
+    def resident(self, session):
+        r = ctypes.c_int()
+        self._chk(lib().pz_server_session_resident(self.h, int(session), ctypes.byref(r)), "session_resident")
+        return bool(r.value)
+
     def add_virtual_session(self, param_id):
         sid = ctypes.c_uint32()
         self._chk(lib().pz_server_add_virtual_session(self.h, int(param_id), ctypes.byref(sid)),

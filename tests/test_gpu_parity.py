@@ -46,6 +46,26 @@ def test_ntt_matches_oracle(gpu_available, param):
     assert np.array_equal(to_host(t).reshape(count, ev.N), x)
 
 
+def test_ntt_batch_many_pairs_odd_count(gpu_available):
+    """The persistent batched NTT: more polynomial pairs than resident CTAs
+    (each CTA streams several pairs through its double-buffered stage), an
+    odd count (a last pair of one), forward and inverse each equal to the
+    oracle's transforms, and no device error raised."""
+    ev, _, _, _ = oracle_setup("NI_8P")
+    eng, _ = engine_and_key("NI_8P")
+    count = 4 * 148 + 3
+    r = rng(0x13)
+    x = r.uniform_mod(ev.Q, count * ev.N).reshape(count, ev.N)
+    t = to_dev(x)
+    eng.ntt_forward_device(t)
+    assert np.array_equal(to_host(t).reshape(count, ev.N), np.stack([ev.ntt_forward(v) for v in x]))
+    y = r.uniform_mod(ev.Q, count * ev.N).reshape(count, ev.N)  # arbitrary evaluation-domain words
+    t = to_dev(y)
+    eng.ntt_backward_device(t)
+    assert np.array_equal(to_host(t).reshape(count, ev.N), np.stack([ev.ntt_backward(v) for v in y]))
+    assert eng.device_error() == 0
+
+
 @pytest.mark.parametrize("param", ["SP_TEST", "I_2P_LB_SR"])
 def test_ntt_negacyclic_product_default_root(gpu_available, param):
     """ntt.rs:510-540 pin: NTT product == schoolbook product (library's own root)."""
@@ -182,10 +202,11 @@ def test_gate_batch_host_api(gpu_available, param):
 
 
 @pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_pbs_variants_bit_exact(gpu_available, param, variant):
     """Every launch-shape variant of the blind rotation (3: one ciphertext on a
-    cluster of two CTAs) gives the oracle's words."""
+    cluster of two CTAs; 4: keys streamed into shared memory by bulk copies)
+    gives the oracle's words."""
     O = oracle()
     ev, secrets, _, okey = oracle_setup(param)
     eng, dkey = engine_and_key(param)
@@ -204,6 +225,7 @@ def test_pbs_variants_bit_exact(gpu_available, param, variant):
         eng.set_split_threshold(-1)
     want = okey.gate_batch(gates, c0, c1, threads=4)
     assert np.array_equal(got, want)
+    assert eng.device_error() == 0
 
 
 def test_ctx_autotune_keeps_results(gpu_available):
@@ -214,7 +236,7 @@ def test_ctx_autotune_keeps_results(gpu_available):
     old = eng.pbs_variant
     try:
         t = eng.autotune(dkey, 296)
-        assert t["variant"] in (0, 1, 2) and t["ms"] > 0 and eng.pbs_variant == t["variant"]
+        assert t["variant"] in (0, 1, 2, 3, 4) and t["ms"] > 0 and eng.pbs_variant == t["variant"]
         bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, 4, 0x7F)
         gates = np.array([O.GATES[g] for g in ["and", "nand", "xor", "nor"]], np.uint8)
         assert np.array_equal(eng.gate_batch(dkey, gates, c0, c1), okey.gate_batch(gates, c0, c1, threads=4))
@@ -224,7 +246,8 @@ def test_ctx_autotune_keeps_results(gpu_available):
 
 def test_split_kernel_many_items_per_cluster(gpu_available):
     """The two-CTA kernel with fewer clusters than ciphertexts (each cluster
-    bootstraps several in turn, reusing its digit slots) == the one-CTA kernel."""
+    bootstraps several in turn, reusing its digit slots) and the staged-key
+    kernel with fewer CTAs than ciphertexts == the one-CTA kernel."""
     O = oracle()
     ev, secrets, _, okey = oracle_setup("NI_8P")
     eng, dkey = engine_and_key("NI_8P")
@@ -236,7 +259,7 @@ def test_split_kernel_many_items_per_cluster(gpu_available):
     outs = []
     old = eng.pbs_variant
     try:
-        for v, limit in [(0, 0), (3, 5)]:
+        for v, limit in [(0, 0), (3, 5), (4, 5)]:
             eng.pbs_variant = v
             eng.set_split_threshold(0)
             eng.set_pbs_grid_limit(limit)
@@ -248,7 +271,9 @@ def test_split_kernel_many_items_per_cluster(gpu_available):
         eng.set_split_threshold(-1)
         eng.set_pbs_grid_limit(0)
     assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[2])  # staged keys: each CTA runs ~5 items, its mbarrier phases carry over
     assert np.array_equal(outs[1][:3], okey.gate_batch(gates[:3], c0[:3], c1[:3], threads=3))
+    assert eng.device_error() == 0
 
 
 def test_pbs_slots_whole_waves(gpu_available):
@@ -258,7 +283,7 @@ def test_pbs_slots_whole_waves(gpu_available):
     import torch
     eng, dkey = engine_and_key("NI_8P")
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    slots = [eng.pbs_slots(v) for v in range(4)]
+    slots = [eng.pbs_slots(v) for v in range(5)]
     assert all(s > 0 for s in slots)
     for v in range(3):
         assert slots[v] % sms == 0
@@ -267,6 +292,6 @@ def test_pbs_slots_whole_waves(gpu_available):
     old = eng.pbs_variant
     try:
         t = eng.autotune(dkey, 2 * slots[2])
-        assert t["variant"] in (0, 1, 2, 3) and t["ms"] > 0
+        assert t["variant"] in (0, 1, 2, 3, 4) and t["ms"] > 0
     finally:
         eng.pbs_variant = old

@@ -202,3 +202,32 @@ def test_autotune_then_run(gpu_available):
     S.run_until_idle()
     assert np.array_equal(S.result(j), C.run(e2, k2, inp))
     assert ev2.decrypt_bool(s2, S.result(j))[0] == 1
+
+
+def test_managed_sessions_evict_and_reimport_keys(gpu_available):
+    """Managed sessions with a key budget of one I_2P key: every job brings
+    its session's key in (evicting the other, idle one) from the device-form
+    blob; a session whose key was evicted and imported again gives the same
+    words as the job run alone, and every output decrypts right."""
+    P = pz()
+    eng, key, ev, s, _ = session("I_2P_LB_SR")
+    blob = key.export()
+    S = P.Server(device=0, arena_bytes=1 << 27, max_items=1024)
+    a = S.add_managed_session(eng, blob)
+    b = S.add_managed_session(eng, blob)
+    S.set_key_budget(len(blob) - 64)
+    C = circuit("add")
+    outs = []
+    for k, sid in enumerate([a, b, a]):
+        x, y = 17 * k + 5, 250 - 9 * k
+        inp = enc_pair(ev, s, x, y, 40 + k)
+        j = S.submit(sid, C, inp)
+        S.run_until_idle()
+        assert S.resident(sid) and not S.resident(b if sid == a else a)
+        got = S.result(j)
+        assert np.array_equal(got, C.run(eng, key, inp)), f"job {k}: words differ from the job alone"
+        expect("add", ev, s, got, x, y)
+        outs.append(got)
+    st = S.stats()
+    assert st["key_imports"] == 3 and st["key_evictions"] == 2 and st["failed"] == 0
+    assert eng.device_error() == 0

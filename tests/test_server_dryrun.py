@@ -168,3 +168,66 @@ def test_schedule_policy_rejects_unknown():
     S, _ = make_server(1 << 16)
     with pytest.raises(Exception):
         S.set_schedule(7)
+
+
+def key_bytes(param):
+    p = pz().params(param)
+    stride = (p.lwe_n + 1 + 31) // 32 * 32
+    return (p.lwe_n * p.rgsw_rows * p.rlwe_n * 8 + p.n_auto_keys * p.auto_rows * p.rlwe_n * 8 +
+            p.lwe_d * p.rlwe_n * stride * 4)
+
+
+def test_managed_keys_admission_and_lru_eviction():
+    """Admission by ciphertext + key bytes: with a key budget for two NI_8P
+    keys and three managed sessions, a job of the third session evicts the
+    least recently used idle key; a session with a job in flight is never
+    evicted (a job waits instead, in arrival order); a key larger than the
+    budget fails its job."""
+    P = pz()
+    S = P.Server(device=P.DRY_RUN, arena_bytes=(1 << 16) * L_of("NI_8P") * 8, max_items=4096)
+    kb = key_bytes("NI_8P")
+    a, b, c = (S.add_virtual_managed_session(P.param_id("NI_8P")) for _ in range(3))
+    S.set_key_budget(2 * kb)
+    assert not any(S.resident(x) for x in (a, b, c))
+    add = u8_circuit("add")
+    ja = S.submit(a, add)
+    S.run_until_idle()
+    jb = S.submit(b, add)
+    S.run_until_idle()
+    st = S.stats()
+    assert st["key_imports"] == 2 and st["key_evictions"] == 0 and st["resident_key_bytes"] == 2 * kb
+    # a was used least recently: the first job of c evicts it
+    jc = S.submit(c, add)
+    S.step()
+    assert S.resident(c) and S.resident(b) and not S.resident(a)
+    assert S.stats()["key_evictions"] == 1
+    # while c and b both have jobs in flight, a new job of a cannot get its key: it waits
+    S.submit(b, u8_circuit("mul"))
+    S.step()
+    ja2 = S.submit(a, add)
+    S.step()
+    assert S.status(ja2)["state"] == P.server.PENDING and not S.resident(a)
+    S.run_until_idle()
+    # c finished first (15 levels vs mul's), so c's idle key made room for a
+    assert S.status(ja2)["state"] == P.server.DONE and S.resident(a) and not S.resident(c)
+    for j in (ja, jb, jc, ja2):
+        assert S.status(j)["state"] == P.server.DONE
+    st = S.stats()
+    assert st["key_imports"] == 4 and st["key_evictions"] == 2 and st["resident_key_bytes"] <= 2 * kb
+    # a key that can never fit the budget fails its job
+    S.set_key_budget(kb // 2)
+    jx = S.submit(c, add)
+    S.step()
+    assert S.status(jx)["state"] == P.server.FAILED
+
+
+def test_unmanaged_sessions_ignore_the_key_budget():
+    """Sessions added with a resident key are always resident; the key budget
+    governs managed sessions only."""
+    P = pz()
+    S, (s0, s1) = make_server(1 << 16)
+    S.set_key_budget(1)
+    j = S.submit(s0, u8_circuit("lt"))
+    S.run_until_idle()
+    assert S.status(j)["state"] == P.server.DONE and S.resident(s0) and S.resident(s1)
+    assert S.stats()["key_imports"] == 0
