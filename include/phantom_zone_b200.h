@@ -215,8 +215,18 @@ const char *pz_kernel_revision(void);
 /* Autotuner: times every blind-rotation variant on synthetic key-switched
  * LWEs with this key -- `batch` of them, or, from one wave up, the largest
  * whole number of that variant's waves not above `batch` -- and keeps the
- * fastest per ciphertext for the context (*ms: its time for `batch`). */
+ * fastest per ciphertext (*ms: its time for `batch`); then times the
+ * key-switch kernel with 8, 16 and 32 ciphertexts per CTA on `batch` inputs
+ * and keeps the fastest.  Both become the context's defaults and the choice
+ * for batches in batch's size bucket (floor(log2(gates))); launches in a
+ * bucket never tuned use the defaults.  Setting a variant or a tile by hand
+ * clears the per-bucket choices.  No reference counterpart. */
 pz_status pz_ctx_autotune(pz_ctx *ctx, const pz_key *key, size_t batch, int *variant, double *ms);
+/* Key-switch ciphertexts per CTA: 8, 16 (default) or 32. */
+pz_status pz_ctx_set_ks_tile(pz_ctx *ctx, int ciphertexts);
+/* The blind-rotation variant and key-switch tile a batch of `gates` gates
+ * would launch with now. */
+pz_status pz_ctx_launch_shape(pz_ctx *ctx, size_t gates, int *variant, int *ks_tile);
 
 /* ---- circuits ------------------------------------------------------------------
  * A circuit records gates instead of executing them (the reference executes
@@ -472,8 +482,9 @@ const char *pz_server_last_error(const pz_server *s);
 pz_status pz_server_add_session(pz_server *s, pz_ctx *ctx, const pz_key *key, uint32_t *session);
 /* dry-run servers only: a session of parameter set param_id without a key */
 pz_status pz_server_add_virtual_session(pz_server *s, int param_id, uint32_t *session);
-/* Managed session: the server keeps a copy of the key's device-form blob
- * (pz_key_export) and holds the device key only while it is needed.  A job of
+/* Managed session: the server holds the session's device key only while it
+ * is needed, importing it from the caller's device-form blob (pz_key_export;
+ * the blob must stay valid and unchanged while the server exists).  A job of
  * a managed session is admitted when its key is resident or fits the key
  * budget after evicting the least recently used resident managed keys of
  * sessions with no job in flight (import: a plain host-to-device copy of the
@@ -499,12 +510,14 @@ pz_status pz_server_step(pz_server *s, size_t *gates);
 pz_status pz_server_job_status(pz_server *s, uint64_t job, int *state, double *latency_ms, double *queue_ms);
 pz_status pz_server_forget(pz_server *s, uint64_t job);
 pz_status pz_server_stats_get(pz_server *s, pz_server_stats *out);
-/* Ragged blind-rotation launch shape (variant as pz_ctx_set_pbs_variant; grid
- * limit 0 = one CTA per gate) */
+/* Ragged blind-rotation launch shape (variant as pz_ctx_set_pbs_variant: 0,
+ * 1, 2 or 4 -- steps of at most half the SMs' gates take the two-CTA shape 3
+ * by themselves; grid limit 0 = one CTA per gate) */
 pz_status pz_server_set_launch(pz_server *s, int pbs_variant, int grid_limit);
-/* Autotuner: times every variant x {one CTA per gate, persistent 2 x SMs}
- * on `batch` synthetic gates spread over the sessions and keeps the fastest.
- * Needs an idle server (no admitted job). */
+/* Autotuner: times the variants 0, 1, 2, 4 x {one CTA per gate, persistent
+ * 2 x SMs} on `batch` synthetic gates spread over the sessions with a
+ * resident key and keeps the fastest.  Needs an idle server (no admitted
+ * job). */
 pz_status pz_server_autotune(pz_server *s, size_t batch, int *variant, int *grid_limit, double *ms);
 /* Which jobs advance a level at each step.  ALL_READY (default): every
  * admitted job.  CRITICAL_PATH: the jobs with the most levels left always

@@ -90,6 +90,8 @@ SIGNATURES = {
     "pz_ctx_pbs_variant": (ctypes.c_int, [vp]),
     "pz_ctx_pbs_slots": (st, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "pz_kernel_revision": (ctypes.c_char_p, []),
+    "pz_ctx_set_ks_tile": (st, [vp, ctypes.c_int]),
+    "pz_ctx_launch_shape": (st, [vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "pz_ctx_device_error": (st, [vp, ctypes.POINTER(ctypes.c_uint32)]),
     "pz_chacha_block": (st, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),
     "pz_uniform_mod_word": (st, [ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),

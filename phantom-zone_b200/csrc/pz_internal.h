@@ -27,6 +27,13 @@ struct pz_ctx {
   int grid_limit = 0;
   int pbs_variant = 0;  // blind-rotation launch shape (see pz::PBS_VARIANTS)
   int split_below = -1;  // batches of at most this many gates use the two-CTA kernel (-1: half the SMs)
+  int ks_ct = 16;        // key-switch ciphertexts per CTA (8, 16, 32)
+  // autotuned launch shapes per batch-size bucket floor(log2(gates)); a
+  // bucket the autotuner has not seen uses the defaults above
+  struct Tuned {
+    int variant = -1, ks_ct = 0;
+  };
+  Tuned tuned[48];
   // host-API scratch (guarded by mu)
   std::mutex mu;
   size_t cap = 0;
@@ -51,6 +58,9 @@ struct pz_ni_ksk {
 };
 
 namespace pz {
+inline int size_bucket(size_t n) { return n ? 63 - __builtin_clzll((unsigned long long)n) : 0; }
+int effective_variant(pz_ctx *c, size_t count);
+int effective_ks_ct(const pz_ctx *c, size_t count);
 // Launch sequence of one batch of gate bootstraps (ks kernel -> pbs kernel).
 // Optional wire gather/scatter: in0/in1/out_idx (see KsParams, BrParams).
 pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, const u64 *d_c0, const u64 *d_c1,

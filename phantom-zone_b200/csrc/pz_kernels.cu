@@ -542,9 +542,10 @@ __device__ __forceinline__ u64 prelude_moddown(u64 x0, u64 x1, unsigned char gat
   return (u64)round(f);
 }
 
-constexpr int KS_CT = KS_TILE_CT;  // ciphertexts per CTA
 constexpr int KS_IC = 32;    // LWE coefficients per digit chunk
 constexpr int KS_COLS = 128; // output columns per CTA
+// digits of one CTA's chunk: CT ciphertexts x KS_IC coefficients x MAX_KS_D (u32)
+constexpr size_t ks_dig_bytes(int ct) { return (size_t)ct * KS_IC * MAX_KS_D * 4; }
 
 // Input word `i` of gate ct's operand (gathered through a wire index when
 // given; a set WIRE_NEG bit applies not(): q - x, evaluator.rs:2247-2250).
@@ -556,12 +557,13 @@ __device__ __forceinline__ u64 operand(const u64 *base, const u32 *idx, int ct, 
   return (w & WIRE_NEG) ? q - x : x;
 }
 
-// Key switch of ciphertexts [ct0, min(ct0 + KS_CT, count)) for the output
+// Key switch of ciphertexts [ct0, min(ct0 + CT, count)) for the output
 // columns of this CTA (blockIdx.y) over its share of the input coefficients
 // (blockIdx.z of gridDim.z).  With one share the sums are stored reduced mod
 // q_ks; with several, each CTA adds its partial sums into the zeroed output
 // with 32-bit atomics (exact: the result is taken mod q_ks, a power of two
 // <= 2^32) and the consumer reduces (value & (q_ks - 1)).
+template <int CT>
 __device__ __forceinline__ void ks_tile(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
                                         int ct0, int count, u32 *out, u32 (*dig)[KS_IC][MAX_KS_D]) {
   const int tid = threadIdx.x;
@@ -572,12 +574,12 @@ __device__ __forceinline__ void ks_tile(const KsParams &P, const unsigned char *
   const u32 i_begin = blockIdx.z * per * KS_IC;
   const u32 i_end = min(P.N, i_begin + per * KS_IC);
   if (i_begin >= P.N) return;  // uniform per CTA
-  u32 acc[KS_CT];
+  u32 acc[CT];
 #pragma unroll
-  for (int c = 0; c < KS_CT; c++) acc[c] = 0;
+  for (int c = 0; c < CT; c++) acc[c] = 0;
   for (u32 i0 = i_begin; i0 < i_end; i0 += KS_IC) {
     __syncthreads();
-    for (int e = tid; e < KS_CT * KS_IC; e += KS_COLS) {
+    for (int e = tid; e < CT * KS_IC; e += KS_COLS) {
       const int c = e / KS_IC, ii = e % KS_IC;
       const int ct = ct0 + c;
       if (ct < count) {
@@ -598,14 +600,14 @@ __device__ __forceinline__ void ks_tile(const KsParams &P, const unsigned char *
           const u32 kv = __ldg(kp);
           kp += P.ksk_stride;
 #pragma unroll
-          for (int c = 0; c < KS_CT; c++) acc[c] += dig[c][ii][jd] * kv;
+          for (int c = 0; c < CT; c++) acc[c] += dig[c][ii][jd] * kv;
         }
       }
     }
   }
   if (col <= (int)P.n) {
 #pragma unroll
-    for (int c = 0; c < KS_CT; c++) {
+    for (int c = 0; c < CT; c++) {
       const int ct = ct0 + c;
       if (ct < count) {
         u32 v = acc[c];
@@ -621,10 +623,13 @@ __device__ __forceinline__ void ks_tile(const KsParams &P, const unsigned char *
   }
 }
 
+// CT ciphertexts per CTA (8, 16 or 32: picked per batch by the autotuner);
+// the digit buffer is dynamic shared memory of ks_dig_bytes(CT).
+template <int CT>
 __global__ void __launch_bounds__(KS_COLS)
     ks_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
-  __shared__ u32 dig[KS_CT][KS_IC][MAX_KS_D];
-  ks_tile(P, gates, c0, c1, blockIdx.x * KS_CT, count, out, dig);
+  extern __shared__ __align__(16) u32 ks_dig[];
+  ks_tile<CT>(P, gates, c0, c1, blockIdx.x * CT, count, out, (u32 (*)[KS_IC][MAX_KS_D])ks_dig);
 }
 
 // Ragged batch: tile blockIdx.x holds up to KS_CT ciphertexts of one session
@@ -633,7 +638,7 @@ __global__ void __launch_bounds__(KS_COLS)
 __global__ void __launch_bounds__(KS_COLS)
     ks_ragged_kernel(const KsParams *descs, const KsTile *tiles, const unsigned char *gates, const u64 *wires,
                      const u32 *in0, const u32 *in1, u32 *out, u32 out_stride) {
-  __shared__ u32 dig[KS_CT][KS_IC][MAX_KS_D];
+  __shared__ u32 dig[KS_TILE_CT][KS_IC][MAX_KS_D];
   __shared__ KsParams sp;
   const KsTile t = tiles[blockIdx.x];
   if (threadIdx.x == 0) {
@@ -645,7 +650,7 @@ __global__ void __launch_bounds__(KS_COLS)
   }
   __syncthreads();
   if (blockIdx.y * KS_COLS > sp.n) return;  // no columns of this session here (uniform per CTA)
-  ks_tile(sp, gates, wires, wires, (int)t.first, (int)(t.first + t.count), out, dig);
+  ks_tile<KS_TILE_CT>(sp, gates, wires, wires, (int)t.first, (int)(t.first + t.count), out, dig);
 }
 
 // ---------------------------------------------------------------------------
@@ -1121,6 +1126,33 @@ __device__ __forceinline__ bool pbs_item_staged(const BrParams &P, int ct, const
   return true;
 }
 
+// The staged-key blind rotation over a ragged batch: item ct uses descriptor
+// item_desc[ct] (parameter set and key of its session) and scatters to
+// out_idx[ct]; the schedule arrays are laid out for the launch's maximum
+// (br_q, n), the mbarrier after them.
+__global__ void __launch_bounds__(256, 2)
+    pbs_bulk_ragged_kernel(const BrParams *descs, const u32 *item_desc, const u32 *ks, u32 ks_stride,
+                           const unsigned char *gates, u64 *out, const u32 *out_idx, int count, u32 max_br_q,
+                           u32 max_n) {
+  extern __shared__ __align__(128) u64 smem[];
+  __shared__ BrParams sp;
+  u64 *bar = bulk_bar(smem, max_br_q, max_n);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+  }
+  u32 phase = 0;
+  for (int ct = blockIdx.x; ct < count; ct += gridDim.x) {
+    __syncthreads();  // the previous item is done with sp (and the mbarrier is initialised)
+    if (threadIdx.x == 0) {
+      sp = descs[item_desc[ct]];
+      sp.out_idx = out_idx;
+    }
+    __syncthreads();
+    if (!pbs_item_staged(sp, ct, ks + (size_t)ct * ks_stride, gates[ct], out, smem, bar, phase)) return;
+  }
+}
+
 __global__ void __launch_bounds__(256, 2)
     pbs_bulk_kernel(BrParams P, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out, int count) {
   extern __shared__ __align__(128) u64 smem[];
@@ -1533,14 +1565,22 @@ __global__ void ks_mask_kernel(u32 *out, size_t count, u32 stride, u32 cols, u32
 }
 
 cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
-                      size_t count, u32 *out, cudaStream_t s, bool reduce_output) {
+                      size_t count, u32 *out, cudaStream_t s, bool reduce_output, int ct) {
   if (count == 0) return cudaSuccess;
   if (P.d > (u32)MAX_KS_D) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)((count + KS_CT - 1) / KS_CT), (unsigned)((P.n + 1 + KS_COLS - 1) / KS_COLS));
+  if (ct != 8 && ct != 16 && ct != 32) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)((count + ct - 1) / ct), (unsigned)((P.n + 1 + KS_COLS - 1) / KS_COLS));
   grid.z = ks_split((size_t)grid.x * grid.y, P.N);
   cudaError_t e;
   if (grid.z > 1 && (e = cudaMemsetAsync(out, 0, count * P.out_stride * sizeof(u32), s)) != cudaSuccess) return e;
-  ks_kernel<<<grid, KS_COLS, 0, s>>>(P, gates, c0, c1, (int)count, out);
+  const size_t smem = ks_dig_bytes(ct);
+#define PZ_KS(CT)                                                              \
+  if ((e = set_smem(ks_kernel<CT>, smem)) != cudaSuccess) return e;           \
+  ks_kernel<CT><<<grid, KS_COLS, smem, s>>>(P, gates, c0, c1, (int)count, out);
+  if (ct == 8) { PZ_KS(8) }
+  else if (ct == 16) { PZ_KS(16) }
+  else { PZ_KS(32) }
+#undef PZ_KS
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (grid.z > 1 && reduce_output) {
     const size_t words = count * (P.n + 1);
@@ -1649,6 +1689,14 @@ cudaError_t launch_pbs_ragged(int logn, bool d1, const BrParams *d_descs, const 
                                                              (int)count);
     return cudaGetLastError();
   }
+  if (logn == 11 && d1 && variant == PBS_BULK) {
+    const size_t bsmem = bulk_smem_bytes(max_br_q, max_n);
+    if ((e = set_smem(pbs_bulk_ragged_kernel, bsmem)) != cudaSuccess) return e;
+    pbs_bulk_ragged_kernel<<<grid, 256, bsmem, s>>>(d_descs, item_desc, ks, ks_stride, gates, out, out_idx,
+                                                    (int)count, max_br_q, max_n);
+    return cudaGetLastError();
+  }
+  if (variant > 2) variant = 0;
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                                    \
   if ((e = set_smem(pbs_ragged_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;                 \
   pbs_ragged_kernel<LN, DD, MB><<<grid, TH, smem, s>>>(d_descs, item_desc, ks, ks_stride, gates, out, out_idx, \

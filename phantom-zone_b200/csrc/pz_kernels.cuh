@@ -70,8 +70,9 @@ cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u
                         int trivial, cudaStream_t s);
 // reduce_output: leave every output word reduced mod q_ks (otherwise the
 // words may carry multiples of q_ks, and consumers mask with q_ks - 1)
+// ct: ciphertexts per CTA (8, 16 or 32)
 cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
-                      size_t count, u32 *out, cudaStream_t s, bool reduce_output);
+                      size_t count, u32 *out, cudaStream_t s, bool reduce_output, int ct = KS_TILE_CT);
 cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
                        const unsigned char *gates, u64 *out, size_t count, u64 *rlwe_dbg,
                        int grid_limit, cudaStream_t s, int variant);

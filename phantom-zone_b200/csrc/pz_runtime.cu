@@ -190,12 +190,19 @@ namespace pz {
 int effective_variant(pz_ctx *c, size_t count) {
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   if (c->logn != 11 || !d1) return c->pbs_variant;
+  const pz_ctx::Tuned &t = c->tuned[size_bucket(count)];
+  if (t.variant >= 0) return t.variant;
   if (c->split_below < 0) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     c->split_below = sms / 2;
   }
   return (count <= (size_t)c->split_below) ? pz::PBS_SPLIT : c->pbs_variant;
+}
+
+int effective_ks_ct(const pz_ctx *c, size_t count) {
+  const pz_ctx::Tuned &t = c->tuned[size_bucket(count)];
+  return t.ks_ct ? t.ks_ct : c->ks_ct;
 }
 
 pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, const u64 *d_c0, const u64 *d_c1,
@@ -214,7 +221,8 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
   u32 *d_ks = d_ks_out ? d_ks_out : d_ks_scratch;
   const u32 ks_out_stride = d_ks_out ? c->P.lwe_n + 1 : stride;
   ks.out_stride = ks_out_stride;
-  cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s, d_ks_out != nullptr);
+  cudaError_t e = pz::launch_ks(ks, d_gates, d_c0, d_c1, count, d_ks, s, d_ks_out != nullptr,
+                                effective_ks_ct(c, count));
   if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   e = pz::launch_pbs((int)c->logn, d1, br, d_ks, ks_out_stride, d_gates, d_out, count, d_rlwe, c->grid_limit, s,
@@ -394,6 +402,7 @@ uint64_t pz_ctx_ntt_root(const pz_ctx *c) { return c ? c->root : 0; }
 
 pz_status pz_ctx_set_pbs_variant(pz_ctx *c, int v) {
   if (!c || v < 0 || v > pz::PBS_MAX_VARIANT) return PZ_ERR_INVALID_ARGUMENT;
+  for (auto &t : c->tuned) t.variant = -1;
   c->pbs_variant = v;
   return PZ_OK;
 }
@@ -674,6 +683,39 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
       bv = v;
     }
   }
+  // key-switch tile: ciphertexts per CTA, timed on `batch` uniform inputs
+  int bct = c->ks_ct;
+  u64 *d_c01 = nullptr;
+  const size_t L = (size_t)c->P.rlwe_n + 1;
+  if (e == cudaSuccess) e = cudaMalloc(&d_c01, 2 * batch * L * 8);
+  if (e == cudaSuccess) {
+    std::vector<u64> c01(2 * batch * L);
+    for (auto &v : c01) { st ^= st << 13; st ^= st >> 7; st ^= st << 17; v = st % c->P.rlwe_q; }
+    e = cudaMemcpy(d_c01, c01.data(), c01.size() * 8, cudaMemcpyHostToDevice);
+  }
+  pz::KsParams ksp = c->ks;
+  ksp.ksk = k->d_ksk;
+  ksp.raw = 0;
+  ksp.out_stride = cols;
+  double best_ks = 1e30;
+  for (int ct : {8, 16, 32}) {
+    if (e != cudaSuccess) break;
+    auto launch = [&]() {
+      return pz::launch_ks(ksp, d_g, d_c01, d_c01 + batch * L, batch, d_ks, c->stream, false, ct);
+    };
+    if ((e = launch()) != cudaSuccess) break;
+    if ((e = cudaEventRecord(a, c->stream)) != cudaSuccess) break;
+    for (int r = 0; r < 3 && e == cudaSuccess; r++) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(b, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float t = 0;
+    if (e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+    if (e == cudaSuccess && t / 3 < best_ks) {
+      best_ks = t / 3;
+      bct = ct;
+    }
+  }
+  cudaFree(d_c01);
   cudaFree(d_ks);
   cudaFree(d_g);
   cudaFree(d_out);
@@ -681,8 +723,24 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
   if (b) cudaEventDestroy(b);
   if (e != cudaSuccess) return cuda_fail(c, "pz_ctx_autotune", e);
   c->pbs_variant = bv;
+  c->ks_ct = bct;
+  c->tuned[pz::size_bucket(batch)] = pz_ctx::Tuned{bv, bct};
   if (variant) *variant = bv;
   if (ms) *ms = best;
+  return PZ_OK;
+}
+
+pz_status pz_ctx_set_ks_tile(pz_ctx *c, int ciphertexts) {
+  if (!c || (ciphertexts != 8 && ciphertexts != 16 && ciphertexts != 32)) return PZ_ERR_INVALID_ARGUMENT;
+  c->ks_ct = ciphertexts;
+  for (auto &t : c->tuned) t = pz_ctx::Tuned{};
+  return PZ_OK;
+}
+
+pz_status pz_ctx_launch_shape(pz_ctx *c, size_t gates, int *variant, int *ks_tile) {
+  if (!c) return PZ_ERR_INVALID_ARGUMENT;
+  if (variant) *variant = pz::effective_variant(c, gates);
+  if (ks_tile) *ks_tile = pz::effective_ks_ct(c, gates);
   return PZ_OK;
 }
 
@@ -796,7 +854,7 @@ pz_status pz_lwe_key_switch_device(pz_ctx *c, const pz_key *k, const uint64_t *d
   ks.Q_f = (double)c->P.lwe_q;
   ks.out_stride = c->P.lwe_n + 1;
   ks.raw = 1;
-  cudaError_t e = pz::launch_ks(ks, nullptr, d_in, nullptr, count, d_out, st, true);
+  cudaError_t e = pz::launch_ks(ks, nullptr, d_in, nullptr, count, d_out, st, true, pz::effective_ks_ct(c, count));
   if (e != cudaSuccess) return cuda_fail(c, "launch_ks", e);
   return PZ_OK;
 }

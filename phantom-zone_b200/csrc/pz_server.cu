@@ -56,10 +56,11 @@ struct pz_server {
     const pz_key *key = nullptr;  // the device key while resident (null: not resident)
     int param_id = 0;
     size_t key_bytes = 0;
-    // managed: the server owns the device key, imported from `blob` (the
-    // pz_key_export form) when a job needs it and released on eviction
+    // managed: the server owns the device key, imported from the caller's
+    // blob (the pz_key_export form) when a job needs it, released on eviction
     bool managed = false;
-    std::vector<unsigned char> blob;
+    const void *blob = nullptr;
+    size_t blob_bytes = 0;
     pz_key *owned = nullptr;
     bool virt_resident = false;  // dry run: residency without a device key
     size_t jobs_in_flight = 0;   // admitted, unfinished jobs: they pin the key
@@ -266,8 +267,9 @@ pz_status add_session_common(pz_server *s, int param_id, pz_ctx *ctx, const pz_k
   se.param_id = param_id;
   se.key_bytes = key ? key->bytes : key_bytes_of(P);
   se.managed = managed;
-  if (blob) se.blob.assign((const unsigned char *)blob, (const unsigned char *)blob + blob_bytes);
-  s->sessions.push_back(std::move(se));
+  se.blob = blob;
+  se.blob_bytes = blob_bytes;
+  s->sessions.push_back(se);
   s->max_n = std::max(s->max_n, P.lwe_n);
   s->max_br_q = std::max(s->max_br_q, P.br_q);
   s->max_d = std::max(s->max_d, P.lwe_d);
@@ -330,7 +332,7 @@ pz_status make_resident(pz_server *s, u32 sid, bool *fits) {
     se.virt_resident = true;
   } else {
     pz_key *k = nullptr;
-    pz_status st = pz_key_import(se.ctx, se.blob.data(), se.blob.size(), &k);
+    pz_status st = pz_key_import(se.ctx, se.blob, se.blob_bytes, &k);
     if (st != PZ_OK) return s->fail(st, std::string("managed session key import: ") + pz_last_error(se.ctx));
     se.owned = k;
     se.key = k;
@@ -485,7 +487,7 @@ void select_jobs(pz_server *s, std::vector<pz_server::Job *> &run) {
     }
   }
   const size_t sms = (size_t)std::max(1, s->sm_count);
-  const size_t cps = s->pbs_variant == 0 ? 2 : s->pbs_variant == 2 ? 4 : 3;
+  const size_t cps = (s->pbs_variant == 0 || s->pbs_variant == pz::PBS_BULK) ? 2 : s->pbs_variant == 2 ? 4 : 3;
   const size_t wave = sms * cps;
   const size_t cap = g <= wave ? std::max<size_t>(1, (g + sms - 1) / sms) * sms : (g + wave - 1) / wave * wave;
   std::stable_sort(opt.begin(), opt.end(), [](const pz_server::Job *a, const pz_server::Job *b) {
@@ -768,7 +770,8 @@ pz_status pz_server_stats_get(pz_server *s, pz_server_stats *out) {
 }
 
 pz_status pz_server_set_launch(pz_server *s, int pbs_variant, int grid_limit) {
-  if (!s || pbs_variant < 0 || pbs_variant >= pz::PBS_VARIANTS || grid_limit < 0) return PZ_ERR_INVALID_ARGUMENT;
+  if (!s || pbs_variant < 0 || pbs_variant > pz::PBS_MAX_VARIANT || pbs_variant == pz::PBS_SPLIT || grid_limit < 0)
+    return PZ_ERR_INVALID_ARGUMENT;
   s->pbs_variant = pbs_variant;
   s->grid_limit = grid_limit;
   return PZ_OK;
@@ -825,8 +828,11 @@ pz_status pz_server_autotune(pz_server *s, size_t batch, int *variant, int *grid
       CK(cudaMemcpy(d_out, outi.data(), batch * 4, cudaMemcpyHostToDevice), "cudaMemcpy") &&
       CK(cudaMemcpy(d_g, g.data(), batch, cudaMemcpyHostToDevice), "cudaMemcpy") &&
       CK(cudaEventCreate(&a), "cudaEventCreate") && CK(cudaEventCreate(&b), "cudaEventCreate")) {
-    const int nv = (s->logn == 11 && s->d1) ? pz::PBS_VARIANTS : 1;
-    for (int v = 0; v < nv && st == PZ_OK; v++) {
+    // one-CTA shapes (register caps 2/3/4 CTAs per SM) and the staged-key shape
+    const int shapes[4] = {0, 1, 2, pz::PBS_BULK};
+    const int nv = (s->logn == 11 && s->d1) ? 4 : 1;
+    for (int vi = 0; vi < nv && st == PZ_OK; vi++) {
+      const int v = shapes[vi];
       for (int gi = 0; gi < 2 && st == PZ_OK; gi++) {
         auto launch = [&]() {
           return pz::launch_pbs_ragged(s->logn, s->d1, s->d_br, d_desc, s->max_br_q, s->max_n, d_ks, s->ks_stride,

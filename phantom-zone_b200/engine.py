@@ -205,11 +205,23 @@ class Engine:
         return n.value
 
     def autotune(self, key, batch=2368):
-        """Pick the fastest blind-rotation variant for this context on `batch` gates."""
+        """Pick the fastest blind-rotation variant and key-switch tile for
+        this context on `batch` gates (cached for batches of that size bucket)."""
         v, ms = ctypes.c_int(), ctypes.c_double()
         check(lib().pz_ctx_autotune(self.h, key.h, int(batch), ctypes.byref(v), ctypes.byref(ms)), self.h,
               "pz_ctx_autotune")
-        return {"variant": v.value, "ms": ms.value}
+        return {"variant": v.value, "ms": ms.value, "ks_tile": self.launch_shape(batch)["ks_tile"]}
+
+    def set_ks_tile(self, ciphertexts):
+        """Key-switch ciphertexts per CTA (8, 16, 32); clears the tuned choices."""
+        check(lib().pz_ctx_set_ks_tile(self.h, int(ciphertexts)), self.h, "pz_ctx_set_ks_tile")
+
+    def launch_shape(self, gates):
+        """The blind-rotation variant and key-switch tile a batch of `gates` uses."""
+        v, t = ctypes.c_int(), ctypes.c_int()
+        check(lib().pz_ctx_launch_shape(self.h, int(gates), ctypes.byref(v), ctypes.byref(t)), self.h,
+              "pz_ctx_launch_shape")
+        return {"variant": v.value, "ks_tile": t.value}
 
     # -- keys --------------------------------------------------------------
     def upload_key(self, rgsw, autos, lwe_ksk):

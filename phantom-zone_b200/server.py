@@ -57,10 +57,13 @@ class Server:
 
     def add_managed_session(self, engine, key_blob):
         """A session whose device key the server imports from `key_blob` (the
-        bytes of DeviceKey.export()) when a job needs it and evicts when the
-        key budget calls for room (least recently used, no job in flight)."""
+        bytes of DeviceKey.export(), kept referenced here) when a job needs it
+        and evicts when the key budget calls for room (least recently used,
+        no job in flight).  Sessions may share one blob object."""
         sid = ctypes.c_uint32()
-        blob = bytes(key_blob)  # the server keeps its own copy
+        blob = key_blob if isinstance(key_blob, bytes) else bytes(key_blob)
+        self._blobs = getattr(self, "_blobs", {})
+        self._blobs[id(blob)] = blob  # the server reads it on every import: keep it alive
         self._chk(lib().pz_server_add_managed_session(self.h, engine.h, blob, len(blob), ctypes.byref(sid)),
                   "add_managed_session")
         self.L = engine.L

@@ -144,6 +144,32 @@ def test_lwe_key_switch(gpu_available, param):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
+@pytest.mark.parametrize("tile", [8, 16, 32])
+def test_lwe_key_switch_every_tile(gpu_available, param, tile):
+    """The key switch with 8, 16 and 32 ciphertexts per CTA (the tiles the
+    autotuner picks from) equals the oracle, on a batch that leaves a partial
+    last tile and on one large enough to run unsplit (grid.z = 1)."""
+    ev, _, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    qk = ev.info.lwe_q
+    r = rng(0x42 + tile)
+    try:
+        eng.set_ks_tile(tile)
+        for count in (tile + 5, 4 * 148 * tile // 8 + 3):
+            x = r.uniform_mod(qk + 1, count * ev.L).reshape(count, ev.L)
+            x[0, :] = qk
+            idx = np.concatenate([np.arange(min(count, 24)), count - 1 - np.arange(8)])
+            want = np.stack([okey.lwe_key_switch(x[i]) for i in idx])
+            out = to_dev(np.zeros((count, ev.n + 1), np.uint32))
+            eng.lwe_key_switch_device(dkey, to_dev(x), out)
+            got = to_host(out, np.uint32).astype(np.uint64).reshape(count, -1)
+            assert np.array_equal(got[idx], want), (tile, count)
+            assert eng.launch_shape(count)["ks_tile"] == tile
+    finally:
+        eng.set_ks_tile(16)
+
+
 def _gate_inputs(ev, secrets, count, tag):
     s = secrets[0]
     r = rng(tag)
@@ -237,11 +263,14 @@ def test_ctx_autotune_keeps_results(gpu_available):
     try:
         t = eng.autotune(dkey, 296)
         assert t["variant"] in (0, 1, 2, 3, 4) and t["ms"] > 0 and eng.pbs_variant == t["variant"]
+        assert t["ks_tile"] in (8, 16, 32)
+        assert eng.launch_shape(296) == {"variant": t["variant"], "ks_tile": t["ks_tile"]}
         bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, 4, 0x7F)
         gates = np.array([O.GATES[g] for g in ["and", "nand", "xor", "nor"]], np.uint8)
         assert np.array_equal(eng.gate_batch(dkey, gates, c0, c1), okey.gate_batch(gates, c0, c1, threads=4))
     finally:
         eng.pbs_variant = old
+        eng.set_ks_tile(16)
 
 
 def test_split_kernel_many_items_per_cluster(gpu_available):

@@ -194,7 +194,7 @@ def test_autotune_then_run(gpu_available):
     e2, k2, ev2, s2, _ = session("I_2P_LB_SR")
     a, b = S.add_session(e8, k8), S.add_session(e2, k2)
     t = S.autotune(296)
-    assert t["variant"] in (0, 1, 2) and t["ms"] > 0 and t["grid_limit"] >= 0
+    assert t["variant"] in (0, 1, 2, 4) and t["ms"] > 0 and t["grid_limit"] >= 0
     inp = enc_pair(ev2, s2, 9, 200, 7)
     C = circuit("lt")
     j = S.submit(b, C, inp)
@@ -231,3 +231,32 @@ def test_managed_sessions_evict_and_reimport_keys(gpu_available):
     st = S.stats()
     assert st["key_imports"] == 3 and st["key_evictions"] == 2 and st["failed"] == 0
     assert eng.device_error() == 0
+
+
+@pytest.mark.parametrize("grid_limit", [0, 5])
+def test_staged_key_ragged_shape(gpu_available, grid_limit):
+    """The staged-key ragged blind rotation (launch shape 4: every operation's
+    key rows come into shared memory by bulk copy, each item with its own
+    session's key) -- one CTA per gate, and a grid of 5 CTAs that each run
+    many items in turn -- gives the words of every job run alone."""
+    P = pz()
+    S = P.Server(device=0, arena_bytes=1 << 28, max_items=4096)
+    S.set_launch(4, grid_limit)
+    params = ["I_2P_LB_SR", "I_8P", "NI_8P"]
+    sids = {p: S.add_session(*session(p)[:2]) for p in params}
+    jobs = []
+    for k, p in enumerate(params):
+        eng, key, ev, s, _ = session(p)
+        for op in ["mul", "lt"]:
+            x, y = 31 * k + 7, 200 - 13 * k
+            C = circuit(op)
+            inp = enc_pair(ev, s, x, y, 60 + 2 * k + (op == "lt"))
+            jobs.append((p, op, x, y, C, inp, S.submit(sids[p], C, inp)))
+    S.run_until_idle()
+    assert S.stats()["failed"] == 0
+    for p, op, x, y, C, inp, j in jobs:
+        eng, key, ev, s, _ = session(p)
+        got = S.result(j)
+        assert np.array_equal(got, C.run(eng, key, inp)), f"{p} {op}: words differ from the job alone"
+        expect(op, ev, s, got, x, y)
+    assert session("NI_8P")[0].device_error() == 0
