@@ -124,6 +124,20 @@ def schedule_work(p, ks):
     return total
 
 
+def measured_hbm_gbs():
+    """HBM copy bandwidth: MEASURED_PEAKS.json's when the file is present,
+    else the fallback figure measured earlier on this pool's B200s."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        rec = json.load(open(path))
+        for k in ("hbm_gbs", "hbm_copy_gbs"):
+            if k in rec:
+                return {"gbs": float(rec[k]), "source": f"MEASURED_PEAKS.json {k}"}
+    except (OSError, ValueError):
+        pass
+    return {"gbs": 6650.0, "source": "fallback (no MEASURED_PEAKS.json): 6.65 TB/s measured earlier on this pool"}
+
+
 def traffic_record(P, variant, B):
     """DRAM bytes per launch of B bootstraps from the committed ncu capture
     (profiles/pbs_kernel_traffic.json, bytes per bootstrap of a warm launch),
@@ -435,13 +449,23 @@ def microbench(P, torch, device, count=4096, reps=5):
     ep_ms = a.elapsed_time(b) / reps
     key.release()
     eng.close()
+    peak_imad = P.probe_imad_rate(device)
+    hbm = measured_hbm_gbs()
+    ntt_mm_s = mm / ((fwd_ms + inv_ms) / 1e3)
+    ntt_gbs = 4 * count * N * 8 / ((fwd_ms + inv_ms) / 1e3) / 1e9
+    ep_mm_s = count * 57344 / (ep_ms / 1e3)
     return {"config": f"{count} polys N={N} mod Q fwd+inv NTT; {count} RLWE x RGSW at I_2P_LB_SR (index i mod n)",
             "ntt_fwd_ms": fwd_ms, "ntt_inv_ms": inv_ms, "ntt_roundtrip_exact": roundtrip_ok,
             "ntt_polys_per_s": count / ((fwd_ms + inv_ms) / 1e3),
-            "ntt_modmul_per_s": mm / ((fwd_ms + inv_ms) / 1e3),
-            "ntt_hbm_gbs": 4 * count * N * 8 / ((fwd_ms + inv_ms) / 1e3) / 1e9,
+            "ntt_modmul_per_s": ntt_mm_s, "ntt_hbm_gbs": ntt_gbs,
+            "ntt_int_frac": ntt_mm_s * C_MM / peak_imad,
+            "ntt_hbm_frac": ntt_gbs / hbm["gbs"] if hbm["gbs"] else None,
             "ext_product_ms": ep_ms, "ext_products_per_s": count / (ep_ms / 1e3),
-            "ext_product_modmul_per_s": count * 57344 / (ep_ms / 1e3)}
+            "ext_product_modmul_per_s": ep_mm_s, "ext_product_int_frac": ep_mm_s * C_MM / peak_imad,
+            "roof": {"int_peak_imad_per_s": peak_imad, "int_peak_source": "pz_probe_imad_rate on this GPU",
+                     "hbm_gbs": hbm["gbs"], "hbm_source": hbm["source"],
+                     "what": "fractions: algorithmic modmuls x 10 IMAD / the IMAD peak; bytes in + out of both "
+                             "passes / the HBM copy bandwidth"}}
 
 
 def ni_ingest_bench(P, torch, device, count=64, reps=3):
