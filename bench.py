@@ -505,13 +505,32 @@ def ni_ingest_bench(P, torch, device, count=64, reps=3):
     all_ms = a.elapsed_time(b) / reps
     ks_ms = b.elapsed_time(c) / reps
     logn = int(np.log2(N))
-    mm = count * (p.ni_ks_d * (N // 2) * logn + 2 * ((N // 2) * logn + N) + 2 * p.ni_ks_d * N)
+    per_rlwe = p.ni_ks_d * (N // 2) * logn + 2 * ((N // 2) * logn + N) + 2 * p.ni_ks_d * N
+    mm = count * per_rlwe
+    del d_l
+    # the key switch alone at a serving-sized batch (the extraction of that
+    # many bools would not fit: N + 1 words per bool)
+    big = 1024
+    d_rb = torch.from_numpy(rng.integers(0, p.rlwe_q, (big, 2, N), dtype=np.uint64).view(np.int64)).cuda()
+    d_kb = torch.empty_like(d_rb)
+    eng.ni_key_switch_device(ksk, d_rb, d_kb)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        eng.ni_key_switch_device(ksk, d_rb, d_kb)
+    b.record()
+    torch.cuda.synchronize()
+    big_ms = a.elapsed_time(b) / reps
+    peak = P.probe_imad_rate(device)
     ksk.release()
     eng.close()
-    del d_l
-    return {"config": f"NI_8P, {count} seeded RLWEs = {count * N} bools: unseed + rlwe_key_switch (d=50) + extract",
+    return {"config": f"NI_8P, {count} seeded RLWEs = {count * N} bools: unseed + rlwe_key_switch (d=50) + extract; "
+                      f"key switch alone also at {big} RLWEs",
             "ingest_ms": all_ms, "bools_per_s": count * N / (all_ms / 1e3), "key_switch_ms": ks_ms,
-            "rlwe_key_switches_per_s": count / (ks_ms / 1e3), "key_switch_modmul_per_s": mm / (ks_ms / 1e3)}
+            "rlwe_key_switches_per_s": count / (ks_ms / 1e3), "key_switch_modmul_per_s": mm / (ks_ms / 1e3),
+            "key_switch_int_frac": mm / (ks_ms / 1e3) * C_MM / peak,
+            f"key_switch_{big}_ms": big_ms, f"rlwe_key_switches_per_s_{big}": big / (big_ms / 1e3),
+            f"key_switch_int_frac_{big}": big * per_rlwe / (big_ms / 1e3) * C_MM / peak}
 
 
 def key_upload_bench(P, device):

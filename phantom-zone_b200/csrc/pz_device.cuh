@@ -168,6 +168,47 @@ __device__ __forceinline__ u64 umulhi_lo2(u64 a, u64 b) {
   return t;
 }
 
+// w v - Q floor~(ws v / 2^64) mod 2^64 for Q = Q_N2048, the quotient from
+// umulhi_lo2 (at most 2 short): the Shoup product of the N = 2048 butterflies,
+// in [0, 4Q) for any 64-bit v.  PZ_BFLY_PTX selects a form written in 32-bit
+// PTX whose 64-bit additions ride on the multiply-adds (a 64-bit addend of
+// mad.wide), an alternative kept for same-box comparisons.
+__device__ __forceinline__ u64 shoup_spq(u64 v, u64 w, u64 ws) {
+#ifndef PZ_BFLY_PTX
+  return w * v - mulq_n2048(umulhi_lo2(ws, v));
+#else
+  u64 r;
+  asm("{\n\t"
+      ".reg .u32 v0, v1, w0, w1, s0, s1, h1, h2, q0, q1, t0, t1, z;\n\t"
+      ".reg .u64 qt, wy, t, hs;\n\t"
+      "mov.b64 {v0, v1}, %1;\n\t"
+      "mov.b64 {w0, w1}, %2;\n\t"
+      "mov.b64 {s0, s1}, %3;\n\t"
+      "mul.hi.u32 h1, s1, v0;\n\t"
+      "mul.hi.u32 h2, s0, v1;\n\t"
+      "add.cc.u32 h1, h1, h2;\n\t"
+      "addc.u32 h2, 0, 0;\n\t"
+      "mov.b64 hs, {h1, h2};\n\t"
+      "mad.wide.u32 qt, s1, v1, hs;\n\t"      // quotient, at most 2 short
+      "mul.wide.u32 wy, w0, v0;\n\t"
+      "mov.b64 {t0, t1}, wy;\n\t"
+      "mad.lo.u32 t1, w0, v1, t1;\n\t"
+      "mad.lo.u32 t1, w1, v0, t1;\n\t"
+      "mov.b64 wy, {t0, t1};\n\t"             // w v mod 2^64
+      "mov.b64 {q0, q1}, qt;\n\t"
+      "mad.wide.u32 t, q0, 77823, wy;\n\t"    // + 77823 qt (low word of qt)
+      "mov.b64 {t0, t1}, t;\n\t"
+      "mad.lo.u32 t1, q1, 77823, t1;\n\t"     // + 77823 qt (high word)
+      "shl.b32 z, q0, 22;\n\t"
+      "sub.u32 t1, t1, z;\n\t"                // - qt 2^54
+      "mov.b64 %0, {t0, t1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(v), "l"(w), "l"(ws));
+  return r;
+#endif
+}
+
 // Forward CT butterfly (the x' = x + wy, y' = x - wy of ntt.rs:31-49) without
 // Harvey's conditional subtraction: wy is a Shoup product, so both outputs
 // grow by a bounded multiple of q per stage and the Shoup product accepts any
@@ -179,7 +220,7 @@ __device__ __forceinline__ u64 umulhi_lo2(u64 a, u64 b) {
 template <bool SPQ>
 __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
   if (SPQ) {
-    const u64 t = w * y - mulq_n2048(umulhi_lo2(ws, y));
+    const u64 t = shoup_spq(y, w, ws);
     y = x + (Q_N2048 << 2) - t;
     x = x + t;
   } else {
@@ -204,7 +245,7 @@ __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
   if (SPQ) {
     const u64 t = x + (u64)K * Q_N2048 - y;
     const u64 u = x + y;
-    y = w * t - mulq_n2048(umulhi_lo2(ws, t));
+    y = shoup_spq(t, w, ws);
     x = u;
   } else {
     const u64 q2 = q << 1;
@@ -274,89 +315,124 @@ __device__ __forceinline__ void inv_round_reduce(u64 (&x)[8], u64 (&y)[8]) {
 }
 
 // Forward radix-8 round k: stages with m = 8^k, 2m and 4m groups; blk is the
-// group index of this thread in the first of them.
-template <int LOGN, bool TWO>
+// group index of this thread in the first of them.  PF: the round's seven
+// twiddle pairs are all loaded before its first butterfly (one load latency
+// per round instead of one per stage; 14 more live registers).
+template <int LOGN, bool TWO, bool PF = false>
 __device__ __forceinline__ void fwd_round8(u64 (&x)[8], u64 (&y)[8], int k, int j, const RingConsts &rc) {
   const int m = 1 << (3 * k);
   const int blk = j >> (LOGN - 3 * k - 3);
   const u64 q = rc.q;
-  u64 w, ws;
-  tw(rc.fw, m + blk, w, ws);
+  u64 w[7], ws[7];  // slots: 0 (stage m), 1-2 (stage 2m), 3-6 (stage 4m)
+  if (PF) {
+    tw(rc.fw, m + blk, w[0], ws[0]);
 #pragma unroll
-  for (int r = 0; r < 4; r++) fbf2<LOGN, TWO>(x, y, r, r + 4, w, ws, q);
+    for (int h = 0; h < 2; h++) tw(rc.fw, 2 * m + 2 * blk + h, w[1 + h], ws[1 + h]);
+#pragma unroll
+    for (int h = 0; h < 4; h++) tw(rc.fw, 4 * m + 4 * blk + h, w[3 + h], ws[3 + h]);
+  }
+  if (!PF) tw(rc.fw, m + blk, w[0], ws[0]);
+#pragma unroll
+  for (int r = 0; r < 4; r++) fbf2<LOGN, TWO>(x, y, r, r + 4, w[0], ws[0], q);
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    tw(rc.fw, 2 * m + 2 * blk + h, w, ws);
-    fbf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    fbf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    if (!PF) tw(rc.fw, 2 * m + 2 * blk + h, w[1 + h], ws[1 + h]);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w[1 + h], ws[1 + h], q);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w[1 + h], ws[1 + h], q);
   }
 #pragma unroll
   for (int h = 0; h < 4; h++) {
-    tw(rc.fw, 4 * m + 4 * blk + h, w, ws);
-    fbf2<LOGN, TWO>(x, y, 2 * h, 2 * h + 1, w, ws, q);
+    if (!PF) tw(rc.fw, 4 * m + 4 * blk + h, w[3 + h], ws[3 + h]);
+    fbf2<LOGN, TWO>(x, y, 2 * h, 2 * h + 1, w[3 + h], ws[3 + h], q);
   }
 }
 
-template <int LOGN, bool TWO>
+template <int LOGN, bool TWO, bool PF = false>
 __device__ __forceinline__ void inv_round8(u64 (&x)[8], u64 (&y)[8], int k, int j, const RingConsts &rc) {
   const int m = 1 << (3 * k);
   const int blk = j >> (LOGN - 3 * k - 3);
   const u64 q = rc.q;
-  u64 w, ws;
+  u64 w[7], ws[7];  // slots: 0-3 (stage 4m), 4-5 (stage 2m), 6 (stage m)
+  if (PF) {
+#pragma unroll
+    for (int h = 0; h < 4; h++) tw(rc.iw, 4 * m + 4 * blk + h, w[h], ws[h]);
+#pragma unroll
+    for (int h = 0; h < 2; h++) tw(rc.iw, 2 * m + 2 * blk + h, w[4 + h], ws[4 + h]);
+    tw(rc.iw, m + blk, w[6], ws[6]);
+  }
   // (N = 2048) inputs < 2Q; sums reach < 4Q, 8Q, 16Q over the three stages
 #pragma unroll
   for (int h = 0; h < 4; h++) {
-    tw(rc.iw, 4 * m + 4 * blk + h, w, ws);
-    ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w, ws, q);
+    if (!PF) tw(rc.iw, 4 * m + 4 * blk + h, w[h], ws[h]);
+    ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w[h], ws[h], q);
   }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    tw(rc.iw, 2 * m + 2 * blk + h, w, ws);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    if (!PF) tw(rc.iw, 2 * m + 2 * blk + h, w[4 + h], ws[4 + h]);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
   }
-  tw(rc.iw, m + blk, w, ws);
+  if (!PF) tw(rc.iw, m + blk, w[6], ws[6]);
 #pragma unroll
-  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO, 8>(x, y, r, r + 4, w, ws, q);
+  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO, 8>(x, y, r, r + 4, w[6], ws[6], q);
   inv_round_reduce<LOGN, TWO>(x, y);
 }
 
-// Trailing 2-stage round (stages with N/4 and N/2 groups).
-template <int LOGN, bool TWO>
+// Trailing 2-stage round (stages with N/4 and N/2 groups); PF as for the
+// radix-8 rounds (six twiddle pairs).
+template <int LOGN, bool TWO, bool PF = false>
 __device__ __forceinline__ void fwd_round4(u64 (&x)[8], u64 (&y)[8], int j, const RingConsts &rc) {
   constexpr int N = 1 << LOGN;
   const u64 q = rc.q;
-  u64 w, ws;
+  u64 w[6], ws[6];  // per h: slot 3h (stage N/4), 3h + 1 + e (stage N/2)
+  if (PF) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
+      tw(rc.fw, N / 4 + g, w[3 * h], ws[3 * h]);
+#pragma unroll
+      for (int e = 0; e < 2; e++) tw(rc.fw, N / 2 + 2 * g + e, w[3 * h + 1 + e], ws[3 * h + 1 + e]);
+    }
+  }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
-    tw(rc.fw, N / 4 + g, w, ws);
-    fbf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    fbf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    if (!PF) tw(rc.fw, N / 4 + g, w[3 * h], ws[3 * h]);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 0, 4 * h + 2, w[3 * h], ws[3 * h], q);
+    fbf2<LOGN, TWO>(x, y, 4 * h + 1, 4 * h + 3, w[3 * h], ws[3 * h], q);
 #pragma unroll
     for (int e = 0; e < 2; e++) {
-      tw(rc.fw, N / 2 + 2 * g + e, w, ws);
-      fbf2<LOGN, TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
+      if (!PF) tw(rc.fw, N / 2 + 2 * g + e, w[3 * h + 1 + e], ws[3 * h + 1 + e]);
+      fbf2<LOGN, TWO>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w[3 * h + 1 + e], ws[3 * h + 1 + e], q);
     }
   }
 }
 
-template <int LOGN, bool TWO>
+template <int LOGN, bool TWO, bool PF = false>
 __device__ __forceinline__ void inv_round4(u64 (&x)[8], u64 (&y)[8], int j, const RingConsts &rc) {
   constexpr int N = 1 << LOGN;
   const u64 q = rc.q;
-  u64 w, ws;
+  u64 w[6], ws[6];  // per h: slots 3h + e (stage N/2), 3h + 2 (stage N/4)
+  if (PF) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
+#pragma unroll
+      for (int e = 0; e < 2; e++) tw(rc.iw, N / 2 + 2 * g + e, w[3 * h + e], ws[3 * h + e]);
+      tw(rc.iw, N / 4 + g, w[3 * h + 2], ws[3 * h + 2]);
+    }
+  }
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     const int g = (j >> 5) * 64 + (j & 31) + (h << 5);
 #pragma unroll
     for (int e = 0; e < 2; e++) {
-      tw(rc.iw, N / 2 + 2 * g + e, w, ws);
-      ibf2<LOGN, TWO, 2>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w, ws, q);
+      if (!PF) tw(rc.iw, N / 2 + 2 * g + e, w[3 * h + e], ws[3 * h + e]);
+      ibf2<LOGN, TWO, 2>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w[3 * h + e], ws[3 * h + e], q);
     }
-    tw(rc.iw, N / 4 + g, w, ws);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    if (!PF) tw(rc.iw, N / 4 + g, w[3 * h + 2], ws[3 * h + 2]);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w[3 * h + 2], ws[3 * h + 2], q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w[3 * h + 2], ws[3 * h + 2], q);
   }
   inv_round_reduce<LOGN, TWO>(x, y);  // (N = 2048) sums < 8Q -> < 2Q
 }
@@ -426,7 +502,7 @@ __device__ __forceinline__ void xchg(u64 (&x)[8], u64 (&y)[8], u64 *sm, int j) {
 // sm: N words (2N with TWO).  The rounds run in a loop (one copy of the round
 // body); the exchanges between them are layout-specialised and picked by a
 // block-uniform switch.
-template <int LOGN, bool TWO>
+template <int LOGN, bool TWO, bool PF = false>
 __device__ __forceinline__ void ntt_fwd(u64 (&x)[8], u64 (&y)[8], u64 *sm, const RingConsts &rc) {
   typedef NttShape<LOGN> S;
   static_assert(S::FULL == 3, "three radix-8 rounds");
@@ -435,11 +511,11 @@ __device__ __forceinline__ void ntt_fwd(u64 (&x)[8], u64 (&y)[8], u64 *sm, const
   for (int k = 0; k < 3; k++) {
     if (k == 1) xchg<LOGN, 0, 1, TWO>(x, y, sm, j);
     else if (k == 2) xchg<LOGN, 1, 2, TWO>(x, y, sm, j);
-    fwd_round8<LOGN, TWO>(x, y, k, j, rc);
+    fwd_round8<LOGN, TWO, PF>(x, y, k, j, rc);
   }
   if constexpr (S::PARTIAL) {
     xchg<LOGN, 2, 3, TWO>(x, y, sm, j);
-    fwd_round4<LOGN, TWO>(x, y, j, rc);
+    fwd_round4<LOGN, TWO, PF>(x, y, j, rc);
   }
 }
 

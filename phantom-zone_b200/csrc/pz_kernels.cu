@@ -122,6 +122,12 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T)
 // its other copy in flight.
 // ---------------------------------------------------------------------------
 constexpr int NTTB_N = 2048;
+// every round's twiddles loaded before its first butterfly (PZ_NTTB_NO_PF: per stage)
+#ifdef PZ_NTTB_NO_PF
+constexpr bool NTTB_PF = false;
+#else
+constexpr bool NTTB_PF = true;
+#endif
 constexpr size_t NTTB_SMEM = (size_t)6 * NTTB_N * 8 + 16;  // exchange 2N | 2 stages of 2N | 2 mbarriers
 
 // Last inverse round (k = 0) with N^{-1} folded into its final stage; values
@@ -130,22 +136,22 @@ template <bool TWO>
 __device__ __forceinline__ void inv_round8_last_scaled(u64 (&x)[8], u64 (&y)[8], const RingConsts &rc) {
   constexpr int LOGN = 11;
   const u64 q = rc.q;
-  u64 w, ws;
+  u64 w[6], ws[6];  // all of the round's twiddles first (one load latency)
 #pragma unroll
-  for (int h = 0; h < 4; h++) {
-    tw(rc.iw, 4 + h, w, ws);
-    ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w, ws, q);
-  }
+  for (int h = 0; h < 4; h++) tw(rc.iw, 4 + h, w[h], ws[h]);
+#pragma unroll
+  for (int h = 0; h < 2; h++) tw(rc.iw, 2 + h, w[4 + h], ws[4 + h]);
+#pragma unroll
+  for (int h = 0; h < 4; h++) ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w[h], ws[h], q);
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    tw(rc.iw, 2 + h, w, ws);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w, ws, q);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w, ws, q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
+    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
   }
   auto last = [&](u64 &a, u64 &b) {  // sums < 16Q, b < 8Q here
     const u64 u = a + b, t = a + 8 * Q_N2048 - b;
-    a = rc.n_inv * u - mulq_n2048(umulhi_lo2(rc.n_inv_s, u));
-    b = rc.iw1n * t - mulq_n2048(umulhi_lo2(rc.iw1n_s, t));
+    a = shoup_spq(u, rc.n_inv, rc.n_inv_s);
+    b = shoup_spq(t, rc.iw1n, rc.iw1n_s);
   };
 #pragma unroll
   for (int r = 0; r < 4; r++) {
@@ -160,11 +166,11 @@ __device__ __forceinline__ void ntt_inv_scaled(u64 (&x)[8], u64 (&y)[8], u64 *sm
   constexpr int LOGN = 11;
   const int j = tid_opaque();
   __syncthreads();
-  inv_round4<LOGN, TWO>(x, y, j, rc);
+  inv_round4<LOGN, TWO, NTTB_PF>(x, y, j, rc);
   xchg<LOGN, 3, 2, TWO>(x, y, sm, j);
-  inv_round8<LOGN, TWO>(x, y, 2, j, rc);
+  inv_round8<LOGN, TWO, NTTB_PF>(x, y, 2, j, rc);
   xchg<LOGN, 2, 1, TWO>(x, y, sm, j);
-  inv_round8<LOGN, TWO>(x, y, 1, j, rc);
+  inv_round8<LOGN, TWO, NTTB_PF>(x, y, 1, j, rc);
   xchg<LOGN, 1, 0, TWO>(x, y, sm, j);
   inv_round8_last_scaled<TWO>(x, y, rc);
 }
@@ -219,7 +225,7 @@ __global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t co
         x[r] = sx[pos_coef<LOGN>(j, r)];
         y[r] = sy[pos_coef<LOGN>(j, r)];
       }
-      ntt_fwd<LOGN, true>(x, y, xs, rc);
+      ntt_fwd<LOGN, true, NTTB_PF>(x, y, xs, rc);
 #pragma unroll
       for (int h = 0; h < 2; h++) {  // registers 4h..4h+3: four consecutive evaluation positions
         const int o = pos_eval<LOGN>(j, 4 * h);
