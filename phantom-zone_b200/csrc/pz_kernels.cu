@@ -298,8 +298,8 @@ __device__ __forceinline__ void mac_pair(u64 (&x)[8], u64 (&y)[8], const u64 *ka
       mul128(xv, b[e], hi2, lo2);
       mac128(yv, c[e], hi, lo);
       mac128(yv, d[e], hi2, lo2);
-      x[r] = redc(hi, lo, q, qi);
-      y[r] = redc(hi2, lo2, q, qi);
+      x[r] = redc_br<LOGN>(hi, lo, q, qi);
+      y[r] = redc_br<LOGN>(hi2, lo2, q, qi);
     }
   }
 }
@@ -323,8 +323,8 @@ __device__ __forceinline__ void mac_auto(u64 (&x)[8], u64 (&y)[8], const u64 *ka
       u64 hi, lo, hi2, lo2;
       mul128(x[r], a[e], hi, lo);
       mul128(x[r], b[e], hi2, lo2);
-      x[r] = redc(hi, lo, q, qi);
-      const u64 v = redc(hi2, lo2, q, qi) + y[r];
+      x[r] = redc_br<LOGN>(hi, lo, q, qi);
+      const u64 v = redc_br<LOGN>(hi2, lo2, q, qi) + y[r];
       y[r] = v >= q2 ? v - q2 : v;
     }
   }
@@ -984,8 +984,8 @@ __device__ __forceinline__ void mac_pair_staged(u64 (&x)[8], u64 (&y)[8], const 
       mul128(xv, b[e], hi2, lo2);
       mac128(yv, c[e], hi, lo);
       mac128(yv, d[e], hi2, lo2);
-      x[r] = redc(hi, lo, q, qi);
-      y[r] = redc(hi2, lo2, q, qi);
+      x[r] = redc_br<LOGN>(hi, lo, q, qi);
+      y[r] = redc_br<LOGN>(hi2, lo2, q, qi);
     }
   }
 }
@@ -1005,8 +1005,8 @@ __device__ __forceinline__ void mac_auto_staged(u64 (&x)[8], u64 (&y)[8], const 
       u64 hi, lo, hi2, lo2;
       mul128(x[r], a[e], hi, lo);
       mul128(x[r], b[e], hi2, lo2);
-      x[r] = redc(hi, lo, q, qi);
-      const u64 v = redc(hi2, lo2, q, qi) + y[r];
+      x[r] = redc_br<LOGN>(hi, lo, q, qi);
+      const u64 v = redc_br<LOGN>(hi2, lo2, q, qi) + y[r];
       y[r] = v >= q2 ? v - q2 : v;
     }
   }
@@ -1209,7 +1209,7 @@ __device__ __forceinline__ void mac_two_rows(u64 (&x)[8], const u64 (&y)[8], con
       u64 hi, lo;
       mul128(x[r], a[e], hi, lo);
       mac128(y[r], b[e], hi, lo);
-      x[r] = redc(hi, lo, q, qi);
+      x[r] = redc_br<LOGN>(hi, lo, q, qi);
     }
   }
 }
