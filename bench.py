@@ -438,15 +438,20 @@ def microbench(P, torch, device, count=4096, reps=5):
     key = eng.upload_key(*synthetic_key(p, 0x5EED))
     rl = torch.from_numpy(rng.integers(0, p.rlwe_q, (count, 2, N), dtype=np.uint64).view(np.int64)).cuda()
     idx = torch.arange(count, dtype=torch.int32, device="cuda") % p.lwe_n
-    eng.rlwe_by_rgsw_device(key, rl, idx)
-    torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(reps):
+    ep_by_shape = {}
+    for v in (0, 1, 2):  # register caps of 2 / 3 / 4 CTAs per SM
+        eng.pbs_variant = v
         eng.rlwe_by_rgsw_device(key, rl, idx)
-    b.record()
-    torch.cuda.synchronize()
-    ep_ms = a.elapsed_time(b) / reps
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(reps):
+            eng.rlwe_by_rgsw_device(key, rl, idx)
+        b.record()
+        torch.cuda.synchronize()
+        ep_by_shape[v] = a.elapsed_time(b) / reps
+    ep_variant = min(ep_by_shape, key=ep_by_shape.get)
+    ep_ms = ep_by_shape[ep_variant]
     key.release()
     eng.close()
     peak_imad = P.probe_imad_rate(device)
@@ -462,6 +467,7 @@ def microbench(P, torch, device, count=4096, reps=5):
             "ntt_hbm_frac": ntt_gbs / hbm["gbs"] if hbm["gbs"] else None,
             "ext_product_ms": ep_ms, "ext_products_per_s": count / (ep_ms / 1e3),
             "ext_product_modmul_per_s": ep_mm_s, "ext_product_int_frac": ep_mm_s * C_MM / peak_imad,
+            "ext_product_ms_by_variant": ep_by_shape, "ext_product_variant": ep_variant,
             "roof": {"int_peak_imad_per_s": peak_imad, "int_peak_source": "pz_probe_imad_rate on this GPU",
                      "hbm_gbs": hbm["gbs"], "hbm_source": hbm["source"],
                      "what": "fractions: algorithmic modmuls x 10 IMAD / the IMAD peak; bytes in + out of both "
@@ -844,14 +850,12 @@ def serving(P, device, sessions=64, rates=SERVING_RATES, arrivals=480, tight_key
     tune = S.autotune(2368)
     key_bytes = S.stats()["resident_key_bytes"]
     points = [serving_point(S, sids, templates, pool, r, arrivals, rng) for r in rates]
-    # the knee: the first offered load the server no longer keeps up with
-    # (throughput below 90 % of the offered gates, or p99 over twice the lightest load's)
+    # the knee: the first offered load at which queueing takes over (median
+    # latency over twice the lightest load's)
     mean_gates = sum(c.info()["gates"] for c in templates) / len(templates)
-    knee = None
     for pt in points:
-        if pt["value"] < 0.9 * pt["offered_circuits_per_s"] * mean_gates or pt["p99_ms"] > 2 * points[0]["p99_ms"]:
-            knee = pt["offered_circuits_per_s"]
-            break
+        pt["offered_gates_per_s"] = pt["offered_circuits_per_s"] * mean_gates
+    knee = next((pt["offered_circuits_per_s"] for pt in points if pt["p50_ms"] > 2 * points[0]["p50_ms"]), None)
     S.set_key_budget(tight_keys * max(kbytes))
     tight = serving_point(S, sids, templates, pool, rates[1], arrivals, rng)
     tight["key_budget_bytes"] = tight_keys * max(kbytes)

@@ -181,7 +181,10 @@ pz_status pz_probe_imad_rate(int device, double *imad_per_second);
 pz_status pz_not_batch_device(pz_ctx *ctx, const uint64_t *d_in, uint64_t *d_out, size_t words,
                               void *stream);
 
-/* Kernel-level entry points (device memory, asynchronous). */
+/* Kernel-level entry points (device memory, asynchronous).  The external
+ * product and the automorphism of the one-digit parameter sets run with the
+ * register cap of the context's blind-rotation variant (0 / 1 / 2: 2 / 3 / 4
+ * CTAs per SM; others: 3). */
 pz_status pz_ntt_forward_device(pz_ctx *ctx, uint64_t *d_polys, size_t count, void *stream);
 pz_status pz_ntt_backward_device(pz_ctx *ctx, uint64_t *d_polys, size_t count, void *stream);
 pz_status pz_rlwe_by_rgsw_device(pz_ctx *ctx, const pz_key *key, uint64_t *d_rlwe,

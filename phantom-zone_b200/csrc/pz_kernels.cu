@@ -471,10 +471,10 @@ __device__ __forceinline__ void bootstrap_op(u64 (&acc)[2][8], u32 op, const BrP
   }
 }
 
-// One-digit (D1) forms are register-capped to 3 CTAs per SM, the shape the
-// blind-rotation autotuner picks for the same operation body.
-template <int LOGN, bool D1>
-__global__ void __launch_bounds__(NttShape<LOGN>::T, D1 ? 3 : 1)
+// One-digit (D1) forms come register-capped for MINB = 2, 3 or 4 CTAs per SM,
+// picked like the blind rotation's launch shapes (the context's variant).
+template <int LOGN, bool D1, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
     ext_product_kernel(BrParams P, u64 *rlwe, const u32 *idx, size_t count, int trivial) {
   constexpr int N = 1 << LOGN;
   extern __shared__ u64 smem[];
@@ -498,8 +498,8 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, D1 ? 3 : 1)
   }
 }
 
-template <int LOGN, bool D1>
-__global__ void __launch_bounds__(NttShape<LOGN>::T, D1 ? 3 : 1)
+template <int LOGN, bool D1, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
     auto_kernel(BrParams P, u64 *rlwe, const u32 *slot, size_t count, int trivial) {
   constexpr int N = 1 << LOGN;
   extern __shared__ u64 smem[];
@@ -1521,34 +1521,42 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
   return e;
 }
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
-                               size_t count, int trivial, cudaStream_t s) {
+                               size_t count, int trivial, cudaStream_t s, int variant) {
   if (count == 0) return cudaSuccess;
   const size_t N = (size_t)1 << logn, smem = OP_REGIONS * N * 8;
   cudaError_t e;
-#define PZ_LAUNCH(LN, DD, TH)                                                                  \
-  if ((e = set_smem(ext_product_kernel<LN, DD>, smem)) != cudaSuccess) return e;              \
-  ext_product_kernel<LN, DD><<<grid_for(count), TH, smem, s>>>(P, rlwe, idx, count, trivial);
-  if (logn == 11 && d1) { PZ_LAUNCH(11, true, 256) }
-  else if (logn == 11) { PZ_LAUNCH(11, false, 256) }
-  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 64) }
-  else if (logn == 9) { PZ_LAUNCH(9, false, 64) }
+#define PZ_LAUNCH(LN, DD, MB, TH)                                                                  \
+  if ((e = set_smem(ext_product_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;              \
+  ext_product_kernel<LN, DD, MB><<<grid_for(count), TH, smem, s>>>(P, rlwe, idx, count, trivial);
+  if (logn == 11 && d1) {
+    if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
+    else if (variant == 2) { PZ_LAUNCH(11, true, 4, 256) }
+    else { PZ_LAUNCH(11, true, 3, 256) }
+  }
+  else if (logn == 11) { PZ_LAUNCH(11, false, 1, 256) }
+  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 1, 64) }
+  else if (logn == 9) { PZ_LAUNCH(9, false, 1, 64) }
   else return cudaErrorInvalidValue;
 #undef PZ_LAUNCH
   return cudaGetLastError();
 }
 
 cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *slot, size_t count,
-                        int trivial, cudaStream_t s) {
+                        int trivial, cudaStream_t s, int variant) {
   if (count == 0) return cudaSuccess;
   const size_t N = (size_t)1 << logn, smem = OP_REGIONS * N * 8;
   cudaError_t e;
-#define PZ_LAUNCH(LN, DD, TH)                                                           \
-  if ((e = set_smem(auto_kernel<LN, DD>, smem)) != cudaSuccess) return e;              \
-  auto_kernel<LN, DD><<<grid_for(count), TH, smem, s>>>(P, rlwe, slot, count, trivial);
-  if (logn == 11 && d1) { PZ_LAUNCH(11, true, 256) }
-  else if (logn == 11) { PZ_LAUNCH(11, false, 256) }
-  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 64) }
-  else if (logn == 9) { PZ_LAUNCH(9, false, 64) }
+#define PZ_LAUNCH(LN, DD, MB, TH)                                                           \
+  if ((e = set_smem(auto_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;              \
+  auto_kernel<LN, DD, MB><<<grid_for(count), TH, smem, s>>>(P, rlwe, slot, count, trivial);
+  if (logn == 11 && d1) {
+    if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
+    else if (variant == 2) { PZ_LAUNCH(11, true, 4, 256) }
+    else { PZ_LAUNCH(11, true, 3, 256) }
+  }
+  else if (logn == 11) { PZ_LAUNCH(11, false, 1, 256) }
+  else if (logn == 9 && d1) { PZ_LAUNCH(9, true, 1, 64) }
+  else if (logn == 9) { PZ_LAUNCH(9, false, 1, 64) }
   else return cudaErrorInvalidValue;
 #undef PZ_LAUNCH
   return cudaGetLastError();

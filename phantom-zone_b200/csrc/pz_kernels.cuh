@@ -64,10 +64,12 @@ cudaError_t launch_key_convert(int logn, const u64 *in, u64 *out, size_t npolys,
 // err: the context's device error word (DEVERR_* bits)
 cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s);
 cudaError_t launch_ntt_inv(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s);
+// variant: register cap of the one-digit forms as the blind rotation's
+// launch shapes 0 / 1 / 2 (2 / 3 / 4 CTAs per SM; other values: 3)
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
-                               size_t count, int trivial, cudaStream_t s);
+                               size_t count, int trivial, cudaStream_t s, int variant = 1);
 cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *slot, size_t count,
-                        int trivial, cudaStream_t s);
+                        int trivial, cudaStream_t s, int variant = 1);
 // reduce_output: leave every output word reduced mod q_ks (otherwise the
 // words may carry multiples of q_ks, and consumers mask with q_ks - 1)
 // ct: ciphertexts per CTA (8, 16 or 32)

@@ -820,7 +820,8 @@ pz_status pz_rlwe_by_rgsw_device(pz_ctx *c, const pz_key *k, uint64_t *d_rlwe, c
   br.rgsw = k->d_rgsw;
   br.autos = k->d_autos;
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
-  PZ_CK(c, pz::launch_ext_product((int)c->logn, d1, br, d_rlwe, d_idx, count, trivial, pick(c, stream)));
+  PZ_CK(c, pz::launch_ext_product((int)c->logn, d1, br, d_rlwe, d_idx, count, trivial, pick(c, stream),
+                                  c->pbs_variant));
   return PZ_OK;
 }
 
@@ -834,7 +835,7 @@ pz_status pz_rlwe_auto_device(pz_ctx *c, const pz_key *k, uint64_t *d_rlwe, cons
   br.rgsw = k->d_rgsw;
   br.autos = k->d_autos;
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
-  PZ_CK(c, pz::launch_auto((int)c->logn, d1, br, d_rlwe, d_slot, count, trivial, pick(c, stream)));
+  PZ_CK(c, pz::launch_auto((int)c->logn, d1, br, d_rlwe, d_slot, count, trivial, pick(c, stream), c->pbs_variant));
   return PZ_OK;
 }
 

@@ -367,8 +367,18 @@ pz_status ensure_device_buffers(pz_server *s) {
 }
 
 // Admit pending jobs in arrival order while their wires fit the arena and
-// their session's key is (or can be made) resident.
+// their session's key is (or can be made) resident.  Resident managed keys
+// over the budget (it may have been lowered) are evicted first, least
+// recently used idle ones, as far as idle ones go.
 pz_status admit(pz_server *s) {
+  while (s->managed_bytes > s->key_budget) {
+    pz_server::Session *victim = nullptr;
+    for (auto &o : s->sessions)
+      if (o.managed && s->resident(o) && o.jobs_in_flight == 0 && (!victim || o.last_use < victim->last_use))
+        victim = &o;
+    if (!victim) break;
+    evict(s, *victim);
+  }
   while (!s->pending.empty()) {
     pz_server::Job *j = s->pending.front();
     const size_t need = j->v.n_inputs + j->v.n_gates;

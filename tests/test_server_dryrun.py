@@ -231,3 +231,25 @@ def test_unmanaged_sessions_ignore_the_key_budget():
     S.run_until_idle()
     assert S.status(j)["state"] == P.server.DONE and S.resident(s0) and S.resident(s1)
     assert S.stats()["key_imports"] == 0
+
+
+def test_lowering_the_key_budget_evicts_idle_keys():
+    """Keys already resident over a lowered budget are evicted at the next
+    step, least recently used first, idle sessions only."""
+    P = pz()
+    S = P.Server(device=P.DRY_RUN, arena_bytes=(1 << 16) * L_of("NI_8P") * 8, max_items=4096)
+    kb = key_bytes("NI_8P")
+    sids = [S.add_virtual_managed_session(P.param_id("NI_8P")) for _ in range(4)]
+    for sid in sids:  # all four resident, used in order
+        S.submit(sid, u8_circuit("lt"))
+        S.run_until_idle()
+    assert all(S.resident(x) for x in sids)
+    j = S.submit(sids[0], u8_circuit("mul"))  # sids[0] busy, most recently used
+    S.step()
+    S.set_key_budget(2 * kb)
+    S.step()
+    # sids[1] and sids[2] were the least recently used idle keys
+    assert [S.resident(x) for x in sids] == [True, False, False, True]
+    assert S.stats()["resident_key_bytes"] == 2 * kb and S.stats()["key_evictions"] == 2
+    S.run_until_idle()
+    assert S.status(j)["state"] == P.server.DONE
