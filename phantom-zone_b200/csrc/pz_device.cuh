@@ -85,6 +85,54 @@ __device__ __forceinline__ u64 redc_br(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
   return redc(hi, lo, q, qinv_neg);
 }
 
+// hi:lo = x a + y c for x, y < 2^60 (lazy forward outputs, < 45 Q) and a, c
+// < Q (keys): in 32-bit limbs the middle column x0 a1 + x1 a0 + y0 c1 + y1 c0
+// stays below 2^62 and the high column below 2^51, so both accumulate with
+// mad.wide and no carries; only the low column and the final merge carry.
+// PZ_MAC_PTX selects it (a same-box comparison); otherwise two 64 x 64
+// products in C.
+__device__ __forceinline__ void sum2_128(u64 x, u64 a, u64 y, u64 c, u64 &hi, u64 &lo) {
+#ifdef PZ_MAC_PTX
+  asm("{\n\t"
+      ".reg .u32 x0, x1, a0, a1, y0, y1, c0, c1, l0, l1, b0, b1, m0, m1, h0, h1;\n\t"
+      ".reg .u64 mid, low, lowb, high;\n\t"
+      "mov.b64 {x0, x1}, %2;\n\t"
+      "mov.b64 {a0, a1}, %3;\n\t"
+      "mov.b64 {y0, y1}, %4;\n\t"
+      "mov.b64 {c0, c1}, %5;\n\t"
+      "mul.wide.u32 mid, y1, c0;\n\t"
+      "mad.wide.u32 mid, y0, c1, mid;\n\t"
+      "mad.wide.u32 mid, x1, a0, mid;\n\t"
+      "mad.wide.u32 mid, x0, a1, mid;\n\t"
+      "mul.wide.u32 high, y1, c1;\n\t"
+      "mad.wide.u32 high, x1, a1, high;\n\t"
+      "mul.wide.u32 low, x0, a0;\n\t"
+      "mul.wide.u32 lowb, y0, c0;\n\t"
+      "mov.b64 {l0, l1}, low;\n\t"
+      "mov.b64 {b0, b1}, lowb;\n\t"
+      "mov.b64 {m0, m1}, mid;\n\t"
+      "mov.b64 {h0, h1}, high;\n\t"
+      "add.cc.u32 l0, l0, b0;\n\t"
+      "addc.cc.u32 l1, l1, b1;\n\t"
+      "addc.cc.u32 h0, h0, m1;\n\t"
+      "addc.u32 h1, h1, 0;\n\t"
+      "add.cc.u32 l1, l1, m0;\n\t"
+      "addc.cc.u32 h0, h0, 0;\n\t"
+      "addc.u32 h1, h1, 0;\n\t"
+      "mov.b64 %0, {h0, h1};\n\t"
+      "mov.b64 %1, {l0, l1};\n\t"
+      "}"
+      : "=l"(hi), "=l"(lo)
+      : "l"(x), "l"(a), "l"(y), "l"(c));
+#else
+  lo = x * a;
+  hi = __umul64hi(x, a);
+  const u64 l = y * c, h = __umul64hi(y, c);
+  lo += l;
+  hi += h + (lo < l ? 1ull : 0ull);
+#endif
+}
+
 __device__ __forceinline__ void mul128(u64 a, u64 b, u64 &hi, u64 &lo) {
   lo = a * b;
   hi = umulhi(a, b);

@@ -294,10 +294,8 @@ __device__ __forceinline__ void mac_pair(u64 (&x)[8], u64 (&y)[8], const u64 *ka
       const int r = 2 * rr + e;
       const u64 xv = x[r], yv = y[r];
       u64 hi, lo, hi2, lo2;
-      mul128(xv, a[e], hi, lo);
-      mul128(xv, b[e], hi2, lo2);
-      mac128(yv, c[e], hi, lo);
-      mac128(yv, d[e], hi2, lo2);
+      sum2_128(xv, a[e], yv, c[e], hi, lo);
+      sum2_128(xv, b[e], yv, d[e], hi2, lo2);
       x[r] = redc_br<LOGN>(hi, lo, q, qi);
       y[r] = redc_br<LOGN>(hi2, lo2, q, qi);
     }
@@ -980,10 +978,8 @@ __device__ __forceinline__ void mac_pair_staged(u64 (&x)[8], u64 (&y)[8], const 
       const int r = 2 * rr + e;
       const u64 xv = x[r], yv = y[r];
       u64 hi, lo, hi2, lo2;
-      mul128(xv, a[e], hi, lo);
-      mul128(xv, b[e], hi2, lo2);
-      mac128(yv, c[e], hi, lo);
-      mac128(yv, d[e], hi2, lo2);
+      sum2_128(xv, a[e], yv, c[e], hi, lo);
+      sum2_128(xv, b[e], yv, d[e], hi2, lo2);
       x[r] = redc_br<LOGN>(hi, lo, q, qi);
       y[r] = redc_br<LOGN>(hi2, lo2, q, qi);
     }
@@ -1207,8 +1203,7 @@ __device__ __forceinline__ void mac_two_rows(u64 (&x)[8], const u64 (&y)[8], con
     for (int e = 0; e < 2; e++) {
       const int r = 2 * rr + e;
       u64 hi, lo;
-      mul128(x[r], a[e], hi, lo);
-      mac128(y[r], b[e], hi, lo);
+      sum2_128(x[r], a[e], y[r], b[e], hi, lo);
       x[r] = redc_br<LOGN>(hi, lo, q, qi);
     }
   }
