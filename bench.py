@@ -995,7 +995,9 @@ def main():
                     help="br-kernel / ks-kernel: only that kernel on --batch items (profiling case)")
     ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--param", default=PARAM)
-    ap.add_argument("--variant", type=int, default=None, help="blind-rotation launch-shape variant")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="blind-rotation launch-shape variant (wavefront mode: fixed instead of autotuned)")
+    ap.add_argument("--ks-tile", type=int, default=16, help="key-switch ciphertexts per CTA with --variant")
     ap.add_argument("--users", type=int, default=8, help="users of the ni-aggregate mode")
     ap.add_argument("--ref-step-seconds", type=float, default=REF_STEP_SECONDS,
                     help="wall time of one timed step of the CPU reference arm")
@@ -1036,7 +1038,12 @@ def main():
     d_out = torch.empty((info["outputs"], L), dtype=torch.int64, device="cuda")
     stream = torch.cuda.current_stream()
 
-    tune = eng.autotune(key, 2368)  # blind-rotation launch variant for this GPU
+    if args.variant is None:
+        tune = eng.autotune(key, 2368)  # blind-rotation launch shape and key-switch tile for this GPU
+    else:  # a fixed launch shape (profiling: the same kernels with and without a profiler)
+        eng.pbs_variant = args.variant
+        eng.set_ks_tile(args.ks_tile)
+        tune = {"variant": args.variant, "ms": None, "ks_tile": args.ks_tile, "fixed": True}
     # warm-up step 1 is a direct run (sets kernel attributes, binds the
     # circuit to the device); the circuit is then captured and replayed
     C.run_device(eng, key, d_in, d_out)
@@ -1137,7 +1144,7 @@ def main():
             "config": {**WORKLOAD_CONFIG, "gates_per_step": gates_per_step, "levels": info["levels"],
                        "max_level_width": info["max_level_width"],
                        "l2": "inputs (537 MB/step) larger than L2; server key resident",
-                       "pbs_variant": tune["variant"]},
+                       "pbs_variant": tune["variant"], "ks_tile": tune["ks_tile"]},
             "latency_ms": {"p50": statistics.median(step_ms), "p99": float(np.percentile(step_ms, 99)),
                            "what": "completion time of every circuit in the wavefront"},
             "e2e": {"value": e2e_value, "unit": "gate bootstraps/s",

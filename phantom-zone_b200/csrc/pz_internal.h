@@ -58,7 +58,11 @@ struct pz_ni_ksk {
 };
 
 namespace pz {
-inline int size_bucket(size_t n) { return n ? 63 - __builtin_clzll((unsigned long long)n) : 0; }
+// floor(log2(n)), clamped to the 48 buckets of pz_ctx::tuned
+inline int size_bucket(size_t n) {
+  const int b = n ? 63 - __builtin_clzll((unsigned long long)n) : 0;
+  return b < 47 ? b : 47;
+}
 int effective_variant(pz_ctx *c, size_t count);
 int effective_ks_ct(const pz_ctx *c, size_t count);
 // Launch sequence of one batch of gate bootstraps (ks kernel -> pbs kernel).
