@@ -288,12 +288,37 @@ __device__ __forceinline__ u64 shoup_spq(u64 v, u64 w, u64 ws) {
 // < q).  Q_N2048 (SPQ): the quotient from umulhi_lo2 is at most 2 short, so
 // wy in [0, 4q), growth 4q per stage (< 45q < 2^60 after 11 stages), and
 // q * quotient comes from the special form of Q.
+// x + t and x + c - t as explicit 32-bit carry chains (PZ_BFLY_ADD_PTX, a
+// same-box comparison): the high words' carries as addc / subc.
+__device__ __forceinline__ void add_sub_ptx(u64 x, u64 t, u64 c, u64 &sum, u64 &dif) {
+  asm("{\n\t"
+      ".reg .u32 x0, x1, t0, t1, c0, c1, s0, s1, d0, d1;\n\t"
+      "mov.b64 {x0, x1}, %2;\n\t"
+      "mov.b64 {t0, t1}, %3;\n\t"
+      "mov.b64 {c0, c1}, %4;\n\t"
+      "add.cc.u32 s0, x0, t0;\n\t"
+      "addc.u32 s1, x1, t1;\n\t"
+      "add.cc.u32 d0, x0, c0;\n\t"
+      "addc.u32 d1, x1, c1;\n\t"
+      "sub.cc.u32 d0, d0, t0;\n\t"
+      "subc.u32 d1, d1, t1;\n\t"
+      "mov.b64 %0, {s0, s1};\n\t"
+      "mov.b64 %1, {d0, d1};\n\t"
+      "}"
+      : "=l"(sum), "=l"(dif)
+      : "l"(x), "l"(t), "l"(c));
+}
+
 template <bool SPQ>
 __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
   if (SPQ) {
     const u64 t = shoup_spq(y, w, ws);
+#ifdef PZ_BFLY_ADD_PTX
+    add_sub_ptx(x, t, Q_N2048 << 2, x, y);
+#else
     y = x + (Q_N2048 << 2) - t;
     x = x + t;
+#endif
   } else {
     const u64 t = shoup_mul(y, w, ws, q);
     y = x + (q << 1) - t;
@@ -315,8 +340,13 @@ __device__ __forceinline__ u64 reduce_n2048(u64 v) {
 template <bool SPQ, int K>
 __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
   if (SPQ) {
+#ifdef PZ_BFLY_ADD_PTX
+    u64 u, t;
+    add_sub_ptx(x, y, (u64)K * Q_N2048, u, t);
+#else
     const u64 t = x + (u64)K * Q_N2048 - y;
     const u64 u = x + y;
+#endif
     y = shoup_spq(t, w, ws);
     x = u;
   } else {
