@@ -730,6 +730,16 @@ __device__ __forceinline__ bool mbar_wait(u64 *bar, u32 parity, long long limit 
     if (clock64() - t0 > limit) return false;
   }
 }
+// One thread: ask L2 to fetch `bytes` (a multiple of 16, 16-byte aligned)
+// from global memory ahead of their use; no completion to wait for.  Used for
+// key rows an operation will read after its transforms (PZ_NO_L2_PF: off,
+// for comparisons).
+__device__ __forceinline__ void prefetch_l2(const void *p, u32 bytes) {
+#ifndef PZ_NO_L2_PF
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+#endif
+}
+
 // Error bits a kernel sets in the context's device error word.
 constexpr u32 DEVERR_MBAR_TIMEOUT = 1u;
 

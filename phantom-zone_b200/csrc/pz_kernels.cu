@@ -479,6 +479,8 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
     if (idx[c] >= P.n) continue;  // out-of-range key index: the ciphertext is left unchanged
+    if (threadIdx.x == 0)  // the key rows, into L2 while the digits are transformed
+      prefetch_l2(P.rgsw + (size_t)idx[c] * P.rgsw_rows * N, P.rgsw_rows * (u32)N * 8);
     u64 *p = rlwe + c * 2 * N;
     u64 acc[2][8];
 #pragma unroll
@@ -504,6 +506,7 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
     if (slot[c] > P.w) continue;  // out-of-range key slot: the ciphertext is left unchanged
+    if (threadIdx.x == 0) prefetch_l2(P.autos + (size_t)slot[c] * P.auto_rows * N, P.auto_rows * (u32)N * 8);
     u64 *p = rlwe + c * 2 * N;
     u64 acc[2][8];
 #pragma unroll
@@ -837,6 +840,19 @@ __device__ __forceinline__ void test_rlwe_b(const BrParams &P, const u32 *kso, u
   }
 }
 
+// L2 prefetch of a blind-rotation operation's key rows (none for a trivial
+// automorphism).
+template <int LOGN>
+__device__ __forceinline__ void prefetch_next_key(const BrParams &P, u32 op) {
+  constexpr size_t N = (size_t)1 << LOGN;
+  if (op & OP_AUTO) {
+    if (!(op & OP_TRIVIAL))
+      prefetch_l2(P.autos + (size_t)(op & OP_SLOT) * P.auto_rows * N, P.auto_rows * (u32)N * 8);
+  } else {
+    prefetch_l2(P.rgsw + (size_t)(op & OP_INDEX) * P.rgsw_rows * N, P.rgsw_rows * (u32)N * 8);
+  }
+}
+
 // MINB: CTAs per SM the register allocation must allow (launch-shape
 // variants chosen at run time, see pz_ctx_set_pbs_variant).
 // One gate bootstrap of ciphertext ct (key-switched LWE kso, gate code
@@ -859,10 +875,14 @@ __device__ __forceinline__ void pbs_item(const BrParams &P, int ct, const u32 *k
     test_rlwe_b<LOGN>(P, kso, gcode, acc[1]);
     __syncthreads();
 
-    // ---- blind rotation: one operation per schedule entry
+    // ---- blind rotation: one operation per schedule entry; the next
+    // operation's key rows are asked into L2 as this one starts
     const u32 nops = *s_nops;
 #pragma unroll 1
-    for (u32 t = 0; t < nops; t++) bootstrap_op<LOGN, D1>(acc, s_ops[t], P, sm);
+    for (u32 t = 0; t < nops; t++) {
+      if (j == 0 && t + 1 < nops) prefetch_next_key<LOGN>(P, s_ops[t + 1]);
+      bootstrap_op<LOGN, D1>(acc, s_ops[t], P, sm);
+    }
 
     // ---- sample extract at index 0 (pbs.rs:423-449)
     u64 *o = out + (size_t)(P.out_idx ? P.out_idx[ct] : (u32)ct) * (N + 1);
@@ -1347,7 +1367,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttShape<LOGN>::T, 2
     __syncthreads();
     const u32 nops = *S.nops;
 #pragma unroll 1
-    for (u32 t = 0; t < nops; t++) split_op<LOGN>(x, S.ops[t], t, P, smem, slots, peer_slots, rank, cl);
+    for (u32 t = 0; t < nops; t++) {
+      if (j == 0 && t + 1 < nops) prefetch_next_key<LOGN>(P, S.ops[t + 1]);
+      split_op<LOGN>(x, S.ops[t], t, P, smem, slots, peer_slots, rank, cl);
+    }
     // sample extract at index 0 (pbs.rs:423-449): rank 0 the a-part, rank 1 b[0]
     u64 *o = out + (size_t)(P.out_idx ? P.out_idx[ct] : (u32)ct) * (N + 1);
 #pragma unroll
@@ -1398,7 +1421,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NttShape<LOGN>::T, 2
     __syncthreads();
     const u32 nops = *S.nops;
 #pragma unroll 1
-    for (u32 t = 0; t < nops; t++) split_op<LOGN>(x, S.ops[t], t, sp, smem, slots, peer_slots, rank, cl);
+    for (u32 t = 0; t < nops; t++) {
+      if (j == 0 && t + 1 < nops) prefetch_next_key<LOGN>(sp, S.ops[t + 1]);
+      split_op<LOGN>(x, S.ops[t], t, sp, smem, slots, peer_slots, rank, cl);
+    }
     u64 *o = out + (size_t)out_idx[ct] * (N + 1);
 #pragma unroll
     for (int r = 0; r < 8; r++) {
