@@ -11,6 +11,9 @@ from .engine import (GATES, PARAMETER_SETS, SELECTORS, DeviceKey, Engine, kernel
                      probe_imad_rate)
 from .circuits import Circuit
 from .server import DRY_RUN, Server
+from .fhe import (FheBool, FheUint8, clear_server_key, div_zero_error_flag, reset_error_flags,
+                  set_server_key)
 
-__all__ = ["Circuit", "Server", "DRY_RUN", "Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "kernel_revision", "param_id", "params",
+__all__ = ["FheBool", "FheUint8", "set_server_key", "clear_server_key", "div_zero_error_flag",
+           "reset_error_flags", "Circuit", "Server", "DRY_RUN", "Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "kernel_revision", "param_id", "params",
            "probe_imad_rate", "_lib"]
