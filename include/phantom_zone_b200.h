@@ -282,9 +282,10 @@ pz_status pz_circuit_replay_graph(pz_circuit *c, void *stream);
 
 /* ---- wire formats (no reference counterpart: the reference serialises nothing) ----
  * Device-form server key as bytes, for checkpoint / restore and for moving a
- * session between processes: a 64-byte header (parameter set, NTT root, sizes)
- * and the device arrays as they are.  Import copies them back without any
- * conversion; a blob from another parameter set or NTT root is refused.  With
+ * session between processes: a 64-byte header (parameter set, NTT root, key
+ * form, sizes) and the device arrays as they are.  Import copies them back
+ * without any conversion; a blob from another parameter set, NTT root or key
+ * form (a build with another multiply-accumulate reduction) is refused.  With
  * buf = NULL, export only writes the required *size. */
 pz_status pz_key_export(const pz_key *key, void *buf, size_t capacity, size_t *size);
 pz_status pz_key_import(pz_ctx *ctx, const void *buf, size_t size, pz_key **out);

@@ -8,10 +8,14 @@
 //     grow to < 16Q inside a radix-8 round and are reduced once per round.
 //     For N = 2048 the products and reductions use the special form
 //     Q = 2^54 - 77823 of that ring's prime.
-//   * The pointwise key product uses Montgomery REDC with R = 2^64.  Device
-//     keys are stored as K * N^{-1} * R mod Q, so REDC(x * K') = x * K * N^{-1}
-//     and the inverse NTT needs no final N^{-1} scaling.  Two products are
-//     summed in 128 bits before one REDC (the d_a = d_b = 1 external product).
+//   * The pointwise key product of the blind rotation for N = 2048 reduces
+//     its 128-bit sums by folding them with 2^54 = 77823 (mod Q) (three
+//     32 x 32-bit multiply-adds); the keys are stored as K * N^{-1} mod Q, so
+//     the inverse NTT needs no final N^{-1} scaling.  Other ring sizes, and
+//     the general-decomposition products of key aggregation and the
+//     non-interactive key switch, use Montgomery REDC with R = 2^64 and keys
+//     stored as K * N^{-1} * R mod Q.  Two products are summed in 128 bits
+//     before one reduction (the d_a = d_b = 1 external product).
 //   All results are exact residues; every value that leaves the device code
 //   (coefficient domain) is reduced to [0, Q), which is what makes the output
 //   independent of the NTT's internal ordering and lazy ranges.
@@ -61,28 +65,6 @@ __device__ __forceinline__ u64 shoup_mul(u64 x, u64 w, u64 ws, u64 q) {
 __device__ __forceinline__ u64 redc(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
   u64 m = lo * qinv_neg;
   return hi + umulhi(m, q) + (lo != 0 ? 1ull : 0ull);
-}
-
-// Montgomery REDC for Q = Q_N2048 = 2^54 - 77823 (same result as redc):
-// hi64(m Q) = (m >> 10) - hi64(77823 m) - borrow, and 77823 m takes two
-// 32 x 17-bit products instead of a 64 x 64-bit high product.
-__device__ __forceinline__ u64 redc_n2048(u64 hi, u64 lo, u64 qinv_neg) {
-  const u64 m = lo * qinv_neg;
-  const u32 m0 = (u32)m, m1 = (u32)(m >> 32);
-  const u64 A = (u64)m0 * 77823u, B = (u64)m1 * 77823u;
-  const u64 Mlo = A + (B << 32);
-  const u64 Mhi = (B >> 32) + (Mlo < A ? 1ull : 0ull);
-  const u64 hq = (m >> 10) - Mhi - ((m << 54) < Mlo ? 1ull : 0ull);
-  return hi + hq + (lo != 0 ? 1ull : 0ull);
-}
-// The REDC of the blind-rotation multiply-accumulates: the special form for
-// N = 2048 when built with PZ_MAC_SPQ (a same-box comparison), else generic.
-template <int LOGN>
-__device__ __forceinline__ u64 redc_br(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
-#ifdef PZ_MAC_SPQ
-  if constexpr (LOGN == 11) return redc_n2048(hi, lo, qinv_neg);
-#endif
-  return redc(hi, lo, q, qinv_neg);
 }
 
 // hi:lo = x a + y c for x, y < 2^60 (lazy forward outputs, < 45 Q) and a, c
@@ -136,6 +118,32 @@ __device__ __forceinline__ void sum2_128(u64 x, u64 a, u64 y, u64 c, u64 &hi, u6
 __device__ __forceinline__ void mul128(u64 a, u64 b, u64 &hi, u64 &lo) {
   lo = a * b;
   hi = umulhi(a, b);
+}
+// hi:lo = x a for x < 2^61 and a < 2^54, in 32-bit limb columns: the middle
+// column x0 a1 + x1 a0 stays below 2^62, so it accumulates with mad.wide and
+// only the merge carries (four multiply-adds against about seven for the
+// 64 x 64-bit low and high products).
+__device__ __forceinline__ void mul128_narrow(u64 x, u64 a, u64 &hi, u64 &lo) {
+  asm("{\n\t"
+      ".reg .u32 x0, x1, a0, a1, l0, l1, m0, m1, h0, h1;\n\t"
+      ".reg .u64 mid, low, high;\n\t"
+      "mov.b64 {x0, x1}, %2;\n\t"
+      "mov.b64 {a0, a1}, %3;\n\t"
+      "mul.wide.u32 mid, x0, a1;\n\t"
+      "mad.wide.u32 mid, x1, a0, mid;\n\t"
+      "mul.wide.u32 high, x1, a1;\n\t"
+      "mul.wide.u32 low, x0, a0;\n\t"
+      "mov.b64 {l0, l1}, low;\n\t"
+      "mov.b64 {m0, m1}, mid;\n\t"
+      "mov.b64 {h0, h1}, high;\n\t"
+      "add.cc.u32 l1, l1, m0;\n\t"
+      "addc.cc.u32 h0, h0, m1;\n\t"
+      "addc.u32 h1, h1, 0;\n\t"
+      "mov.b64 %0, {h0, h1};\n\t"
+      "mov.b64 %1, {l0, l1};\n\t"
+      "}"
+      : "=l"(hi), "=l"(lo)
+      : "l"(x), "l"(a));
 }
 __device__ __forceinline__ void mac128(u64 a, u64 b, u64 &hi, u64 &lo) {
   u64 l = a * b, h = umulhi(a, b);
@@ -331,12 +339,73 @@ __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
 // with reduce_n2048 -- and y' is a Shoup product whose quotient comes from
 // umulhi_lo2 (at most 2 short beyond Shoup's own 1), so y' in [0, 4Q); K Q
 // must bound the incoming y (the caller's stage bound: inputs < 2Q, then
-// outputs < 4Q after one stage and < 8Q after two, hence K = 2, 4, 8).
+// outputs < 4Q after one stage and < 8Q after two, hence K = 2, 4, 8; the
+// trailing round that opens the N = 2048 inverse takes inputs < 2.04 Q --
+// the blind rotation's folded multiply-accumulates -- hence K = 3, 5 there).
 __device__ __forceinline__ u64 reduce_n2048(u64 v) {
   // 2^54 = 77823 (mod Q): v = h 2^54 + l -> l + 77823 h, < 2^54 + 2^27 < 2Q;
   // h < 2^10, so 77823 h < 2^27 is a 32-bit product
   return (v & ((1ull << 54) - 1)) + (u64)((u32)(v >> 54) * 77823u);
 }
+
+// The blind rotation's multiply-accumulate reduction for N = 2048 (the
+// default; PZ_MAC_MONT selects Montgomery REDC there too, for comparisons):
+// X = hi 2^64 + lo with hi < 2^52 is X = (lo mod 2^54) + 2^54 u,
+// u = hi 2^10 + (lo >> 54) < 2^62, and 2^54 = 77823 (mod Q), so
+// X = (lo mod 2^54) + 77823 u0 + 77823 u1 2^32 with u = u1 2^32 + u0; the
+// last term, p 2^32 with p = 77823 u1 < 2^47, is (p mod 2^22) 2^32 +
+// 77823 (p >> 22).  The result is congruent to X and below
+// 2^55 + 2^49 + 2^42 < 2.04 Q: three multiply-adds (two with the 64-bit
+// addend riding on them) instead of REDC's 64-bit low and high products.
+#ifdef PZ_MAC_MONT
+constexpr bool MAC_FOLD_N2048 = false;
+#else
+constexpr bool MAC_FOLD_N2048 = true;
+#endif
+__device__ __forceinline__ u64 fold_n2048(u64 hi, u64 lo) {
+  u64 r;
+  asm("{\n\t"
+      ".reg .u32 l0, l1, h0, h1, u0, u1, p0, p1, ph, b1;\n\t"
+      ".reg .u64 p, base;\n\t"
+      "mov.b64 {l0, l1}, %1;\n\t"
+      "mov.b64 {h0, h1}, %2;\n\t"
+      "shf.l.wrap.b32 u0, l1, h0, 10;\n\t"    // u mod 2^32
+      "shf.l.wrap.b32 u1, h0, h1, 10;\n\t"    // u >> 32 (< 2^30)
+      "mul.wide.u32 p, u1, 77823;\n\t"
+      "mov.b64 {p0, p1}, p;\n\t"
+      "shf.r.wrap.b32 ph, p0, p1, 22;\n\t"    // p >> 22 (< 2^25)
+      "and.b32 p0, p0, 0x3FFFFF;\n\t"         // p mod 2^22
+      "and.b32 b1, l1, 0x3FFFFF;\n\t"         // (lo mod 2^54) >> 32
+      "add.u32 b1, b1, p0;\n\t"
+      "mov.b64 base, {l0, b1};\n\t"           // (lo mod 2^54) + (p mod 2^22) 2^32
+      "mad.wide.u32 base, u0, 77823, base;\n\t"
+      "mad.wide.u32 %0, ph, 77823, base;\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(lo), "l"(hi));
+  return r;
+}
+// Reduction of a multiply-accumulate's 128-bit sum (hi < 2^52): for N = 2048
+// the fold above (< 2.04 Q, keys K N^{-1}), else Montgomery REDC (< 2 Q, keys
+// K N^{-1} 2^64).  Both are exact residues of the same product.
+template <int LOGN>
+__device__ __forceinline__ u64 mac_reduce(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
+  if constexpr (LOGN == 11 && MAC_FOLD_N2048) return fold_n2048(hi, lo);
+  else return redc(hi, lo, q, qinv_neg);
+}
+// The automorphism's b: product + permuted b (each < 2.04 Q for N = 2048,
+// < 2q otherwise), back below 2q.
+template <int LOGN>
+__device__ __forceinline__ void mac_mul(u64 x, u64 a, u64 &hi, u64 &lo) {
+  if constexpr (LOGN == 11) mul128_narrow(x, a, hi, lo);  // x < 45 Q < 2^60, a < Q < 2^54
+  else mul128(x, a, hi, lo);
+}
+template <int LOGN>
+__device__ __forceinline__ u64 mac_add_b(u64 v, u64 q2) {
+  if constexpr (LOGN == 11 && MAC_FOLD_N2048) return reduce_n2048(v);
+  else return v >= q2 ? v - q2 : v;
+}
+
 template <bool SPQ, int K>
 __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
   if (SPQ) {
@@ -530,13 +599,13 @@ __device__ __forceinline__ void inv_round4(u64 (&x)[8], u64 (&y)[8], int j, cons
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       if (!PF) tw(rc.iw, N / 2 + 2 * g + e, w[3 * h + e], ws[3 * h + e]);
-      ibf2<LOGN, TWO, 2>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w[3 * h + e], ws[3 * h + e], q);
+      ibf2<LOGN, TWO, 3>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w[3 * h + e], ws[3 * h + e], q);
     }
     if (!PF) tw(rc.iw, N / 4 + g, w[3 * h + 2], ws[3 * h + 2]);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w[3 * h + 2], ws[3 * h + 2], q);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w[3 * h + 2], ws[3 * h + 2], q);
+    ibf2<LOGN, TWO, 5>(x, y, 4 * h + 0, 4 * h + 2, w[3 * h + 2], ws[3 * h + 2], q);
+    ibf2<LOGN, TWO, 5>(x, y, 4 * h + 1, 4 * h + 3, w[3 * h + 2], ws[3 * h + 2], q);
   }
-  inv_round_reduce<LOGN, TWO>(x, y);  // (N = 2048) sums < 8Q -> < 2Q
+  inv_round_reduce<LOGN, TWO>(x, y);  // (N = 2048) sums < 8.2Q -> < 2Q
 }
 
 // Layout of full round k: thread j holds base + t r, t = N >> (3k + 3).

@@ -20,7 +20,10 @@ struct pz_ctx {
   pz::u64 *d_tv = nullptr;        // 6 x br_q/2
   // constants
   pz::RingConsts rc{};
-  pz::u64 conv_c = 0, conv_cs = 0;
+  // device key form: conv_c scales the transformed rows of the keys that the
+  // Montgomery products use (aggregation, the NI key switch), br_conv_c those
+  // of the blind rotation's RGSW and auto keys (folded products for N = 2048)
+  pz::u64 conv_c = 0, conv_cs = 0, br_conv_c = 0, br_conv_cs = 0;
   pz::BrParams br{};
   pz::KsParams ks{};
   pz::u32 *d_err = nullptr;  // device error word: DEVERR_* bits set by kernels whose bounded waits ran out

@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t co
 // auto key rows A x d, B x d.
 // ---------------------------------------------------------------------------
 
-// x <- x (pointwise, Montgomery) from two device-layout key rows, y likewise.
+// x <- x (pointwise, mac_reduce) from two device-layout key rows, y likewise.
 template <int LOGN>
 __device__ __forceinline__ void mac_pair(u64 (&x)[8], u64 (&y)[8], const u64 *ka, const u64 *kb,
                                          const u64 *kc, const u64 *kd, const RingConsts &rc) {
@@ -296,14 +296,15 @@ __device__ __forceinline__ void mac_pair(u64 (&x)[8], u64 (&y)[8], const u64 *ka
       u64 hi, lo, hi2, lo2;
       sum2_128(xv, a[e], yv, c[e], hi, lo);
       sum2_128(xv, b[e], yv, d[e], hi2, lo2);
-      x[r] = redc_br<LOGN>(hi, lo, q, qi);
-      y[r] = redc_br<LOGN>(hi2, lo2, q, qi);
+      x[r] = mac_reduce<LOGN>(hi, lo, q, qi);
+      y[r] = mac_reduce<LOGN>(hi2, lo2, q, qi);
     }
   }
 }
 
 // Automorphism product: x' = x ka, y' = x kb + y, with y the permuted b in
-// the evaluation domain (< 2q); outputs < 2q.
+// the evaluation domain (< 2q; for N = 2048 < 2.04 Q, a folded product); x'
+// as mac_reduce leaves it, y' < 2q.
 template <int LOGN>
 __device__ __forceinline__ void mac_auto(u64 (&x)[8], u64 (&y)[8], const u64 *ka, const u64 *kb,
                                          const RingConsts &rc) {
@@ -319,11 +320,10 @@ __device__ __forceinline__ void mac_auto(u64 (&x)[8], u64 (&y)[8], const u64 *ka
     for (int e = 0; e < 2; e++) {
       const int r = 2 * rr + e;
       u64 hi, lo, hi2, lo2;
-      mul128(x[r], a[e], hi, lo);
-      mul128(x[r], b[e], hi2, lo2);
-      x[r] = redc_br<LOGN>(hi, lo, q, qi);
-      const u64 v = redc_br<LOGN>(hi2, lo2, q, qi) + y[r];
-      y[r] = v >= q2 ? v - q2 : v;
+      mac_mul<LOGN>(x[r], a[e], hi, lo);
+      mac_mul<LOGN>(x[r], b[e], hi2, lo2);
+      x[r] = mac_reduce<LOGN>(hi, lo, q, qi);
+      y[r] = mac_add_b<LOGN>(mac_reduce<LOGN>(hi2, lo2, q, qi) + y[r], q2);
     }
   }
 }
@@ -1000,8 +1000,8 @@ __device__ __forceinline__ void mac_pair_staged(u64 (&x)[8], u64 (&y)[8], const 
       u64 hi, lo, hi2, lo2;
       sum2_128(xv, a[e], yv, c[e], hi, lo);
       sum2_128(xv, b[e], yv, d[e], hi2, lo2);
-      x[r] = redc_br<LOGN>(hi, lo, q, qi);
-      y[r] = redc_br<LOGN>(hi2, lo2, q, qi);
+      x[r] = mac_reduce<LOGN>(hi, lo, q, qi);
+      y[r] = mac_reduce<LOGN>(hi2, lo2, q, qi);
     }
   }
 }
@@ -1019,11 +1019,10 @@ __device__ __forceinline__ void mac_auto_staged(u64 (&x)[8], u64 (&y)[8], const 
     for (int e = 0; e < 2; e++) {
       const int r = 2 * rr + e;
       u64 hi, lo, hi2, lo2;
-      mul128(x[r], a[e], hi, lo);
-      mul128(x[r], b[e], hi2, lo2);
-      x[r] = redc_br<LOGN>(hi, lo, q, qi);
-      const u64 v = redc_br<LOGN>(hi2, lo2, q, qi) + y[r];
-      y[r] = v >= q2 ? v - q2 : v;
+      mac_mul<LOGN>(x[r], a[e], hi, lo);
+      mac_mul<LOGN>(x[r], b[e], hi2, lo2);
+      x[r] = mac_reduce<LOGN>(hi, lo, q, qi);
+      y[r] = mac_add_b<LOGN>(mac_reduce<LOGN>(hi2, lo2, q, qi) + y[r], q2);
     }
   }
 }
@@ -1207,7 +1206,7 @@ __global__ void __launch_bounds__(256, 2)
 // ---------------------------------------------------------------------------
 namespace cg = cooperative_groups;
 
-// out = REDC(x ka + y kb), x, y in the evaluation layout, key rows in the device layout
+// out = mac_reduce(x ka + y kb), x, y in the evaluation layout, key rows in the device layout
 template <int LOGN>
 __device__ __forceinline__ void mac_two_rows(u64 (&x)[8], const u64 (&y)[8], const u64 *ka, const u64 *kb,
                                              const RingConsts &rc) {
@@ -1224,7 +1223,7 @@ __device__ __forceinline__ void mac_two_rows(u64 (&x)[8], const u64 (&y)[8], con
       const int r = 2 * rr + e;
       u64 hi, lo;
       sum2_128(x[r], a[e], y[r], b[e], hi, lo);
-      x[r] = redc_br<LOGN>(hi, lo, q, qi);
+      x[r] = mac_reduce<LOGN>(hi, lo, q, qi);
     }
   }
 }
@@ -1300,10 +1299,7 @@ __device__ __forceinline__ void split_op(u64 (&x)[8], u32 op, u32 t, const BrPar
       }
       mac_two_rows<LOGN>(d, z, K + N, K + N, P.rc);  // d B
 #pragma unroll
-      for (int r = 0; r < 8; r++) {
-        const u64 v = d[r] + x[r];
-        x[r] = v >= q2 ? v - q2 : v;
-      }
+      for (int r = 0; r < 8; r++) x[r] = mac_add_b<LOGN>(d[r] + x[r], q2);
       if (!keep_b) {
         ntt_inv<LOGN, false>(x, x, sm, P.rc);
 #pragma unroll

@@ -7,7 +7,7 @@ namespace pz {
 constexpr int MAX_KS_D = 16;   // key-switch decomposition count bound
 // Revision of the blind-rotation kernels: bumped with every change to their
 // code, so that a profile taken on one revision is not reported for another.
-constexpr const char *BR_KERNEL_REVISION = "br-v11";
+constexpr const char *BR_KERNEL_REVISION = "br-v12";
 constexpr int MAX_AUTO_SLOTS = 16;
 
 // Everything the blind rotation needs for one parameter set + server key.
@@ -22,7 +22,7 @@ struct BrParams {
   u32 auto_k[MAX_AUTO_SLOTS];      // automorphism element mod 2N per key slot
   const unsigned short *dlog;      // [br_q]
   const u64 *tv;                   // [6][br_q/2] test vectors
-  const u64 *rgsw;                 // [n][rgsw_rows][N] device layout, Montgomery form
+  const u64 *rgsw;                 // [n][rgsw_rows][N] device layout, scaled by the key form
   const u64 *autos;                // [w+1][auto_rows][N]
   const u32 *out_idx;              // optional scatter: output of gate ct -> LWE out_idx[ct]
   u32 *err;                        // the context's device error word (DEVERR_* bits)

@@ -331,8 +331,13 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   rc.fw = c->d_tw;
   rc.iw = c->d_tw + 2 * N;
   const u64 r64 = (u64)(((u128)1 << 64) % Q);
-  c->conv_c = mulmod(rc.n_inv, r64, Q);  // keys stored as K * N^{-1} * 2^64
+  c->conv_c = mulmod(rc.n_inv, r64, Q);  // Montgomery-product keys: K * N^{-1} * 2^64
   c->conv_cs = shoup(c->conv_c, Q);
+  // blind-rotation keys: K * N^{-1} where the multiply-accumulates fold (mac_reduce)
+  // (the one-digit kernels; other decomposition counts run the Montgomery path)
+  const bool fold = c->logn == 11 && pz::MAC_FOLD_N2048 && P.rlrg_d_a == 1 && P.rlrg_d_b == 1 && P.auto_d == 1;
+  c->br_conv_c = fold ? rc.n_inv : c->conv_c;
+  c->br_conv_cs = shoup(c->br_conv_c, Q);
   pz::BrParams &br = c->br;
   br.rc = rc;
   br.err = c->d_err;
@@ -443,7 +448,7 @@ pz_status pz_key_upload(pz_ctx *c, const pz_server_key_view *v, pz_key **out) {
   if ((e = cudaMalloc(&k->d_autos, auto_polys * N * 8)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "auto alloc");
   if ((e = cudaMalloc(&k->d_ksk, ksk_rows * stride * 4)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "ksk alloc");
   k->bytes = (rgsw_polys + auto_polys) * N * 8 + ksk_rows * stride * 4;
-  // coefficient rows -> device staging -> forward NTT + Montgomery/N^{-1} + device layout
+  // coefficient rows -> device staging -> forward NTT + key form (br_conv_c) + device layout
   const size_t chunk = 1024;  // polynomials per staging copy
   u64 *d_stage = nullptr;
   if ((e = cudaMalloc(&d_stage, chunk * N * 8)) != cudaSuccess) return cleanup(PZ_ERR_OUT_OF_MEMORY, "staging alloc");
@@ -452,7 +457,8 @@ pz_status pz_key_upload(pz_ctx *c, const pz_server_key_view *v, pz_key **out) {
       size_t m = std::min(chunk, polys - p0);
       cudaError_t e2 = cudaMemcpyAsync(d_stage, src + p0 * N, m * N * 8, cudaMemcpyHostToDevice, c->stream);
       if (e2 != cudaSuccess) return e2;
-      e2 = pz::launch_key_convert((int)c->logn, d_stage, dst + p0 * N, m, c->rc, c->conv_c, c->conv_cs, c->stream);
+      e2 = pz::launch_key_convert((int)c->logn, d_stage, dst + p0 * N, m, c->rc, c->br_conv_c, c->br_conv_cs,
+                                    c->stream);
       if (e2 != cudaSuccess) return e2;
       e2 = cudaStreamSynchronize(c->stream);
       if (e2 != cudaSuccess) return e2;
@@ -509,7 +515,7 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
   for (size_t p0 = 0; p0 < rgsw_polys; p0 += chunk) {
     const size_t m = std::min(chunk, rgsw_polys - p0);
     if ((e = cudaMemcpyAsync(d_stage, v->rgsw + p0 * N, m * N * 8, cudaMemcpyDefault, c->stream)) != cudaSuccess ||
-        (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_rgsw + p0 * N, m, c->rc, c->conv_c, c->conv_cs,
+        (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_rgsw + p0 * N, m, c->rc, c->br_conv_c, c->br_conv_cs,
                                     c->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
       return cleanup(PZ_ERR_CUDA, std::string("rgsw conversion: ") + cudaGetErrorString(e));
@@ -520,7 +526,7 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
   if (st != PZ_OK) return cleanup(st, c->err);
   if ((e = cudaMemcpy2DAsync(d_stage + d_auto * N, 2 * d_auto * N * 8, v->auto_b, d_auto * N * 8, d_auto * N * 8,
                              P.n_auto_keys, cudaMemcpyDefault, c->stream)) != cudaSuccess ||
-      (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_autos, auto_polys, c->rc, c->conv_c, c->conv_cs,
+      (e = pz::launch_key_convert((int)c->logn, d_stage, k->d_autos, auto_polys, c->rc, c->br_conv_c, c->br_conv_cs,
                                   c->stream)) != cudaSuccess ||
       (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
     return cleanup(PZ_ERR_CUDA, std::string("auto key expansion: ") + cudaGetErrorString(e));

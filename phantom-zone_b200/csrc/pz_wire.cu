@@ -4,11 +4,13 @@
 //
 // Key blob: a 64-byte header followed by the device-form arrays exactly as
 // they sit in device memory (RGSW and auto keys in the evaluation domain,
-// Montgomery form with N^{-1} folded in, per-thread layout; the LWE KSK as
-// u32 rows of ks_stride words).  The evaluation domain depends on the NTT
-// root, so the header records it and an import into a context with another
-// root (or another parameter set) is refused.  Import is a plain copy: no
-// forward NTT, no conversion.
+// scaled by the context's key-form constant -- N^{-1}, or N^{-1} 2^64 for
+// Montgomery products -- in the per-thread layout; the LWE KSK as u32 rows
+// of ks_stride words).  The evaluation domain depends on the NTT root and
+// the scale on the build's multiply-accumulate reduction, so the header
+// (version 2) records both and an import into a context with another root,
+// key form or parameter set is refused.  Import is a plain copy: no forward
+// NTT, no conversion.
 //
 // (The circuit blob lives with the circuit in pz_circuit.cu.)
 #include <cstring>
@@ -28,7 +30,8 @@ struct KeyHeader {
   u32 version, param_id;
   u64 root;
   u64 rgsw_bytes, autos_bytes, ksk_bytes;
-  u64 reserved[2];
+  u64 key_form;  // the scale of the RGSW and auto key rows (br_conv_c)
+  u64 reserved;
 };
 static_assert(sizeof(KeyHeader) == 64, "key header is 64 bytes");
 
@@ -55,7 +58,8 @@ pz_status pz_key_export(const pz_key *k, void *buf, size_t capacity, size_t *siz
   PZ_CK(c, cudaSetDevice(c->device));
   KeyHeader h{};
   h.magic = KEY_MAGIC;
-  h.version = 1;
+  h.version = 2;
+  h.key_form = c->br_conv_c;
   h.param_id = (u32)c->param_id;
   h.root = c->root;
   h.rgsw_bytes = rg;
@@ -78,7 +82,12 @@ pz_status pz_key_import(pz_ctx *c, const void *buf, size_t size, pz_key **out) {
   memcpy(&h, buf, sizeof h);
   size_t rg, au, ks;
   key_sizes(c, &rg, &au, &ks);
-  if (h.magic != KEY_MAGIC || h.version != 1) return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "pz_key_import: not a key blob");
+  if (h.magic != KEY_MAGIC || h.version < 1 || h.version > 2)
+    return pz::fail(c, PZ_ERR_INVALID_ARGUMENT, "pz_key_import: not a key blob");
+  // version 1 blobs carried Montgomery-form rows without recording it
+  const u64 form = h.version == 1 ? c->conv_c : h.key_form;
+  if (form != c->br_conv_c)
+    return pz::fail(c, PZ_ERR_KEY_MISMATCH, "pz_key_import: key rows in another device form (other build)");
   if (h.param_id != (u32)c->param_id) return pz::fail(c, PZ_ERR_KEY_MISMATCH, "pz_key_import: other parameter set");
   if (h.root != c->root) return pz::fail(c, PZ_ERR_KEY_MISMATCH, "pz_key_import: exported under another NTT root");
   if (h.rgsw_bytes != rg || h.autos_bytes != au || h.ksk_bytes != ks || size != sizeof h + rg + au + ks)
