@@ -67,10 +67,11 @@ __device__ __forceinline__ u64 redc(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
   return hi + umulhi(m, q) + (lo != 0 ? 1ull : 0ull);
 }
 
-// hi:lo = x a + y c for x, y < 2^60 (lazy forward outputs, < 45 Q) and a, c
-// < Q (keys): in 32-bit limbs the middle column x0 a1 + x1 a0 + y0 c1 + y1 c0
-// stays below 2^62 and the high column below 2^51, so both accumulate with
-// mad.wide and no carries; only the low column and the final merge carry.
+// hi:lo = x a + y c for x, y < 2^62 (lazy forward outputs: < 238 Q < 2^61.9)
+// and a, c < Q (keys): in 32-bit limbs the middle column x0 a1 + x1 a0 +
+// y0 c1 + y1 c0 stays below 2^63 + 2^55 and the high column below 2^53, so
+// both accumulate with mad.wide and no carries; only the low column and the
+// final merge carry.
 // 1.7 % more blind-rotation throughput on B200 than two 64 x 64 products in
 // C (kept under PZ_MAC_C for comparisons).
 __device__ __forceinline__ void sum2_128(u64 x, u64 a, u64 y, u64 c, u64 &hi, u64 &lo) {
@@ -119,8 +120,8 @@ __device__ __forceinline__ void mul128(u64 a, u64 b, u64 &hi, u64 &lo) {
   lo = a * b;
   hi = umulhi(a, b);
 }
-// hi:lo = x a for x < 2^61 and a < 2^54, in 32-bit limb columns: the middle
-// column x0 a1 + x1 a0 stays below 2^62, so it accumulates with mad.wide and
+// hi:lo = x a for x < 2^62 and a < 2^54, in 32-bit limb columns: the middle
+// column x0 a1 + x1 a0 stays below 2^62 + 2^54, so it accumulates with mad.wide and
 // only the merge carries (four multiply-adds against about seven for the
 // 64 x 64-bit low and high products).
 __device__ __forceinline__ void mul128_narrow(u64 x, u64 a, u64 &hi, u64 &lo) {
@@ -288,6 +289,74 @@ __device__ __forceinline__ u64 shoup_spq(u64 v, u64 w, u64 ws) {
 #endif
 }
 
+__device__ __forceinline__ u64 reduce_n2048(u64 v) {
+  // 2^54 = 77823 (mod Q): v = h 2^54 + l -> l + 77823 h, < 2^54 + 2^27 < 2Q;
+  // h < 2^10, so 77823 h < 2^27 is a 32-bit product
+  return (v & ((1ull << 54) - 1)) + (u64)((u32)(v >> 54) * 77823u);
+}
+
+// Butterfly products with the quotient estimated on the FP64 pipe (the
+// default for N = 2048; PZ_BFLY_SHOUP selects the all-integer Shoup product
+// for comparisons).  The twiddle tables hold (w, w/Q as a double) instead of
+// (w, Shoup(w)).  On B200 the FP64 pipe runs at the integer multiply pipe's
+// rate and concurrently with it, and the 64-bit conversions at about a
+// quarter of it on their own unit, so the Shoup quotient -- two IMAD.HI and
+// an IMAD.WIDE, 2.5-2.65 times an IMAD each -- moves off the busy pipe:
+// v -> vr = reduce_n2048(v) < 2^54 + 2^27, qi = rint(f64(vr) * (w/Q)) within
+// 6.51 of vr w / Q (three roundings of 2^-53 each on a value below 2^54),
+// and raw = w vr - qi Q (mod 2^64) lies in (-6.51 Q, 6.51 Q).  The integer
+// work left is the low words of w vr and qi Q (two IMAD.WIDE, three IMAD).
+#ifdef PZ_BFLY_SHOUP
+constexpr bool BFLY_FP64 = false;
+#else
+constexpr bool BFLY_FP64 = true;
+#endif
+// PZ_FP64_F2I_MAGIC (a comparison): the quotient as the mantissa of
+// qd + 2^55 (a multiple of 8, 4 more of error: raw in (-10.51 Q, 10.51 Q),
+// offset 11 Q) instead of a conversion.  Converting f64(vr) the same way
+// (two 2^52-offset doubles and an FMA) measured 19 % slower than the
+// conversion unit: the extra ALU and FP64 instructions cost more issue
+// slots than the conversions they replace.
+#ifdef PZ_FP64_F2I_MAGIC
+constexpr u64 FP_OFF = 11;  // raw + 11 Q in (0.49 Q, 21.51 Q)
+#else
+constexpr u64 FP_OFF = 7;  // raw + 7 Q in (0.49 Q, 13.51 Q)
+#endif
+__device__ __forceinline__ u64 fp_raw(u64 v, u64 w, u64 wq_bits) {
+  const u64 vr = reduce_n2048(v);
+  u64 qi, r;
+  double vd;
+  asm("cvt.rn.f64.u64 %0, %1;" : "=d"(vd) : "l"(vr));
+  const double qd = __dmul_rn(vd, __longlong_as_double((long long)wq_bits));
+#ifdef PZ_FP64_F2I_MAGIC
+  const double sq = __dadd_rn(qd, 36028797018963968.0);  // + 2^55
+  qi = ((u64)__double_as_longlong(sq) & ((1ull << 52) - 1)) << 3;
+#else
+  asm("cvt.rni.u64.f64 %0, %1;" : "=l"(qi) : "d"(qd));
+#endif
+  asm("{\n\t"
+      ".reg .u32 v0, v1, w0, w1, q0, q1, t0, t1, z;\n\t"
+      ".reg .u64 wy, t;\n\t"
+      "mov.b64 {v0, v1}, %1;\n\t"
+      "mov.b64 {w0, w1}, %2;\n\t"
+      "mov.b64 {q0, q1}, %3;\n\t"
+      "mul.wide.u32 wy, w0, v0;\n\t"
+      "mov.b64 {t0, t1}, wy;\n\t"
+      "mad.lo.u32 t1, w0, v1, t1;\n\t"
+      "mad.lo.u32 t1, w1, v0, t1;\n\t"
+      "mov.b64 wy, {t0, t1};\n\t"            // w vr mod 2^64
+      "mad.wide.u32 t, q0, 77823, wy;\n\t"   // + 77823 qi (low word of qi)
+      "mov.b64 {t0, t1}, t;\n\t"
+      "mad.lo.u32 t1, q1, 77823, t1;\n\t"    // + 77823 qi (high word)
+      "shl.b32 z, q0, 22;\n\t"
+      "sub.u32 t1, t1, z;\n\t"               // - qi 2^54
+      "mov.b64 %0, {t0, t1};\n\t"
+      "}"
+      : "=l"(r)
+      : "l"(vr), "l"(w), "l"(qi));
+  return r;
+}
+
 // Forward CT butterfly (the x' = x + wy, y' = x - wy of ntt.rs:31-49) without
 // Harvey's conditional subtraction: wy is a Shoup product, so both outputs
 // grow by a bounded multiple of q per stage and the Shoup product accepts any
@@ -295,7 +364,8 @@ __device__ __forceinline__ u64 shoup_spq(u64 v, u64 w, u64 ws) {
 // growth 2q per stage (< 23q after the 11 stages of N = 2048 from inputs
 // < q).  Q_N2048 (SPQ): the quotient from umulhi_lo2 is at most 2 short, so
 // wy in [0, 4q), growth 4q per stage (< 45q < 2^60 after 11 stages), and
-// q * quotient comes from the special form of Q.
+// q * quotient comes from the special form of Q; with the FP64 quotient
+// (fp_raw, the default) the growth is < 13.51 Q per stage (< 150 Q).
 // x + t and x + c - t as explicit 32-bit carry chains (PZ_BFLY_ADD_PTX, a
 // same-box comparison): the high words' carries as addc / subc.
 __device__ __forceinline__ void add_sub_ptx(u64 x, u64 t, u64 c, u64 &sum, u64 &dif) {
@@ -319,7 +389,11 @@ __device__ __forceinline__ void add_sub_ptx(u64 x, u64 t, u64 c, u64 &sum, u64 &
 
 template <bool SPQ>
 __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
-  if (SPQ) {
+  if (SPQ && BFLY_FP64) {  // outputs grow by < 13.51 Q per stage (< 150 Q after 11; F2I_MAGIC: 21.51 Q, 238 Q)
+    const u64 raw = fp_raw(y, w, ws), xc = x + FP_OFF * Q_N2048;
+    x = xc + raw;
+    y = xc - raw;
+  } else if (SPQ) {
     const u64 t = shoup_spq(y, w, ws);
 #ifdef PZ_BFLY_ADD_PTX
     add_sub_ptx(x, t, Q_N2048 << 2, x, y);
@@ -342,11 +416,6 @@ __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
 // outputs < 4Q after one stage and < 8Q after two, hence K = 2, 4, 8; the
 // trailing round that opens the N = 2048 inverse takes inputs < 2.04 Q --
 // the blind rotation's folded multiply-accumulates -- hence K = 3, 5 there).
-__device__ __forceinline__ u64 reduce_n2048(u64 v) {
-  // 2^54 = 77823 (mod Q): v = h 2^54 + l -> l + 77823 h, < 2^54 + 2^27 < 2Q;
-  // h < 2^10, so 77823 h < 2^27 is a 32-bit product
-  return (v & ((1ull << 54) - 1)) + (u64)((u32)(v >> 54) * 77823u);
-}
 
 // The blind rotation's multiply-accumulate reduction for N = 2048 (the
 // default; PZ_MAC_MONT selects Montgomery REDC there too, for comparisons):
@@ -397,7 +466,7 @@ __device__ __forceinline__ u64 mac_reduce(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
 // < 2q otherwise), back below 2q.
 template <int LOGN>
 __device__ __forceinline__ void mac_mul(u64 x, u64 a, u64 &hi, u64 &lo) {
-  if constexpr (LOGN == 11) mul128_narrow(x, a, hi, lo);  // x < 45 Q < 2^60, a < Q < 2^54
+  if constexpr (LOGN == 11) mul128_narrow(x, a, hi, lo);  // x < 238 Q < 2^62, a < Q < 2^54
   else mul128(x, a, hi, lo);
 }
 template <int LOGN>
@@ -405,6 +474,15 @@ __device__ __forceinline__ u64 mac_add_b(u64 v, u64 q2) {
   if constexpr (LOGN == 11 && MAC_FOLD_N2048) return reduce_n2048(v);
   else return v >= q2 ? v - q2 : v;
 }
+
+// Stage bounds K of the N = 2048 inverse rounds (stages a, b, c of a round;
+// the round that opens an inverse after the multiply-accumulates takes
+// inputs < 2.04 Q in stage a, K = 3, and IK_MB in stage b).  The Shoup
+// products leave < 4 Q: sums < 4, 8, 16 Q.  The FP64-quotient products
+// leave < 13.51 Q: stage b sees < 13.51 Q, stage c < 27.02 Q.
+// (PZ_FP64_F2I_MAGIC: products < 21.51 Q, stage b < 21.51 Q, stage c < 43.02 Q.)
+constexpr int IK_FB = FP_OFF == 7 ? 14 : 22, IK_FC = FP_OFF == 7 ? 28 : 44;
+constexpr int IK_B = BFLY_FP64 ? IK_FB : 4, IK_C = BFLY_FP64 ? IK_FC : 8, IK_MB = BFLY_FP64 ? IK_FB : 5;
 
 template <bool SPQ, int K>
 __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
@@ -416,7 +494,7 @@ __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
     const u64 t = x + (u64)K * Q_N2048 - y;
     const u64 u = x + y;
 #endif
-    y = shoup_spq(t, w, ws);
+    y = BFLY_FP64 ? fp_raw(t, w, ws) + FP_OFF * Q_N2048 : shoup_spq(t, w, ws);
     x = u;
   } else {
     const u64 q2 = q << 1;
@@ -540,12 +618,12 @@ __device__ __forceinline__ void inv_round8(u64 (&x)[8], u64 (&y)[8], int k, int 
 #pragma unroll
   for (int h = 0; h < 2; h++) {
     if (!PF) tw(rc.iw, 2 * m + 2 * blk + h, w[4 + h], ws[4 + h]);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
-    ibf2<LOGN, TWO, 4>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
+    ibf2<LOGN, TWO, IK_B>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
+    ibf2<LOGN, TWO, IK_B>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
   }
   if (!PF) tw(rc.iw, m + blk, w[6], ws[6]);
 #pragma unroll
-  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO, 8>(x, y, r, r + 4, w[6], ws[6], q);
+  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO, IK_C>(x, y, r, r + 4, w[6], ws[6], q);
   inv_round_reduce<LOGN, TWO>(x, y);
 }
 
@@ -602,8 +680,8 @@ __device__ __forceinline__ void inv_round4(u64 (&x)[8], u64 (&y)[8], int j, cons
       ibf2<LOGN, TWO, 3>(x, y, 4 * h + 2 * e, 4 * h + 2 * e + 1, w[3 * h + e], ws[3 * h + e], q);
     }
     if (!PF) tw(rc.iw, N / 4 + g, w[3 * h + 2], ws[3 * h + 2]);
-    ibf2<LOGN, TWO, 5>(x, y, 4 * h + 0, 4 * h + 2, w[3 * h + 2], ws[3 * h + 2], q);
-    ibf2<LOGN, TWO, 5>(x, y, 4 * h + 1, 4 * h + 3, w[3 * h + 2], ws[3 * h + 2], q);
+    ibf2<LOGN, TWO, IK_MB>(x, y, 4 * h + 0, 4 * h + 2, w[3 * h + 2], ws[3 * h + 2], q);
+    ibf2<LOGN, TWO, IK_MB>(x, y, 4 * h + 1, 4 * h + 3, w[3 * h + 2], ws[3 * h + 2], q);
   }
   inv_round_reduce<LOGN, TWO>(x, y);  // (N = 2048) sums < 8.2Q -> < 2Q
 }
@@ -669,7 +747,7 @@ __device__ __forceinline__ void xchg(u64 (&x)[8], u64 (&y)[8], u64 *sm, int j) {
 }
 
 // Forward negacyclic NTT (CT, ntt.rs:110-143 without reductions): coefficient
-// layout in, values < q; evaluation layout out, values < 45 q (see fbf).
+// layout in, values < q; evaluation layout out, values < 150 q (see fbf).
 // sm: N words (2N with TWO).  The rounds run in a loop (one copy of the round
 // body); the exchanges between them are layout-specialised and picked by a
 // block-uniform switch.

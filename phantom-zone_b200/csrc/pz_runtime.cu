@@ -63,6 +63,18 @@ u64 powmod(u64 a, u64 e, u64 q) {
 }
 u64 invmod(u64 a, u64 q) { return powmod(a, q - 2, q); }  // q prime
 u64 shoup(u64 v, u64 q) { return (u64)(((u128)v << 64) / q); }
+// Second word of a twiddle-table entry: Shoup(w), or for the N = 2048 FP64-
+// quotient butterflies the bits of w/Q rounded once to a double (the
+// quotient in 80-bit long double first, error 2^-64 relative)
+u64 tw_companion(u64 w, u64 q, u32 logn) {
+  if (logn == 11 && pz::BFLY_FP64) {
+    const double d = (double)((long double)w / (long double)q);
+    u64 bits;
+    memcpy(&bits, &d, 8);
+    return bits;
+  }
+  return shoup(w, q);
+}
 u32 log2_exact(u64 v) { return 63 - __builtin_clzll(v); }
 // utils.rs:230-237
 u32 log2_ref(u64 v) { return (v & (v - 1)) == 0 ? 63 - __builtin_clzll(v) : 64 - __builtin_clzll(v); }
@@ -285,7 +297,8 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) { delete c; return PZ_ERR_CUDA; }
   // twiddles: psi^{bitrev(i)} and psi^{-bitrev(i)} (ntt.rs:337-369), each
-  // interleaved with its Shoup companion: [w_0, ws_0, w_1, ws_1, ...]
+  // interleaved with its companion: [w_0, ws_0, w_1, ws_1, ...] (the Shoup
+  // companion, or w/Q as a double for the FP64-quotient butterflies)
   std::vector<u64> tw(4 * N);
   const u64 rinv = invmod(root, Q);
   u64 pw = 1, pwi = 1;
@@ -293,9 +306,9 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
     u64 bo = 0;
     for (u32 b = 0; b < c->logn; b++) bo |= ((i >> b) & 1) << (c->logn - 1 - b);
     tw[2 * bo] = pw;
-    tw[2 * bo + 1] = shoup(pw, Q);
+    tw[2 * bo + 1] = tw_companion(pw, Q, c->logn);
     tw[2 * N + 2 * bo] = pwi;
-    tw[2 * N + 2 * bo + 1] = shoup(pwi, Q);
+    tw[2 * N + 2 * bo + 1] = tw_companion(pwi, Q, c->logn);
     pw = mulmod(pw, root, Q);
     pwi = mulmod(pwi, rinv, Q);
   }
