@@ -956,6 +956,7 @@ def kernel_only(args):
         def launch():
             eng.blind_rotate_device(key, d_ks, d_tv, d_out)
     else:
+        eng.set_ks_tile(args.ks_tile)
         lwe = torch.from_numpy(rng.integers(0, p.lwe_q, (B, L), dtype=np.uint64).view(np.int64)).cuda()
         d_out = torch.empty((B, p.lwe_n + 1), dtype=torch.int32, device="cuda")
 
@@ -973,6 +974,8 @@ def kernel_only(args):
     ms = a.elapsed_time(b) / max(args.steps, 1)
     out = {"mode": args.mode, "param_set": args.param, "batch": B, "variant": eng.pbs_variant,
            "ms_per_launch": ms, "items_per_s": B / ms * 1e3}
+    if args.mode == "ks-kernel":
+        out["ks_tile"] = args.ks_tile
     if args.mode == "br-kernel":
         out["modmuls_per_item"] = schedule_work(p, ks) / B
     print(json.dumps(out), flush=True)
@@ -997,7 +1000,8 @@ def main():
     ap.add_argument("--param", default=PARAM)
     ap.add_argument("--variant", type=int, default=None,
                     help="blind-rotation launch-shape variant (wavefront mode: fixed instead of autotuned)")
-    ap.add_argument("--ks-tile", type=int, default=16, help="key-switch ciphertexts per CTA with --variant")
+    ap.add_argument("--ks-tile", type=int, default=16,
+                    help="key-switch ciphertexts per CTA (8, 16, 32; 64 = tensor cores) with --variant or ks-kernel")
     ap.add_argument("--users", type=int, default=8, help="users of the ni-aggregate mode")
     ap.add_argument("--ref-step-seconds", type=float, default=REF_STEP_SECONDS,
                     help="wall time of one timed step of the CPU reference arm")
@@ -1103,6 +1107,8 @@ def main():
     modmuls = schedule_work(p, ks)
     achieved = modmuls * C_MM / (br_ms / 1e3) / 1e12  # T IMAD/s
     peak = P.probe_imad_rate(local) / 1e12
+    # the other pipes the butterflies use (the quotient runs on the FP64 pipe and the conversion unit)
+    pipes = {k: v / 1e12 for k, v in P.probe_pipe_rates(local).items()}
     traffic, traffic_source = traffic_record(P, tune["variant"], B)
 
     plain = None
@@ -1156,7 +1162,10 @@ def main():
                          "traffic_source": traffic_source,
                          "peak_source": "pz_probe_imad_rate on this GPU (MEASURED_PEAKS.json has no integer peak)",
                          "launch_ms": br_ms, "bootstraps_per_launch": B,
-                         "modmuls_per_bootstrap": modmuls / B},
+                         "modmuls_per_bootstrap": modmuls / B,
+                         "pipe_rates_tips": pipes,
+                         "convention": "10 IMAD per 64-bit modmul; the butterflies' quotient runs on the FP64 "
+                                       "pipe and the conversion unit, so part of the work is off the IMAD pipe"},
             "plain": plain,
             "parity": parity,
             **extras,

@@ -177,6 +177,12 @@ pz_status pz_blind_rotate_batch_device(pz_ctx *ctx, const pz_key *key, const uin
 /* Measured throughput of 32-bit multiply-add (IMAD) instructions on a device:
  * the integer-pipe denominator of the bootstrap's roofline. */
 pz_status pz_probe_imad_rate(int device, double *imad_per_second);
+/* Measured rates (instructions per second, whole device) of the pipes the
+ * butterflies use, rates[k] for k < min(n, PZ_PIPE_PROBES): 0 mad.lo.u32
+ * (IMAD), 1 mad.wide.u32, 2 mad.hi.u32, 3 fma.rn.f64, 4 cvt.rn.f64.u64,
+ * 5 cvt.rni.u64.f64, 6 mad.lo.u32 and fma.rn.f64 interleaved (each). */
+#define PZ_PIPE_PROBES 7
+pz_status pz_probe_pipe_rates(int device, double *rates, size_t n);
 /* out = -in (mod Q, unreduced: -0 = Q) on `words` u64 words. */
 pz_status pz_not_batch_device(pz_ctx *ctx, const uint64_t *d_in, uint64_t *d_out, size_t words,
                               void *stream);
@@ -219,13 +225,16 @@ const char *pz_kernel_revision(void);
  * LWEs with this key -- `batch` of them, or, from one wave up, the largest
  * whole number of that variant's waves not above `batch` -- and keeps the
  * fastest per ciphertext (*ms: its time for `batch`); then times the
- * key-switch kernel with 8, 16 and 32 ciphertexts per CTA on `batch` inputs
- * and keeps the fastest.  Both become the context's defaults and the choice
+ * key-switch kernel with 8, 16 and 32 ciphertexts per CTA and its
+ * tensor-core form (64) on `batch` inputs and keeps the fastest.  Both become the context's defaults and the choice
  * for batches in batch's size bucket (floor(log2(gates))); launches in a
  * bucket never tuned use the defaults.  Setting a variant or a tile by hand
  * clears the per-bucket choices.  No reference counterpart. */
 pz_status pz_ctx_autotune(pz_ctx *ctx, const pz_key *key, size_t batch, int *variant, double *ms);
-/* Key-switch ciphertexts per CTA: 8, 16 (default) or 32. */
+/* Key-switch ciphertexts per CTA: 8, 16 (default) or 32 (integer
+ * multiply-adds), or 64: the tensor-core form (mma.sync s8 digits x u8 KSK
+ * byte planes, 64 ciphertexts x 224 output columns per CTA), which a key
+ * whose digits do not fit s8 runs as 16. */
 pz_status pz_ctx_set_ks_tile(pz_ctx *ctx, int ciphertexts);
 /* The blind-rotation variant and key-switch tile a batch of `gates` gates
  * would launch with now. */

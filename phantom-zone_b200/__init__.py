@@ -8,7 +8,7 @@ interface.  Import it with ``importlib.import_module("phantom-zone_b200")``.
 """
 from . import _lib
 from .engine import (GATES, PARAMETER_SETS, SELECTORS, DeviceKey, Engine, kernel_revision, param_id, params,
-                     probe_imad_rate)
+                     probe_imad_rate, probe_pipe_rates)
 from .circuits import Circuit
 from .server import DRY_RUN, Server
 from .fhe import (FheBool, FheUint8, clear_server_key, div_zero_error_flag, reset_error_flags,
@@ -16,4 +16,4 @@ from .fhe import (FheBool, FheUint8, clear_server_key, div_zero_error_flag, rese
 
 __all__ = ["FheBool", "FheUint8", "set_server_key", "clear_server_key", "div_zero_error_flag",
            "reset_error_flags", "Circuit", "Server", "DRY_RUN", "Engine", "DeviceKey", "GATES", "PARAMETER_SETS", "SELECTORS", "kernel_revision", "param_id", "params",
-           "probe_imad_rate", "_lib"]
+           "probe_imad_rate", "probe_pipe_rates", "_lib"]

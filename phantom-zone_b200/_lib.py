@@ -80,6 +80,7 @@ SIGNATURES = {
     "pz_not_batch_device": (st, [vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_blind_rotate_batch_device": (st, [vp, vp, vp, vp, vp, ctypes.c_size_t, vp]),
     "pz_probe_imad_rate": (st, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "pz_probe_pipe_rates": (st, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]),
     "pz_ntt_forward_device": (st, [vp, vp, ctypes.c_size_t, vp]),
     "pz_ntt_backward_device": (st, [vp, vp, ctypes.c_size_t, vp]),
     "pz_rlwe_by_rgsw_device": (st, [vp, vp, vp, vp, ctypes.c_size_t, ctypes.c_int, vp]),

@@ -175,6 +175,16 @@ __device__ __forceinline__ u64 decomp_next(u64 &v, const Decomp &dp) {
   return ((0ull - c) & dp.q) + k - (c << dp.logb);
 }
 
+// decomp_next with the digit as a signed integer k - c 2^logb (the same
+// residue mod q; |digit| <= 2^(logb-1))
+__device__ __forceinline__ int decomp_next_signed(u64 &v, const Decomp &dp) {
+  const u64 k = v & dp.bmask;
+  v = (v - k) >> dp.logb;
+  const u64 c = (k > dp.bby2 || (k == dp.bby2 && (v & 1ull))) ? 1ull : 0ull;
+  v += c;
+  return (int)k - (int)(c << dp.logb);
+}
+
 // One-digit decomposition (d = 1) with compile-time base 2^LOGB and IGN
 // ignored bits: decomp_init + one decomp_next, with everything after the
 // rounding shift in 32-bit arithmetic (the rounded value's digit and its next

@@ -50,6 +50,7 @@ struct pz_key {
   pz_ctx *ctx = nullptr;
   pz::u64 *d_rgsw = nullptr, *d_autos = nullptr;
   pz::u32 *d_ksk = nullptr;
+  unsigned char *d_ksk8 = nullptr;  // the KSK as byte planes (tensor-core key switch), or null
   size_t bytes = 0;
 };
 
@@ -61,6 +62,13 @@ struct pz_ni_ksk {
 };
 
 namespace pz {
+// Build k->d_ksk8 from k->d_ksk (when the parameter set's digits fit s8 and
+// the rows come in whole 32-row blocks; otherwise, or when the device is out
+// of memory, the key keeps the IMAD key-switch kernels only).
+void build_ksk8(pz_ctx *c, pz_key *k, cudaStream_t s);
+void free_key_arrays(pz_key *k);
+// KsParams of context c bound to key k (both KSK forms)
+void ks_bind_key(const pz_ctx *c, const pz_key *k, KsParams &ks);
 // floor(log2(n)), clamped to the 48 buckets of pz_ctx::tuned
 inline int size_bucket(size_t n) {
   const int b = n ? 63 - __builtin_clzll((unsigned long long)n) : 0;

@@ -661,6 +661,148 @@ __global__ void __launch_bounds__(KS_COLS)
 }
 
 // ---------------------------------------------------------------------------
+// LWE key switch on the tensor cores.  With base-2^logb digits (logb <= 4
+// in every parameter set: digits in [-8, 8]) the key switch of a batch is a
+// matrix product: [ciphertexts x d N digits] (s8) times [d N x (n + 1)] KSK
+// entries mod q_ks.  The KSK is split into byte planes (u8), each plane one
+// mma.sync m16n8k32 s8 x u8 product with exact s32 sums (|sum| < d N 8 255 <
+// 2^27), folded into the u32 result as sum_p 2^(8p) plane_p -- exact mod
+// 2^32, and q_ks divides 2^32.  A CTA owns KSM_ROWS = 64 ciphertexts x
+// KSM_COLS = 224 output columns: 8 warps = 4 row fragments (16) x 2 column
+// halves (112 = 14 column fragments of 8).  Per chunk of 32 input
+// coefficients the CTA writes the 32 d digits of its 64 ciphertexts into
+// shared memory (row stride 32 d + 16 bytes: conflict-free fragment loads);
+// the KSK planes of each 32-row block stream into a double-buffered stage
+// by 16-byte cp.async, one block ahead.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_s8u8(u32 (&d)[4], u32 a0, u32 a1, u32 a2, u32 a3, u32 b0, u32 b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.s8.u8.s32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%10, %10, %10, %10};"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1), "r"(0u));
+}
+
+__host__ __device__ constexpr size_t ksm_astride(u32 d) { return (size_t)32 * d + 16; }
+constexpr size_t ksm_smem_bytes(u32 d, u32 planes) {
+  return (size_t)KSM_ROWS * ksm_astride(d) + 2 * (size_t)planes * KSM_COLS * 32;
+}
+
+template <int NP>
+__global__ void __launch_bounds__(256, 2)
+    ks_mma_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
+  extern __shared__ __align__(16) unsigned char ksm[];
+  const u32 d = P.d, astride = (u32)ksm_astride(d);
+  unsigned char *A = ksm;
+  unsigned char *Bs = ksm + (size_t)KSM_ROWS * astride;  // [2][NP][KSM_COLS][32]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int mf = warp & 3, nh = warp >> 2;
+  const int ct0 = blockIdx.x * KSM_ROWS, cb = blockIdx.y;
+  const size_t L = (size_t)P.N + 1;
+  const u32 kblocks = d * P.N / 32, kb_total = kblocks;
+  const size_t plane_bytes = (size_t)kblocks * P.ksk8_cols * 32;
+  const unsigned char *Bg = P.ksk8 + (size_t)cb * KSM_COLS * 32;
+  constexpr int STAGE = NP * KSM_COLS * 32, CHUNKS16 = NP * KSM_COLS * 2;  // 16-byte pieces per stage
+  auto issue = [&](u32 kb) {
+    unsigned char *dst = Bs + (size_t)(kb & 1) * STAGE;
+    for (int e = tid; e < CHUNKS16; e += 256) {
+      const int p = e / (KSM_COLS * 2), r = e % (KSM_COLS * 2);
+      cp_async16(dst + (size_t)p * KSM_COLS * 32 + r * 16,
+                 Bg + p * plane_bytes + (size_t)kb * P.ksk8_cols * 32 + r * 16);
+    }
+    cp_async_commit();
+  };
+  u32 acc[14][4];
+#pragma unroll
+  for (int f = 0; f < 14; f++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) acc[f][i] = 0;
+  issue(0);
+  u32 kb = 0;
+  for (u32 i0 = 0; i0 < P.N; i0 += 32) {
+    __syncthreads();  // every warp is done with the previous chunk's digits
+    for (int e = tid; e < KSM_ROWS * 32; e += 256) {
+      const int row = e >> 5, cc = e & 31, ct = ct0 + row;
+      unsigned char *dst = A + (size_t)row * astride + (size_t)cc * d;
+      if (ct < count) {
+        const size_t off = 1 + i0 + cc;
+        const u64 x = prelude_moddown(operand(c0, P.in0, ct, off, L, P.Q), operand(c1, P.in1, ct, off, L, P.Q),
+                                      gates ? gates[ct] : 0, false, P);
+        u64 st = decomp_init(x, P.dks);
+        for (u32 j = 0; j < d; j++) dst[j] = (unsigned char)(signed char)decomp_next_signed(st, P.dks);
+      } else {
+        for (u32 j = 0; j < d; j++) dst[j] = 0;
+      }
+    }
+    for (u32 ks = 0; ks < d; ks++, kb++) {
+      cp_async_wait_all();
+      __syncthreads();  // stage kb landed for every thread; stage kb + 1 is free; digits written
+      if (kb + 1 < kb_total) issue(kb + 1);
+      const unsigned char *ar = A + (size_t)(16 * mf + g) * astride + ks * 32 + 4 * t;
+      const u32 a0 = *(const u32 *)ar, a1 = *(const u32 *)(ar + 8 * astride);
+      const u32 a2 = *(const u32 *)(ar + 16), a3 = *(const u32 *)(ar + 8 * astride + 16);
+      const unsigned char *bs = Bs + (size_t)(kb & 1) * STAGE + (size_t)(nh * 112 + g) * 32 + 8 * t;
+#pragma unroll
+      for (int f = 0; f < 14; f++) {
+        u32 r[NP][4];
+#pragma unroll
+        for (int p = 0; p < NP; p++) {
+          const uint2 b = *(const uint2 *)(bs + (size_t)p * KSM_COLS * 32 + f * 8 * 32);
+          mma_s8u8(r[p], a0, a1, a2, a3, b.x, b.y);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          u32 v = r[0][i];
+          if (NP > 1) v += r[1][i] << 8;
+          if (NP > 2) v += r[2][i] << 16;
+          acc[f][i] += v;
+        }
+      }
+    }
+  }
+  // fragment element i of column fragment f: row 16 mf + g (+8 for i >= 2),
+  // column nh 112 + 8 f + 2 t + (i & 1)
+#pragma unroll
+  for (int f = 0; f < 14; f++) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int ct = ct0 + 16 * mf + g + (i >= 2 ? 8 : 0);
+      const u32 col = (u32)cb * KSM_COLS + nh * 112 + 8 * f + 2 * t + (i & 1);
+      if (ct < count && col <= P.n) {
+        u32 v = acc[f][i];
+        if (col == 0)
+          v += (u32)prelude_moddown(operand(c0, P.in0, ct, 0, L, P.Q), operand(c1, P.in1, ct, 0, L, P.Q),
+                                    gates ? gates[ct] : 0, true, P);
+        out[(size_t)ct * P.out_stride + col] = v & P.mask;
+      }
+    }
+  }
+}
+
+// KSK u32 rows -> byte planes in the fragment order of ks_mma_kernel: row r
+// of block r / 32 goes to byte 8 j + 4 h + (k & 3) of its column's 32-byte
+// record, k = r mod 32, h = k / 16, j = (k mod 16) / 4 (thread j of a quad
+// loads bytes 8 j .. 8 j + 7: rows 4j..4j+3 and 16+4j..16+4j+3).
+__global__ void ksk_planes_kernel(const u32 *ksk, u32 rows, u32 stride, u32 n, u32 planes, u32 cols,
+                                  unsigned char *out) {
+  const size_t total = (size_t)rows * cols, plane_bytes = total;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const u32 r = (u32)(e / cols), c = (u32)(e % cols);
+    const u32 v = c <= n ? ksk[(size_t)r * stride + c] : 0u;
+    const u32 k = r & 31, pos = 8 * ((k & 15) >> 2) + 4 * (k >> 4) + (k & 3);
+    const size_t o = ((size_t)(r >> 5) * cols + c) * 32 + pos;
+    for (u32 p = 0; p < planes; p++) out[p * plane_bytes + o] = (unsigned char)(v >> (8 * p));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The bootstrap: one CTA per ciphertext (grid-stride over the batch)
 // ---------------------------------------------------------------------------
 // pbs.rs:416-420
@@ -1462,6 +1604,72 @@ cudaError_t launch_imad_probe(int blocks, int threads, u32 iters, u32 *sink, cud
   return cudaGetLastError();
 }
 
+// Pipe-rate probe behind the butterflies' design: 8 independent chains per
+// thread of one instruction kind, 16 x 8 per iteration.  KIND 0 mad.lo.u32
+// (IMAD), 1 mad.wide.u32 (IMAD.WIDE), 2 mad.hi.u32 (IMAD.HI), 3 fma.rn.f64,
+// 4 cvt.rn.f64.u64, 5 cvt.rni.u64.f64, 6 mad.lo.u32 and fma.rn.f64
+// interleaved (the rate of each).
+template <int KIND>
+__global__ void pipe_probe_kernel(u32 iters, u32 seed, u32 *sink) {
+  u64 x[8];
+  double f[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    x[i] = ((u64)(seed + threadIdx.x * 8 + i) << 20) | i;
+    f[i] = (double)(seed + threadIdx.x + i);
+  }
+  const u32 m = seed | 1u, c = seed ^ 0x9e3779b9u;
+  const double fm = 1.0000001, fc = 1e-9;
+  for (u32 it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        if (KIND == 0 || KIND == 6) {
+          u32 v = (u32)x[i];
+          asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(v) : "r"(m), "r"(c));
+          x[i] = v;
+        }
+        if (KIND == 1) asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(x[i]) : "r"((u32)x[i]), "r"(m));
+        if (KIND == 2) {
+          u32 v = (u32)x[i];
+          asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(v) : "r"(m), "r"(c));
+          x[i] = v;
+        }
+        if (KIND == 3 || KIND == 6) asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(f[i]) : "d"(fm), "d"(fc));
+        if (KIND == 4) {
+          double d;
+          asm volatile("cvt.rn.f64.u64 %0, %1;" : "=d"(d) : "l"(x[i]));
+          x[i] = (u64)__double_as_longlong(d) >> 3;
+        }
+        if (KIND == 5) {
+          u64 q;
+          asm volatile("cvt.rni.u64.f64 %0, %1;" : "=l"(q) : "d"(f[i]));
+          f[i] = __longlong_as_double((long long)(q | 0x4100000000000000ull));
+        }
+      }
+    }
+  }
+  u64 acc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) acc ^= x[i] ^ (u64)__double_as_longlong(f[i]);
+  if (acc == 0x12345678ull) sink[blockIdx.x] = (u32)acc;
+}
+
+cudaError_t launch_pipe_probe(int kind, int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s) {
+  switch (kind) {
+    case 0: pipe_probe_kernel<0><<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink); break;
+    case 1: pipe_probe_kernel<1><<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink); break;
+    case 2: pipe_probe_kernel<2><<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink); break;
+    case 3: pipe_probe_kernel<3><<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink); break;
+    case 4: pipe_probe_kernel<4><<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink); break;
+    case 5: pipe_probe_kernel<5><<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink); break;
+    case 6: pipe_probe_kernel<6><<<blocks, threads, 0, s>>>(iters, 0x2545F491u, sink); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 __global__ void not_kernel(const u64 *in, u64 *out, size_t words, u64 q) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x)
     out[i] = q - in[i];  // neg = q - a, evaluator.rs:2247-2250
@@ -1599,6 +1807,21 @@ cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *
                       size_t count, u32 *out, cudaStream_t s, bool reduce_output, int ct) {
   if (count == 0) return cudaSuccess;
   if (P.d > (u32)MAX_KS_D) return cudaErrorInvalidValue;
+  // the tensor-core form needs the key's byte planes; a key without them
+  // (digits wider than s8, or no memory for the planes) runs the 16-tile
+  if (ct == KS_CT_MMA && (!P.ksk8 || P.planes < 1 || P.planes > 3 || P.d > 16 || (P.d * P.N) % 32 || P.N % 32))
+    ct = 16;
+  if (ct == KS_CT_MMA) {
+    const dim3 grid((unsigned)((count + KSM_ROWS - 1) / KSM_ROWS), P.ksk8_cols / KSM_COLS);
+    const size_t smem = ksm_smem_bytes(P.d, P.planes);
+    cudaError_t e;
+#define PZ_KSM(NP)                                                              if ((e = set_smem(ks_mma_kernel<NP>, smem)) != cudaSuccess) return e;         ks_mma_kernel<NP><<<grid, 256, smem, s>>>(P, gates, c0, c1, (int)count, out);
+    if (P.planes == 1) { PZ_KSM(1) }
+    else if (P.planes == 2) { PZ_KSM(2) }
+    else { PZ_KSM(3) }
+#undef PZ_KSM
+    return cudaGetLastError();
+  }
   if (ct != 8 && ct != 16 && ct != 32) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((count + ct - 1) / ct), (unsigned)((P.n + 1 + KS_COLS - 1) / KS_COLS));
   grid.z = ks_split((size_t)grid.x * grid.y, P.N);
@@ -1620,6 +1843,16 @@ cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *
     return cudaGetLastError();
   }
   return cudaSuccess;
+}
+
+cudaError_t launch_ksk_planes(const u32 *ksk, u32 rows, u32 stride, u32 n, u32 planes, unsigned char *out,
+                              cudaStream_t s) {
+  if (rows % 32 || planes < 1 || planes > 3) return cudaErrorInvalidValue;
+  const u32 cols = ksk8_cols(n);
+  const size_t total = (size_t)rows * cols;
+  ksk_planes_kernel<<<(unsigned)std::min<size_t>((total + 255) / 256, 8192), 256, 0, s>>>(ksk, rows, stride, n,
+                                                                                          planes, cols, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,

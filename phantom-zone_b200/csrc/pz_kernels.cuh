@@ -39,6 +39,13 @@ struct KsParams {
   u32 out_stride;           // u32 words per output LWE (>= n+1)
   u32 raw;                  // inputs are combined LWEs: skip the gate prelude
   const u32 *ksk;           // [d N][ksk_stride]
+  // The same KSK as byte planes for the tensor-core key switch (null: not
+  // built): plane p holds bits 8p..8p+7 of every entry, in blocks of 32 rows
+  // ([planes][d N / 32][ksk8_cols][32], rows permuted inside a block so that
+  // one 8-byte load gives a thread its mma fragment; ksk8_cols = n + 1
+  // rounded up to KSM_COLS, zero-padded).
+  const unsigned char *ksk8;
+  u32 planes, ksk8_cols;
   // Optional gather (circuit wires): input i of gate ct is LWE
   // c{i}[in{i}[ct] & WIRE_MASK], negated (q - x) when bit 31 is set.
   const u32 *in0, *in1;
@@ -73,6 +80,18 @@ cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u
 // reduce_output: leave every output word reduced mod q_ks (otherwise the
 // words may carry multiples of q_ks, and consumers mask with q_ks - 1)
 // ct: ciphertexts per CTA (8, 16 or 32)
+// Tensor-core key switch: KSM_ROWS ciphertexts x KSM_COLS output columns
+// per CTA; launch_ks takes ct = KS_CT_MMA for it.
+constexpr int KSM_ROWS = 64, KSM_COLS = 224, KS_CT_MMA = 64;
+inline u32 ksk8_cols(u32 n) { return (n + 1 + KSM_COLS - 1) / KSM_COLS * KSM_COLS; }
+inline u32 ksk8_planes(u32 mask) {  // bytes of q_ks - 1
+  u32 bits = 0;
+  while (bits < 32 && (mask >> bits)) bits++;
+  return (bits + 7) / 8;
+}
+// KSK rows (u32, stride ksk_stride, d N rows, n + 1 used columns) -> byte planes
+cudaError_t launch_ksk_planes(const u32 *ksk, u32 rows, u32 stride, u32 n, u32 planes, unsigned char *out,
+                              cudaStream_t s);
 cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *c0, const u64 *c1,
                       size_t count, u32 *out, cudaStream_t s, bool reduce_output, int ct = KS_TILE_CT);
 cudaError_t launch_pbs(int logn, bool d1, const BrParams &P, const u32 *ks, u32 ks_stride,
@@ -98,6 +117,7 @@ cudaError_t launch_pbs_ragged(int logn, bool d1, const BrParams *d_descs, const 
                               const u32 *out_idx, size_t count, int grid_limit, cudaStream_t s, int variant);
 cudaError_t launch_not(const u64 *in, u64 *out, size_t words, u64 q, cudaStream_t s);
 cudaError_t launch_imad_probe(int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s);
+cudaError_t launch_pipe_probe(int kind, int blocks, int threads, u32 iters, u32 *sink, cudaStream_t s);
 // per launch: blocks * threads * iters * 16 * 8 multiply-adds
 size_t pbs_smem_bytes(int logn, u32 br_q, u32 n);
 // blind-rotation items resident at once for a launch shape (whole-wave size)

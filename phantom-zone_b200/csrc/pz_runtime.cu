@@ -199,6 +199,41 @@ pz_status check_gates_host(pz_ctx *c, const uint8_t *gates, size_t count, bool r
 }  // namespace
 
 namespace pz {
+void build_ksk8(pz_ctx *c, pz_key *k, cudaStream_t s) {
+  const pz_params &P = c->P;
+  const u32 rows = P.lwe_d * P.rlwe_n;
+  if (!k->d_ksk || rows % 32 || P.rlwe_n % 32 || P.lwe_d > 16 || P.lwe_logb > 7) return;
+  const u32 planes = ksk8_planes(c->ks.mask), cols = ksk8_cols(P.lwe_n);
+  const size_t bytes = (size_t)planes * rows * cols;
+  if (cudaMalloc(&k->d_ksk8, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    k->d_ksk8 = nullptr;
+    return;
+  }
+  if (launch_ksk_planes(k->d_ksk, rows, ks_stride(P), P.lwe_n, planes, k->d_ksk8, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(k->d_ksk8);
+    k->d_ksk8 = nullptr;
+    return;
+  }
+  k->bytes += bytes;
+}
+
+void free_key_arrays(pz_key *k) {
+  cudaFree(k->d_rgsw);
+  cudaFree(k->d_autos);
+  cudaFree(k->d_ksk);
+  cudaFree(k->d_ksk8);
+}
+
+void ks_bind_key(const pz_ctx *c, const pz_key *k, KsParams &ks) {
+  ks.ksk = k->d_ksk;
+  ks.ksk8 = k->d_ksk8;
+  ks.planes = ksk8_planes(c->ks.mask);
+  ks.ksk8_cols = ksk8_cols(c->P.lwe_n);
+}
+
 int effective_variant(pz_ctx *c, size_t count) {
   const bool d1 = c->P.rlrg_d_a == 1 && c->P.rlrg_d_b == 1 && c->P.auto_d == 1;
   if (c->logn != 11 || !d1) return c->pbs_variant;
@@ -225,7 +260,7 @@ pz_status run_gates(pz_ctx *c, const pz_key *k, const unsigned char *d_gates, co
   br.autos = k->d_autos;
   br.out_idx = out_idx;
   pz::KsParams ks = c->ks;
-  ks.ksk = k->d_ksk;
+  pz::ks_bind_key(c, k, ks);
   ks.raw = raw ? 1u : 0u;
   ks.in0 = in0;
   ks.in1 = in1;
@@ -452,7 +487,7 @@ pz_status pz_key_upload(pz_ctx *c, const pz_server_key_view *v, pz_key **out) {
   pz_key *k = new pz_key();
   k->ctx = c;
   auto cleanup = [&](pz_status s, const std::string &m) {
-    cudaFree(k->d_rgsw); cudaFree(k->d_autos); cudaFree(k->d_ksk);
+    pz::free_key_arrays(k);
     delete k;
     return fail(c, s, m);
   };
@@ -491,6 +526,7 @@ pz_status pz_key_upload(pz_ctx *c, const pz_server_key_view *v, pz_key **out) {
     for (size_t col = 0; col < cols; col++) ksk32[r * stride + col] = (u32)(v->lwe_ksk[r * cols + col] & (P.lwe_q - 1));
   if ((e = cudaMemcpy(k->d_ksk, ksk32.data(), ksk32.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
     return cleanup(PZ_ERR_CUDA, std::string("ksk copy: ") + cudaGetErrorString(e));
+  pz::build_ksk8(c, k, c->stream);
   *out = k;
   return PZ_OK;
 }
@@ -512,7 +548,7 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
   u64 *d_stage = nullptr;
   auto cleanup = [&](pz_status s, const std::string &m) {
     cudaFree(d_stage);
-    cudaFree(k->d_rgsw); cudaFree(k->d_autos); cudaFree(k->d_ksk);
+    pz::free_key_arrays(k);
     delete k;
     return fail(c, s, m);
   };
@@ -559,6 +595,8 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
       (e = cudaStreamSynchronize(c->stream)) != cudaSuccess)
     return cleanup(PZ_ERR_CUDA, std::string("ksk b column: ") + cudaGetErrorString(e));
   cudaFree(d_stage);
+  d_stage = nullptr;
+  pz::build_ksk8(c, k, c->stream);
   *out = k;
   return PZ_OK;
 }
@@ -566,7 +604,7 @@ pz_status pz_key_upload_seeded(pz_ctx *c, const pz_seeded_server_key_view *v, pz
 void pz_key_release(pz_key *k) {
   if (!k) return;
   cudaSetDevice(k->ctx->device);
-  cudaFree(k->d_rgsw); cudaFree(k->d_autos); cudaFree(k->d_ksk);
+  pz::free_key_arrays(k);
   delete k;
 }
 size_t pz_key_device_bytes(const pz_key *k) { return k ? k->bytes : 0; }
@@ -713,12 +751,13 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
     e = cudaMemcpy(d_c01, c01.data(), c01.size() * 8, cudaMemcpyHostToDevice);
   }
   pz::KsParams ksp = c->ks;
-  ksp.ksk = k->d_ksk;
+  pz::ks_bind_key(c, k, ksp);
   ksp.raw = 0;
   ksp.out_stride = cols;
   double best_ks = 1e30;
-  for (int ct : {8, 16, 32}) {
+  for (int ct : {8, 16, 32, pz::KS_CT_MMA}) {
     if (e != cudaSuccess) break;
+    if (ct == pz::KS_CT_MMA && !k->d_ksk8) continue;
     auto launch = [&]() {
       return pz::launch_ks(ksp, d_g, d_c01, d_c01 + batch * L, batch, d_ks, c->stream, false, ct);
     };
@@ -750,7 +789,8 @@ pz_status pz_ctx_autotune(pz_ctx *c, const pz_key *k, size_t batch, int *variant
 }
 
 pz_status pz_ctx_set_ks_tile(pz_ctx *c, int ciphertexts) {
-  if (!c || (ciphertexts != 8 && ciphertexts != 16 && ciphertexts != 32)) return PZ_ERR_INVALID_ARGUMENT;
+  if (!c || (ciphertexts != 8 && ciphertexts != 16 && ciphertexts != 32 && ciphertexts != pz::KS_CT_MMA))
+    return PZ_ERR_INVALID_ARGUMENT;
   c->ks_ct = ciphertexts;
   for (auto &t : c->tuned) t = pz_ctx::Tuned{};
   return PZ_OK;
@@ -803,6 +843,39 @@ pz_status pz_probe_imad_rate(int device, double *imad_per_second) {
   cudaEventDestroy(e1);
   cudaFree(sink);
   if (st == PZ_OK) *imad_per_second = (double)blocks * threads * iters * 16 * 8 / (best * 1e-3);
+  return st;
+}
+
+pz_status pz_probe_pipe_rates(int device, double *rates, size_t n) {
+  if (!rates) return PZ_ERR_INVALID_ARGUMENT;
+  for (size_t i = 0; i < n; i++) rates[i] = 0;
+  if (cudaSetDevice(device) != cudaSuccess) return PZ_ERR_CUDA;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return PZ_ERR_CUDA;
+  const int blocks = sms * 8, threads = 256;
+  const u32 iters = 1024;
+  u32 *sink = nullptr;
+  if (cudaMalloc(&sink, blocks * 4) != cudaSuccess) return PZ_ERR_OUT_OF_MEMORY;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  pz_status st = PZ_OK;
+  for (size_t kind = 0; kind < n && kind < PZ_PIPE_PROBES && st == PZ_OK; kind++) {
+    float best = 1e30f;
+    for (int rep = 0; rep < 3 && st == PZ_OK; rep++) {
+      cudaEventRecord(e0, 0);
+      if (pz::launch_pipe_probe((int)kind, blocks, threads, iters, sink, 0) != cudaSuccess) st = PZ_ERR_CUDA;
+      cudaEventRecord(e1, 0);
+      if (cudaEventSynchronize(e1) != cudaSuccess) st = PZ_ERR_CUDA;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0 && ms < best) best = ms;  // first launch is a warm-up
+    }
+    if (st == PZ_OK) rates[kind] = (double)blocks * threads * iters * 16 * 8 / (best * 1e-3);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
   return st;
 }
 
@@ -869,7 +942,7 @@ pz_status pz_lwe_key_switch_device(pz_ctx *c, const pz_key *k, const uint64_t *d
   // raw inputs already mod q_ks: the mod-down step must be the identity, so
   // run the key-switch kernel with Q = q_ks and gate code GATE_RAW.
   pz::KsParams ks = c->ks;
-  ks.ksk = k->d_ksk;
+  pz::ks_bind_key(c, k, ks);
   ks.Q = c->P.lwe_q;
   ks.Q_f = (double)c->P.lwe_q;
   ks.out_stride = c->P.lwe_n + 1;

@@ -105,12 +105,11 @@ pz_status pz_key_import(pz_ctx *c, const void *buf, size_t size, pz_key **out) {
   if (e == cudaSuccess) e = cudaMemcpy(k->d_autos, p + rg, au, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(k->d_ksk, p + rg + au, ks, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
-    cudaFree(k->d_rgsw);
-    cudaFree(k->d_autos);
-    cudaFree(k->d_ksk);
+    pz::free_key_arrays(k);
     delete k;
     return pz::cuda_fail(c, "pz_key_import", e);
   }
+  pz::build_ksk8(c, k, c->stream);  // derived on the device; the blob carries only the u32 rows
   *out = k;
   return PZ_OK;
 }

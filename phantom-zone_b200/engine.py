@@ -48,6 +48,16 @@ def probe_imad_rate(device=0):
     return v.value
 
 
+PIPE_PROBES = ["imad", "imad_wide", "imad_hi", "dfma", "cvt_f64_u64", "cvt_u64_f64", "imad_with_dfma"]
+
+
+def probe_pipe_rates(device=0):
+    """Instructions per second of the pipes the butterflies use, by name."""
+    arr = (ctypes.c_double * len(PIPE_PROBES))()
+    check(lib().pz_probe_pipe_rates(device, arr, len(PIPE_PROBES)), None, "pz_probe_pipe_rates")
+    return dict(zip(PIPE_PROBES, list(arr)))
+
+
 def kernel_revision():
     """Revision tag of the blind-rotation kernel in the loaded library (a
     profile on record applies only to the revision it was taken on)."""
@@ -213,7 +223,8 @@ class Engine:
         return {"variant": v.value, "ms": ms.value, "ks_tile": self.launch_shape(batch)["ks_tile"]}
 
     def set_ks_tile(self, ciphertexts):
-        """Key-switch ciphertexts per CTA (8, 16, 32); clears the tuned choices."""
+        """Key-switch ciphertexts per CTA (8, 16, 32; 64 = the tensor-core form);
+        clears the tuned choices."""
         check(lib().pz_ctx_set_ks_tile(self.h, int(ciphertexts)), self.h, "pz_ctx_set_ks_tile")
 
     def launch_shape(self, gates):

@@ -145,11 +145,13 @@ def test_lwe_key_switch(gpu_available, param):
 
 
 @pytest.mark.parametrize("param", ["I_2P_LB_SR", "NI_8P"])
-@pytest.mark.parametrize("tile", [8, 16, 32])
+@pytest.mark.parametrize("tile", [8, 16, 32, 64])
 def test_lwe_key_switch_every_tile(gpu_available, param, tile):
-    """The key switch with 8, 16 and 32 ciphertexts per CTA (the tiles the
-    autotuner picks from) equals the oracle, on a batch that leaves a partial
-    last tile and on one large enough to run unsplit (grid.z = 1)."""
+    """The key switch with 8, 16 and 32 ciphertexts per CTA and the
+    tensor-core form (64: s8 digits x u8 KSK byte planes) -- the shapes the
+    autotuner picks from -- equals the oracle, on a batch that leaves a
+    partial last tile and on one large enough to run unsplit (grid.z = 1);
+    the inputs include the q_ks edge value."""
     ev, _, _, okey = oracle_setup(param)
     eng, dkey = engine_and_key(param)
     qk = ev.info.lwe_q
@@ -206,6 +208,37 @@ def test_gate_batch_bit_exact(gpu_available, param):
         w_out, w_ks, w_rl, _ = okey.pbs(g, comb)
         assert np.array_equal(got_ks[i].astype(np.uint64), w_ks), f"key switch mismatch at {i} ({g})"
         assert np.array_equal(got_rl[i], w_rl), f"blind rotation mismatch at {i} ({g})"
+        assert np.array_equal(got_out[i], w_out), f"output mismatch at {i} ({g})"
+    dec = ev.decrypt_bool(secrets[0], got_out)
+    want = np.array([TRUTH[names[i % 6]](bits0[i], bits1[i]) for i in range(count)])
+    assert np.array_equal(dec, want)
+
+
+@pytest.mark.parametrize("param", PARAMS)
+def test_gate_batch_tensor_core_key_switch(gpu_available, param):
+    """Gates whose key switch runs on the tensor cores (tile 64: the gate
+    prelude and mod-down feed s8 digits, the KSK comes as u8 byte planes)
+    give the oracle's key-switched LWEs and outputs, across a partial second
+    row tile (70 gates)."""
+    O = oracle()
+    ev, secrets, _, okey = oracle_setup(param)
+    eng, dkey = engine_and_key(param)
+    names = list(TRUTH)
+    count = 70
+    bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, count, 0x57)
+    gates = np.array([O.GATES[names[i % 6]] for i in range(count)], np.uint8)
+    out = to_dev(np.zeros((count, ev.L), np.uint64))
+    ks = to_dev(np.zeros((count, ev.n + 1), np.uint32))
+    try:
+        eng.set_ks_tile(64)
+        eng.gate_batch_device(dkey, to_dev(gates), to_dev(c0), to_dev(c1), out, ks_out=ks)
+    finally:
+        eng.set_ks_tile(16)
+    got_out, got_ks = to_host(out), to_host(ks, np.uint32)
+    for i in list(range(4)) + list(range(63, 70)):
+        g = names[i % 6]
+        w_out, w_ks, _, _ = okey.pbs(g, combine(ev, g, c0[i], c1[i]))
+        assert np.array_equal(got_ks[i].astype(np.uint64), w_ks), f"key switch mismatch at {i} ({g})"
         assert np.array_equal(got_out[i], w_out), f"output mismatch at {i} ({g})"
     dec = ev.decrypt_bool(secrets[0], got_out)
     want = np.array([TRUTH[names[i % 6]](bits0[i], bits1[i]) for i in range(count)])
