@@ -67,7 +67,7 @@ __device__ __forceinline__ u64 redc(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
   return hi + umulhi(m, q) + (lo != 0 ? 1ull : 0ull);
 }
 
-// hi:lo = x a + y c for x, y < 2^62 (lazy forward outputs: < 238 Q < 2^61.9)
+// hi:lo = x a + y c for x, y < 2^62 (lazy forward outputs: < 150 Q < 2^61.3)
 // and a, c < Q (keys): in 32-bit limbs the middle column x0 a1 + x1 a0 +
 // y0 c1 + y1 c0 stays below 2^63 + 2^55 and the high column below 2^53, so
 // both accumulate with mad.wide and no carries; only the low column and the
@@ -321,29 +321,19 @@ constexpr bool BFLY_FP64 = false;
 #else
 constexpr bool BFLY_FP64 = true;
 #endif
-// PZ_FP64_F2I_MAGIC (a comparison): the quotient as the mantissa of
-// qd + 2^55 (a multiple of 8, 4 more of error: raw in (-10.51 Q, 10.51 Q),
-// offset 11 Q) instead of a conversion.  Converting f64(vr) the same way
-// (two 2^52-offset doubles and an FMA) measured 19 % slower than the
-// conversion unit: the extra ALU and FP64 instructions cost more issue
-// slots than the conversions they replace.
-#ifdef PZ_FP64_F2I_MAGIC
-constexpr u64 FP_OFF = 11;  // raw + 11 Q in (0.49 Q, 21.51 Q)
-#else
+// (Magic-number conversions measured slower on B200: both conversions as
+// 2^52-offset doubles and an FMA in, the mantissa of qd + 2^55 out, -19 %;
+// the out conversion alone that way, -10 %: the extra ALU and FP64
+// instructions cost more issue slots than the conversion unit's quarter
+// rate does.)
 constexpr u64 FP_OFF = 7;  // raw + 7 Q in (0.49 Q, 13.51 Q)
-#endif
 __device__ __forceinline__ u64 fp_raw(u64 v, u64 w, u64 wq_bits) {
   const u64 vr = reduce_n2048(v);
   u64 qi, r;
   double vd;
   asm("cvt.rn.f64.u64 %0, %1;" : "=d"(vd) : "l"(vr));
   const double qd = __dmul_rn(vd, __longlong_as_double((long long)wq_bits));
-#ifdef PZ_FP64_F2I_MAGIC
-  const double sq = __dadd_rn(qd, 36028797018963968.0);  // + 2^55
-  qi = ((u64)__double_as_longlong(sq) & ((1ull << 52) - 1)) << 3;
-#else
   asm("cvt.rni.u64.f64 %0, %1;" : "=l"(qi) : "d"(qd));
-#endif
   asm("{\n\t"
       ".reg .u32 v0, v1, w0, w1, q0, q1, t0, t1, z;\n\t"
       ".reg .u64 wy, t;\n\t"
@@ -399,7 +389,7 @@ __device__ __forceinline__ void add_sub_ptx(u64 x, u64 t, u64 c, u64 &sum, u64 &
 
 template <bool SPQ>
 __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
-  if (SPQ && BFLY_FP64) {  // outputs grow by < 13.51 Q per stage (< 150 Q after 11; F2I_MAGIC: 21.51 Q, 238 Q)
+  if (SPQ && BFLY_FP64) {  // outputs grow by < 13.51 Q per stage (< 150 Q after 11)
     const u64 raw = fp_raw(y, w, ws), xc = x + FP_OFF * Q_N2048;
     x = xc + raw;
     y = xc - raw;
@@ -476,7 +466,7 @@ __device__ __forceinline__ u64 mac_reduce(u64 hi, u64 lo, u64 q, u64 qinv_neg) {
 // < 2q otherwise), back below 2q.
 template <int LOGN>
 __device__ __forceinline__ void mac_mul(u64 x, u64 a, u64 &hi, u64 &lo) {
-  if constexpr (LOGN == 11) mul128_narrow(x, a, hi, lo);  // x < 238 Q < 2^62, a < Q < 2^54
+  if constexpr (LOGN == 11) mul128_narrow(x, a, hi, lo);  // x < 150 Q < 2^62, a < Q < 2^54
   else mul128(x, a, hi, lo);
 }
 template <int LOGN>
@@ -490,9 +480,7 @@ __device__ __forceinline__ u64 mac_add_b(u64 v, u64 q2) {
 // inputs < 2.04 Q in stage a, K = 3, and IK_MB in stage b).  The Shoup
 // products leave < 4 Q: sums < 4, 8, 16 Q.  The FP64-quotient products
 // leave < 13.51 Q: stage b sees < 13.51 Q, stage c < 27.02 Q.
-// (PZ_FP64_F2I_MAGIC: products < 21.51 Q, stage b < 21.51 Q, stage c < 43.02 Q.)
-constexpr int IK_FB = FP_OFF == 7 ? 14 : 22, IK_FC = FP_OFF == 7 ? 28 : 44;
-constexpr int IK_B = BFLY_FP64 ? IK_FB : 4, IK_C = BFLY_FP64 ? IK_FC : 8, IK_MB = BFLY_FP64 ? IK_FB : 5;
+constexpr int IK_B = BFLY_FP64 ? 14 : 4, IK_C = BFLY_FP64 ? 28 : 8, IK_MB = BFLY_FP64 ? 14 : 5;
 
 template <bool SPQ, int K>
 __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
