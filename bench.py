@@ -1000,7 +1000,7 @@ def main():
     ap.add_argument("--param", default=PARAM)
     ap.add_argument("--variant", type=int, default=None,
                     help="blind-rotation launch-shape variant (wavefront mode: fixed instead of autotuned)")
-    ap.add_argument("--ks-tile", type=int, default=16,
+    ap.add_argument("--ks-tile", type=int, default=64,
                     help="key-switch ciphertexts per CTA (8, 16, 32; 64 = tensor cores) with --variant or ks-kernel")
     ap.add_argument("--users", type=int, default=8, help="users of the ni-aggregate mode")
     ap.add_argument("--ref-step-seconds", type=float, default=REF_STEP_SECONDS,

@@ -231,10 +231,11 @@ const char *pz_kernel_revision(void);
  * bucket never tuned use the defaults.  Setting a variant or a tile by hand
  * clears the per-bucket choices.  No reference counterpart. */
 pz_status pz_ctx_autotune(pz_ctx *ctx, const pz_key *key, size_t batch, int *variant, double *ms);
-/* Key-switch ciphertexts per CTA: 8, 16 (default) or 32 (integer
- * multiply-adds), or 64: the tensor-core form (mma.sync s8 digits x u8 KSK
- * byte planes, 64 ciphertexts x 224 output columns per CTA), which a key
- * whose digits do not fit s8 runs as 16. */
+/* Key-switch ciphertexts per CTA: 8, 16 or 32 (integer multiply-adds), or
+ * 64 (the default): the tensor-core form (mma.sync s8 digits x u8 KSK byte
+ * planes, 64 ciphertexts x 224 output columns per CTA, the input
+ * coefficients split over more CTAs for small batches), which a key whose
+ * digits do not fit s8 runs as 16. */
 pz_status pz_ctx_set_ks_tile(pz_ctx *ctx, int ciphertexts);
 /* The blind-rotation variant and key-switch tile a batch of `gates` gates
  * would launch with now. */

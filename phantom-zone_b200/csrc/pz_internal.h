@@ -30,7 +30,7 @@ struct pz_ctx {
   int grid_limit = 0;
   int pbs_variant = 0;  // blind-rotation launch shape (see pz::PBS_VARIANTS)
   int split_below = -1;  // batches of at most this many gates use the two-CTA kernel (-1: half the SMs)
-  int ks_ct = 16;        // key-switch ciphertexts per CTA (8, 16, 32)
+  int ks_ct = 64;        // key-switch tile: 8, 16, 32 ciphertexts per CTA, 64 = tensor cores (default)
   // autotuned launch shapes per batch-size bucket floor(log2(gates)); a
   // bucket the autotuner has not seen uses the defaults above
   struct Tuned {

@@ -128,7 +128,15 @@ constexpr bool NTTB_PF = false;
 #else
 constexpr bool NTTB_PF = true;
 #endif
-constexpr size_t NTTB_SMEM = (size_t)6 * NTTB_N * 8 + 16;  // exchange 2N | 2 stages of 2N | 2 mbarriers
+// PZ_NTTB_3CTA (a comparison): one stage instead of two (the next pair's copy
+// is issued once the current pair sits in registers), 64 KB of shared
+// memory, three CTAs per SM at 80 registers instead of two at 128.
+#ifdef PZ_NTTB_3CTA
+constexpr int NTTB_STAGES = 1, NTTB_MINB = 3;
+#else
+constexpr int NTTB_STAGES = 2, NTTB_MINB = 2;
+#endif
+constexpr size_t NTTB_SMEM = (size_t)(2 + 2 * NTTB_STAGES) * NTTB_N * 8 + 16;  // exchange 2N | stages of 2N | mbarriers
 
 // Last inverse round (k = 0) with N^{-1} folded into its final stage; values
 // leave in [0, 4Q).
@@ -183,10 +191,10 @@ __device__ __forceinline__ void lds2(const u64 *p, u64 &a, u64 &b) {
 }
 
 template <bool INV>
-__global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t count, RingConsts rc, u32 *err) {
+__global__ void __launch_bounds__(256, NTTB_MINB) ntt_batch_kernel(u64 *polys, size_t count, RingConsts rc, u32 *err) {
   constexpr int N = NTTB_N, LOGN = 11;
   extern __shared__ __align__(128) u64 smem[];
-  u64 *xs = smem, *stage = smem + 2 * N, *bar = smem + 6 * N;
+  u64 *xs = smem, *stage = smem + 2 * N, *bar = smem + (2 + 2 * NTTB_STAGES) * N;
   const int j = threadIdx.x;
   const size_t pairs = (count + 1) / 2;
   auto issue = [&](size_t p, int b) {  // one thread: pair p -> stage b
@@ -197,21 +205,22 @@ __global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t co
   };
   if (j == 0) {
     mbar_init(bar, 1);
-    mbar_init(bar + 1, 1);
+    if (NTTB_STAGES == 2) mbar_init(bar + 1, 1);
     mbar_init_fence();
   }
   __syncthreads();
   size_t p = blockIdx.x;
   if (j == 0 && p < pairs) issue(p, 0);
   for (u32 it = 0; p < pairs; it++, p += gridDim.x) {
-    const int b = it & 1;
+    const int b = NTTB_STAGES == 2 ? (it & 1) : 0;
     const bool more = p + gridDim.x < pairs;
-    // stage b^1 was read in the previous iteration, before that transform's barriers
-    if (j == 0 && more) issue(p + gridDim.x, b ^ 1);
-    if (!__syncthreads_and(mbar_wait(bar + b, (it >> 1) & 1))) {
+    // (two stages) stage b^1 was read in the previous iteration, before that transform's barriers
+    if (NTTB_STAGES == 2 && j == 0 && more) issue(p + gridDim.x, b ^ 1);
+    const u32 parity = NTTB_STAGES == 2 ? (it >> 1) & 1 : it & 1;
+    if (!__syncthreads_and(mbar_wait(bar + b, parity))) {
       if (j == 0) {
         atomicOr(err, DEVERR_MBAR_TIMEOUT);
-        if (more) mbar_wait(bar + (b ^ 1), ((it + 1) >> 1) & 1);  // bounded: the copy issued above
+        if (NTTB_STAGES == 2 && more) mbar_wait(bar + (b ^ 1), ((it + 1) >> 1) & 1);  // bounded: the copy issued above
       }
       return;
     }
@@ -224,6 +233,10 @@ __global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t co
       for (int r = 0; r < 8; r++) {
         x[r] = sx[pos_coef<LOGN>(j, r)];
         y[r] = sy[pos_coef<LOGN>(j, r)];
+      }
+      if (NTTB_STAGES == 1) {  // the stage is in registers: the next pair's copy may start
+        __syncthreads();
+        if (j == 0 && more) issue(p + gridDim.x, 0);
       }
       ntt_fwd<LOGN, true, NTTB_PF>(x, y, xs, rc);
 #pragma unroll
@@ -244,6 +257,10 @@ __global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t co
         lds2(sx + o + 2, x[4 * h + 2], x[4 * h + 3]);
         lds2(sy + o, y[4 * h], y[4 * h + 1]);
         lds2(sy + o + 2, y[4 * h + 2], y[4 * h + 3]);
+      }
+      if (NTTB_STAGES == 1) {
+        __syncthreads();
+        if (j == 0 && more) issue(p + gridDim.x, 0);
       }
       ntt_inv_scaled<true>(x, y, xs, rc);
 #pragma unroll
@@ -478,6 +495,8 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
   extern __shared__ u64 smem[];
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    if (threadIdx.x == 0 && c + gridDim.x < count)  // the CTA's next ciphertext, into L2
+      prefetch_l2(rlwe + (c + gridDim.x) * 2 * N, 2 * (u32)N * 8);
     if (idx[c] >= P.n) continue;  // out-of-range key index: the ciphertext is left unchanged
     if (threadIdx.x == 0)  // the key rows, into L2 while the digits are transformed
       prefetch_l2(P.rgsw + (size_t)idx[c] * P.rgsw_rows * N, P.rgsw_rows * (u32)N * 8);
@@ -505,6 +524,8 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
   extern __shared__ u64 smem[];
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
+    if (threadIdx.x == 0 && c + gridDim.x < count)  // the CTA's next ciphertext, into L2
+      prefetch_l2(rlwe + (c + gridDim.x) * 2 * N, 2 * (u32)N * 8);
     if (slot[c] > P.w) continue;  // out-of-range key slot: the ciphertext is left unchanged
     if (threadIdx.x == 0) prefetch_l2(P.autos + (size_t)slot[c] * P.auto_rows * N, P.auto_rows * (u32)N * 8);
     u64 *p = rlwe + c * 2 * N;
@@ -706,7 +727,7 @@ __global__ void __launch_bounds__(256, 2)
   const int mf = warp & 3, nh = warp >> 2;
   const int ct0 = blockIdx.x * KSM_ROWS, cb = blockIdx.y;
   const size_t L = (size_t)P.N + 1;
-  const u32 kblocks = d * P.N / 32, kb_total = kblocks;
+  const u32 kblocks = d * P.N / 32;
   const size_t plane_bytes = (size_t)kblocks * P.ksk8_cols * 32;
   const unsigned char *Bg = P.ksk8 + (size_t)cb * KSM_COLS * 32;
   constexpr int STAGE = NP * KSM_COLS * 32, CHUNKS16 = NP * KSM_COLS * 2;  // 16-byte pieces per stage
@@ -724,9 +745,14 @@ __global__ void __launch_bounds__(256, 2)
   for (int f = 0; f < 14; f++)
 #pragma unroll
     for (int i = 0; i < 4; i++) acc[f][i] = 0;
-  issue(0);
-  u32 kb = 0;
-  for (u32 i0 = 0; i0 < P.N; i0 += 32) {
+  // this CTA's share of the 32-coefficient chunks (grid.z shares for small batches)
+  const u32 chunks = P.N / 32, per = (chunks + gridDim.z - 1) / gridDim.z;
+  const u32 c_begin = blockIdx.z * per, c_end = min(chunks, c_begin + per);
+  if (c_begin >= c_end) return;  // uniform per CTA
+  u32 kb = c_begin * d;
+  const u32 kb_end = c_end * d;
+  issue(kb);
+  for (u32 i0 = c_begin * 32; i0 < c_end * 32; i0 += 32) {
     __syncthreads();  // every warp is done with the previous chunk's digits
     for (int e = tid; e < KSM_ROWS * 32; e += 256) {
       const int row = e >> 5, cc = e & 31, ct = ct0 + row;
@@ -744,7 +770,7 @@ __global__ void __launch_bounds__(256, 2)
     for (u32 ks = 0; ks < d; ks++, kb++) {
       cp_async_wait_all();
       __syncthreads();  // stage kb landed for every thread; stage kb + 1 is free; digits written
-      if (kb + 1 < kb_total) issue(kb + 1);
+      if (kb + 1 < kb_end) issue(kb + 1);
       const unsigned char *ar = A + (size_t)(16 * mf + g) * astride + ks * 32 + 4 * t;
       const u32 a0 = *(const u32 *)ar, a1 = *(const u32 *)(ar + 8 * astride);
       const u32 a2 = *(const u32 *)(ar + 16), a3 = *(const u32 *)(ar + 8 * astride + 16);
@@ -777,10 +803,12 @@ __global__ void __launch_bounds__(256, 2)
       const u32 col = (u32)cb * KSM_COLS + nh * 112 + 8 * f + 2 * t + (i & 1);
       if (ct < count && col <= P.n) {
         u32 v = acc[f][i];
-        if (col == 0)
+        if (col == 0 && blockIdx.z == 0)
           v += (u32)prelude_moddown(operand(c0, P.in0, ct, 0, L, P.Q), operand(c1, P.in1, ct, 0, L, P.Q),
                                     gates ? gates[ct] : 0, true, P);
-        out[(size_t)ct * P.out_stride + col] = v & P.mask;
+        u32 *o = out + (size_t)ct * P.out_stride + col;
+        if (gridDim.z == 1) *o = v & P.mask;
+        else atomicAdd(o, v);  // exact mod 2^32; the consumer reduces mod q_ks
       }
     }
   }
@@ -1692,12 +1720,12 @@ cudaError_t launch_key_convert(int logn, const u64 *in, u64 *out, size_t npolys,
 template <typename K>
 static cudaError_t set_smem(K kernel, size_t bytes);
 
-// Persistent grid of the batched NTT: two CTAs per SM, no more CTAs than pairs.
+// Persistent grid of the batched NTT: NTTB_MINB CTAs per SM, no more CTAs than pairs.
 static int ntt_batch_grid(size_t count) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t pairs = (count + 1) / 2;
-  return (int)std::min<size_t>(pairs, (size_t)2 * sms);
+  return (int)std::min<size_t>(pairs, (size_t)NTTB_MINB * sms);
 }
 
 cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s) {
@@ -1745,6 +1773,16 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
   if (e == cudaSuccess) have = bytes;
   return e;
 }
+// Persistent grid for the per-ciphertext operation kernels: MB resident CTAs
+// per SM, each walking its ciphertexts with the next one prefetched into L2.
+// (MB = 1: the unconstrained forms, whose residency the registers and shared
+// memory set -- up to 16 CTAs per SM.)
+static int op_grid(size_t count, int mb) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (int)std::min<size_t>(count, (size_t)sms * (mb > 1 ? mb : 16));
+}
+
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
                                size_t count, int trivial, cudaStream_t s, int variant) {
   if (count == 0) return cudaSuccess;
@@ -1752,7 +1790,7 @@ cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, 
   cudaError_t e;
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                                  \
   if ((e = set_smem(ext_product_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;              \
-  ext_product_kernel<LN, DD, MB><<<grid_for(count), TH, smem, s>>>(P, rlwe, idx, count, trivial);
+  ext_product_kernel<LN, DD, MB><<<op_grid(count, MB), TH, smem, s>>>(P, rlwe, idx, count, trivial);
   if (logn == 11 && d1) {
     if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
     else if (variant == 2) { PZ_LAUNCH(11, true, 4, 256) }
@@ -1773,7 +1811,7 @@ cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u
   cudaError_t e;
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                           \
   if ((e = set_smem(auto_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;              \
-  auto_kernel<LN, DD, MB><<<grid_for(count), TH, smem, s>>>(P, rlwe, slot, count, trivial);
+  auto_kernel<LN, DD, MB><<<op_grid(count, MB), TH, smem, s>>>(P, rlwe, slot, count, trivial);
   if (logn == 11 && d1) {
     if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
     else if (variant == 2) { PZ_LAUNCH(11, true, 4, 256) }
@@ -1812,15 +1850,24 @@ cudaError_t launch_ks(const KsParams &P, const unsigned char *gates, const u64 *
   if (ct == KS_CT_MMA && (!P.ksk8 || P.planes < 1 || P.planes > 3 || P.d > 16 || (P.d * P.N) % 32 || P.N % 32))
     ct = 16;
   if (ct == KS_CT_MMA) {
-    const dim3 grid((unsigned)((count + KSM_ROWS - 1) / KSM_ROWS), P.ksk8_cols / KSM_COLS);
+    dim3 grid((unsigned)((count + KSM_ROWS - 1) / KSM_ROWS), P.ksk8_cols / KSM_COLS);
+    grid.z = ks_split((size_t)grid.x * grid.y, P.N);
     const size_t smem = ksm_smem_bytes(P.d, P.planes);
     cudaError_t e;
+    if (grid.z > 1 && (e = cudaMemsetAsync(out, 0, count * P.out_stride * sizeof(u32), s)) != cudaSuccess) return e;
 #define PZ_KSM(NP)                                                              if ((e = set_smem(ks_mma_kernel<NP>, smem)) != cudaSuccess) return e;         ks_mma_kernel<NP><<<grid, 256, smem, s>>>(P, gates, c0, c1, (int)count, out);
     if (P.planes == 1) { PZ_KSM(1) }
     else if (P.planes == 2) { PZ_KSM(2) }
     else { PZ_KSM(3) }
 #undef PZ_KSM
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (grid.z > 1 && reduce_output) {
+      const size_t words = count * (P.n + 1);
+      ks_mask_kernel<<<(unsigned)std::min<size_t>((words + 255) / 256, 4096), 256, 0, s>>>(out, count, P.out_stride,
+                                                                                          P.n + 1, P.mask);
+      return cudaGetLastError();
+    }
+    return cudaSuccess;
   }
   if (ct != 8 && ct != 16 && ct != 32) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((count + ct - 1) / ct), (unsigned)((P.n + 1 + KS_COLS - 1) / KS_COLS));

@@ -158,7 +158,10 @@ def test_lwe_key_switch_every_tile(gpu_available, param, tile):
     r = rng(0x42 + tile)
     try:
         eng.set_ks_tile(tile)
-        for count in (tile + 5, 4 * 148 * tile // 8 + 3):
+        # the second count leaves one share per tile (grid.z = 1): 4 x 148 CTAs of
+        # 128 threads for the IMAD tiles, 4 x 148 / 3 row tiles of 64 for the tensor cores
+        big = 4 * 148 * tile // 8 + 3 if tile < 64 else 64 * (4 * 148 // 3 + 1) + 3
+        for count in (tile + 5, big):
             x = r.uniform_mod(qk + 1, count * ev.L).reshape(count, ev.L)
             x[0, :] = qk
             idx = np.concatenate([np.arange(min(count, 24)), count - 1 - np.arange(8)])
@@ -169,7 +172,7 @@ def test_lwe_key_switch_every_tile(gpu_available, param, tile):
             assert np.array_equal(got[idx], want), (tile, count)
             assert eng.launch_shape(count)["ks_tile"] == tile
     finally:
-        eng.set_ks_tile(16)
+        eng.set_ks_tile(64)
 
 
 def _gate_inputs(ev, secrets, count, tag):
@@ -233,7 +236,7 @@ def test_gate_batch_tensor_core_key_switch(gpu_available, param):
         eng.set_ks_tile(64)
         eng.gate_batch_device(dkey, to_dev(gates), to_dev(c0), to_dev(c1), out, ks_out=ks)
     finally:
-        eng.set_ks_tile(16)
+        eng.set_ks_tile(64)
     got_out, got_ks = to_host(out), to_host(ks, np.uint32)
     for i in list(range(4)) + list(range(63, 70)):
         g = names[i % 6]
@@ -296,14 +299,14 @@ def test_ctx_autotune_keeps_results(gpu_available):
     try:
         t = eng.autotune(dkey, 296)
         assert t["variant"] in (0, 1, 2, 3, 4) and t["ms"] > 0 and eng.pbs_variant == t["variant"]
-        assert t["ks_tile"] in (8, 16, 32)
+        assert t["ks_tile"] in (8, 16, 32, 64)
         assert eng.launch_shape(296) == {"variant": t["variant"], "ks_tile": t["ks_tile"]}
         bits0, bits1, c0, c1 = _gate_inputs(ev, secrets, 4, 0x7F)
         gates = np.array([O.GATES[g] for g in ["and", "nand", "xor", "nor"]], np.uint8)
         assert np.array_equal(eng.gate_batch(dkey, gates, c0, c1), okey.gate_batch(gates, c0, c1, threads=4))
     finally:
         eng.pbs_variant = old
-        eng.set_ks_tile(16)
+        eng.set_ks_tile(64)
 
 
 def test_split_kernel_many_items_per_cluster(gpu_available):
