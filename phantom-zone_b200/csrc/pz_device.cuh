@@ -314,8 +314,9 @@ __device__ __forceinline__ u64 reduce_n2048(u64 v) {
 // an IMAD.WIDE, 2.5-2.65 times an IMAD each -- moves off the busy pipe:
 // v -> vr = reduce_n2048(v) < 2^54 + 2^27, qi = rint(f64(vr) * (w/Q)) within
 // 6.51 of vr w / Q (three roundings of 2^-53 each on a value below 2^54),
-// and raw = w vr - qi Q (mod 2^64) lies in (-6.51 Q, 6.51 Q).  The integer
-// work left is the low words of w vr and qi Q (two IMAD.WIDE, three IMAD).
+// and raw = w vr - qi Q (mod 2^64) lies in (-6.51 Q, 6.51 Q) (returned with
+// 7 Q added, see fp_raw).  The integer work left is the low words of w vr and
+// qi Q (two IMAD.WIDE, three IMAD).
 #ifdef PZ_BFLY_SHOUP
 constexpr bool BFLY_FP64 = false;
 #else
@@ -327,13 +328,16 @@ constexpr bool BFLY_FP64 = true;
 // instructions cost more issue slots than the conversion unit's quarter
 // rate does.)
 constexpr u64 FP_OFF = 7;  // raw + 7 Q in (0.49 Q, 13.51 Q)
+// fp_raw returns raw + FP_OFF Q: the offset rides on the quotient as
+// qi = rint(f64(vr) (w/Q) - FP_OFF) (one FMA, signed: qi may be negative),
+// so w vr - qi Q mod 2^64 is already in (0.49 Q, 13.51 Q).
 __device__ __forceinline__ u64 fp_raw(u64 v, u64 w, u64 wq_bits) {
   const u64 vr = reduce_n2048(v);
   u64 qi, r;
   double vd;
   asm("cvt.rn.f64.u64 %0, %1;" : "=d"(vd) : "l"(vr));
-  const double qd = __dmul_rn(vd, __longlong_as_double((long long)wq_bits));
-  asm("cvt.rni.u64.f64 %0, %1;" : "=l"(qi) : "d"(qd));
+  const double qd = __fma_rn(vd, __longlong_as_double((long long)wq_bits), -(double)FP_OFF);
+  asm("cvt.rni.s64.f64 %0, %1;" : "=l"(qi) : "d"(qd));
   asm("{\n\t"
       ".reg .u32 v0, v1, w0, w1, q0, q1, t0, t1, z;\n\t"
       ".reg .u64 wy, t;\n\t"
@@ -390,9 +394,9 @@ __device__ __forceinline__ void add_sub_ptx(u64 x, u64 t, u64 c, u64 &sum, u64 &
 template <bool SPQ>
 __device__ __forceinline__ void fbf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
   if (SPQ && BFLY_FP64) {  // outputs grow by < 13.51 Q per stage (< 150 Q after 11)
-    const u64 raw = fp_raw(y, w, ws), xc = x + FP_OFF * Q_N2048;
-    x = xc + raw;
-    y = xc - raw;
+    const u64 r7 = fp_raw(y, w, ws);  // w y + 7 Q (mod Q), in (0.49 Q, 13.51 Q)
+    y = x + 2 * FP_OFF * Q_N2048 - r7;
+    x = x + r7;
   } else if (SPQ) {
     const u64 t = shoup_spq(y, w, ws);
 #ifdef PZ_BFLY_ADD_PTX
@@ -492,7 +496,7 @@ __device__ __forceinline__ void ibf(u64 &x, u64 &y, u64 w, u64 ws, u64 q) {
     const u64 t = x + (u64)K * Q_N2048 - y;
     const u64 u = x + y;
 #endif
-    y = BFLY_FP64 ? fp_raw(t, w, ws) + FP_OFF * Q_N2048 : shoup_spq(t, w, ws);
+    y = BFLY_FP64 ? fp_raw(t, w, ws) : shoup_spq(t, w, ws);
     x = u;
   } else {
     const u64 q2 = q << 1;

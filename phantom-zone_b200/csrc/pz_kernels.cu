@@ -128,15 +128,7 @@ constexpr bool NTTB_PF = false;
 #else
 constexpr bool NTTB_PF = true;
 #endif
-// PZ_NTTB_3CTA (a comparison): one stage instead of two (the next pair's copy
-// is issued once the current pair sits in registers), 64 KB of shared
-// memory, three CTAs per SM at 80 registers instead of two at 128.
-#ifdef PZ_NTTB_3CTA
-constexpr int NTTB_STAGES = 1, NTTB_MINB = 3;
-#else
-constexpr int NTTB_STAGES = 2, NTTB_MINB = 2;
-#endif
-constexpr size_t NTTB_SMEM = (size_t)(2 + 2 * NTTB_STAGES) * NTTB_N * 8 + 16;  // exchange 2N | stages of 2N | mbarriers
+constexpr size_t NTTB_SMEM = (size_t)6 * NTTB_N * 8 + 16;  // exchange 2N | 2 stages of 2N | 2 mbarriers
 
 // Last inverse round (k = 0) with N^{-1} folded into its final stage; values
 // leave in [0, 4Q).
@@ -191,10 +183,10 @@ __device__ __forceinline__ void lds2(const u64 *p, u64 &a, u64 &b) {
 }
 
 template <bool INV>
-__global__ void __launch_bounds__(256, NTTB_MINB) ntt_batch_kernel(u64 *polys, size_t count, RingConsts rc, u32 *err) {
+__global__ void __launch_bounds__(256, 2) ntt_batch_kernel(u64 *polys, size_t count, RingConsts rc, u32 *err) {
   constexpr int N = NTTB_N, LOGN = 11;
   extern __shared__ __align__(128) u64 smem[];
-  u64 *xs = smem, *stage = smem + 2 * N, *bar = smem + (2 + 2 * NTTB_STAGES) * N;
+  u64 *xs = smem, *stage = smem + 2 * N, *bar = smem + 6 * N;
   const int j = threadIdx.x;
   const size_t pairs = (count + 1) / 2;
   auto issue = [&](size_t p, int b) {  // one thread: pair p -> stage b
@@ -205,22 +197,21 @@ __global__ void __launch_bounds__(256, NTTB_MINB) ntt_batch_kernel(u64 *polys, s
   };
   if (j == 0) {
     mbar_init(bar, 1);
-    if (NTTB_STAGES == 2) mbar_init(bar + 1, 1);
+    mbar_init(bar + 1, 1);
     mbar_init_fence();
   }
   __syncthreads();
   size_t p = blockIdx.x;
   if (j == 0 && p < pairs) issue(p, 0);
   for (u32 it = 0; p < pairs; it++, p += gridDim.x) {
-    const int b = NTTB_STAGES == 2 ? (it & 1) : 0;
+    const int b = it & 1;
     const bool more = p + gridDim.x < pairs;
-    // (two stages) stage b^1 was read in the previous iteration, before that transform's barriers
-    if (NTTB_STAGES == 2 && j == 0 && more) issue(p + gridDim.x, b ^ 1);
-    const u32 parity = NTTB_STAGES == 2 ? (it >> 1) & 1 : it & 1;
-    if (!__syncthreads_and(mbar_wait(bar + b, parity))) {
+    // stage b^1 was read in the previous iteration, before that transform's barriers
+    if (j == 0 && more) issue(p + gridDim.x, b ^ 1);
+    if (!__syncthreads_and(mbar_wait(bar + b, (it >> 1) & 1))) {
       if (j == 0) {
         atomicOr(err, DEVERR_MBAR_TIMEOUT);
-        if (NTTB_STAGES == 2 && more) mbar_wait(bar + (b ^ 1), ((it + 1) >> 1) & 1);  // bounded: the copy issued above
+        if (more) mbar_wait(bar + (b ^ 1), ((it + 1) >> 1) & 1);  // bounded: the copy issued above
       }
       return;
     }
@@ -233,10 +224,6 @@ __global__ void __launch_bounds__(256, NTTB_MINB) ntt_batch_kernel(u64 *polys, s
       for (int r = 0; r < 8; r++) {
         x[r] = sx[pos_coef<LOGN>(j, r)];
         y[r] = sy[pos_coef<LOGN>(j, r)];
-      }
-      if (NTTB_STAGES == 1) {  // the stage is in registers: the next pair's copy may start
-        __syncthreads();
-        if (j == 0 && more) issue(p + gridDim.x, 0);
       }
       ntt_fwd<LOGN, true, NTTB_PF>(x, y, xs, rc);
 #pragma unroll
@@ -257,10 +244,6 @@ __global__ void __launch_bounds__(256, NTTB_MINB) ntt_batch_kernel(u64 *polys, s
         lds2(sx + o + 2, x[4 * h + 2], x[4 * h + 3]);
         lds2(sy + o, y[4 * h], y[4 * h + 1]);
         lds2(sy + o + 2, y[4 * h + 2], y[4 * h + 3]);
-      }
-      if (NTTB_STAGES == 1) {
-        __syncthreads();
-        if (j == 0 && more) issue(p + gridDim.x, 0);
       }
       ntt_inv_scaled<true>(x, y, xs, rc);
 #pragma unroll
@@ -495,8 +478,6 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
   extern __shared__ u64 smem[];
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
-    if (threadIdx.x == 0 && c + gridDim.x < count)  // the CTA's next ciphertext, into L2
-      prefetch_l2(rlwe + (c + gridDim.x) * 2 * N, 2 * (u32)N * 8);
     if (idx[c] >= P.n) continue;  // out-of-range key index: the ciphertext is left unchanged
     if (threadIdx.x == 0)  // the key rows, into L2 while the digits are transformed
       prefetch_l2(P.rgsw + (size_t)idx[c] * P.rgsw_rows * N, P.rgsw_rows * (u32)N * 8);
@@ -524,8 +505,6 @@ __global__ void __launch_bounds__(NttShape<LOGN>::T, MINB)
   extern __shared__ u64 smem[];
   const int j = threadIdx.x;
   for (size_t c = blockIdx.x; c < count; c += gridDim.x) {
-    if (threadIdx.x == 0 && c + gridDim.x < count)  // the CTA's next ciphertext, into L2
-      prefetch_l2(rlwe + (c + gridDim.x) * 2 * N, 2 * (u32)N * 8);
     if (slot[c] > P.w) continue;  // out-of-range key slot: the ciphertext is left unchanged
     if (threadIdx.x == 0) prefetch_l2(P.autos + (size_t)slot[c] * P.auto_rows * N, P.auto_rows * (u32)N * 8);
     u64 *p = rlwe + c * 2 * N;
@@ -1720,12 +1699,12 @@ cudaError_t launch_key_convert(int logn, const u64 *in, u64 *out, size_t npolys,
 template <typename K>
 static cudaError_t set_smem(K kernel, size_t bytes);
 
-// Persistent grid of the batched NTT: NTTB_MINB CTAs per SM, no more CTAs than pairs.
+// Persistent grid of the batched NTT: two CTAs per SM, no more CTAs than pairs.
 static int ntt_batch_grid(size_t count) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t pairs = (count + 1) / 2;
-  return (int)std::min<size_t>(pairs, (size_t)NTTB_MINB * sms);
+  return (int)std::min<size_t>(pairs, (size_t)2 * sms);
 }
 
 cudaError_t launch_ntt_fwd(int logn, u64 *polys, size_t count, const RingConsts &rc, u32 *err, cudaStream_t s) {
@@ -1773,16 +1752,6 @@ static cudaError_t set_smem(K kernel, size_t bytes) {
   if (e == cudaSuccess) have = bytes;
   return e;
 }
-// Persistent grid for the per-ciphertext operation kernels: MB resident CTAs
-// per SM, each walking its ciphertexts with the next one prefetched into L2.
-// (MB = 1: the unconstrained forms, whose residency the registers and shared
-// memory set -- up to 16 CTAs per SM.)
-static int op_grid(size_t count, int mb) {
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (int)std::min<size_t>(count, (size_t)sms * (mb > 1 ? mb : 16));
-}
-
 cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, const u32 *idx,
                                size_t count, int trivial, cudaStream_t s, int variant) {
   if (count == 0) return cudaSuccess;
@@ -1790,7 +1759,7 @@ cudaError_t launch_ext_product(int logn, bool d1, const BrParams &P, u64 *rlwe, 
   cudaError_t e;
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                                  \
   if ((e = set_smem(ext_product_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;              \
-  ext_product_kernel<LN, DD, MB><<<op_grid(count, MB), TH, smem, s>>>(P, rlwe, idx, count, trivial);
+  ext_product_kernel<LN, DD, MB><<<grid_for(count), TH, smem, s>>>(P, rlwe, idx, count, trivial);
   if (logn == 11 && d1) {
     if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
     else if (variant == 2) { PZ_LAUNCH(11, true, 4, 256) }
@@ -1811,7 +1780,7 @@ cudaError_t launch_auto(int logn, bool d1, const BrParams &P, u64 *rlwe, const u
   cudaError_t e;
 #define PZ_LAUNCH(LN, DD, MB, TH)                                                           \
   if ((e = set_smem(auto_kernel<LN, DD, MB>, smem)) != cudaSuccess) return e;              \
-  auto_kernel<LN, DD, MB><<<op_grid(count, MB), TH, smem, s>>>(P, rlwe, slot, count, trivial);
+  auto_kernel<LN, DD, MB><<<grid_for(count), TH, smem, s>>>(P, rlwe, slot, count, trivial);
   if (logn == 11 && d1) {
     if (variant == 0) { PZ_LAUNCH(11, true, 2, 256) }
     else if (variant == 2) { PZ_LAUNCH(11, true, 4, 256) }
