@@ -694,25 +694,28 @@ constexpr size_t ksm_smem_bytes(u32 d, u32 planes) {
   return (size_t)KSM_ROWS * ksm_astride(d) + 2 * (size_t)planes * KSM_COLS * 32;
 }
 
+// One CTA's tile: ciphertexts [ct0, min(ct0 + KSM_ROWS, count)), output
+// column block cb, this CTA's share (blockIdx.z of gridDim.z) of the input
+// coefficients.  NP bounds the planes (P.planes <= NP, checked per plane).
 template <int NP>
-__global__ void __launch_bounds__(256, 2)
-    ks_mma_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
-  extern __shared__ __align__(16) unsigned char ksm[];
-  const u32 d = P.d, astride = (u32)ksm_astride(d);
+__device__ __forceinline__ void ks_mma_tile(const KsParams &P, const unsigned char *gates, const u64 *c0,
+                                            const u64 *c1, int ct0, int count, u32 *out, int cb,
+                                            unsigned char *ksm) {
+  const u32 d = P.d, astride = (u32)ksm_astride(d), planes = P.planes;
   unsigned char *A = ksm;
   unsigned char *Bs = ksm + (size_t)KSM_ROWS * astride;  // [2][NP][KSM_COLS][32]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int mf = warp & 3, nh = warp >> 2;
-  const int ct0 = blockIdx.x * KSM_ROWS, cb = blockIdx.y;
   const size_t L = (size_t)P.N + 1;
   const u32 kblocks = d * P.N / 32;
   const size_t plane_bytes = (size_t)kblocks * P.ksk8_cols * 32;
   const unsigned char *Bg = P.ksk8 + (size_t)cb * KSM_COLS * 32;
-  constexpr int STAGE = NP * KSM_COLS * 32, CHUNKS16 = NP * KSM_COLS * 2;  // 16-byte pieces per stage
+  constexpr int STAGE = NP * KSM_COLS * 32;
+  const int chunks16 = (int)planes * KSM_COLS * 2;  // 16-byte pieces per stage
   auto issue = [&](u32 kb) {
     unsigned char *dst = Bs + (size_t)(kb & 1) * STAGE;
-    for (int e = tid; e < CHUNKS16; e += 256) {
+    for (int e = tid; e < chunks16; e += 256) {
       const int p = e / (KSM_COLS * 2), r = e % (KSM_COLS * 2);
       cp_async16(dst + (size_t)p * KSM_COLS * 32 + r * 16,
                  Bg + p * plane_bytes + (size_t)kb * P.ksk8_cols * 32 + r * 16);
@@ -759,8 +762,12 @@ __global__ void __launch_bounds__(256, 2)
         u32 r[NP][4];
 #pragma unroll
         for (int p = 0; p < NP; p++) {
-          const uint2 b = *(const uint2 *)(bs + (size_t)p * KSM_COLS * 32 + f * 8 * 32);
-          mma_s8u8(r[p], a0, a1, a2, a3, b.x, b.y);
+          if (p < (int)planes) {
+            const uint2 b = *(const uint2 *)(bs + (size_t)p * KSM_COLS * 32 + f * 8 * 32);
+            mma_s8u8(r[p], a0, a1, a2, a3, b.x, b.y);
+          } else {
+            r[p][0] = r[p][1] = r[p][2] = r[p][3] = 0;
+          }
         }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -791,6 +798,34 @@ __global__ void __launch_bounds__(256, 2)
       }
     }
   }
+}
+
+template <int NP>
+__global__ void __launch_bounds__(256, 2)
+    ks_mma_kernel(KsParams P, const unsigned char *gates, const u64 *c0, const u64 *c1, int count, u32 *out) {
+  extern __shared__ __align__(16) unsigned char ksm[];
+  ks_mma_tile<NP>(P, gates, c0, c1, blockIdx.x * KSM_ROWS, count, out, blockIdx.y, ksm);
+}
+
+// Ragged batch on the tensor cores: tile blockIdx.x holds up to KSM_ROWS
+// consecutive items of one session (descriptor), whose KSK planes it streams;
+// operands are gathered from `wires` through in0/in1 (bit 31 = not()).
+__global__ void __launch_bounds__(256, 2)
+    ks_mma_ragged_kernel(const KsParams *descs, const KsTile *tiles, const unsigned char *gates, const u64 *wires,
+                         const u32 *in0, const u32 *in1, u32 *out, u32 out_stride) {
+  extern __shared__ __align__(16) unsigned char ksm[];
+  __shared__ KsParams sp;
+  const KsTile t = tiles[blockIdx.x];
+  if (threadIdx.x == 0) {
+    sp = descs[t.desc];
+    sp.in0 = in0;
+    sp.in1 = in1;
+    sp.out_stride = out_stride;
+    sp.raw = 0;
+  }
+  __syncthreads();
+  if (blockIdx.y * KSM_COLS > sp.n) return;  // no columns of this session here (uniform per CTA)
+  ks_mma_tile<3>(sp, gates, wires, wires, (int)t.first, (int)(t.first + t.count), out, blockIdx.y, ksm);
 }
 
 // KSK u32 rows -> byte planes in the fragment order of ks_mma_kernel: row r
@@ -1951,6 +1986,21 @@ cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, siz
   cudaError_t e;
   if (grid.z > 1 && (e = cudaMemsetAsync(out, 0, count * out_stride * sizeof(u32), s)) != cudaSuccess) return e;
   ks_ragged_kernel<<<grid, KS_COLS, 0, s>>>(d_descs, d_tiles, gates, wires, in0, in1, out, out_stride);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ks_mma_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,
+                                 u32 max_n, u32 max_N, u32 max_d, const unsigned char *gates, const u64 *wires,
+                                 const u32 *in0, const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s) {
+  if (ntiles == 0) return cudaSuccess;
+  if (max_d > 16) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)ntiles, ksk8_cols(max_n) / KSM_COLS);
+  grid.z = ks_split((size_t)grid.x * grid.y, max_N);
+  const size_t smem = ksm_smem_bytes(max_d, 3);
+  cudaError_t e;
+  if (grid.z > 1 && (e = cudaMemsetAsync(out, 0, count * out_stride * sizeof(u32), s)) != cudaSuccess) return e;
+  if ((e = set_smem(ks_mma_ragged_kernel, smem)) != cudaSuccess) return e;
+  ks_mma_ragged_kernel<<<grid, 256, smem, s>>>(d_descs, d_tiles, gates, wires, in0, in1, out, out_stride);
   return cudaGetLastError();
 }
 

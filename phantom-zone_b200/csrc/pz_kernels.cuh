@@ -112,6 +112,11 @@ constexpr int PBS_MAX_VARIANT = PBS_BULK;
 cudaError_t launch_ks_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,
                              u32 max_n, u32 max_N, u32 max_d, const unsigned char *gates, const u64 *wires,
                              const u32 *in0, const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s);
+// The ragged key switch on the tensor cores: tiles of up to KSM_ROWS items,
+// every session's key with its byte planes (KsParams::ksk8), d <= 16.
+cudaError_t launch_ks_mma_ragged(const KsParams *d_descs, const KsTile *d_tiles, size_t ntiles, size_t count,
+                                 u32 max_n, u32 max_N, u32 max_d, const unsigned char *gates, const u64 *wires,
+                                 const u32 *in0, const u32 *in1, u32 *out, u32 out_stride, cudaStream_t s);
 cudaError_t launch_pbs_ragged(int logn, bool d1, const BrParams *d_descs, const u32 *item_desc, u32 max_br_q,
                               u32 max_n, const u32 *ks, u32 ks_stride, const unsigned char *gates, u64 *out,
                               const u32 *out_idx, size_t count, int grid_limit, cudaStream_t s, int variant);

@@ -71,6 +71,7 @@ struct pz_server {
   size_t key_budget = SIZE_MAX, managed_bytes = 0;
   u64 use_clock = 0, key_imports = 0, key_evictions = 0;
   bool descs_dirty = false;
+  bool ks_mma = false;  // every session with a resident key has its KSK byte planes: tensor-core key switch
   int logn = -1;
   bool d1 = true;
   size_t L = 0;
@@ -231,8 +232,13 @@ pz_status upload_descs(pz_server *s) {
     br[i].autos = se.key ? se.key->d_autos : nullptr;
     br[i].out_idx = nullptr;
     ks[i] = se.ctx->ks;
-    ks[i].ksk = se.key ? se.key->d_ksk : nullptr;
+    ks[i].ksk = nullptr;
+    if (se.key) pz::ks_bind_key(se.ctx, se.key, ks[i]);
   }
+  bool mma = s->max_d <= 16;
+  for (size_t i = 0; i < s->sessions.size(); i++)
+    if (s->sessions[i].key && !s->sessions[i].key->d_ksk8) mma = false;
+  s->ks_mma = mma;
   s->descs_dirty = false;
   cudaFree(s->d_br);
   cudaFree(s->d_ksp);
@@ -433,6 +439,7 @@ pz_status run_items(pz_server *s, const std::vector<Item> &items) {
     u32 *hd = (u32 *)(h + lay.desc);
     pz::KsTile *ht = (pz::KsTile *)(h + lay.tiles);
     size_t ntiles = 0;
+    const u32 tile_cap = s->ks_mma ? (u32)pz::KSM_ROWS : (u32)pz::KS_TILE_CT;
     for (size_t i = 0; i < n; i++) {
       const Item &it = items[c0 + i];
       hg[i] = it.gate;
@@ -440,7 +447,7 @@ pz_status run_items(pz_server *s, const std::vector<Item> &items) {
       h1[i] = it.in1;
       ho[i] = it.out;
       hd[i] = it.session;
-      if (ntiles == 0 || ht[ntiles - 1].desc != it.session || ht[ntiles - 1].count == (u32)pz::KS_TILE_CT)
+      if (ntiles == 0 || ht[ntiles - 1].desc != it.session || ht[ntiles - 1].count == tile_cap)
         ht[ntiles++] = pz::KsTile{it.session, (u32)i, 0};
       ht[ntiles - 1].count++;
     }
@@ -448,10 +455,9 @@ pz_status run_items(pz_server *s, const std::vector<Item> &items) {
     if ((e = cudaMemcpyAsync(d, h, lay.total, cudaMemcpyHostToDevice, s->stream)) != cudaSuccess)
       return s->cuda("item upload", e);
     if ((e = cudaEventRecord(s->buf_free[b], s->stream)) != cudaSuccess) return s->cuda("cudaEventRecord", e);
-    e = pz::launch_ks_ragged(s->d_ksp, (const pz::KsTile *)(d + lay.tiles), ntiles, n, s->max_n,
-                             (u32)(s->L - 1), s->max_d,
-                             d + lay.gate, s->d_arena, (const u32 *)(d + lay.in0), (const u32 *)(d + lay.in1),
-                             s->d_ksout, s->ks_stride, s->stream);
+    e = (s->ks_mma ? pz::launch_ks_mma_ragged : pz::launch_ks_ragged)(
+        s->d_ksp, (const pz::KsTile *)(d + lay.tiles), ntiles, n, s->max_n, (u32)(s->L - 1), s->max_d, d + lay.gate,
+        s->d_arena, (const u32 *)(d + lay.in0), (const u32 *)(d + lay.in1), s->d_ksout, s->ks_stride, s->stream);
     if (e != cudaSuccess) return s->cuda("launch_ks_ragged", e);
     // a step of at most half the SMs' gates: one cluster of two CTAs per gate (the latency form)
     const int variant = (s->logn == 11 && s->d1 && n <= (size_t)s->sm_count / 2) ? pz::PBS_SPLIT : s->pbs_variant;
