@@ -553,6 +553,19 @@ __device__ __forceinline__ void ibf2(u64 (&x)[8], u64 (&y)[8], int a, int b, u64
   ibf<LOGN == 11, K>(x[a], x[b], w, ws, q);
   if (TWO) ibf<LOGN == 11, K>(y[a], y[b], w, ws, q);
 }
+// With the FP64-quotient butterflies the round that opens an inverse
+// transform (2 stages, inputs < 2.04 Q, K = 3 and 14) skips its reduction
+// (PZ_INV_REDUCE_EVERY_ROUND: reduces, a comparison): its products leave
+// < 13.51 Q whatever their input, so its sums stay < 27.02 Q, and every
+// radix-8 round takes inputs that large (K = 28, 55, 109; sums < 216.2 Q)
+// before its own reduction.
+#ifdef PZ_INV_REDUCE_EVERY_ROUND
+constexpr bool INV_SKIP = false;
+#else
+constexpr bool INV_SKIP = BFLY_FP64;
+#endif
+constexpr int IK_A8 = INV_SKIP ? 28 : 2, IK_B8 = INV_SKIP ? 55 : IK_B, IK_C8 = INV_SKIP ? 109 : IK_C;
+
 // End of an inverse round for N = 2048: every value back below 2Q.
 template <int LOGN, bool TWO>
 __device__ __forceinline__ void inv_round_reduce(u64 (&x)[8], u64 (&y)[8]) {
@@ -598,11 +611,34 @@ __device__ __forceinline__ void fwd_round8(u64 (&x)[8], u64 (&y)[8], int k, int 
   }
 }
 
+// The round's three stages with compile-time bounds (IK_A8..C8 above; the
+// Shoup butterflies: inputs < 2Q, sums < 4Q, 8Q, 16Q), then the once-per-round
+// reduction.
+template <int LOGN, bool TWO, bool PF>
+__device__ __forceinline__ void inv_round8_stages(u64 (&x)[8], u64 (&y)[8], int m, int blk, u64 (&w)[7],
+                                                  u64 (&ws)[7], const RingConsts &rc) {
+  const u64 q = rc.q;
+#pragma unroll
+  for (int h = 0; h < 4; h++) {
+    if (!PF) tw(rc.iw, 4 * m + 4 * blk + h, w[h], ws[h]);
+    ibf2<LOGN, TWO, IK_A8>(x, y, 2 * h, 2 * h + 1, w[h], ws[h], q);
+  }
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    if (!PF) tw(rc.iw, 2 * m + 2 * blk + h, w[4 + h], ws[4 + h]);
+    ibf2<LOGN, TWO, IK_B8>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
+    ibf2<LOGN, TWO, IK_B8>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
+  }
+  if (!PF) tw(rc.iw, m + blk, w[6], ws[6]);
+#pragma unroll
+  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO, IK_C8>(x, y, r, r + 4, w[6], ws[6], q);
+  inv_round_reduce<LOGN, TWO>(x, y);
+}
+
 template <int LOGN, bool TWO, bool PF = false>
 __device__ __forceinline__ void inv_round8(u64 (&x)[8], u64 (&y)[8], int k, int j, const RingConsts &rc) {
   const int m = 1 << (3 * k);
   const int blk = j >> (LOGN - 3 * k - 3);
-  const u64 q = rc.q;
   u64 w[7], ws[7];  // slots: 0-3 (stage 4m), 4-5 (stage 2m), 6 (stage m)
   if (PF) {
 #pragma unroll
@@ -611,22 +647,7 @@ __device__ __forceinline__ void inv_round8(u64 (&x)[8], u64 (&y)[8], int k, int 
     for (int h = 0; h < 2; h++) tw(rc.iw, 2 * m + 2 * blk + h, w[4 + h], ws[4 + h]);
     tw(rc.iw, m + blk, w[6], ws[6]);
   }
-  // (N = 2048) inputs < 2Q; sums reach < 4Q, 8Q, 16Q over the three stages
-#pragma unroll
-  for (int h = 0; h < 4; h++) {
-    if (!PF) tw(rc.iw, 4 * m + 4 * blk + h, w[h], ws[h]);
-    ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w[h], ws[h], q);
-  }
-#pragma unroll
-  for (int h = 0; h < 2; h++) {
-    if (!PF) tw(rc.iw, 2 * m + 2 * blk + h, w[4 + h], ws[4 + h]);
-    ibf2<LOGN, TWO, IK_B>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
-    ibf2<LOGN, TWO, IK_B>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
-  }
-  if (!PF) tw(rc.iw, m + blk, w[6], ws[6]);
-#pragma unroll
-  for (int r = 0; r < 4; r++) ibf2<LOGN, TWO, IK_C>(x, y, r, r + 4, w[6], ws[6], q);
-  inv_round_reduce<LOGN, TWO>(x, y);
+  inv_round8_stages<LOGN, TWO, PF>(x, y, m, blk, w, ws, rc);
 }
 
 // Trailing 2-stage round (stages with N/4 and N/2 groups); PF as for the
@@ -685,7 +706,7 @@ __device__ __forceinline__ void inv_round4(u64 (&x)[8], u64 (&y)[8], int j, cons
     ibf2<LOGN, TWO, IK_MB>(x, y, 4 * h + 0, 4 * h + 2, w[3 * h + 2], ws[3 * h + 2], q);
     ibf2<LOGN, TWO, IK_MB>(x, y, 4 * h + 1, 4 * h + 3, w[3 * h + 2], ws[3 * h + 2], q);
   }
-  inv_round_reduce<LOGN, TWO>(x, y);  // (N = 2048) sums < 8.2Q -> < 2Q
+  if (!INV_SKIP) inv_round_reduce<LOGN, TWO>(x, y);  // (N = 2048) sums < 8.2Q -> < 2Q
 }
 
 // Layout of full round k: thread j holds base + t r, t = N >> (3k + 3).

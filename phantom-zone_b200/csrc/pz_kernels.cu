@@ -141,15 +141,17 @@ __device__ __forceinline__ void inv_round8_last_scaled(u64 (&x)[8], u64 (&y)[8],
   for (int h = 0; h < 4; h++) tw(rc.iw, 4 + h, w[h], ws[h]);
 #pragma unroll
   for (int h = 0; h < 2; h++) tw(rc.iw, 2 + h, w[4 + h], ws[4 + h]);
+  // the last radix-8 round's bounds
+  constexpr int KA = IK_A8, KB = IK_B8, KC = IK_C8;
 #pragma unroll
-  for (int h = 0; h < 4; h++) ibf2<LOGN, TWO, 2>(x, y, 2 * h, 2 * h + 1, w[h], ws[h], q);
+  for (int h = 0; h < 4; h++) ibf2<LOGN, TWO, KA>(x, y, 2 * h, 2 * h + 1, w[h], ws[h], q);
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    ibf2<LOGN, TWO, IK_B>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
-    ibf2<LOGN, TWO, IK_B>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
+    ibf2<LOGN, TWO, KB>(x, y, 4 * h + 0, 4 * h + 2, w[4 + h], ws[4 + h], q);
+    ibf2<LOGN, TWO, KB>(x, y, 4 * h + 1, 4 * h + 3, w[4 + h], ws[4 + h], q);
   }
-  auto last = [&](u64 &a, u64 &b) {  // a, b < IK_C Q here
-    const u64 u = a + b, t = a + (u64)IK_C * Q_N2048 - b;
+  auto last = [&](u64 &a, u64 &b) {  // a, b < KC Q here
+    const u64 u = a + b, t = a + (u64)KC * Q_N2048 - b;
     a = shoup_spq(u, rc.n_inv, rc.n_inv_s);
     b = shoup_spq(t, rc.iw1n, rc.iw1n_s);
   };

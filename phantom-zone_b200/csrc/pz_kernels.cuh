@@ -7,7 +7,7 @@ namespace pz {
 constexpr int MAX_KS_D = 16;   // key-switch decomposition count bound
 // Revision of the blind-rotation kernels: bumped with every change to their
 // code, so that a profile taken on one revision is not reported for another.
-constexpr const char *BR_KERNEL_REVISION = "br-v14";
+constexpr const char *BR_KERNEL_REVISION = "br-v15";
 constexpr int MAX_AUTO_SLOTS = 16;
 
 // Everything the blind rotation needs for one parameter set + server key.
