@@ -24,6 +24,7 @@ struct pz_ctx {
   // Montgomery products use (aggregation, the NI key switch), br_conv_c those
   // of the blind rotation's RGSW and auto keys (folded products for N = 2048)
   pz::u64 conv_c = 0, conv_cs = 0, br_conv_c = 0, br_conv_cs = 0;
+  pz::u64 ni_conv_c = 0, ni_conv_cs = 0;  // the NI key-switch keys (ni_mac: folded when MAC_FOLD_N2048)
   pz::BrParams br{};
   pz::KsParams ks{};
   pz::u32 *d_err = nullptr;  // device error word: DEVERR_* bits set by kernels whose bounded waits ran out
@@ -56,7 +57,7 @@ struct pz_key {
 
 struct pz_ni_ksk {
   pz_ctx *ctx = nullptr;
-  pz::u64 *d_ksk = nullptr;  // [2 d][N] evaluation domain, Montgomery form with N^{-1}
+  pz::u64 *d_ksk = nullptr;  // [2 d][N] evaluation domain, scaled by ni_conv_c (N^{-1})
   pz::u32 d = 0;
   size_t bytes = 0;
 };

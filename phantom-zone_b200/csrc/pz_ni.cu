@@ -15,9 +15,9 @@
 //   key switch   rlwe_key_switch (runtime.rs:1001-1063) from the user's RLWE
 //                secret u_j to the ideal secret s: the 50 one-bit signed
 //                digits of -A are transformed two at a time and accumulated
-//                against the user's ui_to_s key rows (Montgomery form,
-//                N^{-1} folded in), then one inverse transform of both
-//                outputs and B' += B.
+//                against the user's ui_to_s key rows (N^{-1} folded in;
+//                sums folded with 2^54 = 77823, see ni_mac), then one
+//                inverse transform of both outputs and B' += B.
 //   extract      BatchedFheBools::extract (ni_mp_api.rs:217-236): bool i is
 //                sample_extract (pbs.rs:423-449) at coefficient i % N of
 //                RLWE i / N.
@@ -392,7 +392,7 @@ pz_status pz_ni_ksk_upload(pz_ctx *c, const uint64_t *ksk, pz_ni_ksk **out) {
   cudaError_t e = cudaMalloc(&k->d_ksk, k->bytes);
   if (e == cudaSuccess) e = cudaMalloc(&stage, k->bytes);
   if (e == cudaSuccess) e = cudaMemcpyAsync(stage, ksk, k->bytes, cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess) e = pz::launch_key_convert((int)c->logn, stage, k->d_ksk, polys, c->rc, c->conv_c, c->conv_cs, c->stream);
+  if (e == cudaSuccess) e = pz::launch_key_convert((int)c->logn, stage, k->d_ksk, polys, c->rc, c->ni_conv_c, c->ni_conv_cs, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFree(stage);
   if (e != cudaSuccess) {
@@ -424,7 +424,7 @@ pz_status pz_ni_ksk_upload_seeded(pz_ctx *c, const uint64_t *ksk_b, const uint8_
   if (e == cudaSuccess && s == PZ_OK)
     e = cudaMemcpyAsync(stage + d * N, ksk_b, d * N * 8, cudaMemcpyDefault, c->stream);
   if (e == cudaSuccess && s == PZ_OK)
-    e = pz::launch_key_convert((int)c->logn, stage, k->d_ksk, polys, c->rc, c->conv_c, c->conv_cs, c->stream);
+    e = pz::launch_key_convert((int)c->logn, stage, k->d_ksk, polys, c->rc, c->ni_conv_c, c->ni_conv_cs, c->stream);
   if (e == cudaSuccess && s == PZ_OK) e = cudaStreamSynchronize(c->stream);
   cudaFree(stage);
   if (e != cudaSuccess || s != PZ_OK) {

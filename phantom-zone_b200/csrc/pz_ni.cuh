@@ -79,8 +79,11 @@ __host__ __device__ __forceinline__ bool uniform_from_word(u64 v, u64 q, u64 zon
   return v * q <= zone;
 }
 
-// oa += REDC(x ka + y kc), ob += REDC(x kb + y kd), lazily in [0, 2q); the
-// key rows are in the device layout (register pair -> one 16-byte word).
+// oa += x ka + y kc, ob += x kb + y kd (mod Q), kept below 2Q; the key rows
+// are in the device layout (register pair -> one 16-byte word) and, with the
+// blind rotation's folded reduction (MAC_FOLD_N2048), scaled by N^{-1} only:
+// each 128-bit sum is folded with 2^54 = 77823 and the running sum brought
+// back below 2Q by reduce_n2048.  Otherwise Montgomery REDC, keys with 2^64.
 __device__ __forceinline__ void ni_mac(u64 (&oa)[8], u64 (&ob)[8], const u64 (&x)[8], const u64 (&y)[8],
                                        const u64 *ka, const u64 *kb, const u64 *kc, const u64 *kd, bool two,
                                        const RingConsts &rc) {
@@ -100,15 +103,27 @@ __device__ __forceinline__ void ni_mac(u64 (&oa)[8], u64 (&ob)[8], const u64 (&x
     for (int e = 0; e < 2; e++) {
       const int r = 2 * rr + e;
       u64 hi, lo, hi2, lo2;
-      mul128(x[r], a[e], hi, lo);
-      mul128(x[r], b[e], hi2, lo2);
-      if (two) {
-        mac128(y[r], c[e], hi, lo);
-        mac128(y[r], d[e], hi2, lo2);
+      if constexpr (MAC_FOLD_N2048) {  // x, y < 150 Q (lazy forward outputs), keys < Q
+        if (two) {
+          sum2_128(x[r], a[e], y[r], c[e], hi, lo);
+          sum2_128(x[r], b[e], y[r], d[e], hi2, lo2);
+        } else {
+          mul128_narrow(x[r], a[e], hi, lo);
+          mul128_narrow(x[r], b[e], hi2, lo2);
+        }
+        oa[r] = reduce_n2048(oa[r] + fold_n2048(hi, lo));
+        ob[r] = reduce_n2048(ob[r] + fold_n2048(hi2, lo2));
+      } else {
+        mul128(x[r], a[e], hi, lo);
+        mul128(x[r], b[e], hi2, lo2);
+        if (two) {
+          mac128(y[r], c[e], hi, lo);
+          mac128(y[r], d[e], hi2, lo2);
+        }
+        const u64 va = oa[r] + redc(hi, lo, q, qi), vb = ob[r] + redc(hi2, lo2, q, qi);
+        oa[r] = va >= q2 ? va - q2 : va;
+        ob[r] = vb >= q2 ? vb - q2 : vb;
       }
-      const u64 va = oa[r] + redc(hi, lo, q, qi), vb = ob[r] + redc(hi2, lo2, q, qi);
-      oa[r] = va >= q2 ? va - q2 : va;
-      ob[r] = vb >= q2 ? vb - q2 : vb;
     }
   }
 }

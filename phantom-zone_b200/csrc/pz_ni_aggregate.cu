@@ -322,7 +322,7 @@ pz_status pz_ni_aggregate_device(pz_ctx *c, const uint8_t crs[32], const pz_ni_s
     ps = pz::seeded_fill_u64(c, seed, P.rlwe_q, (u64)d * N, d * N, 2 * d * N, 0, d_stage, st);
     if (ps == PZ_OK) e = cudaMemcpyAsync(d_stage + d * N, d_ksk_b + j * d * N, d * N * 8, cudaMemcpyDeviceToDevice, st);
     if (ps == PZ_OK && e == cudaSuccess)
-      e = pz::launch_key_convert(NI_LOGN, d_stage, d_keys + j * 2 * d * N, 2 * d, c->rc, c->conv_c, c->conv_cs, st);
+      e = pz::launch_key_convert(NI_LOGN, d_stage, d_keys + j * 2 * d * N, 2 * d, c->rc, c->ni_conv_c, c->ni_conv_cs, st);
   }
   std::vector<NiUser> hu(users);
   for (size_t u = 0; u < users; u++) {

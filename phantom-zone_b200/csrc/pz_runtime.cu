@@ -386,6 +386,8 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   const bool fold = c->logn == 11 && pz::MAC_FOLD_N2048 && P.rlrg_d_a == 1 && P.rlrg_d_b == 1 && P.auto_d == 1;
   c->br_conv_c = fold ? rc.n_inv : c->conv_c;
   c->br_conv_cs = shoup(c->br_conv_c, Q);
+  c->ni_conv_c = (c->logn == 11 && pz::MAC_FOLD_N2048) ? rc.n_inv : c->conv_c;
+  c->ni_conv_cs = shoup(c->ni_conv_c, Q);
   pz::BrParams &br = c->br;
   br.rc = rc;
   br.err = c->d_err;
