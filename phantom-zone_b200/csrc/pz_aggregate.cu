@@ -55,7 +55,7 @@ pz_status pz_aggregate_rgsw_device(pz_ctx *c, uint64_t *d_rgsw0, const uint64_t 
     for (size_t c0 = 0; c0 < count && e == cudaSuccess; c0 += chunk) {
       const size_t m = std::min(chunk, count - c0);
       const u64 *src = d_others + (t * count + c0) * rows1 * N;
-      e = pz::launch_key_convert((int)c->logn, src, d_eval, m * rows1, c->rc, c->conv_c, c->conv_cs, st);
+      e = pz::launch_key_convert((int)c->logn, src, d_eval, m * rows1, c->rc, c->br_conv_c, c->br_conv_cs, st);
       if (e != cudaSuccess) break;
       br.rgsw = d_eval;
       br.n = (u32)m;

@@ -330,7 +330,7 @@ __device__ __forceinline__ void mac_auto(u64 (&x)[8], u64 (&y)[8], const u64 *ka
   }
 }
 
-// Lazy accumulation for the general decomposition path: o += REDC(...) in [0, 2q).
+// Lazy accumulation for the general decomposition path: o += x k (mod q), kept in [0, 2q).
 template <int LOGN>
 __device__ __forceinline__ void mac_accum(u64 (&oa)[8], u64 (&ob)[8], const u64 (&x)[8], const u64 (&y)[8],
                                           const u64 *ka, const u64 *kb, const u64 *kc, const u64 *kd, bool hx,
@@ -342,11 +342,26 @@ __device__ __forceinline__ void mac_accum(u64 (&oa)[8], u64 (&ob)[8], const u64 
 #pragma unroll
   for (int r = 0; r < 8; r++) {
     u64 hi = 0, lo = 0, hi2 = 0, lo2 = 0;
-    if (hx) { mac128(x[r], a[r], hi, lo); mac128(x[r], b[r], hi2, lo2); }
-    if (hy) { mac128(y[r], c[r], hi, lo); mac128(y[r], d[r], hi2, lo2); }
-    const u64 va = oa[r] + redc(hi, lo, q, qi), vb = ob[r] + redc(hi2, lo2, q, qi);
-    oa[r] = va >= 2 * q ? va - 2 * q : va;
-    ob[r] = vb >= 2 * q ? vb - 2 * q : vb;
+    if constexpr (LOGN == 11 && MAC_FOLD_N2048) {  // keys K N^{-1}; sums folded, kept below 2Q
+      if (hx && hy) {
+        sum2_128(x[r], a[r], y[r], c[r], hi, lo);
+        sum2_128(x[r], b[r], y[r], d[r], hi2, lo2);
+      } else if (hx) {
+        mul128_narrow(x[r], a[r], hi, lo);
+        mul128_narrow(x[r], b[r], hi2, lo2);
+      } else if (hy) {
+        mul128_narrow(y[r], c[r], hi, lo);
+        mul128_narrow(y[r], d[r], hi2, lo2);
+      }
+      oa[r] = reduce_n2048(oa[r] + fold_n2048(hi, lo));
+      ob[r] = reduce_n2048(ob[r] + fold_n2048(hi2, lo2));
+    } else {
+      if (hx) { mac128(x[r], a[r], hi, lo); mac128(x[r], b[r], hi2, lo2); }
+      if (hy) { mac128(y[r], c[r], hi, lo); mac128(y[r], d[r], hi2, lo2); }
+      const u64 va = oa[r] + redc(hi, lo, q, qi), vb = ob[r] + redc(hi2, lo2, q, qi);
+      oa[r] = va >= 2 * q ? va - 2 * q : va;
+      ob[r] = vb >= 2 * q ? vb - 2 * q : vb;
+    }
   }
 }
 

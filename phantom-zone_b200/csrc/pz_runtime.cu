@@ -382,8 +382,8 @@ pz_status pz_ctx_create_ex(int id, int device, uint64_t root, pz_ctx **out) {
   c->conv_c = mulmod(rc.n_inv, r64, Q);  // Montgomery-product keys: K * N^{-1} * 2^64
   c->conv_cs = shoup(c->conv_c, Q);
   // blind-rotation keys: K * N^{-1} where the multiply-accumulates fold (mac_reduce)
-  // (the one-digit kernels; other decomposition counts run the Montgomery path)
-  const bool fold = c->logn == 11 && pz::MAC_FOLD_N2048 && P.rlrg_d_a == 1 && P.rlrg_d_b == 1 && P.auto_d == 1;
+  // (every N = 2048 multiply-accumulate of the blind rotation and aggregation folds)
+  const bool fold = c->logn == 11 && pz::MAC_FOLD_N2048;
   c->br_conv_c = fold ? rc.n_inv : c->conv_c;
   c->br_conv_cs = shoup(c->br_conv_c, Q);
   c->ni_conv_c = (c->logn == 11 && pz::MAC_FOLD_N2048) ? rc.n_inv : c->conv_c;
